@@ -1,0 +1,602 @@
+"""CPU oracle for the paces adaptive-basis time step (Holstein chain, single exciton).
+
+TEST INFRASTRUCTURE ONLY.  This module is a plain NumPy/SciPy restatement of
+the reference algorithm, used by `tests/`, by `__graft_entry__.smoke()` as the
+checker, and by `bench.py` as the timed CPU baseline.  The product path
+(`paces_b200`) never imports it.
+
+Pinning: `tests/test_oracle_pins.py` checks every function here against golden
+fixtures produced by the unmodified reference (rkevk/paces 1.2.0) run on CPU
+behind `oracle/refshim` (a NumPy stand-in for CuPy); see
+`tests/golden/gen_golden.py`.
+
+Keys use the reference layout: each basis state (pos, n_0, ..., n_{N-1}) is
+packed MSB-first into W uint32 words, field widths ceil(log2(max_dim)), and a
+field may straddle two words (paces/core/hamiltonian.py:140-160, :218-248).
+
+Two features the reference lacks are restated here so the same code can serve
+as the oracle for the extended configurations:
+
+* periodic=True: hopping wraps pos L-1 <-> 0 (the reference raises,
+  paces/models/holstein.py:183-184).  Requires L >= 3.
+* site_eps: per-site exciton energy added to the diagonal
+  (paces/models/holstein.py:280-287 has only eps_sys + hbar_omega*sum(n) +
+  delta_eps*pos).
+With periodic=False and site_eps=None every function reduces to the reference.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+import scipy.sparse as sp
+
+TAYLOR_TOL_F64 = 2.0 ** -53   # paces/core/time_evolution.py:484
+TAYLOR_TOL_F32 = 2.0 ** -24   # single-precision unit roundoff (paces/aux/_scipy/_expm_multiply.py)
+
+# --------------------------------------------------------------------------------------------
+# model description and key layout
+# --------------------------------------------------------------------------------------------
+
+
+@dataclasses.dataclass
+class Model:
+    """Holstein-chain parameters (paces/models/holstein.py:24-66, use_terms dict)."""
+    nchain: int
+    max_ho_dims: list
+    J: float = 1.0
+    g: float = 1.0
+    eps_sys: float = 0.0
+    hbar_omega: float = 1.0
+    delta_eps: float = 0.0
+    periodic: bool = False
+    site_eps: np.ndarray | None = None
+
+    def __post_init__(self):
+        self.max_ho_dims = [int(x) for x in self.max_ho_dims]
+        if len(self.max_ho_dims) != self.nchain:
+            raise ValueError("nchain should match the number of QHOs.")
+        if self.periodic and self.nchain < 3:
+            raise ValueError("periodic hopping needs at least 3 sites")
+        max_dims = np.array([self.nchain] + self.max_ho_dims, dtype=np.float64)
+        # hamiltonian.py:155 bitwidths = ceil(log2(max_dims))
+        self.bitwidths = np.ceil(np.log2(max_dims)).astype(np.int64)
+        self.posbitwidth = int(self.bitwidths[0])
+        self.totwordwidth = int(math.ceil(self.bitwidths.sum() / 32))       # hamiltonian.py:160
+        self.bit_offset = np.concatenate([[0], np.cumsum(self.bitwidths)[:-1]])
+        if self.site_eps is not None:
+            self.site_eps = np.asarray(self.site_eps, dtype=np.float64)
+
+    @property
+    def n_sites(self):
+        return self.nchain + 1
+
+
+def _window(keys, wi):
+    """64-bit window of words (wi, wi+1) for every row (wi may vary per row)."""
+    rows = np.arange(keys.shape[0])
+    wi = np.broadcast_to(np.asarray(wi, dtype=np.int64), rows.shape)
+    hi = keys[rows, wi].astype(np.uint64)
+    has_lo = wi + 1 < keys.shape[1]
+    lo = np.zeros_like(hi)
+    lo[has_lo] = keys[rows[has_lo], wi[has_lo] + 1]
+    return (hi << np.uint64(32)) | lo, rows, wi, has_lo
+
+
+def get_field(model: Model, keys, index):
+    """n at field `index` (0 = exciton position) -- paces/core/hamiltonian.py:291-318."""
+    index = np.asarray(index, dtype=np.int64)
+    b0 = model.bit_offset[index]
+    w = model.bitwidths[index]
+    wi = b0 // 32
+    n2 = b0 + w - 32 * wi
+    val, *_ = _window(keys, wi)
+    sh = np.broadcast_to((64 - n2).astype(np.uint64), val.shape)
+    mask = (np.uint64(1) << np.broadcast_to(w.astype(np.uint64), val.shape)) - np.uint64(1)
+    return ((val >> sh) & mask).astype(np.uint32)
+
+
+def add_field(model: Model, keys, n, index):
+    """In place: field `index` += n with carry/borrow across words.
+
+    paces/core/hamiltonian.py:321-360 and the per-row variant
+    paces/models/_kernels/_holstein_kernels.py:96-149 (index may vary per row).
+    """
+    index = np.asarray(index, dtype=np.int64)
+    b0 = model.bit_offset[index]
+    w = model.bitwidths[index]
+    wi = b0 // 32
+    n2 = b0 + w - 32 * wi
+    val, rows, wi, has_lo = _window(keys, wi)
+    inc = (np.uint64(abs(n)) << np.broadcast_to((64 - n2).astype(np.uint64), val.shape))
+    val = val + inc if n > 0 else val - inc
+    keys[rows, wi] = (val >> np.uint64(32)).astype(np.uint32)
+    keys[rows[has_lo], wi[has_lo] + 1] = (val[has_lo] & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+
+
+def set_field(model: Model, keys, values, index):
+    """In place: field `index` := values (per row)."""
+    cur = get_field(model, keys, index).astype(np.int64)
+    values = np.broadcast_to(np.asarray(values, dtype=np.int64), cur.shape)
+    up = values > cur
+    dn = values < cur
+    for mask, sign in ((up, 1), (dn, -1)):
+        if mask.any():
+            sub = keys[mask]
+            delta = np.abs(values[mask] - cur[mask])
+            for d in np.unique(delta):
+                m2 = delta == d
+                s2 = sub[m2]
+                add_field(model, s2, sign * int(d), index)
+                sub[m2] = s2
+            keys[mask] = sub
+
+
+def compress(model: Model, raw):
+    """(R, N+1) occupations -> (R, W) uint32 keys.  paces/core/hamiltonian.py:218-248."""
+    raw = np.asarray(raw)
+    keys = np.zeros((raw.shape[0], model.totwordwidth), dtype=np.uint32)
+    for i in range(model.n_sites):
+        col = raw[:, i].astype(np.uint64)
+        if np.any(col >= (np.uint64(1) << np.uint64(model.bitwidths[i]))):
+            raise ValueError(f"occupation exceeds field width at field {i}")
+        b0 = int(model.bit_offset[i])
+        w = int(model.bitwidths[i])
+        wi = b0 // 32
+        n2 = b0 + w - 32 * wi
+        val = col << np.uint64(64 - n2)
+        keys[:, wi] |= (val >> np.uint64(32)).astype(np.uint32)
+        if wi + 1 < model.totwordwidth:
+            keys[:, wi + 1] |= (val & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    return keys
+
+
+def decompress(model: Model, keys):
+    """(R, W) keys -> (R, N+1) occupations.  paces/core/hamiltonian.py:210-215."""
+    out = np.zeros((keys.shape[0], model.n_sites), dtype=np.uint32)
+    for i in range(model.n_sites):
+        out[:, i] = get_field(model, keys, i)
+    return out
+
+
+def get_pos(model, keys):
+    return get_field(model, keys, 0).astype(np.int64)
+
+
+def phonon_at_exc(model, keys):
+    """paces/models/_kernels/_holstein_kernels.py:153-179 (get_occ_pte_kernel)."""
+    return get_field(model, keys, get_pos(model, keys) + 1)
+
+
+def sum_all_phonons(model, keys):
+    """Sum_s n_s in float64, accumulated site by site (_holstein_kernels.py:183-210)."""
+    res = np.zeros(keys.shape[0], dtype=np.float64)
+    for s in range(model.nchain):
+        res += get_field(model, keys, s + 1) * 1.0
+    return res
+
+
+# --------------------------------------------------------------------------------------------
+# sorting, uniqueness, lookup
+# --------------------------------------------------------------------------------------------
+
+
+def _rows_as_bytes(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return np.ascontiguousarray(a.astype(">u4")).view(f"S{4 * a.shape[1]}").reshape(a.shape[0])
+
+
+def lexsort_rows(a):
+    """Row order with column 0 most significant (paces/aux/helpers.py:71)."""
+    return np.lexsort(a.T[::-1])
+
+
+def unique_rows(a):
+    """Sorted unique rows.  paces/aux/helpers.py:63-75 (cupy_unique)."""
+    if a.shape[0] == 0:
+        return a.copy()
+    s = a[lexsort_rows(a)]
+    mask = np.empty(s.shape[0], dtype=bool)
+    mask[0] = True
+    mask[1:] = np.any(s[1:] != s[:-1], axis=1)
+    return s[mask]
+
+
+def searchsorted(phonebook, findme, allow_escapes=False):
+    """Lower bound of each row of `findme` in the sorted `phonebook`.
+
+    paces/aux/cupy_search.py:78-93 with the kernel at :149-228.  With
+    allow_escapes=False every row must be present (the CUDA kernel asserts).
+    Escapes return len(phonebook), as the CUDA kernel does.
+    """
+    if findme.shape[0] == 0:
+        return np.zeros(0, dtype=np.int64)
+    pb = _rows_as_bytes(phonebook)
+    q = _rows_as_bytes(findme)
+    left = np.searchsorted(pb, q, side="left")
+    if not allow_escapes:
+        hit = left < len(pb)
+        hit[hit] = pb[left[hit]] == q[hit]
+        if not hit.all():
+            raise LookupError("a looked-up basis state is not in the phonebook")
+    return left.astype(np.int64)
+
+
+def lookup_with_mask(phonebook, findme):
+    """(index, found) pairs; index valid only where found (used by the remap and o-star mask)."""
+    idx = searchsorted(phonebook, findme, allow_escapes=True)
+    found = np.zeros(idx.shape[0], dtype=bool)
+    ok = idx < phonebook.shape[0]
+    found[ok] = np.all(phonebook[idx[ok]] == findme[ok], axis=1)
+    return idx, found
+
+
+# --------------------------------------------------------------------------------------------
+# Hamiltonian terms (Holstein), expansion and assembly
+# --------------------------------------------------------------------------------------------
+
+
+def hopping_images(model: Model, basis):
+    """Right/left hop images and their masks.  paces/models/holstein.py:151-207 (order 1, 1D).
+
+    Returns (plus_inds, plus_mask, minus_inds_all, minus_mask): plus_inds are
+    the images of basis[plus_mask]; minus_inds_all[i] is the image of basis[i]
+    (only meaningful where minus_mask).
+    """
+    L = model.nchain
+    pos = get_pos(model, basis)
+    if model.periodic:
+        plus_mask = np.ones(basis.shape[0], dtype=bool)
+        minus_mask = np.ones(basis.shape[0], dtype=bool)
+        plus = basis.copy()
+        minus = basis.copy()
+        set_field(model, plus, (pos + 1) % L, 0)
+        set_field(model, minus, (pos - 1) % L, 0)
+        return plus, plus_mask, minus, minus_mask
+    plus_mask = pos < (L - 1)
+    plus = basis[plus_mask].copy()
+    add_field(model, plus, 1, 0)
+    minus = basis.copy()
+    add_field(model, minus, -1, 0)
+    minus_mask = pos > 0
+    return plus, plus_mask, minus, minus_mask
+
+
+def vib_images(model: Model, basis):
+    """b^dagger / b at the exciton site.  paces/models/holstein.py:242-277."""
+    occ = phonon_at_exc(model, basis).astype(np.int64)
+    pos = get_pos(model, basis)
+    maxd = np.asarray(model.max_ho_dims, dtype=np.int64)[pos]
+    plus_mask = occ < (maxd - 1)                      # holstein.py:254 (ceiling)
+    plus = basis[plus_mask].copy()
+    add_field(model, plus, 1, pos[plus_mask] + 1)
+    minus = basis.copy()
+    # the reference subtracts on every row (holstein.py:259-260) and masks afterwards; rows
+    # with n=0 would borrow from the neighbouring field, so subtract only where n>0 here --
+    # the masked rows are discarded either way.
+    minus_mask = occ > 0                              # holstein.py:261 (floor)
+    sub = minus[minus_mask]
+    add_field(model, sub, -1, pos[minus_mask] + 1)
+    minus[minus_mask] = sub
+    return plus, plus_mask, minus, minus_mask, occ
+
+
+def enlarge(model: Model, basis):
+    """basis U all raw images, unique.  paces/core/hamiltonian.py:550-577."""
+    hp, _, hm, hmm = hopping_images(model, basis)
+    vp, _, vm, vmm, _ = vib_images(model, basis)
+    allk = np.concatenate([basis, hp, hm[hmm], vp, vm[vmm]])
+    return unique_rows(allk)
+
+
+def o_star_mask(basis, plus):
+    """True where a basis state is NOT a plus image.  paces/core/hamiltonian.py:363-374."""
+    if plus.shape[0] == 0:
+        return np.ones(basis.shape[0], dtype=bool)
+    sortplus = plus[lexsort_rows(plus)]
+    _, found = lookup_with_mask(sortplus, basis)
+    return ~found
+
+
+def diag_values(model: Model, keys):
+    """eps_sys + hbar_omega*sum(n) (+ delta_eps*pos) (+ site_eps[pos]).  holstein.py:280-287."""
+    d = model.eps_sys + model.hbar_omega * sum_all_phonons(model, keys)
+    if model.delta_eps != 0:
+        d = d + model.delta_eps * get_pos(model, keys)
+    if model.site_eps is not None:
+        d = d + model.site_eps[get_pos(model, keys)]
+    return d
+
+
+@dataclasses.dataclass
+class Assembly:
+    new_inds: np.ndarray           # (S, W) sorted unique keys
+    diag: np.ndarray               # (S,) float64
+    mats: dict                     # term -> scipy CSR (S x S), float64
+    basis: np.ndarray              # the enlarged basis B1 the images were generated from
+    basis_lookup: np.ndarray       # positions of B1 in new_inds
+    ceiling_hits: int
+
+
+def generate_mel(model: Model, select, enlarge_steps):
+    """Images, unique, diagonal, lookups, COO with h.c.  paces/core/hamiltonian.py:383-547."""
+    basis = select
+    for _ in range(enlarge_steps):
+        basis = enlarge(model, basis)
+    n = basis.shape[0]
+    hp, hpm, hm_all, hmm = hopping_images(model, basis)
+    hmm = hmm & o_star_mask(basis, hp)
+    hm = hm_all[hmm]
+    vp, vpm, vm_all, vmm, occ = vib_images(model, basis)
+    ceiling_hits = int(n - vpm.sum())
+    vmm = vmm & o_star_mask(basis, vp)
+    vm = vm_all[vmm]
+    new_inds = unique_rows(np.concatenate([basis, hp, hm, vp, vm]))
+    S = new_inds.shape[0]
+    if S >= 2 ** 31:
+        raise ValueError("The number of states is too large for signed 32-bit-integer indices.")
+    diag = diag_values(model, new_inds)
+    blook = searchsorted(new_inds, basis)
+    g = float(model.g)
+    J = float(model.J)
+    triples = {
+        "hopping": [(hp, np.full(hp.shape[0], J), hpm), (hm, np.full(hm.shape[0], J), hmm)],
+        "vib_coupling": [
+            (vp, np.sqrt(occ[vpm] + 1, dtype=np.float64) * g, vpm),
+            (vm, np.sqrt(occ[vmm], dtype=np.float64) * g, vmm),
+        ],
+    }
+    mats = {}
+    for term, lst in triples.items():
+        rows, cols, vals = [], [], []
+        for inds, v, mask in lst:
+            src = blook[mask]
+            img = searchsorted(new_inds, inds)
+            rows += [img, src]
+            cols += [src, img]
+            vals += [v, np.conj(v)]
+        r = np.concatenate(rows)
+        c = np.concatenate(cols)
+        v = np.concatenate(vals)
+        mats[term] = sp.coo_matrix((v, (r, c)), shape=(S, S)).tocsr()
+    return Assembly(new_inds, diag, mats, basis, blook, ceiling_hits)
+
+
+# --------------------------------------------------------------------------------------------
+# truncation, remap, propagation, observables
+# --------------------------------------------------------------------------------------------
+
+
+def truncate(whoami, vector, maxstates, rng=None):
+    """Keep the `maxstates` largest |psi| states, lexicographically sorted.
+
+    paces/core/time_evolution.py:833-910.  Stable ascending argsort of |psi| and
+    the last `maxstates` entries: among equal values at the cut the highest
+    original indices are kept (shuffle_seed=None).  With `rng` the tied states
+    at the cut are drawn at random instead (the reference's shuffle, whose
+    cuRAND stream cannot be reproduced: parity unpinned for that branch).
+    """
+    w = np.abs(vector)
+    order = np.argsort(w, kind="stable")
+    ms = int(maxstates)
+    if rng is None or len(vector) < ms or w[order[-ms - 1]] < w[order[-ms]]:
+        sel = order[-ms:]
+    else:
+        sv = w[order]
+        decision = sv[-ms]
+        first = np.searchsorted(sv, decision, "left")
+        last = np.searchsorted(sv, decision, "right")
+        if (last - first) > 0.9 * len(vector):
+            raise ValueError("This operation would shuffle too many states.")
+        back = len(vector) - last
+        tied = order[first:last]
+        sel = np.concatenate([rng.permutation(tied)[: ms - back], order[last:]])
+    sel = np.sort(sel)          # whoami is sorted, so index order == lexicographic order
+    return whoami[sel]
+
+
+def remap(old_whoami, vector, new_inds):
+    """New psi = old psi on states present in both bases, else 0.  time_evolution.py:781-797."""
+    idx, found = lookup_with_mask(old_whoami, new_inds)
+    out = np.zeros(new_inds.shape[0], dtype=vector.dtype)
+    out[found] = vector[idx[found]]
+    return out
+
+
+def apply_h(asm: Assembly, v):
+    """diag*v + sum_term CSR_term @ v.  paces/core/time_evolution.py:382-400."""
+    res = asm.diag * v
+    for m in asm.mats.values():
+        res = res + m.dot(v)
+    return res
+
+
+def taylor(asm: Assembly, v, dt, m_star=100, tol=TAYLOR_TOL_F64):
+    """Truncated Taylor series of exp(-i dt H) v.  paces/core/time_evolution.py:482-512.
+
+    Returns (res, [converged, j_ind, c1_plus_c2, term_ratio]).
+    """
+    converged = False
+    term = v
+    res = v.copy()
+    c1 = np.linalg.norm(res, np.inf)
+    c1_plus_c2 = 0.0
+    term_ratio = 0.0
+    j_ind = 0
+    for j_ind in range(m_star):
+        coeff = -1j * dt / float(j_ind + 1)
+        term = apply_h(asm, term)
+        term = term * coeff
+        c2 = np.linalg.norm(term, np.inf)
+        res += term
+        c1_plus_c2 = c1 + c2
+        term_ratio = c1_plus_c2 / np.linalg.norm(res, np.inf)
+        if term_ratio <= tol:
+            converged = True
+            break
+        c1 = c2
+    return res, [converged, j_ind, c1_plus_c2, term_ratio]
+
+
+def n_exc(model, whoami, vector):
+    """Sum |psi|^2 per exciton position.  paces/models/holstein.py:311-314, :380-396."""
+    pos = get_pos(model, whoami)
+    return np.bincount(pos, weights=np.abs(vector) ** 2, minlength=model.nchain)
+
+
+def n_pho(model, whoami, vector):
+    """Sum_states n_site |psi|^2 per site.  holstein.py:317-322, _holstein_kernels.py:215-255."""
+    w = np.abs(vector) ** 2
+    return np.array([(get_field(model, whoami, s + 1) * w).sum() for s in range(model.nchain)])
+
+
+def total_energy(asm, vector):
+    """<psi|H|psi>.  paces/core/observables.py:95-99."""
+    return complex(np.vdot(vector, apply_h(asm, vector)))
+
+
+# --------------------------------------------------------------------------------------------
+# full trajectory (generate_timeline)
+# --------------------------------------------------------------------------------------------
+
+
+def initial_basis(model: Model, minpos, maxpos=None):
+    """Single-exciton, phonon-vacuum basis on positions [minpos, maxpos).
+
+    paces/models/holstein.py:427-476 with truncate_d_list = [1]*N.
+    """
+    if maxpos is None:
+        maxpos = minpos + 1
+    raw = np.zeros((maxpos - minpos, model.n_sites), dtype=np.uint32)
+    raw[:, 0] = np.arange(minpos, maxpos)
+    return compress(model, raw)
+
+
+def grow_optimal_basis(model, whoami, maxstates, n_max=np.inf, fillfac=1.0):
+    """paces/core/time_evolution.py:290-319."""
+    n = 0
+    prev = whoami
+    while len(whoami) <= maxstates * fillfac:
+        if n >= n_max:
+            break
+        n += 1
+        prev = whoami
+        whoami = enlarge(model, prev)
+    return prev
+
+
+@dataclasses.dataclass
+class StepRecord:
+    t: float
+    norm: float
+    numstates: int
+    n_exc: np.ndarray
+    n_pho: np.ndarray
+    energy: complex
+    post_adapt_norm: float
+    post_adapt_energy: float
+    expm_dbg: list
+    ceiling_hits: int
+
+
+class Trajectory:
+    """A CPU run of `generate_timeline` (paces/core/time_evolution.py:426-458, :552-650)."""
+
+    def __init__(self, model, whoami, vector, maxstates, enlarge_steps, m_star=100,
+                 tol=TAYLOR_TOL_F64, diagnostics=True, shuffle_rng=None, renormalize=False,
+                 explosion_cutoff=2.0):
+        self.model = model
+        self.whoami = whoami
+        self.vector = np.asarray(vector, dtype=np.complex128)
+        self.maxstates = maxstates
+        self.enlarge_steps = enlarge_steps
+        self.m_star = m_star
+        self.tol = tol
+        self.diagnostics = diagnostics
+        self.rng = shuffle_rng
+        self.renormalize = renormalize
+        self.explosion_cutoff = explosion_cutoff
+        self.asm = None
+        self.records = []
+
+    def _new_space(self):
+        """paces/core/time_evolution.py:735-807."""
+        select = truncate(self.whoami, self.vector, self.maxstates, self.rng)
+        asm = generate_mel(self.model, select, self.enlarge_steps)
+        self.vector = remap(self.whoami, self.vector, asm.new_inds)
+        self.whoami = asm.new_inds
+        self.asm = asm
+        pan, pae = -1.0, float("nan")
+        if self.diagnostics:
+            pan = float(np.linalg.norm(self.vector))
+            e = total_energy(asm, self.vector)
+            if e.imag > 1e-12:
+                raise RuntimeError(f"Energy has non-zero imaginary part: {e.imag}.")
+            pae = e.real
+        return pan, pae
+
+    def _observe(self, t, expm_dbg, pan, pae):
+        norm = float(np.linalg.norm(self.vector))
+        rec = StepRecord(t, norm, self.whoami.shape[0], n_exc(self.model, self.whoami, self.vector),
+                         n_pho(self.model, self.whoami, self.vector),
+                         total_energy(self.asm, self.vector), pan, pae, expm_dbg,
+                         self.asm.ceiling_hits)
+        self.records.append(rec)
+        return rec
+
+    def first_step(self, t):
+        """paces/core/time_evolution.py:616-650."""
+        pan, pae = self._new_space()
+        return self._observe(t, [0, 0, 0, 0], pan, pae)
+
+    def step(self, t, dt):
+        """paces/core/time_evolution.py:552-613."""
+        pan, pae = self._new_space()
+        self.vector, dbg = taylor(self.asm, self.vector, dt, self.m_star, self.tol)
+        nrm = np.linalg.norm(self.vector)
+        if self.renormalize:
+            self.vector /= nrm
+        elif nrm > self.explosion_cutoff:
+            raise RuntimeError("Norm has exceeded preset explosion cutoff value"
+                               f" ({self.explosion_cutoff})!")
+        return self._observe(t, dbg, pan, pae)
+
+    def run(self, t_array):
+        for i, t in enumerate(t_array):
+            if i == 0:
+                self.first_step(t)
+            else:
+                self.step(t, t - t_array[i - 1])
+        return self.records
+
+
+def exact_dynamics(model: Model, maxstates_full, t_array, init_pos=0):
+    """Full-Hilbert-space reference via scipy expm_multiply (known-answer test, no truncation).
+
+    Builds the complete basis of dimension L*prod(max_ho_dims), the full H with
+    the same terms, and propagates |init_pos, vacuum>.  Returns n_exc per time.
+    """
+    import itertools
+    import scipy.sparse.linalg as spla
+    L = model.nchain
+    ranges = [range(L)] + [range(d) for d in model.max_ho_dims]
+    raw = np.array(list(itertools.product(*ranges)), dtype=np.uint32)
+    if raw.shape[0] > maxstates_full:
+        raise ValueError("Hilbert space too large for exact dynamics")
+    keys = unique_rows(compress(model, raw))
+    asm = generate_mel(model, keys, 0)
+    H = sp.diags(asm.diag) + sum(asm.mats.values())
+    init = initial_basis(model, init_pos)
+    idx = searchsorted(asm.new_inds, init)
+    v = np.zeros(asm.new_inds.shape[0], dtype=np.complex128)
+    v[idx[0]] = 1.0
+    out = []
+    prev_t = t_array[0]
+    for t in t_array:
+        if t != prev_t:
+            v = spla.expm_multiply(-1j * (t - prev_t) * H, v)
+        prev_t = t
+        out.append(n_exc(model, asm.new_inds, v))
+    return np.array(out)

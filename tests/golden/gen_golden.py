@@ -1,0 +1,300 @@
+"""Generate golden fixtures by running the unmodified reference (rkevk/paces 1.2.0) on CPU.
+
+Usage (in a container that has the reference source; it never runs on the GPU host):
+
+    python tests/golden/gen_golden.py /path/to/reference [--long]
+
+The reference is imported behind `oracle/refshim` (a NumPy stand-in for CuPy).
+Nothing of the reference is copied: only its outputs on seeded, synthetic
+inputs are stored, as compressed .npz files next to this script.
+
+Fixtures written:
+  layout_<name>.npz   compress_ind_arr, field get/add kernels, sum_all_phonons,
+                      calculate_bath_n_b, searchsorted_full_binary, cupy_unique
+  stages_<name>.npz   per-step stage data of a short trajectory: truncation input
+                      and output, generate_mel output (diag, new_inds, CSR per term),
+                      remap output, Taylor output and diagnostics, observables
+  traj_<name>.npz     observables and diagnostics of every step of a trajectory
+  ed_n4.npz           exact-diagonalisation known answer (full Hilbert space)
+"""
+
+import argparse
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+LAYOUTS = {
+    # name: (nchain, max_ho_dim) -- 4-bit fields (N=16: W=3, N=32: W=5), 7-bit straddling
+    # fields (N=25 as in the reference's example driver), 3-bit fields.
+    "n16c16": (16, 16),
+    "n32c16": (32, 16),
+    "n25c128": (25, 128),
+    "n6c8": (6, 8),
+}
+
+STAGE_RUNS = {
+    # name: (nchain, max_ho_dim, g, maxstates, enlarge_steps, steps, initpos)
+    "n6c8": (6, 8, 1.0, 200, 1, 8, 2),
+    "n16c16": (16, 16, 1.0, 1500, 1, 5, 0),
+    "n32c16": (32, 16, 1.5, 2000, 1, 4, 0),
+    "n25c128": (25, 128, 4.0, 1000, 1, 4, 12),
+    "n8c16es0": (8, 16, 1.5, 600, 0, 6, 3),
+}
+
+TRAJ_RUNS = {
+    # name: (nchain, max_ho_dim, g, maxstates, enlarge_steps, steps, initpos)
+    "n8c16": (8, 16, 1.5, 4000, 1, 60, 0),
+    "n16c16_m4096": (16, 16, 1.0, 4096, 1, 100, 0),
+}
+LONG_TRAJ_RUNS = {
+    # the small plain-method configuration (open chain): N=16, g=1, maxstates=2^16, 200 steps
+    "n16c16_m65536": (16, 16, 1.0, 65536, 1, 200, 0),
+}
+
+
+def import_reference(ref_root):
+    sys.path.insert(0, os.path.join(REPO, "oracle", "refshim"))
+    sys.path.insert(0, ref_root)
+    import cupy  # the stand-in
+    import paces
+    cupy.adapt_reference(paces)
+    from paces.config import devices
+    if not devices.configure_called:
+        devices.configure()
+    return paces
+
+
+def terms(g):
+    return {"diag": dict(eps_sys=0.0, hbar_omega=1.0, delta_eps=0.0),
+            "hopping": dict(J=1.0), "vib_coupling": dict(g=g)}
+
+
+def make_objects(paces, nchain, dim, g, maxstates, es, initpos, workdir):
+    from paces.models import holstein
+    from paces.core.time_evolution import ExpmParams, TimeEvoParams
+    from paces.config import devices
+    with devices.vector_dev:
+        ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain,
+                                   use_terms=terms(g), debug_verb=0)
+        te = holstein.TimeEvolution(ham, holstein.Observables, ["n_exc", "n_pho", "total_energy"],
+                                    workdir, TimeEvoParams(maxstates=maxstates, enlarge_steps=es,
+                                                           shuffle_seed=None),
+                                    ExpmParams(), os.path.join(workdir, "params.log"))
+        te.create_nonuniform_basis([1] * nchain, minpos=initpos, maxpos=initpos + 1)
+        te.create_initial_vector([1.0], [[initpos] + [0] * nchain])
+    return ham, te
+
+
+def gen_layout(paces, name, nchain, dim, rng):
+    from paces.models import holstein
+    from paces.models._kernels import _holstein_kernels as holke
+    from paces.aux import cupy_search
+    from paces.aux.helpers import cupy_unique
+    from paces.config import devices
+    ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain, use_terms=terms(1.0),
+                               debug_verb=0)
+    R = 3000
+    raw = np.zeros((R, nchain + 1), dtype=np.uint32)
+    raw[:, 0] = rng.integers(0, nchain, R)
+    # sparse occupations (most sites empty, like the physical states) plus some dense rows
+    occ = rng.integers(0, dim, (R, nchain)) * (rng.random((R, nchain)) < 0.25)
+    occ[: R // 10] = rng.integers(0, dim, (R // 10, nchain))
+    raw[:, 1:] = occ
+    keys = ham.compress_ind_arr(raw.copy())
+    out = dict(raw=raw, keys=keys, bitwidths=np.asarray(ham.bitwidths_v),
+               posbitwidth=np.int64(ham.posbitwidth))
+    out["get_occ"] = holke.get_phonon_at_exc(keys, ham.posbitwidth, ham.qhobitwidth_v)
+    n_at = out["get_occ"].astype(np.int64)
+    can_up = n_at < dim - 1
+    can_dn = n_at > 0
+    k_up = keys[can_up].copy()
+    holke.add_phonon_at_exc(k_up, ham.posbitwidth, ham.qhobitwidth_v)
+    k_dn = keys[can_dn].copy()
+    holke.rem_phonon_at_exc(k_dn, ham.posbitwidth, ham.qhobitwidth_v)
+    out.update(can_up=can_up, can_dn=can_dn, keys_up=k_up, keys_dn=k_dn)
+    out["sum_all"] = ham.sum_all_phonons(keys)
+    w = rng.random(R)
+    out["bath_weights"] = w
+    out["bath_n_b"] = holke.calculate_bath_n_b(w, keys, ham.posbitwidth, ham.qhobitwidth_v)
+    # hopping shifts via the generic field adder
+    pos = raw[:, 0].astype(np.int64)
+    kr = keys[pos < nchain - 1].copy()
+    ham.add_n_to_pos(kr, 1)
+    kl = keys[pos > 0].copy()
+    ham.add_n_to_pos(kl, -1)
+    out.update(keys_right=kr, keys_left=kl)
+    # unique + search
+    dup = np.concatenate([keys, keys[rng.integers(0, R, R // 2)]])
+    uniq = cupy_unique(dup)
+    out["unique_in"] = dup
+    out["unique_out"] = uniq
+    q_hit = uniq[rng.integers(0, len(uniq), 2000)]
+    out["search_hit_q"] = q_hit
+    out["search_hit_idx"] = cupy_search.searchsorted_full_binary(uniq, q_hit, False)
+    q_any = ham.compress_ind_arr(np.concatenate(
+        [raw[:500], np.column_stack([rng.integers(0, nchain, 500),
+                                      rng.integers(0, dim, (500, nchain))])]).astype(np.uint32))
+    out["search_any_q"] = q_any
+    # the reference clamps nothing here: escapes come back as len(phonebook) from the CUDA
+    # kernel; the stand-in clamps them to len-1, so store the boolean hit mask instead
+    idx = cupy_search.searchsorted_full_binary(uniq, q_any, True)
+    out["search_any_hit"] = np.all(uniq[idx] == q_any, axis=1)
+    out["search_any_idx"] = idx
+    np.savez_compressed(os.path.join(HERE, f"layout_{name}.npz"), **out)
+
+
+def gen_stages(paces, name, cfg, workdir):
+    nchain, dim, g, maxstates, es, steps, initpos = cfg
+    ham, te = make_objects(paces, nchain, dim, g, maxstates, es, initpos, workdir)
+    from paces.core.time_evolution import CoeffSaveParams
+    rec = {}
+    state = {"step": 0}
+
+    orig_select = te._determine_select_whoami
+    orig_gen = ham.generate_mel
+    orig_post = te._post_assignment_diagnostics
+    orig_taylor = te._simple_taylor
+    orig_enlarge = ham.enlarge_basis_set
+
+    def k(s):
+        return f"s{state['step']}_{s}"
+
+    def select(vector, **kw):
+        rec[k("trunc_whoami")] = np.array(te.whoami)
+        rec[k("trunc_vector")] = np.array(vector)
+        out = orig_select(vector, **kw)
+        rec[k("select")] = np.array(out)
+        return out
+
+    def enlarge(basis):
+        out = orig_enlarge(basis)
+        if k("enlarged") not in rec:
+            rec[k("enlarged")] = np.array(out)
+        return out
+
+    def gen(basis, enlarge_steps=0, log_ind=1.2):
+        out = orig_gen(basis, enlarge_steps=enlarge_steps, log_ind=log_ind)
+        (diag, new_inds), coo, dbg = out
+        rec[k("new_inds")] = np.array(new_inds)
+        rec[k("diag")] = np.array(diag)
+        rec[k("ceiling_hits")] = np.array([int(x) for x in dbg.get("vib_coupling", [0])])
+        return out
+
+    def post():
+        rec[k("remap_vector")] = np.array(te.vector)
+        for term, m in te.sparse_mats_dict.items():
+            m = m.copy()
+            m.sort_indices()
+            rec[k(f"csr_{term}_indptr")] = m.indptr.astype(np.int64)
+            rec[k(f"csr_{term}_indices")] = m.indices.astype(np.int64)
+            rec[k(f"csr_{term}_data")] = m.data
+        out = orig_post()
+        rec[k("post_adapt")] = np.array(out, dtype=np.float64)
+        return out
+
+    def taylor(dt):
+        rec[k("taylor_in")] = np.array(te.vector)
+        res, dbg = orig_taylor(dt)
+        rec[k("taylor_out")] = np.array(res)
+        rec[k("taylor_dbg")] = np.array([float(dbg[0]), float(dbg[1]), float(dbg[2]),
+                                         float(dbg[3])])
+        return res, dbg
+
+    te._determine_select_whoami = select
+    ham.generate_mel = gen
+    ham.enlarge_basis_set = enlarge
+    te._post_assignment_diagnostics = post
+    te._simple_taylor = taylor
+
+    orig_post_proc = te._postprocess
+
+    def postprocess(t, norm, i):
+        rec[k("final_vector")] = np.array(te.vector)
+        rec[k("final_whoami")] = np.array(te.whoami)
+        orig_post_proc(t, norm, i)
+        state["step"] += 1
+
+    te._postprocess = postprocess
+    from paces.config import devices
+    with devices.vector_dev:
+        te.generate_timeline(np.arange(steps + 1) * 0.05, CoeffSaveParams())
+    obs = os.path.join(workdir, "observables")
+    rec["n_exc"] = np.loadtxt(os.path.join(obs, "n_exc.real"))
+    rec["n_pho"] = np.loadtxt(os.path.join(obs, "n_pho.real"))
+    rec["energy"] = np.loadtxt(os.path.join(obs, "total_energy.real"))
+    rec["diagnostics"] = np.loadtxt(os.path.join(obs, "diagnostics.log"))
+    rec["config"] = np.array([nchain, dim, g, maxstates, es, steps, initpos], dtype=np.float64)
+    rec["nsteps_recorded"] = np.int64(state["step"])
+    np.savez_compressed(os.path.join(HERE, f"stages_{name}.npz"), **rec)
+
+
+def gen_traj(paces, name, cfg, workdir):
+    nchain, dim, g, maxstates, es, steps, initpos = cfg
+    ham, te = make_objects(paces, nchain, dim, g, maxstates, es, initpos, workdir)
+    from paces.core.time_evolution import CoeffSaveParams
+    from paces.config import devices
+    with devices.vector_dev:
+        te.generate_timeline(np.arange(steps + 1) * 0.05, CoeffSaveParams())
+    obs = os.path.join(workdir, "observables")
+    np.savez_compressed(
+        os.path.join(HERE, f"traj_{name}.npz"),
+        n_exc=np.loadtxt(os.path.join(obs, "n_exc.real")),
+        n_pho=np.loadtxt(os.path.join(obs, "n_pho.real")),
+        energy=np.loadtxt(os.path.join(obs, "total_energy.real")),
+        energy_imag=np.loadtxt(os.path.join(obs, "total_energy.imag")),
+        diagnostics=np.loadtxt(os.path.join(obs, "diagnostics.log")),
+        config=np.array([nchain, dim, g, maxstates, es, steps, initpos], dtype=np.float64))
+
+
+def gen_ed(paces, workdir):
+    """N=4, max_ho_dims=4, J=g=omega=1: the full space (1024 states) fits, so paces == exact."""
+    ham, te = make_objects(paces, 4, 4, 1.0, 100000, 1, 0, workdir)
+    from paces.core.time_evolution import CoeffSaveParams
+    from paces.config import devices
+    with devices.vector_dev:
+        te.generate_timeline(np.arange(21) * 0.05, CoeffSaveParams())
+    obs = os.path.join(workdir, "observables")
+    np.savez_compressed(os.path.join(HERE, "ed_n4.npz"),
+                        n_exc=np.loadtxt(os.path.join(obs, "n_exc.real")),
+                        n_pho=np.loadtxt(os.path.join(obs, "n_pho.real")))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("reference", help="path of the reference checkout (read only)")
+    ap.add_argument("--long", action="store_true", help="also the 2^16-state, 200-step run")
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    paces = import_reference(os.path.abspath(args.reference))
+    rng = np.random.default_rng(20260101)
+
+    def fresh():
+        d = tempfile.mkdtemp(prefix="paces_golden_")
+        return d
+
+    jobs = []
+    for name, (n, d) in LAYOUTS.items():
+        jobs.append((f"layout_{name}", lambda name=name, n=n, d=d: gen_layout(paces, name, n, d, rng)))
+    for name, cfg in STAGE_RUNS.items():
+        jobs.append((f"stages_{name}", lambda name=name, cfg=cfg: gen_stages(paces, name, cfg, fresh())))
+    for name, cfg in TRAJ_RUNS.items():
+        jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))
+    jobs.append(("ed_n4", lambda: gen_ed(paces, fresh())))
+    if args.long:
+        for name, cfg in LONG_TRAJ_RUNS.items():
+            jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))
+    for jname, fn in jobs:
+        if args.only and args.only not in jname:
+            continue
+        print("generating", jname, flush=True)
+        fn()
+
+
+if __name__ == "__main__":
+    main()

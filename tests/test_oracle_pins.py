@@ -1,0 +1,175 @@
+"""Pin the CPU oracle to the reference: every oracle function against golden fixtures.
+
+The fixtures come from the unmodified reference run on CPU (tests/golden/gen_golden.py).
+Keys, sort order, dedup and lookup indices are compared bit-exactly; amplitudes and
+observables to 1e-12 (complex128, summation order differs between SciPy and the
+reference's NumPy stand-in only in the last bits).
+"""
+
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import paces_oracle as po
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+LAYOUTS = sorted(glob.glob(os.path.join(GOLDEN, "layout_*.npz")))
+STAGES = sorted(glob.glob(os.path.join(GOLDEN, "stages_*.npz")))
+TRAJS = sorted(glob.glob(os.path.join(GOLDEN, "traj_*.npz")))
+
+
+def _model_from_raw(f):
+    raw = f["raw"]
+    nchain = raw.shape[1] - 1
+    bw = f["bitwidths"]
+    dim = 2 ** int(bw[1])
+    return po.Model(nchain, [dim] * nchain)
+
+
+@pytest.mark.parametrize("path", LAYOUTS, ids=os.path.basename)
+def test_layout_pack_and_fields(path):
+    f = np.load(path)
+    m = _model_from_raw(f)
+    assert np.array_equal(m.bitwidths, f["bitwidths"])
+    keys = po.compress(m, f["raw"])
+    assert np.array_equal(keys, f["keys"])
+    assert np.array_equal(po.decompress(m, keys), f["raw"])
+    assert np.array_equal(po.phonon_at_exc(m, keys), f["get_occ"])
+    assert np.array_equal(po.sum_all_phonons(m, keys), f["sum_all"])
+    pos = po.get_pos(m, keys)
+    occ = po.phonon_at_exc(m, keys).astype(np.int64)
+    up = keys[f["can_up"]].copy()
+    po.add_field(m, up, 1, pos[f["can_up"]] + 1)
+    assert np.array_equal(up, f["keys_up"])
+    dn = keys[f["can_dn"]].copy()
+    po.add_field(m, dn, -1, pos[f["can_dn"]] + 1)
+    assert np.array_equal(dn, f["keys_dn"])
+    assert np.array_equal(f["can_up"], occ < m.max_ho_dims[0] - 1)
+    r = keys[pos < m.nchain - 1].copy()
+    po.add_field(m, r, 1, 0)
+    assert np.array_equal(r, f["keys_right"])
+    l_ = keys[pos > 0].copy()
+    po.add_field(m, l_, -1, 0)
+    assert np.array_equal(l_, f["keys_left"])
+    nb = po.n_pho(m, keys, np.sqrt(f["bath_weights"]))
+    np.testing.assert_allclose(nb, f["bath_n_b"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("path", LAYOUTS, ids=os.path.basename)
+def test_layout_unique_and_search(path):
+    f = np.load(path)
+    u = po.unique_rows(f["unique_in"])
+    assert np.array_equal(u, f["unique_out"])
+    assert np.array_equal(po.searchsorted(u, f["search_hit_q"]), f["search_hit_idx"])
+    idx, found = po.lookup_with_mask(u, f["search_any_q"])
+    assert np.array_equal(found, f["search_any_hit"])
+    assert np.array_equal(idx[found], f["search_any_idx"][found].astype(np.int64))
+    with pytest.raises(LookupError):
+        if (~found).any():
+            po.searchsorted(u, f["search_any_q"], allow_escapes=False)
+        else:
+            raise LookupError
+
+
+def _stage_model(f):
+    nchain, dim, g = int(f["config"][0]), int(f["config"][1]), float(f["config"][2])
+    return po.Model(nchain, [dim] * nchain, g=g), int(f["config"][3]), int(f["config"][4])
+
+
+@pytest.mark.parametrize("path", STAGES, ids=os.path.basename)
+def test_stage_by_stage(path):
+    """Each stage of each step, fed the reference's own inputs, reproduces its outputs."""
+    f = np.load(path)
+    m, maxstates, es = _stage_model(f)
+    nsteps = int(f["nsteps_recorded"])
+    assert nsteps >= 3
+    for s in range(nsteps):
+        k = f"s{s}_"
+        sel = po.truncate(f[k + "trunc_whoami"], f[k + "trunc_vector"], maxstates)
+        assert np.array_equal(sel, f[k + "select"]), f"truncation differs at step {s}"
+        if es >= 1:
+            assert np.array_equal(po.enlarge(m, sel), f[k + "enlarged"])
+        asm = po.generate_mel(m, sel, es)
+        assert np.array_equal(asm.new_inds, f[k + "new_inds"]), f"new_inds differ at step {s}"
+        assert np.array_equal(asm.diag, f[k + "diag"])
+        assert asm.ceiling_hits == int(f[k + "ceiling_hits"][0])
+        for term, mat in asm.mats.items():
+            mat = mat.copy()
+            mat.sort_indices()
+            assert np.array_equal(mat.indptr, f[k + f"csr_{term}_indptr"])
+            assert np.array_equal(mat.indices, f[k + f"csr_{term}_indices"])
+            assert np.array_equal(mat.data, f[k + f"csr_{term}_data"])
+        v = po.remap(f[k + "trunc_whoami"], f[k + "trunc_vector"], asm.new_inds)
+        assert np.array_equal(v, f[k + "remap_vector"])
+        if k + "taylor_in" in f:
+            res, dbg = po.taylor(asm, f[k + "taylor_in"], 0.05)
+            np.testing.assert_allclose(res, f[k + "taylor_out"], rtol=0, atol=1e-13)
+            assert dbg[0] == bool(f[k + "taylor_dbg"][0])
+            assert dbg[1] == int(f[k + "taylor_dbg"][1])
+        fv, fw = f[k + "final_vector"], f[k + "final_whoami"]
+        np.testing.assert_allclose(po.n_exc(m, fw, fv), f["n_exc"][s, 2:], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(po.n_pho(m, fw, fv), f["n_pho"][s, 2:], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(po.total_energy(asm, fv).real, f["energy"][s, 2], rtol=1e-12,
+                                   atol=1e-14)
+
+
+@pytest.mark.parametrize("path", TRAJS, ids=os.path.basename)
+def test_trajectory(path):
+    """The whole oracle trajectory reproduces the reference's observables and diagnostics."""
+    f = np.load(path)
+    m, maxstates, es = _stage_model(f)
+    steps, initpos = int(f["config"][5]), int(f["config"][6])
+    if maxstates > 10000:
+        pytest.skip("long trajectory: covered by the GPU parity test")
+    t = np.arange(steps + 1) * 0.05
+    tr = po.Trajectory(m, po.initial_basis(m, initpos), np.array([1.0 + 0j]), maxstates, es)
+    recs = tr.run(t)
+    ne = np.array([r.n_exc for r in recs])
+    nph = np.array([r.n_pho for r in recs])
+    np.testing.assert_allclose(ne, f["n_exc"][:, 2:], rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(nph, f["n_pho"][:, 2:], rtol=1e-10, atol=1e-14)
+    diag = f["diagnostics"]
+    assert np.array_equal(np.array([r.numstates for r in recs]), diag[:, 9].astype(int))
+    assert np.array_equal(np.array([int(r.expm_dbg[1]) for r in recs]), diag[:, 6].astype(int))
+
+
+def test_exact_diagonalisation_known_answer():
+    """N=4, cutoff 4: the adaptive basis covers the full space, so paces == exact dynamics.
+
+    The value at t=1 is the known answer the reference reproduces to all printed digits.
+    """
+    f = np.load(os.path.join(GOLDEN, "ed_n4.npz"))
+    m = po.Model(4, [4] * 4)
+    t = np.arange(21) * 0.05
+    exact = po.exact_dynamics(m, 5000, t)
+    np.testing.assert_allclose(f["n_exc"][:, 2:], exact, atol=1e-12)
+    np.testing.assert_allclose(
+        f["n_exc"][-1, 2:],
+        [0.4217194563555634, 0.4335225805672021, 0.1270492529005554, 0.0177087101766804],
+        atol=1e-15)
+    tr = po.Trajectory(m, po.initial_basis(m, 0), np.array([1.0 + 0j]), 100000, 1)
+    recs = tr.run(t)
+    np.testing.assert_allclose(np.array([r.n_exc for r in recs]), exact, atol=1e-12)
+
+
+def test_periodic_extension_reduces_and_is_exact():
+    """Periodic hopping (not in the reference) against exact dynamics on the full space."""
+    m = po.Model(3, [4] * 3, g=0.7, periodic=True)
+    t = np.arange(11) * 0.05
+    exact = po.exact_dynamics(m, 5000, t, init_pos=1)
+    tr = po.Trajectory(m, po.initial_basis(m, 1), np.array([1.0 + 0j]), 100000, 1)
+    recs = tr.run(t)
+    np.testing.assert_allclose(np.array([r.n_exc for r in recs]), exact, atol=1e-12)
+    # ring symmetry: starting on the middle site of 3, sites 0 and 2 stay equal
+    np.testing.assert_allclose(exact[:, 0], exact[:, 2], atol=1e-12)
+
+
+def test_site_disorder_extension_is_exact():
+    m = po.Model(4, [3] * 4, g=0.9, site_eps=np.array([0.3, -0.2, 0.1, 0.0]))
+    t = np.arange(11) * 0.05
+    exact = po.exact_dynamics(m, 5000, t, init_pos=2)
+    tr = po.Trajectory(m, po.initial_basis(m, 2), np.array([1.0 + 0j]), 100000, 1)
+    recs = tr.run(t)
+    np.testing.assert_allclose(np.array([r.n_exc for r in recs]), exact, atol=1e-12)
