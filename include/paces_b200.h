@@ -1,0 +1,217 @@
+/*
+ * paces_b200.h -- C ABI of libpaces_b200.so, the sm_100a implementation of the
+ * paces adaptive-basis time step (truncate -> expand -> sort/unique -> lookup ->
+ * assemble H -> expm-multiply -> observables) for the single-exciton Holstein chain.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (PACES_OK == 0).  Errors raised
+ *     inside kernels (capacity overflow, failed lookup, non-finite values, a
+ *     bounded wait that ran out) are written to the device-side status word of
+ *     the step record / context and returned by the next call that reads it.
+ *   - Device buffers are owned by the caller.  No entry point allocates device
+ *     memory after paces_create (which allocates a few bytes of status words).
+ *     Scratch comes from a caller-provided workspace sized by
+ *     paces_workspace_bytes.
+ *   - All work is enqueued on the caller's stream; nothing synchronises the
+ *     host except paces_read_record-style helpers the caller invokes itself.
+ *   - A context is not re-entrant: one host thread/stream per context.
+ *
+ * Basis layout (device)
+ *   A basis is a set of states (pos, n_0..n_{N-1}) sorted lexicographically,
+ *   stored blocked by exciton position: keys[i] holds only the phonon
+ *   occupations, packed MSB-first into `nw` uint64 words (fields never
+ *   straddle a word); blk[p] is the index of the first state with pos == p and
+ *   blk[nchain] is the number of states.  Within a block, uint64-word order is
+ *   the lexicographic order of (n_0, ..., n_{N-1}), so (pos, words) order is
+ *   the reference's MSB-first uint32 row order.  paces_keys_to_ref /
+ *   paces_keys_from_ref convert to and from the reference's whoami layout.
+ *
+ * Reference interfaces replaced (paths within rkevk/paces 1.2.0):
+ *   paces_expand       HamiltonianFramework.enlarge_basis_set  paces/core/hamiltonian.py:550-577
+ *                      + cupy_unique                          paces/aux/helpers.py:63-75
+ *   paces_assemble     HamiltonianFramework.generate_mel       paces/core/hamiltonian.py:383-547
+ *                      + TimeEvolutionFramework.create_matrices paces/core/time_evolution.py:365-372
+ *   paces_truncate     _determine_select_whoami                paces/core/time_evolution.py:833-910
+ *   paces_remap        vector remap in _generate_new_hilbert_space_cupy
+ *                                                             paces/core/time_evolution.py:781-797
+ *   paces_taylor       _simple_taylor + total_ham              paces/core/time_evolution.py:482-512, :382-400
+ *   paces_observables  calculate_n_exc / calculate_n_pho / calculate_total_energy / norm
+ *                      paces/models/holstein.py:299-322, paces/core/observables.py:95-99,
+ *                      paces/core/time_evolution.py:585-602
+ *   paces_lookup       searchsorted_full_binary                paces/aux/cupy_search.py:78-93
+ *   paces_step         TimeEvolutionFramework._evolve_single_step / _perform_first_step
+ *                      paces/core/time_evolution.py:552-650
+ */
+#ifndef PACES_B200_H
+#define PACES_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *paces_stream_t; /* a cudaStream_t */
+
+enum paces_status {
+    PACES_OK = 0,
+    PACES_ERR_CAPACITY = 1,   /* a result did not fit the caller's buffers: grow and retry */
+    PACES_ERR_LOOKUP = 2,     /* a state that must be present in a basis was not found */
+    PACES_ERR_NONFINITE = 3,  /* NaN/Inf amplitudes */
+    PACES_ERR_TIMEOUT = 4,    /* a bounded device-side wait ran out */
+    PACES_ERR_BADARG = 5,
+    PACES_ERR_CUDA = 6,       /* a CUDA runtime call failed (see paces_last_error) */
+    PACES_ERR_EXPLOSION = 7,  /* norm above ExpmParams.explosion_cutoff */
+    PACES_ERR_SHUFFLE = 8     /* tie shuffle would touch > 90% of the states */
+};
+
+enum paces_precision {
+    PACES_C128 = 0, /* complex128 amplitudes, float64 matrix elements (reference precision) */
+    PACES_C64 = 1   /* complex64 amplitudes/SpMV with fp32 accumulation; fp64 norms and scalars */
+};
+
+#define PACES_MAX_SITES 128
+
+typedef struct paces_model_desc {
+    int32_t nchain;            /* number of sites L (1D chain), 1 <= L <= 128 */
+    int32_t periodic;          /* 0: open chain (reference); 1: ring (L >= 3) */
+    int32_t precision;         /* enum paces_precision */
+    int32_t reserved;
+    const int32_t *max_ho_dims; /* host array, nchain entries, 2..256 */
+    double eps_sys;            /* use_terms["diag"]["eps_sys"] */
+    double hbar_omega;         /* use_terms["diag"]["hbar_omega"] */
+    double delta_eps;          /* use_terms["diag"]["delta_eps"] */
+    double J;                  /* use_terms["hopping"]["J"] (real) */
+    double g;                  /* use_terms["vib_coupling"]["g"] (real) */
+    const double *site_eps;    /* host array of nchain per-site energies, or NULL */
+} paces_model_desc;
+
+typedef struct paces_ctx paces_ctx;
+
+typedef struct paces_basis {
+    uint64_t *keys; /* device [cap][nw] */
+    int32_t *blk;   /* device [nchain+1]; blk[nchain] = number of states */
+    int64_t cap;    /* capacity in states */
+} paces_basis;
+
+/* H on a basis: neighbour table + per-row metadata.  nbr[k*cap + r] is the row index of
+ * the k-th neighbour of row r (k: 0 = exciton one site left, 1 = right, 2 = one phonon
+ * less at the exciton site, 3 = one phonon more), or -1 when that coupling is absent from
+ * the reference's H (both rows outside the enlarged basis, or a boundary/ceiling/floor).
+ * meta[r] = pos | n_exc << 8 | n_total << 16, from which the diagonal element is
+ * eps_sys + hbar_omega*n_total (+ delta_eps*pos) (+ site_eps[pos]). */
+typedef struct paces_hmat {
+    int32_t *nbr;
+    uint32_t *meta;
+    int64_t cap;
+} paces_hmat;
+
+typedef struct paces_step_params {
+    int64_t maxstates;       /* TimeEvoParams.maxstates */
+    int32_t enlarge_steps;   /* TimeEvoParams.enlarge_steps */
+    int32_t evolve;          /* 0: first step (no propagation), 1: propagate by dt */
+    double dt;
+    int32_t m_star;          /* ExpmParams.m_star */
+    int32_t diagnostics;     /* TimeEvoParams.diagnostics: post-remap norm and energy */
+    double tol;              /* Taylor stop tolerance (2^-53 for C128, 2^-24 for C64) */
+    int32_t shuffle;         /* 1: shuffle equal-weight states at the cut (shuffle_seed set) */
+    int32_t renormalize;     /* ExpmParams.renormalize */
+    uint64_t shuffle_seed;
+    uint64_t step_index;     /* mixes into the shuffle stream */
+    double explosion_cutoff; /* ExpmParams.explosion_cutoff */
+} paces_step_params;
+
+/* Written on the device by paces_step; the caller copies it back (one transfer per step). */
+typedef struct paces_step_record {
+    int32_t status;          /* first error raised by a kernel of this step */
+    int32_t n_select;        /* states kept by the truncation */
+    int32_t n_enlarged;      /* size of the enlarged basis the matrix elements come from */
+    int32_t n_states;        /* size of the new basis (numstates) */
+    int32_t converged;       /* Taylor: stop criterion met */
+    int32_t final_m;         /* Taylor: index of the last term (j_ind) */
+    int32_t ceiling_hits;    /* enlarged-basis states at the phonon ceiling */
+    int32_t n_tied;          /* states tied with the truncation threshold */
+    double c1_plus_c2;
+    double term_ratio;
+    double post_adapt_norm;  /* -1 when diagnostics are off */
+    double post_adapt_energy_re;
+    double post_adapt_energy_im;
+    double norm;
+    double energy_re;
+    double energy_im;
+    double n_exc[PACES_MAX_SITES];
+    double n_pho[PACES_MAX_SITES];
+} paces_step_record;
+
+/* Taylor diagnostics (device), as returned by _simple_taylor (time_evolution.py:510-511). */
+typedef struct paces_expm_info {
+    int32_t converged;
+    int32_t final_m;
+    double c1_plus_c2;
+    double term_ratio;
+} paces_expm_info;
+
+/* Observables (device output of paces_observables): [0] norm, [1] energy re, [2] energy im,
+ * [3 .. 3+L) n_exc, [3+L .. 3+2L) n_pho.  `what` is a bit set of PACES_OBS_*. */
+enum { PACES_OBS_NORM = 1, PACES_OBS_ENERGY = 2, PACES_OBS_SITES = 4 };
+
+/* ---- context ----------------------------------------------------------------------- */
+int paces_create(const paces_model_desc *desc, paces_ctx **out);
+int paces_destroy(paces_ctx *ctx);
+const char *paces_last_error(const paces_ctx *ctx);
+int paces_key_words(const paces_ctx *ctx);         /* nw: uint64 words per key */
+int paces_ref_words(const paces_ctx *ctx);         /* uint32 words per reference row */
+/* Internal key layout, nchain entries each: word index, LSB position, field width of site s. */
+int paces_key_layout(const paces_ctx *ctx, int32_t *word, int32_t *shift, int32_t *bits);
+int paces_version(void);                            /* 10000*major + 100*minor + patch */
+/* Copy the context's device status word (errors raised by kernels of the stage entry points)
+ * to the host, synchronising `stream`, and clear it. */
+int paces_read_status(paces_ctx *ctx, paces_stream_t stream, int32_t *host_status);
+/* Workspace bytes for every entry point on bases of up to `cap` states. */
+int paces_workspace_bytes(const paces_ctx *ctx, int64_t cap, size_t *bytes);
+
+/* ---- layout conversion --------------------------------------------------------------- */
+/* Reference rows (pos in the leading bits, MSB-first uint32 words, ref_words per row) ->
+ * keys + positions.  Rows need not be sorted. */
+int paces_keys_from_ref(paces_ctx *ctx, const uint32_t *ref, int64_t n, int32_t ref_words,
+                        uint64_t *keys_out, int32_t *pos_out, paces_stream_t stream);
+/* A basis -> reference rows (ref_words uint32 per row). */
+int paces_keys_to_ref(paces_ctx *ctx, const paces_basis *b, int32_t ref_words, uint32_t *ref_out,
+                      paces_stream_t stream);
+
+/* ---- stages -------------------------------------------------------------------------- */
+int paces_expand(paces_ctx *ctx, const paces_basis *in, paces_basis *out, void *ws,
+                 size_t ws_bytes, paces_stream_t stream);
+int paces_assemble(paces_ctx *ctx, const paces_basis *in, paces_basis *out, paces_hmat *h,
+                   int32_t *dev_ceiling_hits, void *ws, size_t ws_bytes, paces_stream_t stream);
+int paces_truncate(paces_ctx *ctx, const paces_basis *in, const void *psi, int64_t maxstates,
+                   int32_t shuffle, uint64_t shuffle_seed, uint64_t step_index,
+                   paces_basis *out, void *ws, size_t ws_bytes, paces_stream_t stream);
+int paces_remap(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi,
+                const paces_basis *new_b, void *new_psi, void *ws, size_t ws_bytes,
+                paces_stream_t stream);
+int paces_taylor(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi_in,
+                 void *psi_out, double dt, int32_t m_star, double tol,
+                 paces_expm_info *dev_info, void *ws, size_t ws_bytes, paces_stream_t stream);
+int paces_observables(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi,
+                      int32_t what, double *dev_out, void *ws, size_t ws_bytes,
+                      paces_stream_t stream);
+/* Lower-bound lookup of (pos, key) queries in a basis; out[i] = row index or -1 if absent.
+ * With must_exist != 0 a miss also raises PACES_ERR_LOOKUP (reference: noesc kernel). */
+int paces_lookup(paces_ctx *ctx, const paces_basis *phonebook, const uint64_t *q_keys,
+                 const int32_t *q_pos, int64_t nq, int32_t must_exist, int64_t *out,
+                 void *ws, size_t ws_bytes, paces_stream_t stream);
+
+/* One full time step: truncate(old) -> expand^enlarge_steps -> assemble -> remap ->
+ * [diagnostics] -> [Taylor] -> observables.  The old basis and amplitudes are read only;
+ * the new basis, new amplitudes, h and rec are written.
+ * Returns PACES_OK once enqueued; kernel-side errors land in rec->status. */
+int paces_step(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi, paces_basis *new_b,
+               void *new_psi, paces_hmat *h, const paces_step_params *prm,
+               paces_step_record *dev_rec, void *ws, size_t ws_bytes, paces_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PACES_B200_H */

@@ -1,0 +1,536 @@
+// C ABI of libpaces_b200 (declared in include/paces_b200.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "kernels.cuh"
+
+using namespace paces;
+
+struct paces_ctx {
+    ModelDev m;
+    RefLayout rl;
+    int nw;
+    int precision;
+    int device;
+    int num_sms;
+    int taylor_grid;
+    int* d_status;  // device status word for the stage entry points
+    char err[512];
+};
+
+namespace {
+
+int fail(const paces_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(const_cast<paces_ctx*>(c)->err, sizeof(c->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int cuda_fail(const paces_ctx* c, const char* where) {
+    const cudaError_t e = cudaGetLastError();
+    return fail(c, PACES_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define PACES_CHECK_LAUNCH(c, rc, where)                          \
+    do {                                                          \
+        const int _rc = (rc);                                     \
+        if (_rc == PACES_ERR_CUDA) return cuda_fail((c), (where)); \
+        if (_rc != PACES_OK) return fail((c), _rc, "%s failed", (where)); \
+    } while (0)
+
+// Workspace regions for bases of up to `cap` states.
+struct Layout {
+    size_t total = 0;
+    int64_t cap = 0;
+    size_t keysA, blkA, keysB, blkB, maps;
+    size_t m_run_lo, m_run_len, m_split_off, m_tile_off, m_counters, m_split_co, m_split_rank, m_ord_co,
+        m_tile_state;
+    int64_t split_cap, tile_cap;
+    size_t t_hist, t_cand, t_cand_idx, t_sel, t_tile_cnt, t_tile_pre;
+    int t_tiles;
+    size_t r_tile_off, r_counters;
+    int r_tiles;
+    size_t v_V, v_TA, v_TB, v_partials, v_bar;
+    size_t o_partials, o_out;
+};
+
+Layout make_layout(const paces_ctx* c, int64_t cap) {
+    Layout l;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) & ~size_t(255);
+        return o;
+    };
+    const int L = c->m.L, nw = c->nw;
+    const size_t cs = c->precision == PACES_C64 ? 8 : 16;
+    const size_t ucap = size_t(cap);
+    l.cap = cap;
+    l.keysA = take(ucap * nw * 8);
+    l.blkA = take(size_t(L + 1) * 4);
+    l.keysB = take(ucap * nw * 8);
+    l.blkB = take(size_t(L + 1) * 4);
+    l.maps = take(size_t(kRuns) * ucap * 4);
+    l.split_cap = merge_split_cap(cap, nw, L);
+    l.tile_cap = merge_tile_cap(l.split_cap, L);
+    l.m_run_lo = take(size_t(L) * kRuns * 4);
+    l.m_run_len = take(size_t(L) * kRuns * 4);
+    l.m_split_off = take((size_t(L) * kRuns + 1) * 4);
+    l.m_tile_off = take(size_t(L + 1) * 4);
+    l.m_counters = take(16 * 4);
+    l.m_split_co = take(size_t(l.split_cap) * kRuns * 4);
+    l.m_split_rank = take(size_t(l.split_cap) * 4);
+    l.m_ord_co = take(size_t(l.split_cap) * kRuns * 4);
+    l.m_tile_state = take(size_t(l.tile_cap) * 8);
+    l.t_tiles = trunc_tiles_cap(cap);
+    l.t_hist = take(4096 * 4);
+    l.t_cand = take(ucap * 8);
+    l.t_cand_idx = take(ucap * 4);
+    l.t_sel = take(16 * 8);
+    l.t_tile_cnt = take(size_t(l.t_tiles) * 3 * 4);
+    l.t_tile_pre = take(size_t(l.t_tiles) * 3 * 4);
+    l.r_tiles = remap_tile_cap(cap, nw, L);
+    l.r_tile_off = take(size_t(L + 1) * 4);
+    l.r_counters = take(16);
+    l.v_V = take(ucap * cs);
+    l.v_TA = take(ucap * cs);
+    l.v_TB = take(ucap * cs);
+    l.v_partials = take(size_t(2) * c->taylor_grid * 4 * 8);
+    l.v_bar = take(16);
+    l.o_partials = take(size_t(obs_max_grid(c->num_sms)) * (3 + 2 * L) * 8);
+    l.o_out = take(size_t(3 + 2 * L) * 8);
+    l.total = off;
+    return l;
+}
+
+// Largest capacity whose layout fits `bytes`.
+Layout fit_layout(const paces_ctx* c, size_t bytes) {
+    int64_t lo = 0, hi = int64_t(bytes / 8) + 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) / 2;
+        if (make_layout(c, mid).total <= bytes) lo = mid; else hi = mid - 1;
+    }
+    return make_layout(c, lo);
+}
+
+template <typename T>
+T* at(void* ws, size_t off) {
+    return reinterpret_cast<T*>(static_cast<unsigned char*>(ws) + off);
+}
+
+MergeWs merge_ws(const Layout& l, void* ws) {
+    MergeWs w;
+    w.run_lo = at<int>(ws, l.m_run_lo);
+    w.run_len = at<int>(ws, l.m_run_len);
+    w.split_off = at<int>(ws, l.m_split_off);
+    w.tile_off = at<int>(ws, l.m_tile_off);
+    w.counters = at<int>(ws, l.m_counters);
+    w.split_co = at<int>(ws, l.m_split_co);
+    w.split_rank = at<int>(ws, l.m_split_rank);
+    w.ord_co = at<int>(ws, l.m_ord_co);
+    w.tile_state = at<unsigned long long>(ws, l.m_tile_state);
+    w.split_cap = int(l.split_cap);
+    w.tile_cap = int(l.tile_cap);
+    return w;
+}
+
+TruncWs trunc_ws(const Layout& l, void* ws) {
+    TruncWs w;
+    w.hist = at<unsigned>(ws, l.t_hist);
+    w.cand = at<unsigned long long>(ws, l.t_cand);
+    w.cand_idx = at<int>(ws, l.t_cand_idx);
+    w.sel = at<long long>(ws, l.t_sel);
+    w.tile_cnt = at<int>(ws, l.t_tile_cnt);
+    w.tile_pre = at<int>(ws, l.t_tile_pre);
+    w.cap = l.cap;
+    w.ntiles_cap = l.t_tiles;
+    return w;
+}
+
+RemapWs remap_ws(const Layout& l, void* ws) {
+    RemapWs w;
+    w.tile_off = at<int>(ws, l.r_tile_off);
+    w.counters = at<int>(ws, l.r_counters);
+    w.tile_cap = l.r_tiles;
+    return w;
+}
+
+TaylorWs taylor_ws(const Layout& l, void* ws) {
+    TaylorWs w;
+    w.ta = at<void>(ws, l.v_TA);
+    w.tb = at<void>(ws, l.v_TB);
+    w.partials = at<double>(ws, l.v_partials);
+    w.barrier = at<unsigned>(ws, l.v_bar);
+    return w;
+}
+
+bool valid_basis(const paces_basis* b) { return b && b->keys && b->blk && b->cap >= 0; }
+
+__global__ void record_init_kernel(paces_step_record* rec, int diagnostics) {
+    if (threadIdx.x != 0) return;
+    memset(rec, 0, sizeof(paces_step_record));
+    rec->post_adapt_norm = -1.0;
+    rec->post_adapt_energy_re = __longlong_as_double(0x7ff8000000000000ll);
+    rec->post_adapt_energy_im = 0.0;
+    (void)diagnostics;
+}
+
+__global__ void record_counts_kernel(paces_step_record* rec, const int* sel_blk, const int* enl_blk,
+                                     const int* new_blk, int L) {
+    if (threadIdx.x != 0) return;
+    rec->n_select = sel_blk[L];
+    rec->n_enlarged = enl_blk[L];
+    rec->n_states = new_blk[L];
+}
+
+}  // namespace
+
+extern "C" {
+
+int paces_version(void) { return 10200; }
+
+int paces_create(const paces_model_desc* d, paces_ctx** out) {
+    if (!out) return PACES_ERR_BADARG;
+    *out = nullptr;
+    if (!d || !d->max_ho_dims) return PACES_ERR_BADARG;
+    const int L = d->nchain;
+    if (L < 2 || L > kMaxSites) return PACES_ERR_BADARG;
+    if (d->periodic && L < 3) return PACES_ERR_BADARG;
+    if (d->precision != PACES_C128 && d->precision != PACES_C64) return PACES_ERR_BADARG;
+    paces_ctx* c = new paces_ctx();
+    std::memset(c, 0, sizeof(*c));
+    ModelDev& m = c->m;
+    m.L = L;
+    m.periodic = d->periodic ? 1 : 0;
+    m.eps_sys = d->eps_sys;
+    m.hbar_omega = d->hbar_omega;
+    m.delta_eps = d->delta_eps;
+    m.J = d->J;
+    m.g = d->g;
+    m.has_site_eps = d->site_eps ? 1 : 0;
+    int word = 0, used = 0, total_bits = 0;
+    for (int s = 0; s < L; ++s) {
+        const int md = d->max_ho_dims[s];
+        if (md < 2 || md > 256) {
+            delete c;
+            return PACES_ERR_BADARG;
+        }
+        int b = 0;
+        while ((1 << b) < md) ++b;  // ceil(log2(max_dim)), paces/core/hamiltonian.py:155
+        if (used + b > 64) {
+            ++word;
+            used = 0;
+        }
+        m.word[s] = uint8_t(word);
+        m.shift[s] = uint8_t(64 - used - b);
+        m.bits[s] = uint8_t(b);
+        m.maxd[s] = uint16_t(md);
+        m.site_eps[s] = d->site_eps ? d->site_eps[s] : 0.0;
+        used += b;
+        total_bits += b;
+    }
+    c->nw = word + 1;
+    m.nw = c->nw;
+    if (c->nw > 8) {
+        delete c;
+        return PACES_ERR_BADARG;
+    }
+    // reference row layout: position field first, then the sites (hamiltonian.py:140-160)
+    int pb = 0;
+    while ((1 << pb) < L) ++pb;
+    c->rl.nfields = L + 1;
+    c->rl.off[0] = 0;
+    c->rl.bits[0] = pb;
+    for (int s = 0; s < L; ++s) {
+        c->rl.off[s + 1] = c->rl.off[s] + c->rl.bits[s];
+        c->rl.bits[s + 1] = m.bits[s];
+    }
+    c->rl.words = (pb + total_bits + 31) / 32;
+    if (c->rl.words > kMaxRefWords) {
+        delete c;
+        return PACES_ERR_BADARG;
+    }
+    c->precision = d->precision;
+    if (cudaGetDevice(&c->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) {
+        delete c;
+        return PACES_ERR_CUDA;
+    }
+    c->taylor_grid = taylor_max_grid(c->precision == PACES_C64, c->num_sms);
+    if (cudaMalloc(&c->d_status, 64) != cudaSuccess || cudaMemset(c->d_status, 0, 64) != cudaSuccess) {
+        delete c;
+        return PACES_ERR_CUDA;
+    }
+    *out = c;
+    return PACES_OK;
+}
+
+int paces_destroy(paces_ctx* c) {
+    if (!c) return PACES_OK;
+    if (c->d_status) cudaFree(c->d_status);
+    delete c;
+    return PACES_OK;
+}
+
+const char* paces_last_error(const paces_ctx* c) { return c ? c->err : "no context"; }
+
+int paces_key_words(const paces_ctx* c) { return c ? c->nw : 0; }
+
+int paces_ref_words(const paces_ctx* c) { return c ? c->rl.words : 0; }
+
+int paces_key_layout(const paces_ctx* c, int32_t* word, int32_t* shift, int32_t* bits) {
+    if (!c) return PACES_ERR_BADARG;
+    for (int s = 0; s < c->m.L; ++s) {
+        if (word) word[s] = c->m.word[s];
+        if (shift) shift[s] = c->m.shift[s];
+        if (bits) bits[s] = c->m.bits[s];
+    }
+    return PACES_OK;
+}
+
+int paces_workspace_bytes(const paces_ctx* c, int64_t cap, size_t* bytes) {
+    if (!c || !bytes || cap < 0) return PACES_ERR_BADARG;
+    *bytes = make_layout(c, cap).total;
+    return PACES_OK;
+}
+
+int paces_read_status(paces_ctx* c, paces_stream_t stream, int32_t* host_status) {
+    if (!c || !host_status) return PACES_ERR_BADARG;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(host_status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess || cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), st) != cudaSuccess)
+        return cuda_fail(c, "paces_read_status");
+    return PACES_OK;
+}
+
+int paces_keys_from_ref(paces_ctx* c, const uint32_t* ref, int64_t n, int32_t ref_words,
+                        uint64_t* keys_out, int32_t* pos_out, paces_stream_t stream) {
+    if (!c) return PACES_ERR_BADARG;
+    if (ref_words != c->rl.words) return fail(c, PACES_ERR_BADARG, "reference rows have %d words, model needs %d", ref_words, c->rl.words);
+    PACES_CHECK_LAUNCH(c, launch_keys_from_ref(c->nw, c->m, c->rl, ref, n, keys_out, pos_out, c->d_status,
+                                               c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
+                       "keys_from_ref");
+    return PACES_OK;
+}
+
+int paces_keys_to_ref(paces_ctx* c, const paces_basis* b, int32_t ref_words, uint32_t* ref_out,
+                      paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !ref_out) return PACES_ERR_BADARG;
+    if (ref_words != c->rl.words) return fail(c, PACES_ERR_BADARG, "reference rows have %d words, model needs %d", ref_words, c->rl.words);
+    PACES_CHECK_LAUNCH(c, launch_keys_to_ref(c->nw, c->m, c->rl, b->keys, b->blk, ref_out, c->num_sms,
+                                             reinterpret_cast<cudaStream_t>(stream)),
+                       "keys_to_ref");
+    return PACES_OK;
+}
+
+int paces_expand(paces_ctx* c, const paces_basis* in, paces_basis* out, void* ws, size_t ws_bytes,
+                 paces_stream_t stream) {
+    if (!c || !valid_basis(in) || !valid_basis(out) || !ws) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
+    MergeOut mo{};
+    mo.keys = out->keys;
+    mo.blk = out->blk;
+    mo.cap = out->cap;
+    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->m, in->keys, in->blk, merge_ws(l, ws), mo, nullptr,
+                                       c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
+                       "expand");
+    return PACES_OK;
+}
+
+int paces_assemble(paces_ctx* c, const paces_basis* in, paces_basis* out, paces_hmat* h,
+                   int32_t* dev_ceiling_hits, void* ws, size_t ws_bytes, paces_stream_t stream) {
+    if (!c || !valid_basis(in) || !valid_basis(out) || !h || !h->nbr || !h->meta || !ws) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
+    MergeOut mo{};
+    mo.keys = out->keys;
+    mo.blk = out->blk;
+    mo.cap = out->cap;
+    mo.meta = h->meta;
+    mo.nbr = h->nbr;
+    mo.nbr_cap = h->cap;
+    mo.maps = at<int>(ws, l.maps);
+    mo.map_cap = l.cap;
+    if (h->cap < out->cap) mo.cap = h->cap;
+    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->m, in->keys, in->blk, merge_ws(l, ws), mo, dev_ceiling_hits,
+                                       c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
+                       "assemble");
+    return PACES_OK;
+}
+
+int paces_truncate(paces_ctx* c, const paces_basis* in, const void* psi, int64_t maxstates, int32_t shuffle,
+                   uint64_t shuffle_seed, uint64_t step_index, paces_basis* out, void* ws, size_t ws_bytes,
+                   paces_stream_t stream) {
+    if (!c || !valid_basis(in) || !valid_basis(out) || !psi || !ws || maxstates < 1) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
+    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, psi, maxstates,
+                                          shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys, out->blk,
+                                          out->cap, nullptr, c->d_status, c->num_sms,
+                                          reinterpret_cast<cudaStream_t>(stream)),
+                       "truncate");
+    return PACES_OK;
+}
+
+int paces_remap(paces_ctx* c, const paces_basis* old_b, const void* old_psi, const paces_basis* new_b,
+                void* new_psi, void* ws, size_t ws_bytes, paces_stream_t stream) {
+    if (!c || !valid_basis(old_b) || !valid_basis(new_b) || !old_psi || !new_psi || !ws) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    if (old_b->cap > l.cap || new_b->cap > l.cap)
+        return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states", (long long)l.cap);
+    PACES_CHECK_LAUNCH(c, launch_remap(c->nw, c->precision == PACES_C64, c->m, old_b->keys, old_b->blk, old_psi,
+                                       new_b->keys, new_b->blk, new_psi, remap_ws(l, ws), c->d_status, c->num_sms,
+                                       reinterpret_cast<cudaStream_t>(stream)),
+                       "remap");
+    return PACES_OK;
+}
+
+int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi_in, void* psi_out,
+                 double dt, int32_t m_star, double tol, paces_expm_info* dev_info, void* ws, size_t ws_bytes,
+                 paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !psi_in || !psi_out || psi_in == psi_out || !ws || m_star < 1)
+        return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    if (h->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states", (long long)l.cap);
+    TaylorOut o{};
+    if (dev_info) {
+        o.converged = &dev_info->converged;
+        o.final_m = &dev_info->final_m;
+        o.c1_plus_c2 = &dev_info->c1_plus_c2;
+        o.term_ratio = &dev_info->term_ratio;
+    }
+    PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->cap, h->meta, psi_in,
+                                        psi_out, dt, m_star, tol, taylor_ws(l, ws), o, c->d_status, c->num_sms,
+                                        reinterpret_cast<cudaStream_t>(stream)),
+                       "taylor");
+    return PACES_OK;
+}
+
+int paces_observables(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi, int32_t what,
+                      double* dev_out, void* ws, size_t ws_bytes, paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !psi || !dev_out || !ws) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    const int L = c->m.L;
+    ObsTarget t{dev_out, dev_out + 1, dev_out + 2, dev_out + 3, dev_out + 3 + L};
+    PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c->precision == PACES_C64, c->m, b->keys, b->blk, h->nbr, h->cap,
+                                             h->meta, psi, what, at<double>(ws, l.o_partials), t, c->num_sms,
+                                             reinterpret_cast<cudaStream_t>(stream)),
+                       "observables");
+    return PACES_OK;
+}
+
+int paces_lookup(paces_ctx* c, const paces_basis* pb, const uint64_t* q_keys, const int32_t* q_pos, int64_t nq,
+                 int32_t must_exist, int64_t* out, void* ws, size_t ws_bytes, paces_stream_t stream) {
+    (void)ws;
+    (void)ws_bytes;
+    if (!c || !valid_basis(pb) || (nq > 0 && (!q_keys || !q_pos || !out))) return PACES_ERR_BADARG;
+    PACES_CHECK_LAUNCH(c, launch_lookup(c->nw, c->m, pb->keys, pb->blk, q_keys, q_pos, nq, must_exist, out,
+                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
+                       "lookup");
+    return PACES_OK;
+}
+
+int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces_basis* new_b, void* new_psi,
+               paces_hmat* h, const paces_step_params* prm, paces_step_record* rec, void* ws, size_t ws_bytes,
+               paces_stream_t stream) {
+    if (!c || !valid_basis(old_b) || !valid_basis(new_b) || !old_psi || !new_psi || !h || !h->nbr || !h->meta ||
+        !prm || !rec || !ws)
+        return fail(c, PACES_ERR_BADARG, "paces_step: null argument");
+    if (prm->maxstates < 1 || prm->enlarge_steps < 0 || (prm->evolve && prm->m_star < 1))
+        return fail(c, PACES_ERR_BADARG, "paces_step: bad parameters");
+    const Layout l = fit_layout(c, ws_bytes);
+    if (old_b->cap > l.cap || new_b->cap > l.cap || h->cap > l.cap)
+        return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states; bases hold %lld/%lld", (long long)l.cap,
+                    (long long)old_b->cap, (long long)new_b->cap);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const bool c64 = c->precision == PACES_C64;
+    const int L = c->m.L;
+    int* status = &rec->status;
+    record_init_kernel<<<1, 32, 0, st>>>(rec, prm->diagnostics);
+
+    paces_basis A{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap};
+    paces_basis B{at<uint64_t>(ws, l.keysB), at<int32_t>(ws, l.blkB), l.cap};
+    // 1. truncation of the old state
+    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, old_b->keys, old_b->blk, old_psi, prm->maxstates,
+                                          prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), A.keys,
+                                          A.blk, A.cap, &rec->n_tied, status, c->num_sms, st),
+                       "step/truncate");
+    // 2. enlargement (enlarge_steps times)
+    const MergeWs mws = merge_ws(l, ws);
+    paces_basis* cur = &A;
+    paces_basis* other = &B;
+    for (int e = 0; e < prm->enlarge_steps; ++e) {
+        MergeOut mo{};
+        mo.keys = other->keys;
+        mo.blk = other->blk;
+        mo.cap = other->cap;
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->m, cur->keys, cur->blk, mws, mo, nullptr, status,
+                                           c->num_sms, st),
+                           "step/expand");
+        paces_basis* t = cur;
+        cur = other;
+        other = t;
+    }
+    // 3. new basis + H
+    {
+        MergeOut mo{};
+        mo.keys = new_b->keys;
+        mo.blk = new_b->blk;
+        mo.cap = new_b->cap < h->cap ? new_b->cap : h->cap;
+        mo.meta = h->meta;
+        mo.nbr = h->nbr;
+        mo.nbr_cap = h->cap;
+        mo.maps = at<int>(ws, l.maps);
+        mo.map_cap = l.cap;
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->m, cur->keys, cur->blk, mws, mo, &rec->ceiling_hits,
+                                           status, c->num_sms, st),
+                           "step/assemble");
+    }
+    // 4. amplitudes into the new basis
+    void* target = prm->evolve ? at<void>(ws, l.v_V) : new_psi;
+    PACES_CHECK_LAUNCH(c, launch_remap(c->nw, c64, c->m, old_b->keys, old_b->blk, old_psi, new_b->keys, new_b->blk,
+                                       target, remap_ws(l, ws), status, c->num_sms, st),
+                       "step/remap");
+    double* opart = at<double>(ws, l.o_partials);
+    // 5. post-adaptation diagnostics
+    if (prm->diagnostics) {
+        ObsTarget t{&rec->post_adapt_norm, &rec->post_adapt_energy_re, &rec->post_adapt_energy_im, nullptr, nullptr};
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, new_b->keys, new_b->blk, h->nbr, h->cap, h->meta,
+                                                 target, PACES_OBS_NORM | PACES_OBS_ENERGY, opart, t, c->num_sms, st),
+                           "step/diagnostics");
+    }
+    // 6. propagation
+    if (prm->evolve) {
+        TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
+        PACES_CHECK_LAUNCH(c, launch_taylor(c64, c->m, new_b->blk, h->nbr, h->cap, h->meta, target, new_psi, prm->dt,
+                                            prm->m_star, prm->tol, taylor_ws(l, ws), o, status, c->num_sms, st),
+                           "step/taylor");
+        if (prm->renormalize) {
+            ObsTarget t{&rec->norm, nullptr, nullptr, nullptr, nullptr};
+            PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, new_b->keys, new_b->blk, h->nbr, h->cap, h->meta,
+                                                     new_psi, PACES_OBS_NORM, opart, t, c->num_sms, st),
+                               "step/norm");
+            PACES_CHECK_LAUNCH(c, launch_scale(c64, c->m, new_b->blk, new_psi, &rec->norm, c->num_sms, st),
+                               "step/renormalize");
+        }
+    }
+    // 7. observables of the new state
+    {
+        ObsTarget t{&rec->norm, &rec->energy_re, &rec->energy_im, rec->n_exc, rec->n_pho};
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, new_b->keys, new_b->blk, h->nbr, h->cap, h->meta,
+                                                 new_psi, PACES_OBS_NORM | PACES_OBS_ENERGY | PACES_OBS_SITES, opart, t,
+                                                 c->num_sms, st),
+                           "step/observables");
+    }
+    record_counts_kernel<<<1, 32, 0, st>>>(rec, A.blk, cur->blk, new_b->blk, L);
+    if (cudaGetLastError() != cudaSuccess) return cuda_fail(c, "step/record");
+    return PACES_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,136 @@
+// Shared device definitions of libpaces_b200: model descriptor, packed Fock keys,
+// key comparison, status reporting and bounded waits.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/paces_b200.h"
+
+namespace paces {
+
+constexpr int kMaxSites = PACES_MAX_SITES;
+constexpr int kRuns = 5;  // candidate runs per exciton block: self, from-left, from-right, up, down
+enum Run : int { RUN_SELF = 0, RUN_FROM_LEFT = 1, RUN_FROM_RIGHT = 2, RUN_UP = 3, RUN_DOWN = 4 };
+// neighbour slots of the H table (paces_hmat.nbr)
+enum Slot : int { NB_LEFT = 0, NB_RIGHT = 1, NB_DOWN = 2, NB_UP = 3 };
+
+// Model constants passed by value to every kernel (fits the 32 KB parameter space).
+struct ModelDev {
+    int L;             // sites == exciton positions
+    int nw;            // uint64 words per key
+    int periodic;
+    int has_site_eps;
+    double eps_sys, hbar_omega, delta_eps, J, g;
+    uint8_t word[kMaxSites];   // word holding site s
+    uint8_t shift[kMaxSites];  // bit position of the field's least significant bit
+    uint8_t bits[kMaxSites];   // field width
+    uint16_t maxd[kMaxSites];  // max_ho_dims[s]
+    double site_eps[kMaxSites];
+};
+
+template <int NW>
+struct Key {
+    uint64_t w[NW];
+};
+
+template <int NW>
+__device__ __forceinline__ Key<NW> load_key(const uint64_t* __restrict__ base, int64_t i) {
+    Key<NW> k;
+    const uint64_t* q = base + i * NW;
+    if constexpr (NW % 2 == 0) {
+#pragma unroll
+        for (int w = 0; w < NW; w += 2) {
+            ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(q + w));
+            k.w[w] = v.x;
+            k.w[w + 1] = v.y;
+        }
+    } else {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) k.w[w] = __ldg(q + w);
+    }
+    return k;
+}
+
+template <int NW>
+__device__ __forceinline__ void store_key(uint64_t* __restrict__ base, int64_t i, const Key<NW>& k) {
+    uint64_t* q = base + i * NW;
+    if constexpr (NW % 2 == 0) {
+#pragma unroll
+        for (int w = 0; w < NW; w += 2)
+            *reinterpret_cast<ulonglong2*>(q + w) = make_ulonglong2(k.w[w], k.w[w + 1]);
+    } else {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) q[w] = k.w[w];
+    }
+}
+
+// -1 / 0 / +1 lexicographic comparison of the word sequences.
+template <int NW>
+__device__ __forceinline__ int key_cmp(const Key<NW>& a, const Key<NW>& b) {
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        if (a.w[w] != b.w[w]) return a.w[w] < b.w[w] ? -1 : 1;
+    }
+    return 0;
+}
+
+template <int NW>
+__device__ __forceinline__ bool key_eq(const Key<NW>& a, const Key<NW>& b) {
+    bool eq = true;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) eq &= (a.w[w] == b.w[w]);
+    return eq;
+}
+
+template <int NW>
+__device__ __forceinline__ uint32_t get_field(const ModelDev& m, const Key<NW>& k, int s) {
+    const uint64_t mask = (uint64_t(1) << m.bits[s]) - 1;
+    uint64_t word = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w)
+        if (w == m.word[s]) word = k.w[w];
+    return uint32_t((word >> m.shift[s]) & mask);
+}
+
+// field s += delta (caller guarantees no overflow out of the field)
+template <int NW>
+__device__ __forceinline__ void add_field(const ModelDev& m, Key<NW>& k, int s, int delta) {
+    const uint64_t one = uint64_t(1) << m.shift[s];
+#pragma unroll
+    for (int w = 0; w < NW; ++w)
+        if (w == m.word[s]) k.w[w] = delta > 0 ? k.w[w] + one : k.w[w] - one;
+}
+
+template <int NW>
+__device__ __forceinline__ uint32_t total_phonons(const ModelDev& m, const Key<NW>& k) {
+    uint32_t t = 0;
+    for (int s = 0; s < m.L; ++s) t += get_field(m, k, s);
+    return t;
+}
+
+// ---- status words ------------------------------------------------------------------------
+__device__ __forceinline__ void raise_status(int* status, int code) {
+    if (status) atomicCAS(status, 0, code);
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Upper bound on any device-side wait (look-back, grid barrier): 2 s.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+// Block id of `i` in block offsets blk[0..L] (blk sorted): largest p with blk[p] <= i.
+__device__ __forceinline__ int block_of(const int* blk, int L, int64_t i) {
+    int lo = 0, hi = L - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (blk[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+}  // namespace paces

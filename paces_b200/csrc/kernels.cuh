@@ -1,0 +1,87 @@
+// Declarations shared between the stage kernels and the C ABI layer.
+#pragma once
+
+#include <type_traits>
+
+#include "common.cuh"
+#include "merge.cuh"
+#include "truncate.cuh"
+
+namespace paces {
+
+// Largest r with off[r] <= s (off non-decreasing with n+1 entries, s < off[n]).
+__device__ __forceinline__ int find_segment(const int* off, int n, int s) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= s) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---- remap ------------------------------------------------------------------------------
+struct RemapWs {
+    int* tile_off;  // [L+1]
+    int* counters;  // [0] tiles
+    int tile_cap;
+};
+__host__ __device__ constexpr int remap_tile(int nw) { return nw <= 2 ? 2048 : (nw <= 4 ? 1024 : 512); }
+inline int remap_tile_cap(int64_t cap, int nw, int L) { return int((2 * cap) / remap_tile(nw) + L + 8); }
+int launch_remap(int nw, bool c64, const ModelDev& m, const uint64_t* ok, const int* ob,
+                 const void* opsi, const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws,
+                 int* status, int num_sms, cudaStream_t st);
+
+// ---- Taylor -----------------------------------------------------------------------------
+struct TaylorOut {
+    int* converged;
+    int* final_m;
+    double* c1_plus_c2;
+    double* term_ratio;
+};
+struct TaylorWs {
+    void* ta;            // [cap] complex
+    void* tb;            // [cap] complex
+    double* partials;    // [2][max_grid][4]
+    unsigned* barrier;   // [2]
+};
+int taylor_max_grid(bool c64, int num_sms);
+int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,
+                  const uint32_t* meta, const void* v_in, void* res, double dt, int m_star,
+                  double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
+                  cudaStream_t st);
+
+// ---- observables --------------------------------------------------------------------------
+struct ObsTarget {
+    double* norm;        // may be null
+    double* energy_re;
+    double* energy_im;
+    double* n_exc;       // [L] or null
+    double* n_pho;       // [L] or null
+};
+constexpr int kObsGridPerSm = 4;
+inline int obs_max_grid(int num_sms) { return num_sms * kObsGridPerSm; }
+int launch_observables(int nw, bool c64, const ModelDev& m, const uint64_t* keys, const int* blk,
+                       const int* nbr, int64_t nbr_cap, const uint32_t* meta, const void* psi,
+                       int what, double* partials, const ObsTarget& out, int num_sms,
+                       cudaStream_t st);
+int launch_scale(bool c64, const ModelDev& m, const int* blk, void* psi, const double* norm,
+                 int num_sms, cudaStream_t st);
+
+// ---- lookup and layout conversion -------------------------------------------------------
+struct RefLayout {
+    int words;                    // uint32 words per reference row
+    int nfields;                  // L + 1 (field 0 = exciton position)
+    int off[kMaxSites + 1];       // bit offset of each field from the row's MSB
+    int bits[kMaxSites + 1];
+};
+constexpr int kMaxRefWords = 40;
+int launch_lookup(int nw, const ModelDev& m, const uint64_t* pk, const int* pblk,
+                  const uint64_t* qk, const int* qpos, int64_t nq, int must_exist, int64_t* out,
+                  int* status, int num_sms, cudaStream_t st);
+int launch_keys_to_ref(int nw, const ModelDev& m, const RefLayout& rl, const uint64_t* keys,
+                       const int* blk, uint32_t* ref, int num_sms, cudaStream_t st);
+int launch_keys_from_ref(int nw, const ModelDev& m, const RefLayout& rl, const uint32_t* ref,
+                         int64_t n, uint64_t* keys, int* pos, int* status, int num_sms,
+                         cudaStream_t st);
+
+}  // namespace paces

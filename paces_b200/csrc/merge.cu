@@ -1,0 +1,549 @@
+// Structured k-way merge kernels (see merge.cuh for the design).
+#include "kernels.cuh"
+
+namespace paces {
+
+namespace {
+
+constexpr int kTileThreads = 256;
+constexpr unsigned long long kLbAgg = 1ull << 62;
+constexpr unsigned long long kLbInc = 2ull << 62;
+constexpr unsigned long long kLbMask = (1ull << 62) - 1;
+
+// Source block of run j of output block p, or -1.
+__device__ __forceinline__ int run_source(const ModelDev& m, int p, int j) {
+    if (j == RUN_FROM_LEFT) return p >= 1 ? p - 1 : (m.periodic ? m.L - 1 : -1);
+    if (j == RUN_FROM_RIGHT) return p + 1 < m.L ? p + 1 : (m.periodic ? 0 : -1);
+    return p;
+}
+
+// Element `src` of X as it appears in run j of block p: key and order flag
+// (0 = floor hole, 1 = real, 2 = ceiling hole).
+template <int NW>
+__device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __restrict__ X, int p,
+                                         int j, int64_t src, Key<NW>& k, int& flag) {
+    k = load_key<NW>(X, src);
+    flag = 1;
+    if (j == RUN_UP || j == RUN_DOWN) {
+        const int w = m.word[p];
+        const int sh = m.shift[p];
+        const uint32_t n = get_field(m, k, p);
+        const uint64_t low = sh == 0 ? 0ull : ((uint64_t(1) << sh) - 1);
+        if (j == RUN_UP) {
+            if (n + 1 >= m.maxd[p]) {
+                flag = 2;
+#pragma unroll
+                for (int q = 0; q < NW; ++q) {
+                    if (q == w) k.w[q] |= low;
+                    else if (q > w) k.w[q] = ~0ull;
+                }
+            } else {
+                add_field(m, k, p, +1);
+            }
+        } else {
+            if (n == 0) {
+                flag = 0;
+#pragma unroll
+                for (int q = 0; q < NW; ++q) {
+                    if (q == w) k.w[q] &= ~low;
+                    else if (q > w) k.w[q] = 0ull;
+                }
+            } else {
+                add_field(m, k, p, -1);
+            }
+        }
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ int cmp_kf(const Key<NW>& a, int fa, const Key<NW>& b, int fb) {
+    int c = key_cmp(a, b);
+    return c != 0 ? c : (fa - fb);
+}
+
+// Elements of run (p, j) that precede (key, flag): strictly smaller, or not larger when
+// `upper` (the element's own run index is larger than j).
+template <int NW>
+__device__ int run_bound(const ModelDev& m, const uint64_t* __restrict__ X, int p, int j, int lo,
+                         int len, const Key<NW>& key, int flag, bool upper) {
+    int a = 0, b = len;
+    while (a < b) {
+        const int mid = (a + b) >> 1;
+        Key<NW> k2;
+        int f2;
+        run_elem<NW>(m, X, p, j, lo + mid, k2, f2);
+        const int c = cmp_kf(k2, f2, key, flag);
+        if (upper ? (c <= 0) : (c < 0)) a = mid + 1; else b = mid;
+    }
+    return a;
+}
+
+template <int NW>
+__device__ __forceinline__ int smem_bound(const Key<NW>* keys, const uint8_t* flags, int off, int len,
+                                          const Key<NW>& key, int flag, bool upper) {
+    int a = 0, b = len;
+    while (a < b) {
+        const int mid = (a + b) >> 1;
+        const int c = cmp_kf(keys[off + mid], int(flags[off + mid]), key, flag);
+        if (upper ? (c <= 0) : (c < 0)) a = mid + 1; else b = mid;
+    }
+    return a;
+}
+
+__global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, MergeWs ws, int stride,
+                                  int* status) {
+    __shared__ int s_len[kMaxSites * kRuns];
+    __shared__ int s_tiles;
+    const int L = m.L;
+    for (int idx = threadIdx.x; idx < L * kRuns; idx += blockDim.x) {
+        const int p = idx / kRuns, j = idx % kRuns;
+        const int src = run_source(m, p, j);
+        int lo = 0, len = 0;
+        if (src >= 0) {
+            lo = x_blk[src];
+            len = x_blk[src + 1] - lo;
+        }
+        ws.run_lo[idx] = lo;
+        ws.run_len[idx] = len;
+        s_len[idx] = len;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0, tacc = 0;
+        for (int p = 0; p < L; ++p) {
+            const int first = acc;
+            for (int j = 0; j < kRuns; ++j) {
+                ws.split_off[p * kRuns + j] = acc;
+                acc += (s_len[p * kRuns + j] + stride - 1) / stride;
+            }
+            ws.tile_off[p] = tacc;
+            tacc += (acc - first + kMergeGroup - 1) / kMergeGroup;
+        }
+        ws.split_off[L * kRuns] = acc;
+        ws.tile_off[L] = tacc;
+        const bool ok = acc <= ws.split_cap && tacc <= ws.tile_cap;
+        if (!ok) raise_status(status, PACES_ERR_CAPACITY);
+        ws.counters[0] = ok ? acc : 0;
+        ws.counters[1] = ok ? tacc : 0;
+        ws.counters[2] = 0;
+        ws.counters[3] = 0;
+        ws.counters[4] = 0;
+        s_tiles = ok ? tacc : 0;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < s_tiles; t += blockDim.x) ws.tile_state[t] = 0ull;
+}
+
+template <int NW>
+__global__ void __launch_bounds__(256) merge_split_kernel(ModelDev m, const uint64_t* __restrict__ X,
+                                                          MergeWs ws, int stride) {
+    const int total = ws.counters[0];
+    const int nr = m.L * kRuns;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
+        const int r = find_segment(ws.split_off, nr, s);
+        const int p = r / kRuns, j = r % kRuns;
+        const int i = (s - ws.split_off[r]) * stride;
+        Key<NW> k;
+        int f;
+        run_elem<NW>(m, X, p, j, ws.run_lo[r] + i, k, f);
+        int rank = 0;
+#pragma unroll 1
+        for (int jj = 0; jj < kRuns; ++jj) {
+            int co;
+            if (jj == j) co = i;
+            else co = run_bound<NW>(m, X, p, jj, ws.run_lo[p * kRuns + jj], ws.run_len[p * kRuns + jj],
+                                    k, f, jj < j);
+            ws.split_co[int64_t(s) * kRuns + jj] = co;
+            rank += co;
+        }
+        ws.split_rank[s] = rank;
+    }
+}
+
+__global__ void __launch_bounds__(256) merge_order_kernel(ModelDev m, MergeWs ws) {
+    const int total = ws.counters[0];
+    const int nr = m.L * kRuns;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
+        const int r = find_segment(ws.split_off, nr, s);
+        const int p = r / kRuns, j = r % kRuns;
+        const int own = s - ws.split_off[r];
+        const int rank = ws.split_rank[s];
+        int o = own;
+        for (int jj = 0; jj < kRuns; ++jj) {
+            if (jj == j) continue;
+            int a = ws.split_off[p * kRuns + jj], b = ws.split_off[p * kRuns + jj + 1];
+            const int base = a;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                if (ws.split_rank[mid] < rank) a = mid + 1; else b = mid;
+            }
+            o += a - base;
+        }
+        const int64_t dst = int64_t(ws.split_off[p * kRuns]) + o;
+        if (dst >= ws.split_off[(p + 1) * kRuns]) continue;  // inconsistent ranks: cannot happen for sorted runs
+#pragma unroll
+        for (int jj = 0; jj < kRuns; ++jj) ws.ord_co[dst * kRuns + jj] = ws.split_co[int64_t(s) * kRuns + jj];
+    }
+}
+
+// Exclusive prefix of `count` over tiles taken in ticket order (decoupled look-back).
+__device__ int lookback_prefix(unsigned long long* state, int t, int count, int* status) {
+    if (t == 0) {
+        atomicExch(&state[0], kLbInc | (unsigned long long)count);
+        return 0;
+    }
+    atomicExch(&state[t], kLbAgg | (unsigned long long)count);
+    long long excl = 0;
+    int pred = t - 1;
+    const uint64_t t0 = global_ns();
+    while (pred >= 0) {
+        const unsigned long long v = atomicAdd(&state[pred], 0ull);
+        const unsigned long long fl = v >> 62;
+        if (fl == 0) {
+            if (global_ns() - t0 > kWaitLimitNs) {
+                raise_status(status, PACES_ERR_TIMEOUT);
+                break;
+            }
+            __nanosleep(64);
+            continue;
+        }
+        excl += (long long)(v & kLbMask);
+        if (fl == 2) break;
+        --pred;
+    }
+    __threadfence();
+    atomicExch(&state[t], kLbInc | (unsigned long long)(excl + count));
+    return int(excl);
+}
+
+template <int NW, bool ASM>
+__global__ void __launch_bounds__(kTileThreads)
+merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tmax, MergeOut out,
+                  int* status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    Key<NW>* s_key = reinterpret_cast<Key<NW>*>(smem);
+    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_key + tmax);
+    uint8_t* s_first = s_flag + tmax;
+    uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_first + ((tmax + 15) & ~15));
+
+    __shared__ int s_t, s_p, s_tl, s_n, s_base, s_total;
+    __shared__ int s_start[kRuns], s_off[kRuns + 1], s_lo[kRuns];
+    __shared__ Key<NW> s_pred;
+    __shared__ int s_pred_flag, s_has_pred;
+    __shared__ int s_warp[kTileThreads / 32];
+    __shared__ int s_ceil;
+
+    const int tid = threadIdx.x;
+    const int L = m.L;
+    const int ntiles = ws.counters[1];
+
+    for (;;) {
+        if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
+        __syncthreads();
+        const int t = s_t;
+        if (t >= ntiles) return;
+
+        if (tid == 0) {
+            const int p = find_segment(ws.tile_off, L, t);
+            const int tl = t - ws.tile_off[p];
+            const int ob = ws.split_off[p * kRuns];
+            const int nsb = ws.split_off[(p + 1) * kRuns] - ob;
+            const int a = ob + tl * kMergeGroup;
+            const int bidx = tl * kMergeGroup + kMergeGroup;
+            int n = 0;
+            for (int j = 0; j < kRuns; ++j) {
+                const int st = ws.ord_co[int64_t(a) * kRuns + j];
+                const int en = bidx < nsb ? ws.ord_co[int64_t(ob + bidx) * kRuns + j]
+                                          : ws.run_len[p * kRuns + j];
+                s_start[j] = st;
+                s_off[j] = n;
+                s_lo[j] = ws.run_lo[p * kRuns + j];
+                n += en - st;
+            }
+            s_off[kRuns] = n;
+            s_n = n;
+            s_p = p;
+            s_tl = tl;
+            s_ceil = 0;
+            // merged predecessor of the tile: the largest element before the start of any run
+            int has = 0, pf = 0, pj = -1;
+            Key<NW> pk;
+            for (int j = 0; j < kRuns; ++j) {
+                if (s_start[j] == 0) continue;
+                Key<NW> k;
+                int f;
+                run_elem<NW>(m, X, p, j, int64_t(s_lo[j]) + s_start[j] - 1, k, f);
+                bool larger = !has;
+                if (has) {
+                    const int c = cmp_kf(k, f, pk, pf);
+                    larger = c > 0 || (c == 0 && j > pj);
+                }
+                if (larger) {
+                    pk = k;
+                    pf = f;
+                    pj = j;
+                    has = 1;
+                }
+            }
+            s_has_pred = has;
+            if (has) {
+                s_pred = pk;
+                s_pred_flag = pf;
+            }
+            if (n > tmax) raise_status(status, PACES_ERR_CAPACITY);
+        }
+        __syncthreads();
+        const int n = min(s_n, tmax);
+        const int p = s_p;
+
+        // 1. load the tile's segments (transforms applied on the fly)
+        for (int e = tid; e < n; e += kTileThreads) {
+            int j = 0;
+#pragma unroll
+            for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
+            Key<NW> k;
+            int f;
+            run_elem<NW>(m, X, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
+            s_key[e] = k;
+            s_flag[e] = uint8_t(f);
+            s_perm[e] = 0xffff;  // every rank must be claimed below
+        }
+        __syncthreads();
+
+        // 2. merged rank of every element
+        for (int e = tid; e < n; e += kTileThreads) {
+            int j = 0;
+#pragma unroll
+            for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
+            const Key<NW> k = s_key[e];
+            const int f = s_flag[e];
+            int r = e - s_off[j];
+#pragma unroll 1
+            for (int jj = 0; jj < kRuns; ++jj) {
+                if (jj == j) continue;
+                r += smem_bound<NW>(s_key, s_flag, s_off[jj], s_off[jj + 1] - s_off[jj], k, f, jj < j);
+            }
+            if (r < n) s_perm[r] = uint16_t(e);
+            else raise_status(status, PACES_ERR_BADARG);
+        }
+        __syncthreads();
+
+        // 3. first-occurrence flags over a contiguous chunk per thread, then a block scan
+        const int per = (n + kTileThreads - 1) / kTileThreads;
+        const int q0 = min(tid * per, n);
+        const int q1 = min(q0 + per, n);
+        int cnt = 0;
+        for (int q = q0; q < q1; ++q) {
+            const int e = s_perm[q];
+            int first = 0;
+            if (e >= n) {
+                raise_status(status, PACES_ERR_BADARG);
+            } else if (s_flag[e] == 1) {
+                if (q == 0) {
+                    first = !s_has_pred || s_pred_flag != 1 || !key_eq(s_pred, s_key[e]);
+                } else {
+                    const int pe = s_perm[q - 1];
+                    first = pe >= n || s_flag[pe] != 1 || !key_eq(s_key[pe], s_key[e]);
+                }
+            }
+            s_first[q] = uint8_t(first);
+            cnt += first;
+        }
+        // block exclusive scan of cnt
+        const int lane = tid & 31, wid = tid >> 5;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_warp[wid] = incl;
+        __syncthreads();
+        if (tid == 0) {
+            int acc = 0;
+            for (int w = 0; w < kTileThreads / 32; ++w) {
+                const int v = s_warp[w];
+                s_warp[w] = acc;
+                acc += v;
+            }
+            s_total = acc;
+            s_base = lookback_prefix(ws.tile_state, t, acc, status);
+            if (s_tl == 0) out.blk[p] = s_base;
+        }
+        __syncthreads();
+        const int base = s_base;
+        int run = s_warp[wid] + incl - cnt;  // exclusive count of firsts before q0
+
+        // 4. outputs
+        int ceil_local = 0;
+        for (int q = q0; q < q1; ++q) {
+            const int e = s_perm[q];
+            if (e >= n) continue;
+            int j = 0;
+#pragma unroll
+            for (int qq = 1; qq < kRuns; ++qq) j += (e >= s_off[qq]);
+            const int64_t src = int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]);
+            const int f = s_flag[e];
+            if (f != 1) {
+                if constexpr (ASM) {
+                    if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = -1;
+                }
+                ceil_local += (f == 2);
+                continue;
+            }
+            const int first = s_first[q];
+            run += first;
+            const int64_t u = int64_t(base) + run - 1;
+            if (first) {
+                if (u < out.cap) {
+                    store_key<NW>(out.keys, u, s_key[e]);
+                    if constexpr (ASM) {
+                        const Key<NW> k = s_key[e];
+                        const uint32_t nex = get_field(m, k, p);
+                        const uint32_t ntot = total_phonons(m, k);
+                        if (u < out.nbr_cap) {
+                            out.meta[u] = uint32_t(p) | (nex << 8) | (ntot << 16);
+#pragma unroll
+                            for (int sl = 0; sl < 4; ++sl) out.nbr[int64_t(sl) * out.nbr_cap + u] = -1;
+                        }
+                    }
+                } else {
+                    raise_status(status, PACES_ERR_CAPACITY);
+                }
+            }
+            if constexpr (ASM) {
+                if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = int(u);
+            }
+        }
+        if constexpr (ASM) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ceil_local += __shfl_xor_sync(0xffffffffu, ceil_local, o);
+            if (lane == 0 && ceil_local) atomicAdd(&s_ceil, ceil_local);
+            __syncthreads();
+            if (tid == 0 && s_ceil) atomicAdd(&ws.counters[3], s_ceil);
+        }
+        __syncthreads();
+    }
+}
+
+// Output block offsets for blocks without tiles, the output count, capacity check.
+__global__ void merge_finalize_kernel(ModelDev m, MergeWs ws, MergeOut out, int* ceiling_out,
+                                      int* status) {
+    if (threadIdx.x != 0) return;
+    const int L = m.L;
+    const int ntiles = ws.counters[1];
+    long long total = 0;
+    if (ntiles > 0) total = (long long)(ws.tile_state[ntiles - 1] & kLbMask);
+    if (total > out.cap) {
+        raise_status(status, PACES_ERR_CAPACITY);
+        total = out.cap;
+    }
+    out.blk[L] = int(total);
+    for (int p = L - 1; p >= 0; --p) {
+        if (ntiles == 0 || ws.tile_off[p] == ws.tile_off[p + 1]) out.blk[p] = out.blk[p + 1];
+        if (out.blk[p] > total) out.blk[p] = int(total);
+    }
+    ws.counters[4] = int(total);
+    if (ceiling_out) *ceiling_out = ws.counters[3];
+}
+
+// H neighbour table from the per-source index maps (assemble only).
+__global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __restrict__ x_blk,
+                                                       MergeOut out) {
+    __shared__ int s_blk[kMaxSites + 1];
+    const int L = m.L;
+    for (int i = threadIdx.x; i <= L; i += blockDim.x) s_blk[i] = x_blk[i];
+    __syncthreads();
+    const int nx = s_blk[L];
+    const int64_t mc = out.map_cap, nc = out.nbr_cap;
+    const int* map = out.maps;
+    int* nb = out.nbr;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const int p = block_of(s_blk, L, i);
+        const int q = map[0 * mc + i];
+        if (q < 0 || q >= nc) continue;
+        if (p + 1 < L || m.periodic) {
+            const int s = map[int64_t(RUN_FROM_LEFT) * mc + i];
+            if (s >= 0 && s < nc) {
+                nb[int64_t(NB_RIGHT) * nc + q] = s;
+                nb[int64_t(NB_LEFT) * nc + s] = q;
+            }
+        }
+        if (p > 0 || m.periodic) {
+            const int s = map[int64_t(RUN_FROM_RIGHT) * mc + i];
+            if (s >= 0 && s < nc) {
+                nb[int64_t(NB_LEFT) * nc + q] = s;
+                nb[int64_t(NB_RIGHT) * nc + s] = q;
+            }
+        }
+        {
+            const int s = map[int64_t(RUN_UP) * mc + i];
+            if (s >= 0 && s < nc) {
+                nb[int64_t(NB_UP) * nc + q] = s;
+                nb[int64_t(NB_DOWN) * nc + s] = q;
+            }
+        }
+        {
+            const int s = map[int64_t(RUN_DOWN) * mc + i];
+            if (s >= 0 && s < nc) {
+                nb[int64_t(NB_DOWN) * nc + q] = s;
+                nb[int64_t(NB_UP) * nc + s] = q;
+            }
+        }
+    }
+}
+
+template <int NW>
+size_t tile_smem_bytes() {
+    const int tmax = merge_tmax(NW);
+    return size_t(tmax) * sizeof(Key<NW>) + 2 * size_t((tmax + 15) & ~15) + size_t(tmax) * 2;
+}
+
+template <int NW>
+int launch_merge_t(bool assemble, const ModelDev& m, const uint64_t* X, const int* x_blk,
+                   const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status, int num_sms,
+                   cudaStream_t st) {
+    const int stride = merge_stride(NW);
+    const int tmax = merge_tmax(NW);
+    merge_plan_kernel<<<1, 1024, 0, st>>>(m, x_blk, ws, stride, status);
+    const int g = num_sms * 8;
+    merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, ws, stride);
+    merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
+    const size_t smem = tile_smem_bytes<NW>();
+    if (assemble) {
+        auto kfn = merge_tile_kernel<NW, true>;
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTileThreads, smem);
+        kfn<<<num_sms * max(per_sm, 1), kTileThreads, smem, st>>>(m, X, ws, tmax, out, status);
+    } else {
+        auto kfn = merge_tile_kernel<NW, false>;
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTileThreads, smem);
+        kfn<<<num_sms * max(per_sm, 1), kTileThreads, smem, st>>>(m, X, ws, tmax, out, status);
+    }
+    merge_finalize_kernel<<<1, 32, 0, st>>>(m, ws, out, ceiling_out, status);
+    if (assemble) nbr_fill_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, out);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
+}
+
+}  // namespace
+
+int launch_merge(int nw, bool assemble, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+                 const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status, int num_sms,
+                 cudaStream_t st) {
+    switch (nw) {
+        case 1: return launch_merge_t<1>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        case 2: return launch_merge_t<2>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        case 3: return launch_merge_t<3>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        case 4: return launch_merge_t<4>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        case 5: return launch_merge_t<5>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        case 6: return launch_merge_t<6>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        case 7: return launch_merge_t<7>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        case 8: return launch_merge_t<8>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        default: return PACES_ERR_BADARG;
+    }
+}
+
+}  // namespace paces

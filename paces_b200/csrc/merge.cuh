@@ -1,0 +1,73 @@
+// Structured k-way merge: basis expansion, sort and dedup without a general sort.
+//
+// Reference behaviour (paces/core/hamiltonian.py:550-577 enlarge_basis_set,
+// :383-492 generate_mel, paces/aux/helpers.py:63-75 cupy_unique): collect the
+// basis and every image of every basis state under the off-diagonal terms, lexsort
+// the rows and drop duplicates.
+//
+// B200 design: keys carry only the phonon words; the exciton position is the block.
+// For a sorted basis X the candidates of output block p are five runs, each already
+// sorted because every Holstein term maps a sorted block monotonically:
+//   SELF       X_p                      (the basis itself)
+//   FROM_LEFT  X_{p-1}                  (right hops land in block p, phonon words unchanged)
+//   FROM_RIGHT X_{p+1}                  (left hops)
+//   UP         X_p with n_p + 1         (b^dagger at the exciton site; ceiling n_p = maxd-1 is a hole)
+//   DOWN       X_p with n_p - 1         (b at the exciton site; floor n_p = 0 is a hole)
+// A hole keeps a placeholder key that preserves the run's order (DOWN: fields after p
+// cleared; UP: all bits below field p set) and a flag that sorts it before (DOWN) or
+// after (UP) real keys with the same words, so holes never produce output.
+//
+// The merge is tiled with splitters: every `stride`-th element of every run is ranked
+// against all runs (binary search), splitters are put in merged order, and every
+// `group` consecutive splitters bound one tile of at most (group + 4) * stride elements.
+// A tile is merged in shared memory (rank = own index + bounds in the other segments),
+// duplicates are flagged against the merged predecessor, and output offsets come from a
+// decoupled look-back over tiles taken in ticket order.  Every input element learns the
+// index of its key in the output, which gives the H neighbour table without any lookup.
+#pragma once
+
+#include "common.cuh"
+
+namespace paces {
+
+struct MergeWs {
+    int* run_lo;     // [L*kRuns] first source index in X of each run
+    int* run_len;    // [L*kRuns]
+    int* split_off;  // [L*kRuns + 1] prefix of splitter counts
+    int* tile_off;   // [L + 1] prefix of tile counts
+    int* counters;   // [0] splitters [1] tiles [2] tile ticket [3] ceiling holes [4] output count
+    int* split_co;   // [split_cap * kRuns]
+    int* split_rank; // [split_cap]
+    int* ord_co;     // [split_cap * kRuns]
+    unsigned long long* tile_state;  // [tile_cap] look-back words
+    int split_cap;
+    int tile_cap;
+};
+
+struct MergeOut {
+    uint64_t* keys;
+    int* blk;
+    int64_t cap;
+    // assemble only
+    uint32_t* meta;
+    int* nbr;        // [4][nbr_cap]
+    int64_t nbr_cap;
+    int* maps;       // [kRuns][map_cap], indexed by source index in X
+    int64_t map_cap;
+};
+
+// Tiling constants by key width (shared memory of one tile stays below ~100 KB).
+__host__ __device__ constexpr int merge_stride(int nw) { return nw <= 4 ? 256 : 128; }
+constexpr int kMergeGroup = 8;
+__host__ __device__ constexpr int merge_tmax(int nw) { return (kMergeGroup + kRuns - 1) * merge_stride(nw); }
+
+inline int64_t merge_split_cap(int64_t in_cap, int nw, int L) {
+    return kRuns * (in_cap / merge_stride(nw) + 1) * 1 + int64_t(kRuns) * L + 8;
+}
+inline int64_t merge_tile_cap(int64_t split_cap, int L) { return split_cap / kMergeGroup + L + 8; }
+
+int launch_merge(int nw, bool assemble, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+                 const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status,
+                 int num_sms, cudaStream_t st);
+
+}  // namespace paces

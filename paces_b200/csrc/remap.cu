@@ -1,0 +1,129 @@
+// Amplitude remap into the new basis.
+//
+// Reference (paces/core/time_evolution.py:781-797): for every new state, binary-search
+// the old basis; where the state exists, copy its old amplitude, else 0 (states that
+// the previous truncation dropped but the expansion re-created get their old amplitude
+// back).
+//
+// B200 design: both bases are sorted and blocked by exciton position, so the lookup is
+// a merge-path sorted search per block: tiles of 2048 merged (old + new) elements,
+// split by a diagonal binary search, the tile's old keys staged in shared memory, and
+// each new key resolved by a shared-memory upper bound (old before new on equal keys;
+// a match is the old element just before the new one).
+#include "kernels.cuh"
+
+namespace paces {
+
+namespace {
+
+template <int NW>
+__device__ int merge_path(const uint64_t* __restrict__ A, int na, const uint64_t* __restrict__ B, int nb,
+                          int diag) {
+    int begin = max(0, diag - nb), end = min(diag, na);
+    while (begin < end) {
+        const int mid = (begin + end) >> 1;
+        const Key<NW> a = load_key<NW>(A, mid);
+        const Key<NW> b = load_key<NW>(B, diag - 1 - mid);
+        if (!(key_cmp(b, a) < 0)) begin = mid + 1; else end = mid;
+    }
+    return begin;
+}
+
+__global__ void remap_plan_kernel(ModelDev m, const int* __restrict__ ob, const int* __restrict__ nb,
+                                  RemapWs ws, int tile, int* status) {
+    if (threadIdx.x != 0) return;
+    int acc = 0;
+    for (int p = 0; p < m.L; ++p) {
+        ws.tile_off[p] = acc;
+        const int tot = (ob[p + 1] - ob[p]) + (nb[p + 1] - nb[p]);
+        acc += (tot + tile - 1) / tile;
+    }
+    ws.tile_off[m.L] = acc;
+    if (acc > ws.tile_cap) {
+        raise_status(status, PACES_ERR_CAPACITY);
+        acc = 0;
+    }
+    ws.counters[0] = acc;
+}
+
+template <int NW, bool C64>
+__global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint64_t* __restrict__ old_keys,
+                                                         const int* __restrict__ ob,
+                                                         const void* __restrict__ old_psi,
+                                                         const uint64_t* __restrict__ new_keys,
+                                                         const int* __restrict__ nb, void* __restrict__ new_psi,
+                                                         RemapWs ws) {
+    using C = typename std::conditional<C64, float2, double2>::type;
+    constexpr int kTile = remap_tile(NW);
+    __shared__ Key<NW> s_old[kTile + 1];
+    __shared__ int s_a[2];
+    const int ntiles = ws.counters[0];
+    const C* op = reinterpret_cast<const C*>(old_psi);
+    C* np = reinterpret_cast<C*>(new_psi);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int p = find_segment(ws.tile_off, m.L, t);
+        const int tl = t - ws.tile_off[p];
+        const int o0 = ob[p], no = ob[p + 1] - o0;
+        const int n0 = nb[p], nn = nb[p + 1] - n0;
+        const uint64_t* O = old_keys + int64_t(o0) * NW;
+        const uint64_t* N = new_keys + int64_t(n0) * NW;
+        const int d0 = tl * kTile, d1 = min(d0 + kTile, no + nn);
+        if (threadIdx.x < 2) s_a[threadIdx.x] = merge_path<NW>(O, no, N, nn, threadIdx.x == 0 ? d0 : d1);
+        __syncthreads();
+        const int a0 = s_a[0], a1 = s_a[1];
+        const int h = a0 > 0 ? 1 : 0;  // halo: the old element before the tile
+        for (int e = threadIdx.x; e < a1 - a0 + h; e += blockDim.x) s_old[e] = load_key<NW>(O, a0 - h + e);
+        __syncthreads();
+        const int b0 = d0 - a0, b1 = d1 - a1;
+        const int nold = a1 - a0;
+        for (int x = b0 + threadIdx.x; x < b1; x += blockDim.x) {
+            const Key<NW> k = load_key<NW>(N, x);
+            int lo = 0, hi = nold;  // upper bound among s_old[h .. h+nold)
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (key_cmp(s_old[h + mid], k) <= 0) lo = mid + 1; else hi = mid;
+            }
+            const int aa = a0 + lo;  // old elements before k in merged order
+            C v;
+            v.x = 0;
+            v.y = 0;
+            if (aa > 0 && key_eq(s_old[h + lo - 1], k)) v = op[int64_t(o0) + aa - 1];
+            np[int64_t(n0) + x] = v;
+        }
+        __syncthreads();
+    }
+}
+
+template <int NW, bool C64>
+int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const void* opsi,
+                   const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws, int* status,
+                   int num_sms, cudaStream_t st) {
+    remap_plan_kernel<<<1, 32, 0, st>>>(m, ob, nb, ws, remap_tile(NW), status);
+    remap_tile_kernel<NW, C64><<<num_sms * 4, 256, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi, ws);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
+}
+
+}  // namespace
+
+int launch_remap(int nw, bool c64, const ModelDev& m, const uint64_t* ok, const int* ob,
+                 const void* opsi, const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws,
+                 int* status, int num_sms, cudaStream_t st) {
+#define PACES_REMAP_CASE(N)                                                                         \
+    case N:                                                                                         \
+        return c64 ? launch_remap_t<N, true>(m, ok, ob, opsi, nk, nb, npsi, ws, status, num_sms, st) \
+                   : launch_remap_t<N, false>(m, ok, ob, opsi, nk, nb, npsi, ws, status, num_sms, st);
+    switch (nw) {
+        PACES_REMAP_CASE(1)
+        PACES_REMAP_CASE(2)
+        PACES_REMAP_CASE(3)
+        PACES_REMAP_CASE(4)
+        PACES_REMAP_CASE(5)
+        PACES_REMAP_CASE(6)
+        PACES_REMAP_CASE(7)
+        PACES_REMAP_CASE(8)
+        default: return PACES_ERR_BADARG;
+    }
+#undef PACES_REMAP_CASE
+}
+
+}  // namespace paces

@@ -1,0 +1,201 @@
+// Truncated-Taylor exp(-i dt H) psi as one persistent cooperative kernel.
+//
+// Reference (paces/core/time_evolution.py:482-512, _simple_taylor): term_{j+1} =
+// (-i dt/(j+1)) H term_j, res += term_{j+1}, stop when (|term_j|_inf + |term_{j+1}|_inf) /
+// |res|_inf <= tol, at most m_star terms; one host sync per term in the reference.
+//
+// B200 design: every term is one grid-stride sweep over the rows (neighbour-table SpMV,
+// term write, res update and the two inf-norms fused), separated by a bounded grid
+// barrier; every block reduces the per-block maxima itself and takes the same stop
+// decision, so the whole series runs in one launch with no host round trip.  The
+// neighbour indices of consecutive rows are monotone (images of a sorted block are
+// sorted), so the four gathers stream through L2.  complex128 rounds every operation
+// like the reference; complex64 uses fp32 FMA with fp64 stop arithmetic.
+#include "hrow.cuh"
+#include "kernels.cuh"
+
+namespace paces {
+
+namespace {
+
+constexpr int kTThreads = 256;
+constexpr int kTWarps = kTThreads / 32;
+
+// Bounded grid-wide barrier (all blocks are co-resident: cooperative launch).
+__device__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen, int* status) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&bar[0], 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            while (atomicAdd(&bar[1], 0u) == gen) {
+                if (global_ns() - t0 > kWaitLimitNs) {
+                    raise_status(status, PACES_ERR_TIMEOUT);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        ++gen;
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// max-reduce four values over the block; result in out[0..3] (shared), valid after return.
+__device__ void block_max4(double v[4], double (*red)[kTWarps], double* out) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] = fmax(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+        if (lane == 0) red[k][wid] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double r = 0.0;
+        for (int w = 0; w < kTWarps; ++w) r = fmax(r, red[threadIdx.x][w]);
+        out[threadIdx.x] = r;
+    }
+    __syncthreads();
+}
+
+template <bool C64>
+__global__ void __launch_bounds__(kTThreads)
+taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nbr, int64_t cap,
+              const uint32_t* __restrict__ meta, const void* v_in, void* res_out, TaylorWs ws,
+              double dt, int m_star, double tol, TaylorOut out, int* status) {
+    using C = typename std::conditional<C64, float2, double2>::type;
+    using R = typename std::conditional<C64, float, double>::type;
+    __shared__ R s_sq[260];
+    __shared__ double s_red[4][kTWarps];
+    __shared__ double s_fin[4];
+    for (int k = threadIdx.x; k < 260; k += kTThreads) s_sq[k] = R(__dmul_rn(sqrt(double(k)), m.g));
+    __syncthreads();
+
+    const int64_t S = blk[m.L];
+    const unsigned nblocks = gridDim.x;
+    unsigned gen = 0;
+    const C* v = reinterpret_cast<const C*>(v_in);
+    C* res = reinterpret_cast<C*>(res_out);
+    C* ta = reinterpret_cast<C*>(ws.ta);
+    C* tb = reinterpret_cast<C*>(ws.tb);
+    const R J = R(m.J);
+    double c1 = 0.0, c1c2 = 0.0, ratio = 0.0;
+    int conv = 0, fin_j = 0;
+
+    for (int j = 0; j < m_star; ++j) {
+        const C* src = j == 0 ? v : ((j & 1) ? ta : tb);
+        C* dst = (j & 1) ? tb : ta;
+        const C* rin = j == 0 ? v : res;
+        const double cd = dt / double(j + 1);
+        const R c = R(cd);
+        double mx[4] = {0.0, 0.0, 0.0, 0.0};  // |term|, |res|, |v|, non-finite
+        for (int64_t r = int64_t(blockIdx.x) * kTThreads + threadIdx.x; r < S;
+             r += int64_t(gridDim.x) * kTThreads) {
+            const uint32_t mm = __ldg(meta + r);
+            C t, rr;
+            const C a = rin[r];
+            if constexpr (C64) {
+                const float2 y = h_row_c64(m, s_sq, J, r, nbr, cap, mm, src);
+                t = make_float2(c * y.y, -(c * y.x));
+                rr = make_float2(a.x + t.x, a.y + t.y);
+                mx[0] = fmax(mx[0], double(hypotf(t.x, t.y)));
+                mx[1] = fmax(mx[1], double(hypotf(rr.x, rr.y)));
+                if (j == 0) mx[2] = fmax(mx[2], double(hypotf(a.x, a.y)));
+            } else {
+                const double2 y = h_row_c128(m, s_sq, r, nbr, cap, mm, src);
+                t = make_double2(__dmul_rn(cd, y.y), -__dmul_rn(cd, y.x));
+                rr = make_double2(__dadd_rn(a.x, t.x), __dadd_rn(a.y, t.y));
+                mx[0] = fmax(mx[0], hypot(t.x, t.y));
+                mx[1] = fmax(mx[1], hypot(rr.x, rr.y));
+                if (j == 0) mx[2] = fmax(mx[2], hypot(a.x, a.y));
+            }
+            if (!(isfinite(double(rr.x)) && isfinite(double(rr.y)))) mx[3] = 1.0;
+            dst[r] = t;
+            res[r] = rr;
+        }
+        block_max4(mx, s_red, s_fin);
+        if (threadIdx.x == 0) {
+            double* pp = ws.partials + (size_t((j & 1) * nblocks) + blockIdx.x) * 4;
+            pp[0] = s_fin[0];
+            pp[1] = s_fin[1];
+            pp[2] = s_fin[2];
+            pp[3] = s_fin[3];
+        }
+        if (!grid_barrier(ws.barrier, nblocks, gen, status)) {
+            fin_j = j;
+            break;
+        }
+        double g4[4] = {0.0, 0.0, 0.0, 0.0};
+        for (unsigned b = threadIdx.x; b < nblocks; b += kTThreads) {
+            const double* pp = ws.partials + (size_t((j & 1) * nblocks) + b) * 4;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) g4[k] = fmax(g4[k], __ldcg(pp + k));
+        }
+        block_max4(g4, s_red, s_fin);
+        fin_j = j;
+        if (s_fin[3] != 0.0) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) raise_status(status, PACES_ERR_NONFINITE);
+            break;
+        }
+        if (j == 0) c1 = s_fin[2];
+        const double c2 = s_fin[0];
+        c1c2 = c1 + c2;
+        ratio = c1c2 / s_fin[1];
+        if (ratio <= tol) {
+            conv = 1;
+            break;
+        }
+        c1 = c2;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (out.converged) *out.converged = conv;
+        if (out.final_m) *out.final_m = fin_j;
+        if (out.c1_plus_c2) *out.c1_plus_c2 = c1c2;
+        if (out.term_ratio) *out.term_ratio = ratio;
+    }
+}
+
+template <bool C64>
+int occupancy() {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, taylor_kernel<C64>, kTThreads, 0);
+    return per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+}
+
+}  // namespace
+
+int taylor_max_grid(bool c64, int num_sms) { return num_sms * (c64 ? occupancy<true>() : occupancy<false>()); }
+
+int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,
+                  const uint32_t* meta, const void* v_in, void* res, double dt, int m_star,
+                  double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
+                  cudaStream_t st) {
+    if (m_star < 1) return PACES_ERR_BADARG;
+    if (cudaMemsetAsync(ws.barrier, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return PACES_ERR_CUDA;
+    const int grid = taylor_max_grid(c64, num_sms);
+    ModelDev mm = m;
+    TaylorWs w = ws;
+    TaylorOut o = out;
+    int64_t cap = nbr_cap;
+    void* args[] = {&mm, (void*)&blk, (void*)&nbr, &cap, (void*)&meta, (void*)&v_in, &res, &w,
+                    &dt, &m_star, &tol, &o, &status};
+    cudaError_t e;
+    if (c64)
+        e = cudaLaunchCooperativeKernel((const void*)taylor_kernel<true>, dim3(grid), dim3(kTThreads), args, 0, st);
+    else
+        e = cudaLaunchCooperativeKernel((const void*)taylor_kernel<false>, dim3(grid), dim3(kTThreads), args, 0, st);
+    return e == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
+}
+
+}  // namespace paces

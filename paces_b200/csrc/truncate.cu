@@ -1,0 +1,510 @@
+// Amplitude-ranked truncation (see truncate.cuh).
+#include "truncate.cuh"
+
+namespace paces {
+
+namespace {
+
+// selection state words (TruncWs.sel)
+enum : int {
+    SEL_S = 0,        // number of input states
+    SEL_ALL = 1,      // 1: keep everything (S <= maxstates)
+    SEL_W = 2,        // weight select: [2] prefix [3] mask [4] need [5] active
+    SEL_H = 6,        // hash select:   [6] prefix [7] mask [8] need [9] active
+    SEL_CAND = 10,    // candidate count
+    SEL_TIES = 11,    // states equal to the threshold
+    SEL_SHUFFLE = 12, // 1: ties at the cut are shuffled
+    SEL_WORDS = 16
+};
+
+constexpr int kRounds = 6;
+__host__ __device__ constexpr int round_shift(int r) { return r < 5 ? 52 - 12 * r : 0; }
+__host__ __device__ constexpr int round_bits(int r) { return r < 5 ? 12 : 4; }
+
+template <bool C64>
+__device__ __forceinline__ unsigned long long weight_bits(const void* psi, int64_t i, int* status) {
+    double w;
+    if constexpr (C64) {
+        const float2 z = reinterpret_cast<const float2*>(psi)[i];
+        w = double(hypotf(z.x, z.y));
+    } else {
+        const double2 z = reinterpret_cast<const double2*>(psi)[i];
+        w = hypot(z.x, z.y);
+    }
+    if (!(w <= 1.7976931348623157e308)) raise_status(status, PACES_ERR_NONFINITE);
+    return (unsigned long long)__double_as_longlong(w);
+}
+
+// splitmix64 finaliser applied to (index + stream offset): a bijection of the index, so
+// hashes of distinct states never collide.
+__device__ __forceinline__ unsigned long long tie_hash(uint64_t seed, uint64_t step, int64_t i) {
+    unsigned long long z = (unsigned long long)i + seed * 0x9E3779B97F4A7C15ull + step * 0xD1B54A32D192ED03ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    return ~z;  // keep the largest ~hash == the smallest hash
+}
+
+__global__ void trunc_init_kernel(ModelDev m, const int* __restrict__ x_blk, int64_t maxstates,
+                                  TruncWs ws) {
+    const int tid = threadIdx.x;
+    for (int b = tid; b < 4096; b += blockDim.x) ws.hist[b] = 0;
+    if (tid == 0) {
+        const long long S = x_blk[m.L];
+        for (int k = 0; k < SEL_WORDS; ++k) ws.sel[k] = 0;
+        ws.sel[SEL_S] = S;
+        ws.sel[SEL_ALL] = S <= maxstates ? 1 : 0;
+        ws.sel[SEL_W + 2] = maxstates;
+        ws.sel[SEL_W + 3] = S <= maxstates ? 0 : 1;
+    }
+}
+
+template <bool C64>
+__global__ void __launch_bounds__(256) trunc_hist_all_kernel(const void* __restrict__ psi, TruncWs ws,
+                                                             int* status) {
+    __shared__ unsigned h[4096];
+    if (!ws.sel[SEL_W + 3]) return;
+    for (int b = threadIdx.x; b < 4096; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const int64_t S = ws.sel[SEL_S];
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < S; i += int64_t(gridDim.x) * blockDim.x) {
+        const unsigned long long k = weight_bits<C64>(psi, i, status);
+        atomicAdd(&h[(k >> 52) & 4095], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 4096; b += blockDim.x)
+        if (h[b]) atomicAdd(&ws.hist[b], h[b]);
+}
+
+// One radix round: find the digit holding the need-th largest key, narrow the prefix.
+__global__ void __launch_bounds__(1024) trunc_select_kernel(TruncWs ws, int base, int round,
+                                                            int record_ties) {
+    __shared__ long long s_warp[32];
+    __shared__ int s_bin;
+    __shared__ long long s_above;
+    if (!ws.sel[base + 3]) return;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int bits = round_bits(round), shift = round_shift(round);
+    const int nb = 1 << bits;
+    const int per = (nb + 1023) / 1024;  // 4 or 1
+    const long long need = ws.sel[base + 2];
+    long long mine = 0;
+    for (int q = 0; q < per; ++q) {
+        const int b = tid * per + q;
+        if (b < nb) mine += ws.hist[b];
+    }
+    // suffix sums: threads above me
+    long long incl = mine;  // inclusive suffix within the warp (lanes >= lane)
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long v = __shfl_down_sync(0xffffffffu, incl, o);
+        if (lane + o < 32) incl += v;
+    }
+    if (lane == 0) s_warp[wid] = incl;
+    if (tid == 0) s_bin = -1;
+    __syncthreads();
+    long long warps_above = 0;
+    for (int w = wid + 1; w < 32; ++w) warps_above += s_warp[w];
+    const long long above_me = warps_above + (incl - mine);  // sum of bins above my range
+    if (mine > 0 && above_me < need && need <= above_me + mine) {
+        long long acc = above_me;
+        for (int q = per - 1; q >= 0; --q) {
+            const int b = tid * per + q;
+            if (b >= nb) continue;
+            const long long hb = ws.hist[b];
+            if (acc < need && need <= acc + hb) {
+                s_bin = b;
+                s_above = acc;
+                break;
+            }
+            acc += hb;
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && s_bin >= 0) {
+        const int b = s_bin;
+        ws.sel[base + 2] = need - s_above;
+        ws.sel[base + 0] |= (long long)((unsigned long long)b << shift);
+        ws.sel[base + 1] |= (long long)((unsigned long long)(nb - 1) << shift);
+        if (record_ties && round == kRounds - 1) ws.sel[SEL_TIES] = ws.hist[b];
+    }
+    __syncthreads();
+    for (int b = tid; b < 4096; b += blockDim.x) ws.hist[b] = 0;
+}
+
+template <bool C64>
+__global__ void __launch_bounds__(256) trunc_collect_kernel(const void* __restrict__ psi, TruncWs ws,
+                                                            int* status) {
+    if (!ws.sel[SEL_W + 3]) return;
+    const int64_t S = ws.sel[SEL_S];
+    const unsigned long long pre = (unsigned long long)ws.sel[SEL_W + 0];
+    const unsigned long long msk = (unsigned long long)ws.sel[SEL_W + 1];
+    const int lane = threadIdx.x & 31;
+    for (int64_t i0 = blockIdx.x * int64_t(blockDim.x); i0 < S; i0 += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        unsigned long long k = 0;
+        bool take = false;
+        if (i < S) {
+            k = weight_bits<C64>(psi, i, status);
+            take = (k & msk) == pre;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, take);
+        if (!ballot) continue;
+        int basei = 0;
+        if (lane == 0) basei = int(atomicAdd(reinterpret_cast<unsigned long long*>(&ws.sel[SEL_CAND]),
+                                            (unsigned long long)__popc(ballot)));
+        basei = __shfl_sync(0xffffffffu, basei, 0);
+        if (take) {
+            const int slot = basei + __popc(ballot & ((1u << lane) - 1));
+            if (slot < ws.cap) {
+                ws.cand[slot] = k;
+                ws.cand_idx[slot] = int(i);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) trunc_hist_cand_kernel(TruncWs ws, int base, int round) {
+    __shared__ unsigned h[4096];
+    if (!ws.sel[base + 3]) return;
+    const int bits = round_bits(round), shift = round_shift(round);
+    const unsigned long long dm = (1ull << bits) - 1;
+    for (int b = threadIdx.x; b < 4096; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const long long nc = min(ws.sel[SEL_CAND], (long long)ws.cap);
+    const unsigned long long pre = (unsigned long long)ws.sel[base + 0];
+    const unsigned long long msk = (unsigned long long)ws.sel[base + 1];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = ws.cand[c];
+        if ((k & msk) == pre) atomicAdd(&h[(k >> shift) & dm], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < (1 << bits); b += blockDim.x)
+        if (h[b]) atomicAdd(&ws.hist[b], h[b]);
+}
+
+// Decide whether the tie at the cut is shuffled; if so, collect the tied states' hashes.
+__global__ void trunc_shuffle_prep_kernel(TruncWs ws, int* status) {
+    if (threadIdx.x != 0) return;
+    const long long ties = ws.sel[SEL_TIES];
+    const long long need = ws.sel[SEL_W + 2];
+    const bool active = ws.sel[SEL_W + 3] && ties > need;
+    ws.sel[SEL_SHUFFLE] = active ? 1 : 0;
+    if (active && double(ties) > 0.9 * double(ws.sel[SEL_S])) raise_status(status, PACES_ERR_SHUFFLE);
+    ws.sel[SEL_H + 0] = 0;
+    ws.sel[SEL_H + 1] = 0;
+    ws.sel[SEL_H + 2] = need;
+    ws.sel[SEL_H + 3] = active ? 1 : 0;
+    ws.sel[SEL_CAND] = 0;
+}
+
+template <bool C64>
+__global__ void __launch_bounds__(256) trunc_collect_ties_kernel(const void* __restrict__ psi, TruncWs ws,
+                                                                 uint64_t seed, uint64_t step, int* status) {
+    if (!ws.sel[SEL_H + 3]) return;
+    const int64_t S = ws.sel[SEL_S];
+    const unsigned long long vstar = (unsigned long long)ws.sel[SEL_W + 0];
+    const int lane = threadIdx.x & 31;
+    for (int64_t i0 = blockIdx.x * int64_t(blockDim.x); i0 < S; i0 += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        bool take = false;
+        if (i < S) take = weight_bits<C64>(psi, i, status) == vstar;
+        const unsigned ballot = __ballot_sync(0xffffffffu, take);
+        if (!ballot) continue;
+        int basei = 0;
+        if (lane == 0) basei = int(atomicAdd(reinterpret_cast<unsigned long long*>(&ws.sel[SEL_CAND]),
+                                            (unsigned long long)__popc(ballot)));
+        basei = __shfl_sync(0xffffffffu, basei, 0);
+        if (take) {
+            const int slot = basei + __popc(ballot & ((1u << lane) - 1));
+            if (slot < ws.cap) {
+                ws.cand[slot] = tie_hash(seed, step, i);
+                ws.cand_idx[slot] = int(i);
+            }
+        }
+    }
+}
+
+// Per tile: states above the threshold, tied states, tied states kept by the hash rule.
+template <bool C64>
+__global__ void __launch_bounds__(256) trunc_count_kernel(const void* __restrict__ psi, TruncWs ws,
+                                                          uint64_t seed, uint64_t step, int* status) {
+    __shared__ int s_c[3];
+    const int64_t S = ws.sel[SEL_S];
+    const int ntiles = int((S + kTruncTile - 1) / kTruncTile);
+    if (ws.sel[SEL_ALL]) return;
+    const unsigned long long vstar = (unsigned long long)ws.sel[SEL_W + 0];
+    const bool shuf = ws.sel[SEL_SHUFFLE] != 0;
+    const unsigned long long hstar = (unsigned long long)ws.sel[SEL_H + 0];
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (threadIdx.x < 3) s_c[threadIdx.x] = 0;
+        __syncthreads();
+        int a = 0, ti = 0, hk = 0;
+        const int64_t i1 = min(S, int64_t(t + 1) * kTruncTile);
+        for (int64_t i = int64_t(t) * kTruncTile + threadIdx.x; i < i1; i += blockDim.x) {
+            const unsigned long long k = weight_bits<C64>(psi, i, status);
+            a += k > vstar;
+            if (k == vstar) {
+                ++ti;
+                if (shuf) hk += tie_hash(seed, step, i) >= hstar;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            ti += __shfl_xor_sync(0xffffffffu, ti, o);
+            hk += __shfl_xor_sync(0xffffffffu, hk, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&s_c[0], a);
+            atomicAdd(&s_c[1], ti);
+            atomicAdd(&s_c[2], hk);
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) ws.tile_cnt[t * 3 + threadIdx.x] = s_c[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(1024) trunc_scan_kernel(TruncWs ws) {
+    __shared__ int s_w[32][3];
+    if (ws.sel[SEL_ALL]) return;
+    const int64_t S = ws.sel[SEL_S];
+    const int ntiles = int((S + kTruncTile - 1) / kTruncTile);
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int per = (ntiles + 1023) / 1024;
+    const int t0 = min(tid * per, ntiles), t1 = min(t0 + per, ntiles);
+    int c[3] = {0, 0, 0};
+    for (int t = t0; t < t1; ++t)
+        for (int k = 0; k < 3; ++k) c[k] += ws.tile_cnt[t * 3 + k];
+    int incl[3];
+    for (int k = 0; k < 3; ++k) {
+        incl[k] = c[k];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl[k], o);
+            if (lane >= o) incl[k] += v;
+        }
+        if (lane == 31) s_w[wid][k] = incl[k];
+    }
+    __syncthreads();
+    if (tid < 3) {
+        int acc = 0;
+        for (int w = 0; w < 32; ++w) {
+            const int v = s_w[w][tid];
+            s_w[w][tid] = acc;
+            acc += v;
+        }
+    }
+    __syncthreads();
+    int run[3];
+    for (int k = 0; k < 3; ++k) run[k] = s_w[wid][k] + incl[k] - c[k];
+    for (int t = t0; t < t1; ++t)
+        for (int k = 0; k < 3; ++k) {
+            ws.tile_pre[t * 3 + k] = run[k];
+            run[k] += ws.tile_cnt[t * 3 + k];
+        }
+}
+
+template <int NW, bool C64>
+__global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint64_t* __restrict__ x_keys,
+                                                          const int* __restrict__ x_blk,
+                                                          const void* __restrict__ psi, TruncWs ws,
+                                                          uint64_t seed, uint64_t step,
+                                                          uint64_t* __restrict__ out_keys,
+                                                          int* __restrict__ out_blk, int64_t out_cap,
+                                                          int* status) {
+    __shared__ unsigned long long s_k[kTruncTile];
+    __shared__ int s_blk[kMaxSites + 1];
+    __shared__ int s_w[8][3];
+    const int L = m.L;
+    for (int i = threadIdx.x; i <= L; i += blockDim.x) s_blk[i] = x_blk[i];
+    const int64_t S = ws.sel[SEL_S];
+    const bool all = ws.sel[SEL_ALL] != 0;
+    const int ntiles = int((S + kTruncTile - 1) / kTruncTile);
+    const unsigned long long vstar = (unsigned long long)ws.sel[SEL_W + 0];
+    const long long need = ws.sel[SEL_W + 2];
+    const long long ties = ws.sel[SEL_TIES];
+    const bool shuf = ws.sel[SEL_SHUFFLE] != 0;
+    const unsigned long long hstar = (unsigned long long)ws.sel[SEL_H + 0];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int kPer = kTruncTile / 256;
+    __syncthreads();
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t i0 = int64_t(t) * kTruncTile;
+        const int n = int(min(int64_t(kTruncTile), S - i0));
+        if (!all)
+            for (int e = tid; e < n; e += 256) s_k[e] = weight_bits<C64>(psi, i0 + e, status);
+        __syncthreads();
+        // per-thread chunk [q0, q1): counts of above / tied / hash-kept tied states
+        const int q0 = min(tid * kPer, n), q1 = min(q0 + kPer, n);
+        int ca = 0, ct = 0, ch = 0;
+        if (!all)
+            for (int q = q0; q < q1; ++q) {
+                ca += s_k[q] > vstar;
+                if (s_k[q] == vstar) {
+                    ++ct;
+                    if (shuf) ch += tie_hash(seed, step, i0 + q) >= hstar;
+                }
+            }
+        int ia = ca, it = ct, ih = ch;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int va = __shfl_up_sync(0xffffffffu, ia, o);
+            const int vt = __shfl_up_sync(0xffffffffu, it, o);
+            const int vh = __shfl_up_sync(0xffffffffu, ih, o);
+            if (lane >= o) {
+                ia += va;
+                it += vt;
+                ih += vh;
+            }
+        }
+        if (lane == 31) {
+            s_w[wid][0] = ia;
+            s_w[wid][1] = it;
+            s_w[wid][2] = ih;
+        }
+        __syncthreads();
+        long long A = 0, T = 0, H = 0;
+        if (!all) {
+            A = ws.tile_pre[t * 3 + 0];
+            T = ws.tile_pre[t * 3 + 1];
+            H = ws.tile_pre[t * 3 + 2];
+        }
+        for (int w = 0; w < wid; ++w) {
+            A += s_w[w][0];
+            T += s_w[w][1];
+            H += s_w[w][2];
+        }
+        A += ia - ca;
+        T += it - ct;
+        H += ih - ch;
+        for (int q = q0; q < q1; ++q) {
+            const int64_t i = i0 + q;
+            bool keep;
+            long long out;
+            if (all) {
+                keep = true;
+                out = i;
+            } else {
+                const unsigned long long k = s_k[q];
+                const long long kept_ties = shuf ? H : max(0ll, T - (ties - need));
+                out = A + kept_ties;
+                if (k > vstar) {
+                    keep = true;
+                    ++A;
+                } else if (k == vstar) {
+                    if (shuf) {
+                        keep = tie_hash(seed, step, i) >= hstar;
+                        H += keep;
+                    } else {
+                        keep = T >= ties - need;
+                    }
+                    ++T;
+                } else {
+                    keep = false;
+                }
+            }
+            // block starts: number of kept states before the first state of the block
+            int p = block_of(s_blk, L, i);
+            if (s_blk[p] == i) out_blk[p] = int(out);
+            if (keep) {
+                if (out < out_cap) {
+                    const uint64_t* src = x_keys + i * NW;
+                    uint64_t* dst = out_keys + out * NW;
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) dst[w] = src[w];
+                } else {
+                    raise_status(status, PACES_ERR_CAPACITY);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void trunc_finalize_kernel(ModelDev m, const int* __restrict__ x_blk, int64_t maxstates,
+                                      TruncWs ws, int* out_blk, int64_t out_cap, int* n_tied_out,
+                                      int* status) {
+    if (threadIdx.x != 0) return;
+    const int L = m.L;
+    const long long S = ws.sel[SEL_S];
+    long long total = ws.sel[SEL_ALL] ? S : maxstates;
+    if (total > out_cap) {
+        raise_status(status, PACES_ERR_CAPACITY);
+        total = out_cap;
+    }
+    if (ws.sel[SEL_CAND] > ws.cap) raise_status(status, PACES_ERR_CAPACITY);
+    out_blk[L] = int(total);
+    for (int p = L - 1; p >= 0; --p)
+        if (x_blk[p] == x_blk[p + 1]) out_blk[p] = out_blk[p + 1];
+    if (n_tied_out) *n_tied_out = int(ws.sel[SEL_ALL] ? 0 : ws.sel[SEL_TIES]);
+}
+
+template <int NW, bool C64>
+int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_blk, const void* psi,
+                      int64_t maxstates, int shuffle, uint64_t seed, uint64_t step, const TruncWs& ws,
+                      uint64_t* out_keys, int* out_blk, int64_t out_cap, int* n_tied_out, int* status,
+                      int num_sms, cudaStream_t st) {
+    const int g = num_sms * 4;
+    trunc_init_kernel<<<1, 1024, 0, st>>>(m, x_blk, maxstates, ws);
+    trunc_hist_all_kernel<C64><<<g, 256, 0, st>>>(psi, ws, status);
+    trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, 0, 1);
+    trunc_collect_kernel<C64><<<g, 256, 0, st>>>(psi, ws, status);
+    for (int r = 1; r < kRounds; ++r) {
+        trunc_hist_cand_kernel<<<g, 256, 0, st>>>(ws, SEL_W, r);
+        trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, r, 1);
+    }
+    if (shuffle) {
+        trunc_shuffle_prep_kernel<<<1, 32, 0, st>>>(ws, status);
+        trunc_collect_ties_kernel<C64><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
+        for (int r = 0; r < kRounds; ++r) {
+            trunc_hist_cand_kernel<<<g, 256, 0, st>>>(ws, SEL_H, r);
+            trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_H, r, 0);
+        }
+    }
+    trunc_count_kernel<C64><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
+    trunc_scan_kernel<<<1, 1024, 0, st>>>(ws);
+    trunc_write_kernel<NW, C64><<<g, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
+                                                   out_blk, out_cap, status);
+    trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out, status);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
+}
+
+template <int NW>
+int dispatch_prec(bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+                  const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
+                  const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
+                  int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
+    if (c64)
+        return launch_truncate_t<NW, true>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
+                                           out_keys, out_blk, out_cap, n_tied_out, status, num_sms, st);
+    return launch_truncate_t<NW, false>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
+                                        out_keys, out_blk, out_cap, n_tied_out, status, num_sms, st);
+}
+
+}  // namespace
+
+int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+                    const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
+                    const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
+                    int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
+#define PACES_TRUNC_CASE(N)                                                                       \
+    case N:                                                                                       \
+        return dispatch_prec<N>(c64, m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,   \
+                                out_keys, out_blk, out_cap, n_tied_out, status, num_sms, st);
+    switch (nw) {
+        PACES_TRUNC_CASE(1)
+        PACES_TRUNC_CASE(2)
+        PACES_TRUNC_CASE(3)
+        PACES_TRUNC_CASE(4)
+        PACES_TRUNC_CASE(5)
+        PACES_TRUNC_CASE(6)
+        PACES_TRUNC_CASE(7)
+        PACES_TRUNC_CASE(8)
+        default: return PACES_ERR_BADARG;
+    }
+#undef PACES_TRUNC_CASE
+}
+
+}  // namespace paces

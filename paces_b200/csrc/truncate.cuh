@@ -1,0 +1,43 @@
+// Amplitude-ranked truncation to `maxstates` states.
+//
+// Reference (paces/core/time_evolution.py:833-910): stable ascending argsort of |psi|,
+// keep the last `maxstates` entries (among equal values the highest indices), lexsort
+// the kept rows.  With shuffle_seed set and a tie at the cut, the tied states at the
+// cut are drawn at random.
+//
+// B200 design: no sort.  The weights |psi| are non-negative doubles, so their bit
+// patterns order like the values; a radix select (12-bit digits, shared-memory
+// histograms) finds the threshold value v* and the number of states equal to v* that
+// must be kept.  Because the basis is already sorted, keeping the selected states in
+// index order *is* the lexsorted result: one order-preserving compaction writes the
+// new basis (keys and block offsets).  Tie rule as in the reference: the states equal
+// to v* with the highest indices; with shuffling, the tied states whose 64-bit hash of
+// (seed, step, index) is smallest -- a uniformly random subset, like the reference's
+// random permutation, but not the same stream (parity unpinned for that branch).
+#pragma once
+
+#include "common.cuh"
+
+namespace paces {
+
+struct TruncWs {
+    unsigned* hist;              // [4096]
+    unsigned long long* cand;    // [cap] candidate weight bits (or hashes)
+    int* cand_idx;               // [cap]
+    long long* sel;              // selection state, see truncate.cu
+    int* tile_cnt;               // [ntiles_cap][3]
+    int* tile_pre;               // [ntiles_cap][3]
+    int64_t cap;
+    int ntiles_cap;
+};
+
+constexpr int kTruncTile = 4096;
+
+inline int trunc_tiles_cap(int64_t cap) { return int(cap / kTruncTile + 2); }
+
+int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+                    const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
+                    const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
+                    int* n_tied_out, int* status, int num_sms, cudaStream_t st);
+
+}  // namespace paces

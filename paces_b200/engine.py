@@ -1,0 +1,374 @@
+"""Device-side engine: owns the native context and the device buffers of one trajectory.
+
+Everything that touches amplitudes or keys runs in libpaces_b200 (sm_100a); this
+module only allocates torch tensors (device memory), passes their pointers through the
+C ABI and reads back the one small record each step produces.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+import torch
+
+from . import _native as nat
+
+TAYLOR_TOL_C128 = 2.0 ** -53   # paces/core/time_evolution.py:484
+TAYLOR_TOL_C64 = 2.0 ** -24    # single-precision unit roundoff
+
+
+@dataclasses.dataclass
+class ModelParams:
+    """Holstein chain (paces/models/holstein.py:24-66 with its use_terms dict)."""
+    nchain: int
+    max_ho_dims: list
+    J: float = 1.0
+    g: float = 1.0
+    eps_sys: float = 0.0
+    hbar_omega: float = 1.0
+    delta_eps: float = 0.0
+    periodic: bool = False
+    site_eps: list | None = None
+    precision: str = "c128"   # "c128" (reference precision) or "c64"
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+class DevBasis:
+    """A sorted basis on the device: keys [cap, nw] (uint64 words in int64 storage) and
+    block offsets by exciton position blk [nchain+1] (blk[nchain] = number of states)."""
+
+    def __init__(self, eng: "Engine", cap: int):
+        self.eng = eng
+        self.cap = int(cap)
+        self.keys = torch.empty((max(self.cap, 1), eng.nw), dtype=torch.int64, device=eng.device)
+        self.blk = torch.zeros(eng.L + 1, dtype=torch.int32, device=eng.device)
+
+    def c(self):
+        return nat.Basis(self.keys.data_ptr(), self.blk.data_ptr(), self.cap)
+
+    def count(self) -> int:
+        return int(self.blk[self.eng.L].item())
+
+
+class DevHMat:
+    """Neighbour table [4, cap] (left, right, down, up; -1 = absent) and row metadata [cap]."""
+
+    def __init__(self, eng: "Engine", cap: int):
+        self.cap = int(cap)
+        self.nbr = torch.empty((4, max(self.cap, 1)), dtype=torch.int32, device=eng.device)
+        self.meta = torch.empty(max(self.cap, 1), dtype=torch.int32, device=eng.device)
+
+    def c(self):
+        return nat.HMat(self.nbr.data_ptr(), self.meta.data_ptr(), self.cap)
+
+
+class Engine:
+    def __init__(self, params: ModelParams, device=None, cap: int = 4096):
+        self.lib = nat.load()
+        if not torch.cuda.is_available():
+            raise RuntimeError("paces_b200 needs a CUDA device (sm_100a); none is visible")
+        self.device = torch.device(device if device is not None else "cuda")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.params = params
+        self.L = int(params.nchain)
+        self.c64 = params.precision == "c64"
+        self.cdtype = torch.complex64 if self.c64 else torch.complex128
+        self.tol = TAYLOR_TOL_C64 if self.c64 else TAYLOR_TOL_C128
+        dims = (ctypes.c_int32 * self.L)(*[int(x) for x in params.max_ho_dims])
+        site = None
+        if params.site_eps is not None:
+            site = (ctypes.c_double * self.L)(*[float(x) for x in params.site_eps])
+        desc = nat.ModelDesc(self.L, 1 if params.periodic else 0, nat.C64 if self.c64 else nat.C128, 0,
+                             dims, float(params.eps_sys), float(params.hbar_omega),
+                             float(params.delta_eps), float(params.J), float(params.g),
+                             site if site is not None else ctypes.POINTER(ctypes.c_double)())
+        self._dims, self._site = dims, site
+        ctx = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            nat.check(self.lib.paces_create(ctypes.byref(desc), ctypes.byref(ctx)), None, "paces_create")
+        self.ctx = ctx
+        self.nw = self.lib.paces_key_words(ctx)
+        self.ref_words = self.lib.paces_ref_words(ctx)
+        self.cap = 0
+        self.ws = None
+        self._grow(cap)
+        self.rec_dev = torch.zeros(ctypes.sizeof(nat.StepRecord), dtype=torch.uint8, device=self.device)
+        self.rec_host = torch.zeros(ctypes.sizeof(nat.StepRecord), dtype=torch.uint8).pin_memory()
+
+    # ---- buffers ------------------------------------------------------------------------
+    def _grow(self, cap):
+        cap = int(max(cap, 64))
+        if cap <= self.cap:
+            return
+        nbytes = ctypes.c_size_t()
+        nat.check(self.lib.paces_workspace_bytes(self.ctx, cap, ctypes.byref(nbytes)), self.ctx, "workspace")
+        self.ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        self.ws_bytes = int(nbytes.value)
+        self.cap = cap
+
+    def workspace(self):
+        return _ptr(self.ws), ctypes.c_size_t(self.ws_bytes)
+
+    def new_basis(self, cap=None):
+        return DevBasis(self, self.cap if cap is None else cap)
+
+    def new_hmat(self, cap=None):
+        return DevHMat(self, self.cap if cap is None else cap)
+
+    def new_vector(self, cap=None):
+        return torch.zeros(max(self.cap if cap is None else cap, 1), dtype=self.cdtype, device=self.device)
+
+    def read_status(self):
+        st = ctypes.c_int32()
+        nat.check(self.lib.paces_read_status(self.ctx, _stream(self.device), ctypes.byref(st)), self.ctx,
+                  "read_status")
+        return int(st.value)
+
+    def raise_status(self, what):
+        st = self.read_status()
+        if st != nat.PACES_OK:
+            if st == nat.ERR_CAPACITY:
+                raise nat.CapacityError(st, what)
+            raise nat.PacesError(st, what)
+
+    # ---- layout conversion ----------------------------------------------------------------
+    def basis_from_ref(self, ref_rows, cap=None) -> DevBasis:
+        """Reference whoami rows (uint32 [n, W], sorted, unique) -> device basis."""
+        ref = torch.as_tensor(np.ascontiguousarray(ref_rows).view(np.int32) if isinstance(ref_rows, np.ndarray)
+                              else ref_rows)
+        ref = ref.to(self.device, torch.int32).contiguous()
+        n = int(ref.shape[0])
+        if n and int(ref.shape[1]) != self.ref_words:
+            raise ValueError(f"rows have {ref.shape[1]} words, the model packs {self.ref_words}")
+        b = self.new_basis(max(cap or 0, n, 1))
+        pos = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        if n:
+            nat.check(self.lib.paces_keys_from_ref(self.ctx, _ptr(ref), n, self.ref_words, _ptr(b.keys), _ptr(pos),
+                                                   _stream(self.device)), self.ctx, "keys_from_ref")
+            self.raise_status("keys_from_ref: occupation or position out of range")
+            counts = torch.bincount(pos[:n].long(), minlength=self.L)
+            b.blk[1:] = torch.cumsum(counts, 0).to(torch.int32)
+            if not bool((pos[1:n] >= pos[: n - 1]).all()):
+                raise ValueError("basis rows must be sorted (exciton position is the leading field)")
+        return b
+
+    def basis_to_ref(self, b: DevBasis, n=None) -> torch.Tensor:
+        n = b.count() if n is None else n
+        out = torch.empty((max(n, 1), self.ref_words), dtype=torch.int32, device=self.device)
+        if n:
+            nat.check(self.lib.paces_keys_to_ref(self.ctx, ctypes.byref(b.c()), self.ref_words, _ptr(out),
+                                                 _stream(self.device)), self.ctx, "keys_to_ref")
+        return out[:n]
+
+    def query_from_ref(self, ref_rows):
+        """Arbitrary reference rows -> (keys, pos) device tensors (no ordering needed)."""
+        ref = torch.as_tensor(np.ascontiguousarray(ref_rows).view(np.int32) if isinstance(ref_rows, np.ndarray)
+                              else ref_rows).to(self.device, torch.int32).contiguous()
+        n = int(ref.shape[0])
+        keys = torch.empty((max(n, 1), self.nw), dtype=torch.int64, device=self.device)
+        pos = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        if n:
+            nat.check(self.lib.paces_keys_from_ref(self.ctx, _ptr(ref), n, self.ref_words, _ptr(keys), _ptr(pos),
+                                                   _stream(self.device)), self.ctx, "keys_from_ref")
+        return keys, pos, n
+
+    # ---- stages ---------------------------------------------------------------------------
+    def expand(self, b: DevBasis, out: DevBasis | None = None) -> DevBasis:
+        out = out or self.new_basis()
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_expand(self.ctx, ctypes.byref(b.c()), ctypes.byref(out.c()), ws, nb,
+                                        _stream(self.device)), self.ctx, "expand")
+        self.raise_status("expand")
+        return out
+
+    def assemble(self, b: DevBasis, out: DevBasis | None = None, h: DevHMat | None = None):
+        out = out or self.new_basis()
+        h = h or self.new_hmat(out.cap)
+        ceil = torch.zeros(1, dtype=torch.int32, device=self.device)
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_assemble(self.ctx, ctypes.byref(b.c()), ctypes.byref(out.c()), ctypes.byref(h.c()),
+                                          _ptr(ceil), ws, nb, _stream(self.device)), self.ctx, "assemble")
+        self.raise_status("assemble")
+        return out, h, int(ceil.item())
+
+    def truncate(self, b: DevBasis, psi, maxstates, shuffle=False, seed=0, step=0, out=None) -> DevBasis:
+        out = out or self.new_basis()
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_truncate(self.ctx, ctypes.byref(b.c()), _ptr(psi), int(maxstates), int(bool(shuffle)),
+                                          int(seed), int(step), ctypes.byref(out.c()), ws, nb,
+                                          _stream(self.device)), self.ctx, "truncate")
+        self.raise_status("truncate")
+        return out
+
+    def remap(self, old: DevBasis, old_psi, new: DevBasis, new_psi=None):
+        new_psi = self.new_vector(new.cap) if new_psi is None else new_psi
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_remap(self.ctx, ctypes.byref(old.c()), _ptr(old_psi), ctypes.byref(new.c()),
+                                       _ptr(new_psi), ws, nb, _stream(self.device)), self.ctx, "remap")
+        self.raise_status("remap")
+        return new_psi
+
+    def taylor(self, b: DevBasis, h: DevHMat, psi_in, dt, m_star=100, tol=None, psi_out=None):
+        psi_out = self.new_vector(b.cap) if psi_out is None else psi_out
+        info = torch.zeros(ctypes.sizeof(nat.ExpmInfo), dtype=torch.uint8, device=self.device)
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_taylor(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(psi_in),
+                                        _ptr(psi_out), float(dt), int(m_star), float(self.tol if tol is None else tol),
+                                        _ptr(info), ws, nb, _stream(self.device)), self.ctx, "taylor")
+        self.raise_status("taylor")
+        raw = info.cpu().numpy().tobytes()
+        e = nat.ExpmInfo.from_buffer_copy(raw)
+        return psi_out, [bool(e.converged), int(e.final_m), float(e.c1_plus_c2), float(e.term_ratio)]
+
+    def observables(self, b: DevBasis, h: DevHMat, psi, what=nat.OBS_NORM | nat.OBS_ENERGY | nat.OBS_SITES):
+        out = torch.zeros(3 + 2 * self.L, dtype=torch.float64, device=self.device)
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_observables(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(psi),
+                                             int(what), _ptr(out), ws, nb, _stream(self.device)), self.ctx,
+                  "observables")
+        o = out.cpu().numpy()
+        return {"norm": o[0], "energy": complex(o[1], o[2]), "n_exc": o[3:3 + self.L],
+                "n_pho": o[3 + self.L:3 + 2 * self.L]}
+
+    def lookup(self, pb: DevBasis, q_keys, q_pos, nq, must_exist=False):
+        out = torch.empty(max(nq, 1), dtype=torch.int64, device=self.device)
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_lookup(self.ctx, ctypes.byref(pb.c()), _ptr(q_keys), _ptr(q_pos), int(nq),
+                                        int(bool(must_exist)), _ptr(out), ws, nb, _stream(self.device)), self.ctx,
+                  "lookup")
+        if must_exist:
+            self.raise_status("lookup: a state that must exist is not in the basis")
+        return out[:nq]
+
+    def step(self, old: DevBasis, old_psi, new: DevBasis, new_psi, h: DevHMat, prm: nat.StepParams,
+             sync=True):
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_step(self.ctx, ctypes.byref(old.c()), _ptr(old_psi), ctypes.byref(new.c()),
+                                      _ptr(new_psi), ctypes.byref(h.c()), ctypes.byref(prm), _ptr(self.rec_dev),
+                                      ws, nb, _stream(self.device)), self.ctx, "step")
+        if not sync:
+            return None
+        return self.read_record()
+
+    def read_record(self) -> nat.StepRecord:
+        self.rec_host.copy_(self.rec_dev, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return nat.StepRecord.from_buffer_copy(self.rec_host.numpy().tobytes())
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.paces_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Trajectory:
+    """One adaptive-basis trajectory on the device, stepped by `paces_step`.
+
+    Two basis/amplitude slots alternate: a step reads the current slot and writes the
+    other, so a capacity overflow leaves the state intact and the step is retried with
+    larger buffers.
+    """
+
+    def __init__(self, eng: Engine, maxstates, enlarge_steps, m_star=100, diagnostics=True,
+                 shuffle_seed=None, renormalize=False, explosion_cutoff=2.0, cap=None):
+        self.eng = eng
+        self.maxstates = int(maxstates)
+        self.enlarge_steps = int(enlarge_steps)
+        self.m_star = int(m_star)
+        self.diagnostics = bool(diagnostics)
+        self.shuffle_seed = shuffle_seed
+        self.renormalize = bool(renormalize)
+        self.explosion_cutoff = float(explosion_cutoff)
+        guess = int((2.5 + 2.0 * (self.enlarge_steps + 1)) * self.maxstates) + 1024
+        eng._grow(cap or guess)
+        self._alloc()
+        self.cur = 0
+        self.step_index = 0
+        self.last = None
+
+    def _alloc(self):
+        e = self.eng
+        self.bases = [e.new_basis(), e.new_basis()]
+        self.psis = [e.new_vector(), e.new_vector()]
+        self.h = e.new_hmat()
+
+    def _regrow(self, factor=1.6):
+        """Grow every buffer, keeping the current state."""
+        e = self.eng
+        old_b, old_psi = self.bases[self.cur], self.psis[self.cur]
+        n = old_b.count()
+        e._grow(int(e.cap * factor))
+        keep_keys, keep_blk, keep_psi = old_b.keys[:n].clone(), old_b.blk.clone(), old_psi[:n].clone()
+        self._alloc()
+        b = self.bases[self.cur]
+        b.keys[:n] = keep_keys
+        b.blk.copy_(keep_blk)
+        self.psis[self.cur][:n] = keep_psi
+
+    def set_state(self, basis: DevBasis, psi):
+        n = basis.count()
+        while n > self.eng.cap:
+            self._regrow()
+        b = self.bases[self.cur]
+        b.keys[:n] = basis.keys[:n]
+        b.blk.copy_(basis.blk)
+        v = self.psis[self.cur]
+        v.zero_()
+        v[:n] = psi[:n].to(self.eng.cdtype)
+
+    @property
+    def basis(self) -> DevBasis:
+        return self.bases[self.cur]
+
+    @property
+    def vector(self):
+        return self.psis[self.cur][: self.basis.count()]
+
+    def params(self, evolve, dt):
+        p = nat.StepParams()
+        p.maxstates = self.maxstates
+        p.enlarge_steps = self.enlarge_steps
+        p.evolve = 1 if evolve else 0
+        p.dt = float(dt)
+        p.m_star = self.m_star
+        p.diagnostics = 1 if self.diagnostics else 0
+        p.tol = self.eng.tol
+        p.shuffle = 0 if self.shuffle_seed is None else 1
+        p.renormalize = 1 if self.renormalize else 0
+        p.shuffle_seed = 0 if self.shuffle_seed is None else int(self.shuffle_seed) & 0xFFFFFFFFFFFFFFFF
+        p.step_index = self.step_index
+        p.explosion_cutoff = self.explosion_cutoff
+        return p
+
+    def step(self, evolve=True, dt=0.0):
+        """One time step (first step: evolve=False).  Returns the step record."""
+        nxt = 1 - self.cur
+        for _ in range(12):
+            rec = self.eng.step(self.bases[self.cur], self.psis[self.cur], self.bases[nxt], self.psis[nxt],
+                                self.h, self.params(evolve, dt))
+            if rec.status == nat.ERR_CAPACITY:
+                self._regrow()
+                continue
+            break
+        if rec.status != nat.PACES_OK:
+            raise nat.PacesError(rec.status, "paces_step")
+        self.cur = nxt
+        self.step_index += 1
+        self.last = rec
+        return rec
