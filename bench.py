@@ -1,0 +1,429 @@
+"""Benchmark of the adaptive-basis time step (Holstein chain, paces) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision c128|c64] [--maxstates M] [--nchain L] [--g G]
+
+Workload (default): 1D periodic Holstein chain, single exciton, N=32 sites, J=1,
+omega0=1, g=1.5, cutoff 15 (4-bit fields, 2 uint64 words per key), dt=0.05,
+maxstates=2^22, enlarge_steps=1, exciton on site 0 with phonon vacuum.  A "step" is
+one full adaptive time step (truncate -> expand -> sort/unique -> assemble H ->
+remap -> Taylor exp(-i dt H) -> observables) once the basis is saturated at
+maxstates.  Untimed preparation steps grow the basis to saturation first.
+
+N > 1 (torchrun): independent replicas, one per GPU ("replicas only": the path is
+not sharded); value = steps of all ranks / max-over-ranks time.
+
+--impl reference times the CPU restatement of the reference (oracle/paces_oracle.py)
+on the host cores, on a bounded sample of the same workload (smaller maxstates,
+scaled linearly to the configured maxstates).
+"""
+
+import argparse
+import ctypes
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="c128", choices=["c128", "c64"])
+    ap.add_argument("--maxstates", type=int, default=1 << 22)
+    ap.add_argument("--nchain", type=int, default=32)
+    ap.add_argument("--g", type=float, default=1.5)
+    ap.add_argument("--dt", type=float, default=0.05)
+    ap.add_argument("--enlarge-steps", type=int, default=1)
+    ap.add_argument("--open-chain", action="store_true", help="open boundaries (the reference's only mode)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(a):
+    bc = "open" if a.open_chain else "periodic"
+    return (f"holstein_{bc}_n{a.nchain}_cutoff15_g{a.g:g}_maxstates{a.maxstates}_dt{a.dt:g}"
+            f"_es{a.enlarge_steps}")
+
+
+def log(a, *msg):
+    if a.verbose:
+        print(*msg, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# --------------------------------------------------------------------------------------------
+# shared workload setup
+# --------------------------------------------------------------------------------------------
+def model_params(a, precision):
+    from paces_b200.engine import ModelParams
+    return ModelParams(nchain=a.nchain, max_ho_dims=[16] * a.nchain, J=1.0, g=a.g, eps_sys=0.0,
+                       hbar_omega=1.0, delta_eps=0.0, periodic=not a.open_chain, precision=precision)
+
+
+def initial_rows(nchain, initpos=0):
+    from paces_b200 import layout
+    raw = np.zeros((1, nchain + 1), dtype=np.uint32)
+    raw[0, 0] = initpos
+    return layout.pack_rows(raw, layout.bitwidths_for([nchain] + [16] * nchain))
+
+
+def prepare(a, eng, maxstates):
+    """Grow the basis (grow_optimal_basis, fillfac=1), first step, then propagate until the
+    truncation keeps exactly maxstates states; returns the saturated trajectory."""
+    import torch
+    from paces_b200.engine import Trajectory
+    tr = Trajectory(eng, maxstates, a.enlarge_steps)
+    b = eng.basis_from_ref(initial_rows(a.nchain))
+    prev = b
+    while True:
+        nxt = eng.expand(prev)
+        if nxt.count() > maxstates:
+            break
+        b, prev = nxt, nxt
+        if nxt.count() == 0:
+            break
+    init = eng.basis_from_ref(initial_rows(a.nchain))
+    keys, pos, n = eng.query_from_ref(initial_rows(a.nchain))
+    idx = int(eng.lookup(b, keys, pos, n, must_exist=True)[0].item())
+    psi = torch.zeros(max(b.count(), 1), dtype=eng.cdtype, device=eng.device)
+    psi[idx] = 1.0
+    del init
+    tr.set_state(b, psi)
+    rec = tr.step(evolve=False)
+    nprep = 1
+    while True:
+        rec = tr.step(evolve=True, dt=a.dt)
+        nprep += 1
+        log(a, f"prep step {nprep}: select={rec.n_select} enlarged={rec.n_enlarged} S={rec.n_states} "
+               f"m={rec.final_m}")
+        if rec.n_select >= maxstates and nprep >= 3:
+            break
+        if nprep > 400:
+            raise RuntimeError("basis did not saturate")
+    return tr, nprep
+
+
+def taylor_bytes_per_term(rec, cs):
+    """Algorithmic bytes of one Taylor term on S rows: neighbour table (16 B), row metadata
+    (4 B), previous term read once, result read and written, new term written (4*cs)."""
+    return rec.n_states * (16 + 4 + 4 * cs)
+
+
+def step_bytes(rec, cs, nw, es):
+    """Algorithmic bytes of a whole step (measurement section)."""
+    kb = 8 * nw
+    S, B, M = rec.n_states, rec.n_enlarged, rec.n_select
+    truncate = S * cs + M * kb                      # read amplitudes, write kept keys
+    expand = es * (M * kb + B * kb)                  # read the basis once, write the enlarged basis
+    assemble = B * kb + S * kb + S * (16 + 4) + 5 * B * 4 + B * 32   # keys in/out, H table, maps, fill
+    remap = 2 * S * kb + 2 * S * cs
+    taylor = (rec.final_m + 1) * S * (16 + 4 + 4 * cs)
+    obs = 2 * S * (cs + 4 + 16) + S * kb
+    return truncate + expand + assemble + remap + taylor + obs
+
+
+def read_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_profile_traffic(precision):
+    """DRAM bytes per row and Taylor term of the Taylor kernel from the committed ncu summary."""
+    p = os.path.join(HERE, "profiles", f"taylor_kernel_{precision}.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        m = re.search(r"dram_bytes_per_row_term:\s*([0-9.]+)", f.read())
+    return float(m.group(1)) if m else None
+
+
+# --------------------------------------------------------------------------------------------
+# CPU restatement (reference arm and cpu_baseline)
+# --------------------------------------------------------------------------------------------
+def oracle_sample(a, m_s, steps, warmup):
+    """Time the CPU oracle on a bounded sample of the workload: the same chain at a reduced
+    maxstates m_s, grown to saturation untimed, then `warmup` + `steps` timed oracle steps.
+    Returns steps/s scaled linearly to a.maxstates (the oracle's cost grows at least
+    linearly with the basis, so the scaled figure favours the CPU), and a description."""
+    from oracle import paces_oracle as po
+    model = po.Model(a.nchain, [16] * a.nchain, g=a.g, periodic=not a.open_chain)
+    tr = po.Trajectory(model, po.initial_basis(model, 0), np.array([1.0 + 0j]), m_s, a.enlarge_steps)
+    t = 0.0
+    tr.first_step(t)
+    n = 0
+    while True:
+        t += a.dt
+        rec = tr.step(t, a.dt)
+        n += 1
+        if len(tr.records) > 3 and rec.numstates > 3 * m_s and n > 3:
+            break
+        if n > 200:
+            break
+    for _ in range(warmup):
+        t += a.dt
+        tr.step(t, a.dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        t += a.dt
+        tr.step(t, a.dt)
+    dt_wall = time.perf_counter() - t0
+    sps = steps / dt_wall
+    scaled = sps * m_s / a.maxstates
+    desc = (f"{steps} oracle steps of the same chain at maxstates={m_s} (saturated, S~{tr.records[-1].numstates}),"
+            f" {dt_wall:.1f} s, scaled by {m_s}/{a.maxstates} (cost linear in maxstates)")
+    return scaled, desc, sps, m_s
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, a.steps)
+    value, desc, _, _ = oracle_sample(a, 1 << 16, steps, max(0, a.warmup))
+    cfg = {"workload": workload_name(a), "nchain": a.nchain, "maxstates": a.maxstates, "g": a.g,
+           "enlarge_steps": a.enlarge_steps, "precision": "c128", "bench_sample": "bounded, see cpu_baseline"}
+    line = {"impl": "reference", "metric": "time-steps/s at 4M states", "value": value, "unit": "time-steps/s",
+            "n_gpus": a.gpus, "steps": steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "time-steps/s", "cores": 1, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "time-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------------------------
+# device arm
+# --------------------------------------------------------------------------------------------
+def run_ours(a):
+    import torch
+    from paces_b200 import _native as nat
+    from paces_b200.engine import Engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    eng = Engine(model_params(a, a.precision), device=f"cuda:{local}")
+    cs = 8 if a.precision == "c64" else 16
+    tr, nprep = prepare(a, eng, a.maxstates)
+    for _ in range(max(a.warmup, 0)):
+        tr.step(evolve=True, dt=a.dt)
+    eng.set_profiling(True)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    stage_sum = {s: 0.0 for s in nat.STAGES}
+    recs = []
+    launches0 = eng.kernel_launches()
+    barrier()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            recs.append(tr.step(evolve=True, dt=a.dt))
+            for k, v in eng.stage_times().items():
+                stage_sum[k] += v
+        ev1.record(stream)
+        ev1.synchronize()
+    launches = eng.kernel_launches() - launches0
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+    barrier()
+    eng.set_profiling(False)
+
+    # e2e: the C ABI called with host buffers -- every step copies the state in from pinned
+    # host memory, runs paces_step, and copies the new state and its record back out.
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_e2e(a, eng, tr, barrier, dist)
+
+    total_steps = a.steps * world
+    value = total_steps / (ms / 1e3)
+    last = recs[-1]
+    taylor_ms = stage_sum["taylor"] / a.steps
+    terms = statistics.mean(r.final_m + 1 for r in recs)
+    S_mean = statistics.mean(r.n_states for r in recs)
+    taylor_alg = statistics.mean(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in recs)
+    achieved = taylor_alg / (taylor_ms / 1e3) / 1e9
+    peak, peak_kind = read_peaks()
+    per_row_term = read_profile_traffic(a.precision)
+    traffic = None if per_row_term is None else per_row_term * S_mean * terms
+    step_alg = statistics.mean(step_bytes(r, cs, eng.nw, a.enlarge_steps) for r in recs)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, desc, _, _ = oracle_sample(a, 1 << 16, 5, 0)
+        cpu = {"value": v, "unit": "time-steps/s", "cores": 1, "kind": "port", "sample": desc}
+    if rank == 0:
+        cfg = {"workload": workload_name(a), "nchain": a.nchain, "cutoff": 15, "g": a.g, "omega0": 1.0, "J": 1.0,
+               "dt": a.dt, "maxstates": a.maxstates, "enlarge_steps": a.enlarge_steps,
+               "boundary": "open" if a.open_chain else "periodic", "precision": a.precision,
+               "states_per_step": int(S_mean), "taylor_terms_per_step": terms, "prep_steps": nprep,
+               "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}"}
+        line = {
+            "metric": "time-steps/s at 4M states", "value": value, "unit": "time-steps/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic", "config": cfg,
+            "roofline": {"bound": "hbm", "kernel": "taylor_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes": taylor_alg, "launch_ms": taylor_ms},
+            "step_roofline": {"achieved": step_alg / (ms / a.steps / 1e3) / 1e9, "unit": "GB/s",
+                              "frac": step_alg / (ms / a.steps / 1e3) / 1e9 / peak},
+            "stage_ms": {k: v / a.steps for k, v in stage_sum.items()},
+            "clocks": clocks, "gpu_launches": launches, "cpu_baseline": cpu, "e2e": e2e,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(a, eng, tr, barrier, dist):
+    import torch
+    e = eng
+    cs = 8 if a.precision == "c64" else 16
+    cap = e.cap
+    hk = [torch.empty((cap, e.nw), dtype=torch.int64).pin_memory() for _ in range(2)]
+    hb = [torch.empty(e.L + 1, dtype=torch.int32).pin_memory() for _ in range(2)]
+    hp = [torch.empty(cap, dtype=e.cdtype).pin_memory() for _ in range(2)]
+    b, v = tr.basis, tr.psis[tr.cur]
+    n = b.count()
+    hk[0][:n].copy_(b.keys[:n])
+    hb[0].copy_(b.blk)
+    hp[0][:n].copy_(v[:n])
+    cur = 0
+    h2d = d2h = 0
+    barrier()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        db, dv = tr.basis, tr.psis[tr.cur]
+        db.keys[:n].copy_(hk[cur][:n], non_blocking=True)
+        db.blk.copy_(hb[cur], non_blocking=True)
+        dv[:n].copy_(hp[cur][:n], non_blocking=True)
+        h2d += n * (e.nw * 8 + cs) + (e.L + 1) * 4
+        rec = tr.step(evolve=True, dt=a.dt)
+        n = rec.n_states
+        nb, nv = tr.basis, tr.psis[tr.cur]
+        nxt = 1 - cur
+        hk[nxt][:n].copy_(nb.keys[:n], non_blocking=True)
+        hb[nxt].copy_(nb.blk, non_blocking=True)
+        hp[nxt][:n].copy_(nv[:n], non_blocking=True)
+        d2h += n * (e.nw * 8 + cs) + (e.L + 1) * 4 + ctypes.sizeof(type(rec))
+        torch.cuda.current_stream().synchronize()
+        cur = nxt
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    world = 1
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        world = dist.get_world_size()
+    return {"value": a.steps * world / (ms / 1e3), "unit": "time-steps/s",
+            "h2d_bytes_per_step": h2d // a.steps, "d2h_bytes_per_step": d2h // a.steps,
+            "api": "paces_step (C ABI) with the state in pinned host memory"}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -168,6 +168,14 @@ int paces_version(void);                            /* 10000*major + 100*minor +
 /* Copy the context's device status word (errors raised by kernels of the stage entry points)
  * to the host, synchronising `stream`, and clear it. */
 int paces_read_status(paces_ctx *ctx, paces_stream_t stream, int32_t *host_status);
+/* Stage timing (no counterpart in the reference, which only prints wall-clock times):
+ * with profiling on, paces_step records CUDA events between its stages, and
+ * paces_stage_times waits for the last step and returns 7 durations in ms: truncate,
+ * expand, assemble, remap, diagnostics, Taylor, observables. */
+int paces_set_profiling(paces_ctx *ctx, int32_t on);
+int paces_stage_times(paces_ctx *ctx, float *ms);
+/* Number of kernels paces_step has enqueued on this context so far. */
+unsigned long long paces_kernel_launches(const paces_ctx *ctx);
 /* Workspace bytes for every entry point on bases of up to `cap` states. */
 int paces_workspace_bytes(const paces_ctx *ctx, int64_t cap, size_t *bytes);
 

@@ -131,8 +131,12 @@ _SIGNATURES = {
                      ctypes.c_size_t, _P],
     "paces_step": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, ctypes.POINTER(HMat),
                    ctypes.POINTER(StepParams), _P, _P, ctypes.c_size_t, _P],
+    "paces_set_profiling": [_P, ctypes.c_int32],
+    "paces_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
+    "paces_kernel_launches": [_P],
 }
-_RESTYPES = {"paces_last_error": ctypes.c_char_p}
+_RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_kernel_launches": ctypes.c_ulonglong}
+STAGES = ("truncate", "expand", "assemble", "remap", "diagnostics", "taylor", "observables")
 
 _lib = None
 

@@ -16,6 +16,9 @@ struct paces_ctx {
     int num_sms;
     int taylor_grid;
     int* d_status;  // device status word for the stage entry points
+    int profiling;  // record stage events in paces_step
+    cudaEvent_t ev[8];
+    unsigned long long launches;  // kernels launched by paces_step since creation
     char err[512];
 };
 
@@ -53,7 +56,7 @@ struct Layout {
     int64_t split_cap, tile_cap;
     size_t t_hist, t_cand, t_cand_idx, t_sel, t_tile_cnt, t_tile_pre;
     int t_tiles;
-    size_t r_tile_off, r_counters;
+    size_t r_tile_off, r_counters, r_split;
     int r_tiles;
     size_t v_V, v_TA, v_TB, v_partials, v_bar;
     size_t o_partials, o_out;
@@ -97,12 +100,13 @@ Layout make_layout(const paces_ctx* c, int64_t cap) {
     l.r_tiles = remap_tile_cap(cap, nw, L);
     l.r_tile_off = take(size_t(L + 1) * 4);
     l.r_counters = take(16);
+    l.r_split = take(size_t(l.r_tiles) * 2 * 4);
     l.v_V = take(ucap * cs);
     l.v_TA = take(ucap * cs);
     l.v_TB = take(ucap * cs);
     l.v_partials = take(size_t(2) * c->taylor_grid * 4 * 8);
     l.v_bar = take(16);
-    l.o_partials = take(size_t(obs_max_grid(c->num_sms)) * (3 + 2 * L) * 8);
+    l.o_partials = take(size_t(obs_max_grid(c->num_sms)) * (4 + 2 * L) * 8);
     l.o_out = take(size_t(3 + 2 * L) * 8);
     l.total = off;
     return l;
@@ -156,6 +160,7 @@ RemapWs remap_ws(const Layout& l, void* ws) {
     RemapWs w;
     w.tile_off = at<int>(ws, l.r_tile_off);
     w.counters = at<int>(ws, l.r_counters);
+    w.split = at<int>(ws, l.r_split);
     w.tile_cap = l.r_tiles;
     return w;
 }
@@ -270,8 +275,33 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
     return PACES_OK;
 }
 
+int paces_set_profiling(paces_ctx* c, int32_t on) {
+    if (!c) return PACES_ERR_BADARG;
+    if (on && !c->profiling) {
+        for (int i = 0; i < 8; ++i)
+            if (cudaEventCreate(&c->ev[i]) != cudaSuccess) return cuda_fail(c, "paces_set_profiling");
+    }
+    if (!on && c->profiling) {
+        for (int i = 0; i < 8; ++i) cudaEventDestroy(c->ev[i]);
+    }
+    c->profiling = on ? 1 : 0;
+    return PACES_OK;
+}
+
+int paces_stage_times(paces_ctx* c, float* ms) {
+    if (!c || !ms || !c->profiling) return PACES_ERR_BADARG;
+    if (cudaEventSynchronize(c->ev[7]) != cudaSuccess) return cuda_fail(c, "paces_stage_times");
+    for (int i = 0; i < 7; ++i)
+        if (cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]) != cudaSuccess)
+            return cuda_fail(c, "paces_stage_times");
+    return PACES_OK;
+}
+
+unsigned long long paces_kernel_launches(const paces_ctx* c) { return c ? c->launches : 0ull; }
+
 int paces_destroy(paces_ctx* c) {
     if (!c) return PACES_OK;
+    if (c->profiling) paces_set_profiling(c, 0);
     if (c->d_status) cudaFree(c->d_status);
     delete c;
     return PACES_OK;
@@ -452,7 +482,15 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
     const bool c64 = c->precision == PACES_C64;
     const int L = c->m.L;
     int* status = &rec->status;
+    auto mark = [&](int i) {
+        if (c->profiling) cudaEventRecord(c->ev[i], st);
+    };
+    // kernels issued by this step (merge: 5, +1 with the neighbour table; truncation: 18,
+    // +14 with tie shuffling; remap 2; observables 2; Taylor 1; renormalisation 3; record 2)
+    c->launches += 2 + (prm->shuffle ? 32 : 18) + 5ull * prm->enlarge_steps + 6 + 3 + (prm->diagnostics ? 2 : 0) +
+                   (prm->evolve ? 1 + (prm->renormalize ? 3 : 0) : 0) + 3;
     record_init_kernel<<<1, 32, 0, st>>>(rec, prm->diagnostics);
+    mark(0);
 
     paces_basis A{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap};
     paces_basis B{at<uint64_t>(ws, l.keysB), at<int32_t>(ws, l.blkB), l.cap};
@@ -461,6 +499,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
                                           prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), A.keys,
                                           A.blk, A.cap, &rec->n_tied, status, c->num_sms, st),
                        "step/truncate");
+    mark(1);
     // 2. enlargement (enlarge_steps times)
     const MergeWs mws = merge_ws(l, ws);
     paces_basis* cur = &A;
@@ -477,6 +516,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
         cur = other;
         other = t;
     }
+    mark(2);
     // 3. new basis + H
     {
         MergeOut mo{};
@@ -492,11 +532,13 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
                                            status, c->num_sms, st),
                            "step/assemble");
     }
+    mark(3);
     // 4. amplitudes into the new basis
     void* target = prm->evolve ? at<void>(ws, l.v_V) : new_psi;
     PACES_CHECK_LAUNCH(c, launch_remap(c->nw, c64, c->m, old_b->keys, old_b->blk, old_psi, new_b->keys, new_b->blk,
                                        target, remap_ws(l, ws), status, c->num_sms, st),
                        "step/remap");
+    mark(4);
     double* opart = at<double>(ws, l.o_partials);
     // 5. post-adaptation diagnostics
     if (prm->diagnostics) {
@@ -505,6 +547,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
                                                  target, PACES_OBS_NORM | PACES_OBS_ENERGY, opart, t, c->num_sms, st),
                            "step/diagnostics");
     }
+    mark(5);
     // 6. propagation
     if (prm->evolve) {
         TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
@@ -520,6 +563,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
                                "step/renormalize");
         }
     }
+    mark(6);
     // 7. observables of the new state
     {
         ObsTarget t{&rec->norm, &rec->energy_re, &rec->energy_im, rec->n_exc, rec->n_pho};
@@ -529,6 +573,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
                            "step/observables");
     }
     record_counts_kernel<<<1, 32, 0, st>>>(rec, A.blk, cur->blk, new_b->blk, L);
+    mark(7);
     if (cudaGetLastError() != cudaSuccess) return cuda_fail(c, "step/record");
     return PACES_OK;
 }

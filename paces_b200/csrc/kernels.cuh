@@ -23,6 +23,7 @@ __device__ __forceinline__ int find_segment(const int* off, int n, int s) {
 struct RemapWs {
     int* tile_off;  // [L+1]
     int* counters;  // [0] tiles
+    int* split;     // [tile_cap][2] old-basis split of each tile's first and last diagonal
     int tile_cap;
 };
 __host__ __device__ constexpr int remap_tile(int nw) { return nw <= 2 ? 2048 : (nw <= 4 ? 1024 : 512); }

@@ -78,13 +78,46 @@ __device__ int run_bound(const ModelDev& m, const uint64_t* __restrict__ X, int 
     return a;
 }
 
+// Tile keys in shared memory, word-major (w[q*stride + e]): a probe reads 8 bytes of word 0
+// and touches the next word only on a tie, which keeps bank conflicts low.
 template <int NW>
-__device__ __forceinline__ int smem_bound(const Key<NW>* keys, const uint8_t* flags, int off, int len,
+struct SKeys {
+    uint64_t* w;
+    int stride;
+    __device__ __forceinline__ Key<NW> get(int e) const {
+        Key<NW> k;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) k.w[q] = w[q * stride + e];
+        return k;
+    }
+    __device__ __forceinline__ void set(int e, const Key<NW>& k) const {
+#pragma unroll
+        for (int q = 0; q < NW; ++q) w[q * stride + e] = k.w[q];
+    }
+    __device__ __forceinline__ int cmp(int e, const Key<NW>& key) const {
+#pragma unroll
+        for (int q = 0; q < NW; ++q) {
+            const uint64_t a = w[q * stride + e];
+            if (a != key.w[q]) return a < key.w[q] ? -1 : 1;
+        }
+        return 0;
+    }
+    __device__ __forceinline__ bool eq(int e1, int e2) const {
+#pragma unroll
+        for (int q = 0; q < NW; ++q)
+            if (w[q * stride + e1] != w[q * stride + e2]) return false;
+        return true;
+    }
+};
+
+template <int NW>
+__device__ __forceinline__ int smem_bound(const SKeys<NW>& keys, const uint8_t* flags, int off, int len,
                                           const Key<NW>& key, int flag, bool upper) {
     int a = 0, b = len;
     while (a < b) {
         const int mid = (a + b) >> 1;
-        const int c = cmp_kf(keys[off + mid], int(flags[off + mid]), key, flag);
+        int c = keys.cmp(off + mid, key);
+        if (c == 0) c = int(flags[off + mid]) - flag;
         if (upper ? (c <= 0) : (c < 0)) a = mid + 1; else b = mid;
     }
     return a;
@@ -186,33 +219,45 @@ __global__ void __launch_bounds__(256) merge_order_kernel(ModelDev m, MergeWs ws
     }
 }
 
-// Exclusive prefix of `count` over tiles taken in ticket order (decoupled look-back).
-__device__ int lookback_prefix(unsigned long long* state, int t, int count, int* status) {
+// Exclusive prefix of `count` over tiles taken in ticket order: decoupled look-back by one
+// warp, 32 predecessors per probe.  Called by all lanes of one warp; returns the prefix.
+__device__ int lookback_warp(unsigned long long* state, int t, int count, int* status) {
+    const int lane = threadIdx.x & 31;
     if (t == 0) {
-        atomicExch(&state[0], kLbInc | (unsigned long long)count);
+        if (lane == 0) atomicExch(&state[0], kLbInc | (unsigned long long)count);
         return 0;
     }
-    atomicExch(&state[t], kLbAgg | (unsigned long long)count);
+    if (lane == 0) atomicExch(&state[t], kLbAgg | (unsigned long long)count);
     long long excl = 0;
-    int pred = t - 1;
+    int top = t - 1;  // window [top-31, top]; lane l looks at top - l
     const uint64_t t0 = global_ns();
-    while (pred >= 0) {
-        const unsigned long long v = atomicAdd(&state[pred], 0ull);
+    while (top >= 0) {
+        const int idx = top - lane;
+        const unsigned long long v = idx >= 0 ? atomicAdd(&state[idx], 0ull) : kLbInc;
         const unsigned long long fl = v >> 62;
-        if (fl == 0) {
+        const unsigned inc = __ballot_sync(0xffffffffu, fl == 2);
+        const unsigned notready = __ballot_sync(0xffffffffu, fl == 0);
+        const int first_inc = inc ? __ffs(inc) - 1 : 32;
+        const unsigned need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
+        if (notready & need) {
             if (global_ns() - t0 > kWaitLimitNs) {
-                raise_status(status, PACES_ERR_TIMEOUT);
+                if (lane == 0) raise_status(status, PACES_ERR_TIMEOUT);
                 break;
             }
-            __nanosleep(64);
+            __nanosleep(32);
             continue;
         }
-        excl += (long long)(v & kLbMask);
-        if (fl == 2) break;
-        --pred;
+        long long val = lane <= first_inc ? (long long)(v & kLbMask) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+        excl += val;
+        if (first_inc < 32) break;
+        top -= 32;
     }
-    __threadfence();
-    atomicExch(&state[t], kLbInc | (unsigned long long)(excl + count));
+    if (lane == 0) {
+        __threadfence();
+        atomicExch(&state[t], kLbInc | (unsigned long long)(excl + count));
+    }
     return int(excl);
 }
 
@@ -221,10 +266,12 @@ __global__ void __launch_bounds__(kTileThreads)
 merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tmax, MergeOut out,
                   int* status) {
     extern __shared__ __align__(16) unsigned char smem[];
-    Key<NW>* s_key = reinterpret_cast<Key<NW>*>(smem);
-    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_key + tmax);
+    const SKeys<NW> s_key{reinterpret_cast<uint64_t*>(smem), tmax};
+    uint8_t* s_flag = smem + size_t(tmax) * NW * 8;
     uint8_t* s_first = s_flag + tmax;
-    uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_first + ((tmax + 15) & ~15));
+    uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_first + ((tmax + 15) & ~15));  // merged pos -> element
+    uint16_t* s_rank = s_perm + tmax;                                                // element -> merged pos
+    uint16_t* s_cnt = s_rank + tmax;  // inclusive count of first occurrences per merged pos
 
     __shared__ int s_t, s_p, s_tl, s_n, s_base, s_total;
     __shared__ int s_start[kRuns], s_off[kRuns + 1], s_lo[kRuns];
@@ -234,8 +281,21 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
     __shared__ int s_ceil;
 
     const int tid = threadIdx.x;
+    __shared__ int s_tile_off[kMaxSites + 1];
+    __shared__ int s_split_off[kMaxSites * kRuns + 1];
+    __shared__ int s_run_lo[kMaxSites * kRuns];
+    __shared__ int s_run_len[kMaxSites * kRuns];
+    __shared__ Key<NW> s_pk[kRuns];
+    __shared__ int s_pf[kRuns], s_pv[kRuns], s_len[kRuns];
+
     const int L = m.L;
     const int ntiles = ws.counters[1];
+    for (int i = tid; i <= L; i += kTileThreads) s_tile_off[i] = ws.tile_off[i];
+    for (int i = tid; i <= L * kRuns; i += kTileThreads) s_split_off[i] = ws.split_off[i];
+    for (int i = tid; i < L * kRuns; i += kTileThreads) {
+        s_run_lo[i] = ws.run_lo[i];
+        s_run_len[i] = ws.run_len[i];
+    }
 
     for (;;) {
         if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
@@ -243,51 +303,63 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
         const int t = s_t;
         if (t >= ntiles) return;
 
-        if (tid == 0) {
-            const int p = find_segment(ws.tile_off, L, t);
-            const int tl = t - ws.tile_off[p];
-            const int ob = ws.split_off[p * kRuns];
-            const int nsb = ws.split_off[(p + 1) * kRuns] - ob;
+        // tile set-up: one thread per run (segment bounds and the element just before it)
+        if (tid < kRuns) {
+            const int j = tid;
+            const int p = find_segment(s_tile_off, L, t);
+            const int tl = t - s_tile_off[p];
+            const int ob = s_split_off[p * kRuns];
+            const int nsb = s_split_off[(p + 1) * kRuns] - ob;
             const int a = ob + tl * kMergeGroup;
             const int bidx = tl * kMergeGroup + kMergeGroup;
+            const int st = __ldcg(ws.ord_co + int64_t(a) * kRuns + j);
+            const int en = bidx < nsb ? __ldcg(ws.ord_co + int64_t(ob + bidx) * kRuns + j) : s_run_len[p * kRuns + j];
+            const int lo = s_run_lo[p * kRuns + j];
+            s_start[j] = st;
+            s_len[j] = en - st;
+            s_lo[j] = lo;
+            s_pv[j] = 0;
+            if (st > 0) {
+                Key<NW> k;
+                int f;
+                run_elem<NW>(m, X, p, j, int64_t(lo) + st - 1, k, f);
+                s_pk[j] = k;
+                s_pf[j] = f;
+                s_pv[j] = 1;
+            }
+            if (j == 0) {
+                s_p = p;
+                s_tl = tl;
+                s_ceil = 0;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
             int n = 0;
             for (int j = 0; j < kRuns; ++j) {
-                const int st = ws.ord_co[int64_t(a) * kRuns + j];
-                const int en = bidx < nsb ? ws.ord_co[int64_t(ob + bidx) * kRuns + j]
-                                          : ws.run_len[p * kRuns + j];
-                s_start[j] = st;
                 s_off[j] = n;
-                s_lo[j] = ws.run_lo[p * kRuns + j];
-                n += en - st;
+                n += s_len[j];
             }
             s_off[kRuns] = n;
             s_n = n;
-            s_p = p;
-            s_tl = tl;
-            s_ceil = 0;
             // merged predecessor of the tile: the largest element before the start of any run
             int has = 0, pf = 0, pj = -1;
-            Key<NW> pk;
             for (int j = 0; j < kRuns; ++j) {
-                if (s_start[j] == 0) continue;
-                Key<NW> k;
-                int f;
-                run_elem<NW>(m, X, p, j, int64_t(s_lo[j]) + s_start[j] - 1, k, f);
+                if (!s_pv[j]) continue;
                 bool larger = !has;
                 if (has) {
-                    const int c = cmp_kf(k, f, pk, pf);
+                    const int c = cmp_kf(s_pk[j], s_pf[j], s_pk[pj], pf);
                     larger = c > 0 || (c == 0 && j > pj);
                 }
                 if (larger) {
-                    pk = k;
-                    pf = f;
+                    pf = s_pf[j];
                     pj = j;
                     has = 1;
                 }
             }
             s_has_pred = has;
             if (has) {
-                s_pred = pk;
+                s_pred = s_pk[pj];
                 s_pred_flag = pf;
             }
             if (n > tmax) raise_status(status, PACES_ERR_CAPACITY);
@@ -304,7 +376,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             Key<NW> k;
             int f;
             run_elem<NW>(m, X, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
-            s_key[e] = k;
+            s_key.set(e, k);
             s_flag[e] = uint8_t(f);
             s_perm[e] = 0xffff;  // every rank must be claimed below
         }
@@ -315,7 +387,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             int j = 0;
 #pragma unroll
             for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
-            const Key<NW> k = s_key[e];
+            const Key<NW> k = s_key.get(e);
             const int f = s_flag[e];
             int r = e - s_off[j];
 #pragma unroll 1
@@ -323,8 +395,12 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                 if (jj == j) continue;
                 r += smem_bound<NW>(s_key, s_flag, s_off[jj], s_off[jj + 1] - s_off[jj], k, f, jj < j);
             }
-            if (r < n) s_perm[r] = uint16_t(e);
-            else raise_status(status, PACES_ERR_BADARG);
+            if (r < n) {
+                s_perm[r] = uint16_t(e);
+                s_rank[e] = uint16_t(r);
+            } else {
+                raise_status(status, PACES_ERR_BADARG);
+            }
         }
         __syncthreads();
 
@@ -340,10 +416,10 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                 raise_status(status, PACES_ERR_BADARG);
             } else if (s_flag[e] == 1) {
                 if (q == 0) {
-                    first = !s_has_pred || s_pred_flag != 1 || !key_eq(s_pred, s_key[e]);
+                    first = !s_has_pred || s_pred_flag != 1 || s_key.cmp(e, s_pred) != 0;
                 } else {
                     const int pe = s_perm[q - 1];
-                    first = pe >= n || s_flag[pe] != 1 || !key_eq(s_key[pe], s_key[e]);
+                    first = pe >= n || s_flag[pe] != 1 || !s_key.eq(pe, e);
                 }
             }
             s_first[q] = uint8_t(first);
@@ -367,52 +443,61 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                 acc += v;
             }
             s_total = acc;
-            s_base = lookback_prefix(ws.tile_state, t, acc, status);
-            if (s_tl == 0) out.blk[p] = s_base;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            const int b = lookback_warp(ws.tile_state, t, s_total, status);
+            if (lane == 0) {
+                s_base = b;
+                if (s_tl == 0) out.blk[p] = b;
+            }
         }
         __syncthreads();
         const int base = s_base;
-        int run = s_warp[wid] + incl - cnt;  // exclusive count of firsts before q0
+        {
+            // inclusive count of firsts at every merged position (for strided writes)
+            int run = s_warp[wid] + incl - cnt;
+            for (int q = q0; q < q1; ++q) {
+                run += s_first[q];
+                s_cnt[q] = uint16_t(run);
+            }
+        }
+        __syncthreads();
 
-        // 4. outputs
-        int ceil_local = 0;
-        for (int q = q0; q < q1; ++q) {
+        // 4a. new keys (and H rows), consecutive threads -> consecutive outputs
+        for (int q = tid; q < n; q += kTileThreads) {
+            if (!s_first[q]) continue;
             const int e = s_perm[q];
-            if (e >= n) continue;
-            int j = 0;
-#pragma unroll
-            for (int qq = 1; qq < kRuns; ++qq) j += (e >= s_off[qq]);
-            const int64_t src = int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]);
-            const int f = s_flag[e];
-            if (f != 1) {
+            const int64_t u = int64_t(base) + s_cnt[q] - 1;
+            if (u < out.cap) {
+                const Key<NW> k = s_key.get(e);
+                store_key<NW>(out.keys, u, k);
                 if constexpr (ASM) {
-                    if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = -1;
-                }
-                ceil_local += (f == 2);
-                continue;
-            }
-            const int first = s_first[q];
-            run += first;
-            const int64_t u = int64_t(base) + run - 1;
-            if (first) {
-                if (u < out.cap) {
-                    store_key<NW>(out.keys, u, s_key[e]);
-                    if constexpr (ASM) {
-                        const Key<NW> k = s_key[e];
-                        const uint32_t nex = get_field(m, k, p);
-                        const uint32_t ntot = total_phonons(m, k);
-                        if (u < out.nbr_cap) {
-                            out.meta[u] = uint32_t(p) | (nex << 8) | (ntot << 16);
+                    const uint32_t nex = get_field(m, k, p);
+                    const uint32_t ntot = total_phonons(m, k);
+                    if (u < out.nbr_cap) {
+                        out.meta[u] = uint32_t(p) | (nex << 8) | (ntot << 16);
 #pragma unroll
-                            for (int sl = 0; sl < 4; ++sl) out.nbr[int64_t(sl) * out.nbr_cap + u] = -1;
-                        }
+                        for (int sl = 0; sl < 4; ++sl) out.nbr[int64_t(sl) * out.nbr_cap + u] = -1;
                     }
-                } else {
-                    raise_status(status, PACES_ERR_CAPACITY);
                 }
+            } else {
+                raise_status(status, PACES_ERR_CAPACITY);
             }
-            if constexpr (ASM) {
-                if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = int(u);
+        }
+        // 4b. index maps in run order: consecutive threads -> consecutive source indices
+        int ceil_local = 0;
+        if constexpr (ASM) {
+            for (int e = tid; e < n; e += kTileThreads) {
+                int j = 0;
+#pragma unroll
+                for (int qq = 1; qq < kRuns; ++qq) j += (e >= s_off[qq]);
+                const int64_t src = int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]);
+                const int f = s_flag[e];
+                int u = -1;
+                if (f == 1) u = base + s_cnt[s_rank[e]] - 1;
+                ceil_local += (f == 2);
+                if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = u;
             }
         }
         if constexpr (ASM) {
@@ -496,7 +581,7 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
 template <int NW>
 size_t tile_smem_bytes() {
     const int tmax = merge_tmax(NW);
-    return size_t(tmax) * sizeof(Key<NW>) + 2 * size_t((tmax + 15) & ~15) + size_t(tmax) * 2;
+    return size_t(tmax) * sizeof(Key<NW>) + 2 * size_t((tmax + 15) & ~15) + size_t(tmax) * 6;
 }
 
 template <int NW>

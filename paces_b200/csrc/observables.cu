@@ -1,4 +1,4 @@
-// Norm, energy and per-site observables in one pass over the state.
+// Norm, energy and per-site observables.
 //
 // Reference: calculate_n_exc (paces/models/holstein.py:311-314, partitioned sum of
 // |psi|^2 by exciton position), calculate_n_pho (holstein.py:317-322 with the CUB
@@ -6,11 +6,14 @@
 // (paces/core/observables.py:95-99, <psi|H psi>) and the norms of
 // paces/core/time_evolution.py:587, :602, :818.
 //
-// B200 design: one grid-stride sweep reads psi, the row metadata and the keys once;
-// every warp broadcasts its 32 rows lane by lane and lane l accumulates the sites
-// l, l+32, l+64, l+96 in registers, so n_pho needs no atomics.  Per-block partials are
-// summed in a fixed order by a second tiny kernel: the result is deterministic, unlike
-// the reference's floating-point atomics.
+// B200 design: two streaming passes with one full wave of resident blocks each.
+//  * energy pass: norm and <psi|H psi> with the neighbour-table SpMV row (gathers);
+//  * site pass: norm, n_exc and n_pho from psi, the keys and the row metadata only.
+//    Rows are sorted by exciton position, so n_exc is a warp-segmented sum; for keys
+//    whose fields all have one width >= 4 bits every thread keeps all per-site sums of
+//    its rows in registers (no atomics, no shuffles per row).
+// Per-block partials are summed in a fixed order by a final kernel, one block per
+// output value: results are deterministic, unlike the reference's float atomics.
 #include "hrow.cuh"
 #include "kernels.cuh"
 
@@ -20,29 +23,86 @@ namespace {
 
 constexpr int kOThreads = 256;
 constexpr int kOWarps = kOThreads / 32;
+constexpr int kFpwMax = 16;  // register fast path: fields of >= 4 bits, at most 16 per word
 
-template <int NW, bool C64>
-__global__ void __launch_bounds__(kOThreads)
-obs_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict__ blk,
-           const int* __restrict__ nbr, int64_t cap, const uint32_t* __restrict__ meta,
-           const void* __restrict__ psi, int what, double* __restrict__ partials) {
+template <bool C64>
+__global__ void __launch_bounds__(kOThreads, 4)
+obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nbr, int64_t cap,
+                  const uint32_t* __restrict__ meta, const void* __restrict__ psi, double* __restrict__ part) {
     using C = typename std::conditional<C64, float2, double2>::type;
     using R = typename std::conditional<C64, float, double>::type;
     __shared__ R s_sq[260];
-    __shared__ double s_site[kOWarps][2 * kMaxSites];
     __shared__ double s_red[kOWarps][3];
-    const int L = m.L;
-    const int nvals = 3 + 2 * L;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int k = threadIdx.x; k < 260; k += kOThreads) s_sq[k] = R(__dmul_rn(sqrt(double(k)), m.g));
     __syncthreads();
-    const int64_t S = blk[L];
+    const int64_t S = blk[m.L];
     const C* x = reinterpret_cast<const C*>(psi);
     const R J = R(m.J);
-    const bool energy = (what & PACES_OBS_ENERGY) != 0;
-    const bool sites = (what & PACES_OBS_SITES) != 0;
     double norm2 = 0.0, er = 0.0, ei = 0.0;
+    for (int64_t r = int64_t(blockIdx.x) * kOThreads + threadIdx.x; r < S; r += int64_t(gridDim.x) * kOThreads) {
+        const C z = x[r];
+        const double zr = double(z.x), zi = double(z.y);
+        const uint32_t mm = __ldg(meta + r);
+        double yr, yi;
+        if constexpr (C64) {
+            const float2 y = h_row_c64(m, s_sq, J, r, nbr, cap, mm, x);
+            yr = y.x;
+            yi = y.y;
+        } else {
+            const double2 y = h_row_c128(m, s_sq, r, nbr, cap, mm, x);
+            yr = y.x;
+            yi = y.y;
+        }
+        norm2 += zr * zr + zi * zi;
+        er += zr * yr + zi * yi;
+        ei += zr * yi - zi * yr;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        norm2 += __shfl_xor_sync(0xffffffffu, norm2, o);
+        er += __shfl_xor_sync(0xffffffffu, er, o);
+        ei += __shfl_xor_sync(0xffffffffu, ei, o);
+    }
+    if (lane == 0) {
+        s_red[wid][0] = norm2;
+        s_red[wid][1] = er;
+        s_red[wid][2] = ei;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double acc = 0.0;
+        for (int w = 0; w < kOWarps; ++w) acc += s_red[w][threadIdx.x];
+        part[size_t(blockIdx.x) * 3 + threadIdx.x] = acc;
+    }
+}
+
+// `uniform`: every field is `ub` bits wide and word q holds sites q*fpw .. q*fpw+fpw-1
+// MSB-first (NW <= 4), so thread-private register accumulators cover all sites.
+template <int NW, bool C64>
+__global__ void __launch_bounds__(kOThreads)
+obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict__ blk,
+                 const uint32_t* __restrict__ meta, const void* __restrict__ psi, double* __restrict__ part,
+                 int uniform_in, int ub, int fpw) {
+    using C = typename std::conditional<C64, float2, double2>::type;
+    constexpr bool kFast = NW <= 4;
+    constexpr int kAcc = kFast ? NW * kFpwMax : 1;
+    __shared__ double s_site[kOWarps][2 * kMaxSites];
+    __shared__ double s_red[kOWarps];
+    const int L = m.L;
+    const int nv = 1 + 2 * L;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const bool uniform = kFast && uniform_in;
+    const uint64_t umask = (uint64_t(1) << ub) - 1;
+    double racc[kAcc];
+#pragma unroll
+    for (int i = 0; i < kAcc; ++i) racc[i] = 0.0;
     double pho[4] = {0.0, 0.0, 0.0, 0.0}, exc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = threadIdx.x; k < kOWarps * 2 * kMaxSites; k += kOThreads) (&s_site[0][0])[k] = 0.0;
+    __syncthreads();
+    const int64_t S = blk[L];
+    const C* x = reinterpret_cast<const C*>(psi);
+    double norm2 = 0.0;
     for (int64_t base = (int64_t(blockIdx.x) * kOWarps + wid) * 32; base < S;
          base += int64_t(gridDim.x) * kOWarps * 32) {
         const int64_t r = base + lane;
@@ -56,25 +116,37 @@ obs_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict_
             const C z = x[r];
             const double zr = double(z.x), zi = double(z.y);
             w = zr * zr + zi * zi;
-            mm = meta[r];
-            if (energy) {
-                double yr, yi;
-                if constexpr (C64) {
-                    const float2 y = h_row_c64(m, s_sq, J, r, nbr, cap, mm, x);
-                    yr = y.x;
-                    yi = y.y;
-                } else {
-                    const double2 y = h_row_c128(m, s_sq, r, nbr, cap, mm, x);
-                    yr = y.x;
-                    yi = y.y;
-                }
-                er += zr * yr + zi * yi;
-                ei += zr * yi - zi * yr;
-            }
-            if (sites) k = load_key<NW>(keys, r);
+            mm = __ldg(meta + r);
+            k = load_key<NW>(keys, r);
         }
         norm2 += w;
-        if (sites) {
+        if (uniform) {
+            // n_exc: a warp spans one or two exciton blocks
+            const int pme = int(mm & 0xffu);
+            const int p0 = __shfl_sync(0xffffffffu, pme, 0);
+            const int vlast = __shfl_sync(0xffffffffu, valid ? pme : -1, 31);
+            const int p1 = vlast < 0 ? L - 1 : vlast;
+            for (int pp = p0; pp <= p1; ++pp) {
+                double v = (valid && pme == pp) ? w : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) s_site[wid][pp] += v;
+            }
+            if (valid && w != 0.0) {
+#pragma unroll
+                for (int q = 0; q < NW; ++q) {
+                    const uint64_t word = k.w[q];
+#pragma unroll
+                    for (int f = 0; f < kFpwMax; ++f) {
+                        if (f < fpw) {
+                            const uint32_t nf = uint32_t((word >> (64 - ub * (f + 1))) & umask);
+                            racc[q * kFpwMax + f] += w * double(nf);
+                        }
+                    }
+                }
+            }
+        } else {
+            // general layout: broadcast each row; lane l owns sites l, l+32, l+64, l+96
             unsigned act = __ballot_sync(0xffffffffu, valid && w != 0.0);
             while (act) {
                 const int src = __ffs(act) - 1;
@@ -95,19 +167,20 @@ obs_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict_
             }
         }
     }
-    // block partials, fixed order
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        norm2 += __shfl_xor_sync(0xffffffffu, norm2, o);
-        er += __shfl_xor_sync(0xffffffffu, er, o);
-        ei += __shfl_xor_sync(0xffffffffu, ei, o);
-    }
-    if (lane == 0) {
-        s_red[wid][0] = norm2;
-        s_red[wid][1] = er;
-        s_red[wid][2] = ei;
-    }
-    if (sites) {
+    for (int o = 16; o > 0; o >>= 1) norm2 += __shfl_xor_sync(0xffffffffu, norm2, o);
+    if (lane == 0) s_red[wid] = norm2;
+    if (uniform) {
+#pragma unroll
+        for (int i = 0; i < kAcc; ++i) {
+            double v = racc[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            const int q = i / kFpwMax, f = i % kFpwMax;
+            const int s = q * fpw + f;
+            if (lane == 0 && f < fpw && s < L) s_site[wid][L + s] = v;
+        }
+    } else {
 #pragma unroll
         for (int qi = 0; qi < 4; ++qi) {
             const int s = lane + 32 * qi;
@@ -118,34 +191,49 @@ obs_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict_
         }
     }
     __syncthreads();
-    double* out = partials + size_t(blockIdx.x) * nvals;
-    for (int v = threadIdx.x; v < nvals; v += kOThreads) {
+    double* out = part + size_t(blockIdx.x) * nv;
+    for (int v = threadIdx.x; v < nv; v += kOThreads) {
         double acc = 0.0;
-        if (v < 3) {
-            for (int w2 = 0; w2 < kOWarps; ++w2) acc += s_red[w2][v];
-        } else if (sites) {
-            for (int w2 = 0; w2 < kOWarps; ++w2) acc += s_site[w2][v - 3];
+        if (v == 0) {
+            for (int w2 = 0; w2 < kOWarps; ++w2) acc += s_red[w2];
+        } else {
+            for (int w2 = 0; w2 < kOWarps; ++w2) acc += s_site[w2][v - 1];
         }
         out[v] = acc;
     }
 }
 
-__global__ void obs_final_kernel(int L, int nblocks, const double* __restrict__ partials, ObsTarget t) {
-    const int nvals = 3 + 2 * L;
-    for (int v = threadIdx.x; v < nvals; v += blockDim.x) {
-        double acc = 0.0;
-        for (int b = 0; b < nblocks; ++b) acc += partials[size_t(b) * nvals + v];
-        if (v == 0) {
-            if (t.norm) *t.norm = sqrt(acc);
-        } else if (v == 1) {
-            if (t.energy_re) *t.energy_re = acc;
-        } else if (v == 2) {
-            if (t.energy_im) *t.energy_im = acc;
-        } else if (v < 3 + L) {
-            if (t.n_exc) t.n_exc[v - 3] = acc;
-        } else {
-            if (t.n_pho) t.n_pho[v - 3 - L] = acc;
-        }
+// One block per output value: strided partial sums then a fixed-shape tree (deterministic).
+// v = 0 norm, 1-2 energy (energy pass), 3.. n_exc and n_pho (site pass).
+__global__ void __launch_bounds__(256) obs_final_kernel(int L, int nb_e, const double* __restrict__ part_e,
+                                                        int nb_s, const double* __restrict__ part_s,
+                                                        ObsTarget t) {
+    __shared__ double s_w[8];
+    const int v = blockIdx.x;
+    const bool from_e = v < 3 && nb_e > 0;
+    const int stride = from_e ? 3 : 1 + 2 * L;
+    const int col = from_e ? v : (v == 0 ? 0 : v - 2);
+    const int nb = from_e ? nb_e : nb_s;
+    const double* part = from_e ? part_e : part_s;
+    double acc_t = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc_t += part[size_t(b) * stride + col];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc_t += __shfl_xor_sync(0xffffffffu, acc_t, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc_t;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double acc = 0.0;
+    for (int w = 0; w < 8; ++w) acc += s_w[w];
+    if (v == 0) {
+        if (t.norm) *t.norm = sqrt(acc);
+    } else if (v == 1) {
+        if (t.energy_re) *t.energy_re = acc;
+    } else if (v == 2) {
+        if (t.energy_im) *t.energy_im = acc;
+    } else if (v < 3 + L) {
+        if (t.n_exc) t.n_exc[v - 3] = acc;
+    } else {
+        if (t.n_pho) t.n_pho[v - 3 - L] = acc;
     }
 }
 
@@ -168,13 +256,43 @@ __global__ void scale_kernel(int L, const int* __restrict__ blk, void* psi, cons
     }
 }
 
+template <typename K>
+int wave_blocks(K kernel, int num_sms) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kOThreads, 0);
+    per_sm = per_sm < 1 ? 1 : (per_sm > kObsGridPerSm ? kObsGridPerSm : per_sm);
+    return num_sms * per_sm;
+}
+
 template <int NW, bool C64>
 int launch_obs_t(const ModelDev& m, const uint64_t* keys, const int* blk, const int* nbr,
                  int64_t nbr_cap, const uint32_t* meta, const void* psi, int what, double* partials,
                  const ObsTarget& out, int num_sms, cudaStream_t st) {
-    const int grid = obs_max_grid(num_sms);
-    obs_kernel<NW, C64><<<grid, kOThreads, 0, st>>>(m, keys, blk, nbr, nbr_cap, meta, psi, what, partials);
-    obs_final_kernel<<<1, 256, 0, st>>>(m.L, grid, partials, out);
+    static int grid_e = 0, grid_s = 0;
+    if (grid_e == 0) {
+        grid_e = wave_blocks(obs_energy_kernel<C64>, num_sms);
+        grid_s = wave_blocks(obs_sites_kernel<NW, C64>, num_sms);
+    }
+    const bool energy = (what & PACES_OBS_ENERGY) != 0;
+    const bool sites = (what & PACES_OBS_SITES) != 0;
+    double* part_e = partials;
+    double* part_s = partials + size_t(obs_max_grid(num_sms)) * 3;
+    int nb_e = 0, nb_s = 0;
+    if (energy || !sites) {
+        obs_energy_kernel<C64><<<grid_e, kOThreads, 0, st>>>(m, blk, nbr, nbr_cap, meta, psi, part_e);
+        nb_e = grid_e;
+    }
+    if (sites) {
+        int ub = m.bits[0];
+        const int fpw = ub > 0 ? 64 / ub : 0;
+        bool uniform = ub >= 4 && NW <= 4;
+        for (int s = 0; s < m.L && uniform; ++s)
+            uniform = m.bits[s] == ub && m.word[s] == s / fpw && m.shift[s] == 64 - ub * (s % fpw + 1);
+        obs_sites_kernel<NW, C64><<<grid_s, kOThreads, 0, st>>>(m, keys, blk, meta, psi, part_s, uniform ? 1 : 0,
+                                                               ub, fpw);
+        nb_s = grid_s;
+    }
+    obs_final_kernel<<<sites ? 3 + 2 * m.L : 3, 256, 0, st>>>(m.L, nb_e, part_e, nb_s, part_s, out);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 

@@ -6,10 +6,11 @@
 // back).
 //
 // B200 design: both bases are sorted and blocked by exciton position, so the lookup is
-// a merge-path sorted search per block: tiles of 2048 merged (old + new) elements,
-// split by a diagonal binary search, the tile's old keys staged in shared memory, and
-// each new key resolved by a shared-memory upper bound (old before new on equal keys;
-// a match is the old element just before the new one).
+// a merge-path sorted search per block.  A first kernel splits every block's merged
+// (old + new) sequence into tiles along diagonals, one thread per diagonal; the tile
+// kernel stages the tile's old keys in shared memory and resolves each new key by a
+// shared-memory upper bound (old before new on equal keys; a match is the old element
+// just before the new one).
 #include "kernels.cuh"
 
 namespace paces {
@@ -46,6 +47,24 @@ __global__ void remap_plan_kernel(ModelDev m, const int* __restrict__ ob, const 
     ws.counters[0] = acc;
 }
 
+// split[2t] / split[2t+1]: old elements before the tile's first / past its last diagonal.
+template <int NW>
+__global__ void __launch_bounds__(256) remap_split_kernel(ModelDev m, const uint64_t* __restrict__ old_keys,
+                                                          const int* __restrict__ ob,
+                                                          const uint64_t* __restrict__ new_keys,
+                                                          const int* __restrict__ nb, RemapWs ws, int tile) {
+    const int ntiles = ws.counters[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * ntiles; i += gridDim.x * blockDim.x) {
+        const int t = i >> 1;
+        const int p = find_segment(ws.tile_off, m.L, t);
+        const int tl = t - ws.tile_off[p];
+        const int o0 = ob[p], no = ob[p + 1] - o0;
+        const int n0 = nb[p], nn = nb[p + 1] - n0;
+        const int d = (i & 1) ? min((tl + 1) * tile, no + nn) : tl * tile;
+        ws.split[i] = merge_path<NW>(old_keys + int64_t(o0) * NW, no, new_keys + int64_t(n0) * NW, nn, d);
+    }
+}
+
 template <int NW, bool C64>
 __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint64_t* __restrict__ old_keys,
                                                          const int* __restrict__ ob,
@@ -56,7 +75,6 @@ __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint6
     using C = typename std::conditional<C64, float2, double2>::type;
     constexpr int kTile = remap_tile(NW);
     __shared__ Key<NW> s_old[kTile + 1];
-    __shared__ int s_a[2];
     const int ntiles = ws.counters[0];
     const C* op = reinterpret_cast<const C*>(old_psi);
     C* np = reinterpret_cast<C*>(new_psi);
@@ -68,9 +86,7 @@ __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint6
         const uint64_t* O = old_keys + int64_t(o0) * NW;
         const uint64_t* N = new_keys + int64_t(n0) * NW;
         const int d0 = tl * kTile, d1 = min(d0 + kTile, no + nn);
-        if (threadIdx.x < 2) s_a[threadIdx.x] = merge_path<NW>(O, no, N, nn, threadIdx.x == 0 ? d0 : d1);
-        __syncthreads();
-        const int a0 = s_a[0], a1 = s_a[1];
+        const int a0 = ws.split[2 * t], a1 = ws.split[2 * t + 1];
         const int h = a0 > 0 ? 1 : 0;  // halo: the old element before the tile
         for (int e = threadIdx.x; e < a1 - a0 + h; e += blockDim.x) s_old[e] = load_key<NW>(O, a0 - h + e);
         __syncthreads();
@@ -99,6 +115,7 @@ int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const v
                    const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws, int* status,
                    int num_sms, cudaStream_t st) {
     remap_plan_kernel<<<1, 32, 0, st>>>(m, ob, nb, ws, remap_tile(NW), status);
+    remap_split_kernel<NW><<<num_sms * 2, 256, 0, st>>>(m, ok, ob, nk, nb, ws, remap_tile(NW));
     remap_tile_kernel<NW, C64><<<num_sms * 4, 256, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi, ws);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }

@@ -70,7 +70,7 @@ __device__ void block_max4(double v[4], double (*red)[kTWarps], double* out) {
 }
 
 template <bool C64>
-__global__ void __launch_bounds__(kTThreads)
+__global__ void __launch_bounds__(kTThreads, 4)
 taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nbr, int64_t cap,
               const uint32_t* __restrict__ meta, const void* v_in, void* res_out, TaylorWs ws,
               double dt, int m_star, double tol, TaylorOut out, int* status) {
@@ -109,16 +109,16 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                 const float2 y = h_row_c64(m, s_sq, J, r, nbr, cap, mm, src);
                 t = make_float2(c * y.y, -(c * y.x));
                 rr = make_float2(a.x + t.x, a.y + t.y);
-                mx[0] = fmax(mx[0], double(hypotf(t.x, t.y)));
-                mx[1] = fmax(mx[1], double(hypotf(rr.x, rr.y)));
-                if (j == 0) mx[2] = fmax(mx[2], double(hypotf(a.x, a.y)));
+                mx[0] = fmax(mx[0], double(fmaf(t.x, t.x, t.y * t.y)));
+                mx[1] = fmax(mx[1], double(fmaf(rr.x, rr.x, rr.y * rr.y)));
+                if (j == 0) mx[2] = fmax(mx[2], double(fmaf(a.x, a.x, a.y * a.y)));
             } else {
                 const double2 y = h_row_c128(m, s_sq, r, nbr, cap, mm, src);
                 t = make_double2(__dmul_rn(cd, y.y), -__dmul_rn(cd, y.x));
                 rr = make_double2(__dadd_rn(a.x, t.x), __dadd_rn(a.y, t.y));
-                mx[0] = fmax(mx[0], hypot(t.x, t.y));
-                mx[1] = fmax(mx[1], hypot(rr.x, rr.y));
-                if (j == 0) mx[2] = fmax(mx[2], hypot(a.x, a.y));
+                mx[0] = fmax(mx[0], fma(t.x, t.x, t.y * t.y));
+                mx[1] = fmax(mx[1], fma(rr.x, rr.x, rr.y * rr.y));
+                if (j == 0) mx[2] = fmax(mx[2], fma(a.x, a.x, a.y * a.y));
             }
             if (!(isfinite(double(rr.x)) && isfinite(double(rr.y)))) mx[3] = 1.0;
             dst[r] = t;
@@ -148,10 +148,11 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
             if (blockIdx.x == 0 && threadIdx.x == 0) raise_status(status, PACES_ERR_NONFINITE);
             break;
         }
-        if (j == 0) c1 = s_fin[2];
-        const double c2 = s_fin[0];
+        // the maxima are of |z|^2; one square root per term gives the inf-norms
+        if (j == 0) c1 = sqrt(s_fin[2]);
+        const double c2 = sqrt(s_fin[0]);
         c1c2 = c1 + c2;
-        ratio = c1c2 / s_fin[1];
+        ratio = c1c2 / sqrt(s_fin[1]);
         if (ratio <= tol) {
             conv = 1;
             break;

@@ -260,6 +260,18 @@ class Engine:
             return None
         return self.read_record()
 
+    def set_profiling(self, on=True):
+        nat.check(self.lib.paces_set_profiling(self.ctx, 1 if on else 0), self.ctx, "set_profiling")
+
+    def stage_times(self):
+        """Per-stage device milliseconds of the last profiled step."""
+        ms = (ctypes.c_float * 7)()
+        nat.check(self.lib.paces_stage_times(self.ctx, ms), self.ctx, "stage_times")
+        return dict(zip(nat.STAGES, [float(x) for x in ms]))
+
+    def kernel_launches(self):
+        return int(self.lib.paces_kernel_launches(self.ctx))
+
     def read_record(self) -> nat.StepRecord:
         self.rec_host.copy_(self.rec_dev, non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
