@@ -95,8 +95,8 @@ typedef struct paces_basis {
     int64_t cap;    /* capacity in states */
 } paces_basis;
 
-/* H on a basis: neighbour table + per-row metadata.  nbr[k*cap + r] is the row index of
- * the k-th neighbour of row r (k: 0 = exciton one site left, 1 = right, 2 = one phonon
+/* H on a basis: neighbour table + per-row metadata.  nbr[4*r + k] (16 bytes per row) is the
+ * row index of the k-th neighbour of row r (k: 0 = exciton one site left, 1 = right, 2 = one phonon
  * less at the exciton site, 3 = one phonon more), or -1 when that coupling is absent from
  * the reference's H (both rows outside the enlarged basis, or a boundary/ceiling/floor).
  * meta[r] = pos | n_exc << 8 | n_total << 16, from which the diagonal element is

@@ -1,4 +1,5 @@
-// One row of H applied to a vector, from the neighbour table and the row metadata.
+// One row of H applied to a vector, from the neighbour table (one int4 per row: left,
+// right, one phonon less, one phonon more; -1 = absent) and the row metadata.
 //
 // Reference: total_ham (paces/core/time_evolution.py:382-400) computes
 //   diag * v + hopping_csr.dot(v) + vib_coupling_csr.dot(v)
@@ -7,6 +8,11 @@
 // holstein.py:271-274).  The complex128 form below keeps exactly that grouping and
 // rounds every product and sum separately (no fused multiply-add), so it reproduces
 // the reference arithmetic row by row.
+//
+// The rows are branch-free: every neighbour load is issued (an absent neighbour re-reads
+// the row's own element, already in flight, and its term is discarded by a select), so
+// the five loads of a row -- and of several rows handled by one thread -- are in flight
+// together without funnelling the absent ones onto one hot cache line.
 #pragma once
 
 #include "common.cuh"
@@ -23,85 +29,64 @@ __device__ __forceinline__ double diag_value(const ModelDev& m, uint32_t meta) {
     return d;
 }
 
+__device__ __forceinline__ int4 load_nbr(const int* __restrict__ nbr, int64_t r) {
+    return __ldg(reinterpret_cast<const int4*>(nbr) + r);
+}
+
 // y = (H x)[r] in complex128.  sq[k] = sqrt(k) * g.
 __device__ __forceinline__ double2 h_row_c128(const ModelDev& m, const double* sq, int64_t r,
-                                              const int* __restrict__ nbr, int64_t cap, uint32_t meta,
+                                              const int* __restrict__ nbr, uint32_t meta,
                                               const double2* __restrict__ x) {
     const int n = int((meta >> 8) & 0xffu);
-    const double d = diag_value(m, meta);
+    const int4 nb = load_nbr(nbr, r);
+    // hopping columns in increasing order (a <= b), as the CSR row sum visits them
+    const bool swap = nb.y >= 0 && (nb.x < 0 || nb.y < nb.x);
+    const int a = swap ? nb.y : nb.x, b = swap ? nb.x : nb.y;
+    const bool ha = a >= 0, hb = b >= 0, hd = nb.z >= 0, hu = nb.w >= 0;
     const double2 xr = __ldcg(x + r);
+    const double2 xa = __ldcg(x + (ha ? a : r));
+    const double2 xb = __ldcg(x + (hb ? b : r));
+    const double2 xd = __ldcg(x + (hd ? nb.z : r));
+    const double2 xu = __ldcg(x + (hu ? nb.w : r));
+    const double d = diag_value(m, meta);
     double2 y = make_double2(__dmul_rn(d, xr.x), __dmul_rn(d, xr.y));
-    int a = __ldg(nbr + r), b = __ldg(nbr + cap + r);
-    const int nd = __ldg(nbr + 2 * cap + r), nu = __ldg(nbr + 3 * cap + r);
-    if (a >= 0 || b >= 0) {
-        if (a < 0 || (b >= 0 && b < a)) {
-            const int tmp = a;
-            a = b;
-            b = tmp;
-        }
-        const double2 xa = __ldcg(x + a);
-        double2 h = make_double2(__dmul_rn(m.J, xa.x), __dmul_rn(m.J, xa.y));
-        if (b >= 0) {
-            const double2 xb = __ldcg(x + b);
-            h.x = __dadd_rn(h.x, __dmul_rn(m.J, xb.x));
-            h.y = __dadd_rn(h.y, __dmul_rn(m.J, xb.y));
-        }
-        y.x = __dadd_rn(y.x, h.x);
-        y.y = __dadd_rn(y.y, h.y);
-    }
-    if (nd >= 0 || nu >= 0) {
-        double2 v;
-        if (nd >= 0) {
-            const double c = sq[n];
-            const double2 xd = __ldcg(x + nd);
-            v = make_double2(__dmul_rn(c, xd.x), __dmul_rn(c, xd.y));
-            if (nu >= 0) {
-                const double c2 = sq[n + 1];
-                const double2 xu = __ldcg(x + nu);
-                v.x = __dadd_rn(v.x, __dmul_rn(c2, xu.x));
-                v.y = __dadd_rn(v.y, __dmul_rn(c2, xu.y));
-            }
-        } else {
-            const double c2 = sq[n + 1];
-            const double2 xu = __ldcg(x + nu);
-            v = make_double2(__dmul_rn(c2, xu.x), __dmul_rn(c2, xu.y));
-        }
-        y.x = __dadd_rn(y.x, v.x);
-        y.y = __dadd_rn(y.y, v.y);
-    }
+    // hopping: (J xa) + (J xb), terms present only
+    const double2 pa = make_double2(__dmul_rn(m.J, xa.x), __dmul_rn(m.J, xa.y));
+    const double2 pb = make_double2(__dmul_rn(m.J, xb.x), __dmul_rn(m.J, xb.y));
+    const double2 hs = (ha && hb) ? make_double2(__dadd_rn(pa.x, pb.x), __dadd_rn(pa.y, pb.y)) : (ha ? pa : pb);
+    if (ha || hb) y = make_double2(__dadd_rn(y.x, hs.x), __dadd_rn(y.y, hs.y));
+    // vibronic: (g sqrt(n) xd) + (g sqrt(n+1) xu); one phonon less sorts first
+    const double cd = sq[n], cu = sq[n + 1];
+    const double2 pd = make_double2(__dmul_rn(cd, xd.x), __dmul_rn(cd, xd.y));
+    const double2 pu = make_double2(__dmul_rn(cu, xu.x), __dmul_rn(cu, xu.y));
+    const double2 vs = (hd && hu) ? make_double2(__dadd_rn(pd.x, pu.x), __dadd_rn(pd.y, pu.y)) : (hd ? pd : pu);
+    if (hd || hu) y = make_double2(__dadd_rn(y.x, vs.x), __dadd_rn(y.y, vs.y));
     return y;
 }
 
 // y = (H x)[r] in complex64 with fp32 accumulation.  sq[k] = float(sqrt(k) * g).
 __device__ __forceinline__ float2 h_row_c64(const ModelDev& m, const float* sq, float J, int64_t r,
-                                            const int* __restrict__ nbr, int64_t cap, uint32_t meta,
+                                            const int* __restrict__ nbr, uint32_t meta,
                                             const float2* __restrict__ x) {
     const int n = int((meta >> 8) & 0xffu);
-    const float d = float(diag_value(m, meta));
+    const int4 nb = load_nbr(nbr, r);
     const float2 xr = __ldcg(x + r);
+    const float2 xa = __ldcg(x + (nb.x >= 0 ? nb.x : r));
+    const float2 xb = __ldcg(x + (nb.y >= 0 ? nb.y : r));
+    const float2 xd = __ldcg(x + (nb.z >= 0 ? nb.z : r));
+    const float2 xu = __ldcg(x + (nb.w >= 0 ? nb.w : r));
+    const float d = float(diag_value(m, meta));
+    const float ja = nb.x >= 0 ? J : 0.f, jb = nb.y >= 0 ? J : 0.f;
+    const float cd = nb.z >= 0 ? sq[n] : 0.f, cu = nb.w >= 0 ? sq[n + 1] : 0.f;
     float2 y = make_float2(d * xr.x, d * xr.y);
-    const int a = __ldg(nbr + r), b = __ldg(nbr + cap + r);
-    const int nd = __ldg(nbr + 2 * cap + r), nu = __ldg(nbr + 3 * cap + r);
-    if (a >= 0) {
-        const float2 v = __ldcg(x + a);
-        y.x = fmaf(J, v.x, y.x);
-        y.y = fmaf(J, v.y, y.y);
-    }
-    if (b >= 0) {
-        const float2 v = __ldcg(x + b);
-        y.x = fmaf(J, v.x, y.x);
-        y.y = fmaf(J, v.y, y.y);
-    }
-    if (nd >= 0) {
-        const float2 v = __ldcg(x + nd);
-        y.x = fmaf(sq[n], v.x, y.x);
-        y.y = fmaf(sq[n], v.y, y.y);
-    }
-    if (nu >= 0) {
-        const float2 v = __ldcg(x + nu);
-        y.x = fmaf(sq[n + 1], v.x, y.x);
-        y.y = fmaf(sq[n + 1], v.y, y.y);
-    }
+    y.x = fmaf(ja, xa.x, y.x);
+    y.y = fmaf(ja, xa.y, y.y);
+    y.x = fmaf(jb, xb.x, y.x);
+    y.y = fmaf(jb, xb.y, y.y);
+    y.x = fmaf(cd, xd.x, y.x);
+    y.y = fmaf(cd, xd.y, y.y);
+    y.x = fmaf(cu, xu.x, y.x);
+    y.y = fmaf(cu, xu.y, y.y);
     return y;
 }
 

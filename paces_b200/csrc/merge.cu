@@ -110,17 +110,40 @@ struct SKeys {
     }
 };
 
+// (key, flag) of tile element x strictly below that of element y.
 template <int NW>
-__device__ __forceinline__ int smem_bound(const SKeys<NW>& keys, const uint8_t* flags, int off, int len,
-                                          const Key<NW>& key, int flag, bool upper) {
-    int a = 0, b = len;
-    while (a < b) {
-        const int mid = (a + b) >> 1;
-        int c = keys.cmp(off + mid, key);
-        if (c == 0) c = int(flags[off + mid]) - flag;
-        if (upper ? (c <= 0) : (c < 0)) a = mid + 1; else b = mid;
+__device__ __forceinline__ bool tile_less(const SKeys<NW>& keys, const uint8_t* flags, int x, int y) {
+#pragma unroll
+    for (int q = 0; q < NW; ++q) {
+        const uint64_t a = keys.w[q * keys.stride + x], b = keys.w[q * keys.stride + y];
+        if (a != b) return a < b;
     }
-    return a;
+    return flags[x] < flags[y];
+}
+
+// Output positions [d0, d1) of the merge of two sorted sequences of tile elements, A
+// (na elements, A(i) = element index) and B; an element of A precedes an equal element of
+// B (A always holds the lower run indices).  Merge-path split, then a sequential merge.
+template <int NW, typename FA, typename FB>
+__device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t* flags, FA A, int na, FB B,
+                                            int nb, int d0, int d1, uint16_t* out) {
+    int lo = max(0, d0 - nb), hi = min(d0, na);
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (!tile_less<NW>(keys, flags, B(d0 - 1 - mid), A(mid))) lo = mid + 1; else hi = mid;
+    }
+    int i = lo, j = d0 - lo;
+    int ea = i < na ? A(i) : 0, eb = j < nb ? B(j) : 0;
+    for (int d = d0; d < d1; ++d) {
+        const bool take_a = j >= nb || (i < na && !tile_less<NW>(keys, flags, eb, ea));
+        if (take_a) {
+            out[d] = uint16_t(ea);
+            if (++i < na) ea = A(i);
+        } else {
+            out[d] = uint16_t(eb);
+            if (++j < nb) eb = B(j);
+        }
+    }
 }
 
 __global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, MergeWs ws, int stride,
@@ -268,8 +291,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
     extern __shared__ __align__(16) unsigned char smem[];
     const SKeys<NW> s_key{reinterpret_cast<uint64_t*>(smem), tmax};
     uint8_t* s_flag = smem + size_t(tmax) * NW * 8;
-    uint8_t* s_first = s_flag + tmax;
-    uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_first + ((tmax + 15) & ~15));  // merged pos -> element
+    uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_flag + ((tmax + 15) & ~15));  // merged pos -> element
     uint16_t* s_rank = s_perm + tmax;                                                // element -> merged pos
     uint16_t* s_cnt = s_rank + tmax;  // inclusive count of first occurrences per merged pos
 
@@ -281,21 +303,11 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
     __shared__ int s_ceil;
 
     const int tid = threadIdx.x;
-    __shared__ int s_tile_off[kMaxSites + 1];
-    __shared__ int s_split_off[kMaxSites * kRuns + 1];
-    __shared__ int s_run_lo[kMaxSites * kRuns];
-    __shared__ int s_run_len[kMaxSites * kRuns];
     __shared__ Key<NW> s_pk[kRuns];
     __shared__ int s_pf[kRuns], s_pv[kRuns], s_len[kRuns];
 
     const int L = m.L;
     const int ntiles = ws.counters[1];
-    for (int i = tid; i <= L; i += kTileThreads) s_tile_off[i] = ws.tile_off[i];
-    for (int i = tid; i <= L * kRuns; i += kTileThreads) s_split_off[i] = ws.split_off[i];
-    for (int i = tid; i < L * kRuns; i += kTileThreads) {
-        s_run_lo[i] = ws.run_lo[i];
-        s_run_len[i] = ws.run_len[i];
-    }
 
     for (;;) {
         if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
@@ -306,15 +318,16 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
         // tile set-up: one thread per run (segment bounds and the element just before it)
         if (tid < kRuns) {
             const int j = tid;
-            const int p = find_segment(s_tile_off, L, t);
-            const int tl = t - s_tile_off[p];
-            const int ob = s_split_off[p * kRuns];
-            const int nsb = s_split_off[(p + 1) * kRuns] - ob;
+            const int p = find_segment(ws.tile_off, L, t);
+            const int tl = t - __ldg(ws.tile_off + p);
+            const int ob = __ldg(ws.split_off + p * kRuns);
+            const int nsb = __ldg(ws.split_off + (p + 1) * kRuns) - ob;
             const int a = ob + tl * kMergeGroup;
             const int bidx = tl * kMergeGroup + kMergeGroup;
             const int st = __ldcg(ws.ord_co + int64_t(a) * kRuns + j);
-            const int en = bidx < nsb ? __ldcg(ws.ord_co + int64_t(ob + bidx) * kRuns + j) : s_run_len[p * kRuns + j];
-            const int lo = s_run_lo[p * kRuns + j];
+            const int en = bidx < nsb ? __ldcg(ws.ord_co + int64_t(ob + bidx) * kRuns + j)
+                                      : __ldg(ws.run_len + p * kRuns + j);
+            const int lo = __ldg(ws.run_lo + p * kRuns + j);
             s_start[j] = st;
             s_len[j] = en - st;
             s_lo[j] = lo;
@@ -362,7 +375,13 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                 s_pred = s_pk[pj];
                 s_pred_flag = pf;
             }
-            if (n > tmax) raise_status(status, PACES_ERR_CAPACITY);
+            if (n > tmax) {
+                // cannot happen for sorted runs (see merge_tmax); flag it and emit nothing
+                raise_status(status, PACES_ERR_CAPACITY);
+                for (int j = 0; j <= kRuns; ++j) s_off[j] = 0;
+                s_n = 0;
+                s_has_pred = 0;
+            }
         }
         __syncthreads();
         const int n = min(s_n, tmax);
@@ -382,24 +401,37 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
         }
         __syncthreads();
 
-        // 2. merged rank of every element
-        for (int e = tid; e < n; e += kTileThreads) {
-            int j = 0;
-#pragma unroll
-            for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
-            const Key<NW> k = s_key.get(e);
-            const int f = s_flag[e];
-            int r = e - s_off[j];
-#pragma unroll 1
-            for (int jj = 0; jj < kRuns; ++jj) {
-                if (jj == j) continue;
-                r += smem_bound<NW>(s_key, s_flag, s_off[jj], s_off[jj + 1] - s_off[jj], k, f, jj < j);
-            }
-            if (r < n) {
-                s_perm[r] = uint16_t(e);
-                s_rank[e] = uint16_t(r);
-            } else {
-                raise_status(status, PACES_ERR_BADARG);
+        // 2. merged order: pairwise merge tree (runs 0+1, 2+3) -> (0123) -> (01234) in shared
+        //    memory; every thread merges a contiguous output range after a merge-path split.
+        //    The level buffers alias s_rank / s_cnt, which are filled only afterwards.
+        {
+            uint16_t* lv1 = s_rank;
+            uint16_t* lv2 = s_cnt;
+            const int o1 = s_off[1], o2 = s_off[2], o3 = s_off[3], o4 = s_off[4];
+            const int n01 = o2, n0123 = o4;
+            auto ident = [](int base) { return [base](int i) { return base + i; }; };
+            auto arr = [](const uint16_t* a) { return [a](int i) { return int(a[i]); }; };
+            int per = (n0123 + kTileThreads - 1) / kTileThreads;
+            int d0 = min(tid * per, n0123), d1 = min(d0 + per, n0123);
+            if (d0 < n01)
+                merge_range<NW>(s_key, s_flag, ident(0), o1, ident(o1), o2 - o1, d0, min(d1, n01), lv1);
+            if (d1 > n01)
+                merge_range<NW>(s_key, s_flag, ident(o2), o3 - o2, ident(o3), o4 - o3, max(d0, n01) - n01,
+                                d1 - n01, lv1 + n01);
+            __syncthreads();
+            d0 = min(tid * per, n0123);
+            d1 = min(d0 + per, n0123);
+            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv1), n01, arr(lv1 + n01), n0123 - n01, d0, d1, lv2);
+            __syncthreads();
+            per = (n + kTileThreads - 1) / kTileThreads;
+            d0 = min(tid * per, n);
+            d1 = min(d0 + per, n);
+            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv2), n0123, ident(o4), n - o4, d0, d1, s_perm);
+            __syncthreads();
+            for (int q = tid; q < n; q += kTileThreads) {
+                const int e = s_perm[q];
+                if (e < n) s_rank[e] = uint16_t(q);
+                else raise_status(status, PACES_ERR_BADARG);
             }
         }
         __syncthreads();
@@ -422,7 +454,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                     first = pe >= n || s_flag[pe] != 1 || !s_key.eq(pe, e);
                 }
             }
-            s_first[q] = uint8_t(first);
+            s_cnt[q] = uint16_t(first);  // turned into an inclusive count below
             cnt += first;
         }
         // block exclusive scan of cnt
@@ -458,7 +490,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             // inclusive count of firsts at every merged position (for strided writes)
             int run = s_warp[wid] + incl - cnt;
             for (int q = q0; q < q1; ++q) {
-                run += s_first[q];
+                run += s_cnt[q];
                 s_cnt[q] = uint16_t(run);
             }
         }
@@ -466,7 +498,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
 
         // 4a. new keys (and H rows), consecutive threads -> consecutive outputs
         for (int q = tid; q < n; q += kTileThreads) {
-            if (!s_first[q]) continue;
+            if (s_cnt[q] == (q > 0 ? s_cnt[q - 1] : 0)) continue;  // not a first occurrence
             const int e = s_perm[q];
             const int64_t u = int64_t(base) + s_cnt[q] - 1;
             if (u < out.cap) {
@@ -477,8 +509,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                     const uint32_t ntot = total_phonons(m, k);
                     if (u < out.nbr_cap) {
                         out.meta[u] = uint32_t(p) | (nex << 8) | (ntot << 16);
-#pragma unroll
-                        for (int sl = 0; sl < 4; ++sl) out.nbr[int64_t(sl) * out.nbr_cap + u] = -1;
+                        reinterpret_cast<int4*>(out.nbr)[u] = make_int4(-1, -1, -1, -1);
                     }
                 }
             } else {
@@ -550,29 +581,29 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
         if (p + 1 < L || m.periodic) {
             const int s = map[int64_t(RUN_FROM_LEFT) * mc + i];
             if (s >= 0 && s < nc) {
-                nb[int64_t(NB_RIGHT) * nc + q] = s;
-                nb[int64_t(NB_LEFT) * nc + s] = q;
+                nb[4 * int64_t(q) + NB_RIGHT] = s;
+                nb[4 * int64_t(s) + NB_LEFT] = q;
             }
         }
         if (p > 0 || m.periodic) {
             const int s = map[int64_t(RUN_FROM_RIGHT) * mc + i];
             if (s >= 0 && s < nc) {
-                nb[int64_t(NB_LEFT) * nc + q] = s;
-                nb[int64_t(NB_RIGHT) * nc + s] = q;
+                nb[4 * int64_t(q) + NB_LEFT] = s;
+                nb[4 * int64_t(s) + NB_RIGHT] = q;
             }
         }
         {
             const int s = map[int64_t(RUN_UP) * mc + i];
             if (s >= 0 && s < nc) {
-                nb[int64_t(NB_UP) * nc + q] = s;
-                nb[int64_t(NB_DOWN) * nc + s] = q;
+                nb[4 * int64_t(q) + NB_UP] = s;
+                nb[4 * int64_t(s) + NB_DOWN] = q;
             }
         }
         {
             const int s = map[int64_t(RUN_DOWN) * mc + i];
             if (s >= 0 && s < nc) {
-                nb[int64_t(NB_DOWN) * nc + q] = s;
-                nb[int64_t(NB_UP) * nc + s] = q;
+                nb[4 * int64_t(q) + NB_DOWN] = s;
+                nb[4 * int64_t(s) + NB_UP] = q;
             }
         }
     }
@@ -581,7 +612,8 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
 template <int NW>
 size_t tile_smem_bytes() {
     const int tmax = merge_tmax(NW);
-    return size_t(tmax) * sizeof(Key<NW>) + 2 * size_t((tmax + 15) & ~15) + size_t(tmax) * 6;
+    // keys, order flags, then three uint16 arrays (merged order, rank, running count)
+    return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) + size_t(tmax) * 6;
 }
 
 template <int NW>

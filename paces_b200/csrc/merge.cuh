@@ -19,8 +19,8 @@
 //
 // The merge is tiled with splitters: every `stride`-th element of every run is ranked
 // against all runs (binary search), splitters are put in merged order, and every
-// `group` consecutive splitters bound one tile of at most (group + 4) * stride elements.
-// A tile is merged in shared memory (rank = own index + bounds in the other segments),
+// `group` consecutive splitters bound one tile of at most (group + 5) * stride elements.
+// A tile is merged in shared memory (a pairwise merge tree with merge-path splits),
 // duplicates are flagged against the merged predecessor, and output offsets come from a
 // decoupled look-back over tiles taken in ticket order.  Every input element learns the
 // index of its key in the output, which gives the H neighbour table without any lookup.
@@ -57,9 +57,12 @@ struct MergeOut {
 };
 
 // Tiling constants by key width (shared memory of one tile stays below ~100 KB).
-__host__ __device__ constexpr int merge_stride(int nw) { return nw <= 4 ? 256 : 128; }
+__host__ __device__ constexpr int merge_stride(int nw) { return nw <= 2 ? 240 : (nw <= 4 ? 128 : 64); }
 constexpr int kMergeGroup = 8;
-__host__ __device__ constexpr int merge_tmax(int nw) { return (kMergeGroup + kRuns - 1) * merge_stride(nw); }
+// A tile holds the merged range of kMergeGroup consecutive splitters; every run contributes
+// fewer than (its splitters in the range + 1) * stride elements, so at most
+// (kMergeGroup + kRuns) * stride elements in total.
+__host__ __device__ constexpr int merge_tmax(int nw) { return (kMergeGroup + kRuns) * merge_stride(nw); }
 
 inline int64_t merge_split_cap(int64_t in_cap, int nw, int L) {
     return kRuns * (in_cap / merge_stride(nw) + 1) * 1 + int64_t(kRuns) * L + 8;

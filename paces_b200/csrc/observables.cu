@@ -46,11 +46,11 @@ obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict
         const uint32_t mm = __ldg(meta + r);
         double yr, yi;
         if constexpr (C64) {
-            const float2 y = h_row_c64(m, s_sq, J, r, nbr, cap, mm, x);
+            const float2 y = h_row_c64(m, s_sq, J, r, nbr, mm, x);
             yr = y.x;
             yi = y.y;
         } else {
-            const double2 y = h_row_c128(m, s_sq, r, nbr, cap, mm, x);
+            const double2 y = h_row_c128(m, s_sq, r, nbr, mm, x);
             yr = y.x;
             yi = y.y;
         }

@@ -70,7 +70,7 @@ __device__ void block_max4(double v[4], double (*red)[kTWarps], double* out) {
 }
 
 template <bool C64>
-__global__ void __launch_bounds__(kTThreads, 4)
+__global__ void __launch_bounds__(kTThreads, C64 ? 4 : 3)
 taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nbr, int64_t cap,
               const uint32_t* __restrict__ meta, const void* v_in, void* res_out, TaylorWs ws,
               double dt, int m_star, double tol, TaylorOut out, int* status) {
@@ -100,20 +100,20 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
         const double cd = dt / double(j + 1);
         const R c = R(cd);
         double mx[4] = {0.0, 0.0, 0.0, 0.0};  // |term|, |res|, |v|, non-finite
-        for (int64_t r = int64_t(blockIdx.x) * kTThreads + threadIdx.x; r < S;
-             r += int64_t(gridDim.x) * kTThreads) {
+        auto hrow = [&](int64_t r) -> C {
             const uint32_t mm = __ldg(meta + r);
+            if constexpr (C64) return h_row_c64(m, s_sq, J, r, nbr, mm, src);
+            else return h_row_c128(m, s_sq, r, nbr, mm, src);
+        };
+        auto finish = [&](int64_t r, const C& y, const C& a) {
             C t, rr;
-            const C a = rin[r];
             if constexpr (C64) {
-                const float2 y = h_row_c64(m, s_sq, J, r, nbr, cap, mm, src);
                 t = make_float2(c * y.y, -(c * y.x));
                 rr = make_float2(a.x + t.x, a.y + t.y);
                 mx[0] = fmax(mx[0], double(fmaf(t.x, t.x, t.y * t.y)));
                 mx[1] = fmax(mx[1], double(fmaf(rr.x, rr.x, rr.y * rr.y)));
                 if (j == 0) mx[2] = fmax(mx[2], double(fmaf(a.x, a.x, a.y * a.y)));
             } else {
-                const double2 y = h_row_c128(m, s_sq, r, nbr, cap, mm, src);
                 t = make_double2(__dmul_rn(cd, y.y), -__dmul_rn(cd, y.x));
                 rr = make_double2(__dadd_rn(a.x, t.x), __dadd_rn(a.y, t.y));
                 mx[0] = fmax(mx[0], fma(t.x, t.x, t.y * t.y));
@@ -123,7 +123,17 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
             if (!(isfinite(double(rr.x)) && isfinite(double(rr.y)))) mx[3] = 1.0;
             dst[r] = t;
             res[r] = rr;
+        };
+        // two rows per thread per pass: all loads of both rows precede the stores
+        const int64_t stride = int64_t(gridDim.x) * kTThreads;
+        int64_t r = int64_t(blockIdx.x) * kTThreads + threadIdx.x;
+        for (; r + stride < S; r += 2 * stride) {
+            const C y0 = hrow(r), y1 = hrow(r + stride);
+            const C a0 = rin[r], a1 = rin[r + stride];
+            finish(r, y0, a0);
+            finish(r + stride, y1, a1);
         }
+        if (r < S) finish(r, hrow(r), rin[r]);
         block_max4(mx, s_red, s_fin);
         if (threadIdx.x == 0) {
             double* pp = ws.partials + (size_t((j & 1) * nblocks) + blockIdx.x) * 4;

@@ -60,11 +60,11 @@ class DevBasis:
 
 
 class DevHMat:
-    """Neighbour table [4, cap] (left, right, down, up; -1 = absent) and row metadata [cap]."""
+    """Neighbour table [cap, 4] (left, right, down, up; -1 = absent) and row metadata [cap]."""
 
     def __init__(self, eng: "Engine", cap: int):
         self.cap = int(cap)
-        self.nbr = torch.empty((4, max(self.cap, 1)), dtype=torch.int32, device=eng.device)
+        self.nbr = torch.empty((max(self.cap, 1), 4), dtype=torch.int32, device=eng.device)
         self.meta = torch.empty(max(self.cap, 1), dtype=torch.int32, device=eng.device)
 
     def c(self):

@@ -19,7 +19,7 @@ def ref_rows(eng, basis):
 def csr_from_table(eng, basis, h, J, g):
     """Per-term CSR (hopping, vib_coupling) and the diagonal, rebuilt from the neighbour table."""
     S = basis.count()
-    nbr = h.nbr[:, :S].cpu().numpy().astype(np.int64)
+    nbr = h.nbr[:S].cpu().numpy().astype(np.int64).T
     meta = h.meta[:S].cpu().numpy().view(np.uint32).astype(np.int64)
     n = (meta >> 8) & 0xFF
     ntot = meta >> 16
