@@ -199,6 +199,19 @@ int paces_truncate(paces_ctx *ctx, const paces_basis *in, const void *psi, int64
 int paces_remap(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi,
                 const paces_basis *new_b, void *new_psi, void *ws, size_t ws_bytes,
                 paces_stream_t stream);
+/* paces_remap without a workspace.  No counterpart in the reference (which allocates
+ * through CuPy's pool on every call).  For callers that cannot allocate device memory
+ * at all: a host application that owns the whole device through its own memory pool, or
+ * a latency-critical loop that must not call cudaMalloc (it can synchronise the device).
+ * The scratch is a 256 KiB array in the library's static device memory, held by every
+ * GPU that loads the library until the process exits; it bounds the two bases together
+ * to about 64M states (2048 per remap tile for keys of 1-2 words, 1024 for 3-4, 512
+ * beyond).  Capacities beyond that return PACES_ERR_CAPACITY before anything is
+ * launched.  The first call on a device looks up the array's device address with that
+ * device current: make it before any stream capture.  All calls share the one array, so
+ * calls that overlap on the GPU (other streams, other threads) race: serialise them. */
+int paces_remap_noalloc(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi,
+                        const paces_basis *new_b, void *new_psi, paces_stream_t stream);
 int paces_taylor(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi_in,
                  void *psi_out, double dt, int32_t m_star, double tol,
                  paces_expm_info *dev_info, void *ws, size_t ws_bytes, paces_stream_t stream);

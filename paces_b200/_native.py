@@ -123,6 +123,7 @@ _SIGNATURES = {
     "paces_truncate": [_P, ctypes.POINTER(Basis), _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64,
                        ctypes.c_uint64, ctypes.POINTER(Basis), _P, ctypes.c_size_t, _P],
     "paces_remap": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P, ctypes.c_size_t, _P],
+    "paces_remap_noalloc": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P],
     "paces_taylor": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, ctypes.c_double, ctypes.c_int32,
                      ctypes.c_double, _P, _P, ctypes.c_size_t, _P],
     "paces_observables": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, ctypes.c_int32, _P, _P,

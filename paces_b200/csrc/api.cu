@@ -421,6 +421,28 @@ int paces_remap(paces_ctx* c, const paces_basis* old_b, const void* old_psi, con
     return PACES_OK;
 }
 
+int paces_remap_noalloc(paces_ctx* c, const paces_basis* old_b, const void* old_psi, const paces_basis* new_b,
+                        void* new_psi, paces_stream_t stream) {
+    if (!c || !valid_basis(old_b) || !valid_basis(new_b) || !old_psi || !new_psi) return PACES_ERR_BADARG;
+    // the tile table must fit the static scratch for any contents of the two bases
+    const int64_t tiles = (old_b->cap + new_b->cap) / remap_tile(c->nw) + c->m.L + 8;
+    if (tiles > remap_static_tile_cap())
+        return fail(c, PACES_ERR_CAPACITY,
+                    "paces_remap_noalloc: bases of %lld + %lld states need %lld remap tiles; the static "
+                    "scratch holds %d (at most %lld states in total with %d key words)",
+                    (long long)old_b->cap, (long long)new_b->cap, (long long)tiles, remap_static_tile_cap(),
+                    (long long)(remap_static_tile_cap() - c->m.L - 8) * remap_tile(c->nw), c->nw);
+    RemapWs ws{};
+    const char* err = nullptr;
+    const int rc = remap_static_ws(&ws, &err);
+    if (rc != PACES_OK) return fail(c, rc, "paces_remap_noalloc: %s", err ? err : "set-up failed");
+    PACES_CHECK_LAUNCH(c, launch_remap(c->nw, c->precision == PACES_C64, c->m, old_b->keys, old_b->blk, old_psi,
+                                       new_b->keys, new_b->blk, new_psi, ws, c->d_status, c->num_sms,
+                                       reinterpret_cast<cudaStream_t>(stream)),
+                       "remap_noalloc");
+    return PACES_OK;
+}
+
 int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi_in, void* psi_out,
                  double dt, int32_t m_star, double tol, paces_expm_info* dev_info, void* ws, size_t ws_bytes,
                  paces_stream_t stream) {

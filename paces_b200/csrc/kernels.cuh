@@ -31,6 +31,9 @@ inline int remap_tile_cap(int64_t cap, int nw, int L) { return int((2 * cap) / r
 int launch_remap(int nw, bool c64, const ModelDev& m, const uint64_t* ok, const int* ob,
                  const void* opsi, const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws,
                  int* status, int num_sms, cudaStream_t st);
+// Workspace of the remap in the library's static device scratch (current device).
+int remap_static_ws(RemapWs* ws, const char** err);
+int remap_static_tile_cap();
 
 // ---- Taylor -----------------------------------------------------------------------------
 struct TaylorOut {

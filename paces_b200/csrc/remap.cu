@@ -11,6 +11,8 @@
 // kernel stages the tile's old keys in shared memory and resolves each new key by a
 // shared-memory upper bound (old before new on equal keys; a match is the old element
 // just before the new one).
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace paces {
@@ -120,7 +122,45 @@ int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const v
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
+// Scratch of the workspace-free remap (paces_remap_noalloc): block tile offsets, the tile
+// counter and two splits per tile, 256 KiB in total.  Every GPU that loads the library
+// holds one copy until the process exits.  Nothing in it has to start at zero: the plan
+// kernel rewrites the offsets and the counter, the split kernel every split it uses.
+constexpr size_t kStaticRemapBytes = size_t(256) << 10;
+constexpr size_t kStaticHeaderBytes = 1024;  // tile_off[kMaxSites+1] and counters
+
 }  // namespace
+
+static __device__ __align__(256) unsigned char g_remap_scratch[kStaticRemapBytes];
+
+int remap_static_tile_cap() { return int((kStaticRemapBytes - kStaticHeaderBytes) / (2 * sizeof(int))); }
+
+int remap_static_ws(RemapWs* ws, const char** err) {
+    static std::mutex mu;
+    static void* addr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        *err = "no current CUDA device";
+        return PACES_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        // host code cannot use the array's name as a device address: ask the runtime, once per
+        // device, with that device current
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_remap_scratch) != cudaSuccess || !p) {
+            *err = "cudaGetSymbolAddress of the static remap scratch failed";
+            return PACES_ERR_CUDA;
+        }
+        addr[dev] = p;
+    }
+    unsigned char* base = static_cast<unsigned char*>(addr[dev]);
+    ws->tile_off = reinterpret_cast<int*>(base);
+    ws->counters = reinterpret_cast<int*>(base + sizeof(int) * (kMaxSites + 8));
+    ws->split = reinterpret_cast<int*>(base + kStaticHeaderBytes);
+    ws->tile_cap = remap_static_tile_cap();
+    return PACES_OK;
+}
 
 int launch_remap(int nw, bool c64, const ModelDev& m, const uint64_t* ok, const int* ob,
                  const void* opsi, const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws,
