@@ -39,7 +39,7 @@ if HERE not in sys.path:
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="c128", choices=["c128", "c64"])
@@ -174,6 +174,17 @@ def prepare(a, eng, maxstates):
         if nprep > 400:
             raise RuntimeError("basis did not saturate")
     return tr, nprep
+
+
+def max_over_ranks(value, dist, device="cuda"):
+    """Largest value over all ranks (the timed region's duration); the value itself when
+    there is no process group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def taylor_bytes_per_term(rec, cs):
@@ -313,11 +324,7 @@ def run_ours(a):
         ev1.record(stream)
         ev1.synchronize()
     launches = eng.kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     clocks = clk.summary()
     barrier()
     eng.set_profiling(False)
@@ -405,13 +412,8 @@ def run_e2e(a, eng, tr, barrier, dist):
         cur = nxt
     ev1.record(stream)
     ev1.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    world = 1
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        world = dist.get_world_size()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
+    world = 1 if dist is None else dist.get_world_size()
     return {"value": a.steps * world / (ms / 1e3), "unit": "time-steps/s",
             "h2d_bytes_per_step": h2d // a.steps, "d2h_bytes_per_step": d2h // a.steps,
             "api": "paces_step (C ABI) with the state in pinned host memory"}

@@ -218,6 +218,10 @@ int paces_taylor(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, cons
 int paces_observables(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi,
                       int32_t what, double *dev_out, void *ws, size_t ws_bytes,
                       paces_stream_t stream);
+/* y = H x on a basis (x and y distinct).  Reference: TimeEvolutionFramework.total_ham,
+ * paces/core/time_evolution.py:382-400. */
+int paces_apply_h(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *x, void *y,
+                  paces_stream_t stream);
 /* Lower-bound lookup of (pos, key) queries in a basis; out[i] = row index or -1 if absent.
  * With must_exist != 0 a miss also raises PACES_ERR_LOOKUP (reference: noesc kernel). */
 int paces_lookup(paces_ctx *ctx, const paces_basis *phonebook, const uint64_t *q_keys,

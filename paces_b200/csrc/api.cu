@@ -477,6 +477,15 @@ int paces_observables(paces_ctx* c, const paces_basis* b, const paces_hmat* h, c
     return PACES_OK;
 }
 
+int paces_apply_h(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* x, void* y,
+                  paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !x || !y || x == y) return PACES_ERR_BADARG;
+    PACES_CHECK_LAUNCH(c, launch_apply_h(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->meta, x, y, c->num_sms,
+                                         reinterpret_cast<cudaStream_t>(stream)),
+                       "apply_h");
+    return PACES_OK;
+}
+
 int paces_lookup(paces_ctx* c, const paces_basis* pb, const uint64_t* q_keys, const int32_t* q_pos, int64_t nq,
                  int32_t must_exist, int64_t* out, void* ws, size_t ws_bytes, paces_stream_t stream) {
     (void)ws;

@@ -70,6 +70,8 @@ int launch_observables(int nw, bool c64, const ModelDev& m, const uint64_t* keys
                        cudaStream_t st);
 int launch_scale(bool c64, const ModelDev& m, const int* blk, void* psi, const double* norm,
                  int num_sms, cudaStream_t st);
+int launch_apply_h(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
+                   const void* x, void* y, int num_sms, cudaStream_t st);
 
 // ---- lookup and layout conversion -------------------------------------------------------
 struct RefLayout {

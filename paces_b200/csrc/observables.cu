@@ -237,6 +237,27 @@ __global__ void __launch_bounds__(256) obs_final_kernel(int L, int nb_e, const d
     }
 }
 
+// y = H x on every row of the basis (total_ham, paces/core/time_evolution.py:382-400).
+template <bool C64>
+__global__ void __launch_bounds__(kOThreads) apply_h_kernel(ModelDev m, const int* __restrict__ blk,
+                                                            const int* __restrict__ nbr,
+                                                            const uint32_t* __restrict__ meta,
+                                                            const void* __restrict__ xin, void* __restrict__ yout) {
+    using C = typename std::conditional<C64, float2, double2>::type;
+    using R = typename std::conditional<C64, float, double>::type;
+    __shared__ R s_sq[260];
+    for (int k = threadIdx.x; k < 260; k += kOThreads) s_sq[k] = R(__dmul_rn(sqrt(double(k)), m.g));
+    __syncthreads();
+    const int64_t S = blk[m.L];
+    const C* x = reinterpret_cast<const C*>(xin);
+    C* y = reinterpret_cast<C*>(yout);
+    for (int64_t r = int64_t(blockIdx.x) * kOThreads + threadIdx.x; r < S; r += int64_t(gridDim.x) * kOThreads) {
+        const uint32_t mm = __ldg(meta + r);
+        if constexpr (C64) y[r] = h_row_c64(m, s_sq, float(m.J), r, nbr, mm, x);
+        else y[r] = h_row_c128(m, s_sq, r, nbr, mm, x);
+    }
+}
+
 template <bool C64>
 __global__ void scale_kernel(int L, const int* __restrict__ blk, void* psi, const double* norm) {
     using C = typename std::conditional<C64, float2, double2>::type;
@@ -320,6 +341,13 @@ int launch_observables(int nw, bool c64, const ModelDev& m, const uint64_t* keys
         default: return PACES_ERR_BADARG;
     }
 #undef PACES_OBS_CASE
+}
+
+int launch_apply_h(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
+                   const void* x, void* y, int num_sms, cudaStream_t st) {
+    if (c64) apply_h_kernel<true><<<num_sms * 4, kOThreads, 0, st>>>(m, blk, nbr, meta, x, y);
+    else apply_h_kernel<false><<<num_sms * 4, kOThreads, 0, st>>>(m, blk, nbr, meta, x, y);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
 int launch_scale(bool c64, const ModelDev& m, const int* blk, void* psi, const double* norm,

@@ -240,6 +240,13 @@ class Engine:
         return {"norm": o[0], "energy": complex(o[1], o[2]), "n_exc": o[3:3 + self.L],
                 "n_pho": o[3 + self.L:3 + 2 * self.L]}
 
+    def apply_h(self, b: DevBasis, h: DevHMat, x, y=None):
+        """y = H x (total_ham)."""
+        y = torch.empty_like(x) if y is None else y
+        nat.check(self.lib.paces_apply_h(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(x), _ptr(y),
+                                         _stream(self.device)), self.ctx, "apply_h")
+        return y
+
     def lookup(self, pb: DevBasis, q_keys, q_pos, nq, must_exist=False):
         out = torch.empty(max(nq, 1), dtype=torch.int64, device=self.device)
         ws, nb = self.workspace()

@@ -80,3 +80,80 @@ def sort_unique_rows(rows):
     keep = np.ones(s.shape[0], dtype=bool)
     keep[1:] = np.any(s[1:] != s[:-1], axis=1)
     return s[keep]
+
+
+# ---- the same field arithmetic on device tensors (host API helpers, off the time step) ----
+
+def field_table(bitwidths):
+    """Per field: bit offset from the row's MSB, width, first word, end bit in its window."""
+    bw = np.asarray(bitwidths, dtype=np.int64)
+    off = np.concatenate([[0], np.cumsum(bw)[:-1]]).astype(np.int64)
+    wi = off // 32
+    n2 = off + bw - 32 * wi
+    return off, bw, wi, n2
+
+
+def rows_i64(rows):
+    """uint32 rows (torch uint32/int32/int64 or numpy) -> int64 tensor with values < 2^32."""
+    import torch
+    if isinstance(rows, np.ndarray):
+        rows = torch.from_numpy(np.ascontiguousarray(rows, dtype=np.uint32).view(np.int32))
+    if rows.dtype == torch.uint32:
+        rows = rows.view(torch.int32)
+    if rows.dtype == torch.int32:
+        return rows.to(torch.int64) & 0xFFFFFFFF
+    return rows.to(torch.int64)
+
+
+def rows_u32(r64):
+    import torch
+    return r64.to(torch.int32).view(torch.uint32) if r64.numel() else r64.to(torch.int32).view(torch.uint32)
+
+
+def _window(r64, wi):
+    import torch
+    n, W = r64.shape
+    pad = torch.cat([r64, torch.zeros((n, 1), dtype=r64.dtype, device=r64.device)], dim=1)
+    if isinstance(wi, torch.Tensor):
+        hi = torch.gather(pad, 1, wi.view(-1, 1)).view(-1)
+        lo = torch.gather(pad, 1, (wi + 1).view(-1, 1)).view(-1)
+    else:
+        hi, lo = pad[:, wi], pad[:, wi + 1]
+    return (hi << 32) | lo
+
+
+def get_field_t(r64, table, idx):
+    """Field `idx` (int, or one index per row) of every row."""
+    import torch
+    off, bw, wi, n2 = table
+    if isinstance(idx, torch.Tensor):
+        dev = r64.device
+        wi_t = torch.as_tensor(wi, device=dev)[idx]
+        n2_t = torch.as_tensor(n2, device=dev)[idx]
+        bw_t = torch.as_tensor(bw, device=dev)[idx]
+        win = _window(r64, wi_t)
+        return (win >> (64 - n2_t)) & ((1 << bw_t) - 1)
+    win = _window(r64, int(wi[idx]))
+    return (win >> int(64 - n2[idx])) & ((1 << int(bw[idx])) - 1)
+
+
+def add_field_t(r64, table, idx, delta):
+    """New rows with field `idx` (int or per-row) increased by `delta` (carry/borrow across words)."""
+    import torch
+    off, bw, wi, n2 = table
+    n, W = r64.shape
+    dev = r64.device
+    if isinstance(idx, torch.Tensor):
+        wi_t = torch.as_tensor(wi, device=dev)[idx]
+        n2_t = torch.as_tensor(n2, device=dev)[idx]
+    else:
+        wi_t = torch.full((n,), int(wi[idx]), dtype=torch.int64, device=dev)
+        n2_t = torch.full((n,), int(n2[idx]), dtype=torch.int64, device=dev)
+    win = _window(r64, wi_t) + (torch.as_tensor(delta, dtype=torch.int64, device=dev) << (64 - n2_t))
+    out = torch.cat([r64, torch.zeros((n, 1), dtype=r64.dtype, device=dev)], dim=1)
+    out.scatter_(1, wi_t.view(-1, 1), ((win >> 32) & 0xFFFFFFFF).view(-1, 1))
+    lo_idx = (wi_t + 1).view(-1, 1)
+    keep_lo = lo_idx < W
+    lo_val = torch.where(keep_lo.view(-1), win & 0xFFFFFFFF, torch.gather(out, 1, lo_idx).view(-1))
+    out.scatter_(1, lo_idx, lo_val.view(-1, 1))
+    return out[:, :W]

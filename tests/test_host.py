@@ -1,0 +1,124 @@
+"""CPU tests of the host side: the C ABI exports, the key layout helpers, the drop-in
+module paths, and the multi-process (replica) timing reduction under gloo."""
+
+import os
+import re
+import socket
+
+import numpy as np
+import pytest
+import torch
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(REPO, "tests", "golden")
+
+
+def _declared_symbols():
+    with open(os.path.join(REPO, "include", "paces_b200.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(paces_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+    from paces_b200 import _native
+    lib = ctypes.CDLL(_native.LIB_PATH)
+    declared = _declared_symbols()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(lib, name), name
+    # and the ctypes binding covers the whole ABI
+    assert set(declared) == set(_native.exported_symbols())
+    _native.load()
+
+
+def test_workspace_query_without_a_device():
+    from paces_b200 import _native
+    lib = _native.load()
+    assert lib.paces_version() == 10200
+    assert lib.paces_create(None, None) == 5  # PACES_ERR_BADARG, no device touched
+
+
+@pytest.mark.parametrize("name", ["n16c16", "n32c16", "n25c128", "n6c8"])
+def test_layout_helpers_match_reference_packing(name):
+    from paces_b200 import layout
+    f = np.load(os.path.join(GOLDEN, f"layout_{name}.npz"))
+    bw = f["bitwidths"]
+    rows = layout.pack_rows(f["raw"], bw)
+    assert np.array_equal(rows, f["keys"])
+    assert np.array_equal(layout.unpack_rows(rows, bw), f["raw"])
+    assert np.array_equal(layout.sort_unique_rows(f["unique_in"]), f["unique_out"])
+    tab = layout.field_table(bw)
+    r64 = layout.rows_i64(rows)
+    pos = layout.get_field_t(r64, tab, 0)
+    assert np.array_equal(layout.get_field_t(r64, tab, pos + 1).numpy(), f["get_occ"])
+    up = torch.from_numpy(f["can_up"])
+    got = layout.rows_u32(layout.add_field_t(r64[up], tab, pos[up] + 1, 1)).numpy()
+    assert np.array_equal(got, f["keys_up"])
+
+
+def test_search_helpers_match_reference():
+    from paces_b200.aux import cupy_search
+    f = np.load(os.path.join(GOLDEN, "layout_n32c16.npz"))
+    uniq = torch.from_numpy(f["unique_out"].view(np.int32))
+    idx = cupy_search.searchsorted_full_binary(uniq, torch.from_numpy(f["search_hit_q"].view(np.int32)))
+    assert np.array_equal(idx.numpy(), f["search_hit_idx"].astype(np.int64))
+    with pytest.raises(LookupError):
+        cupy_search.searchsorted_full_binary(uniq, torch.from_numpy(f["search_any_q"].view(np.int32)))
+
+
+def test_drop_in_module_paths():
+    import paces
+    from paces.config import devices, INIT_VERBOSITY_LEVEL, SEARCHSORTED_TIMING_LEVEL
+    from paces.core.hamiltonian import HamiltonianFramework, MelTriple
+    from paces.core.observables import ObservablesFramework
+    from paces.core.time_evolution import CoeffSaveParams, ExpmParams, TimeEvoParams, TimeEvolutionFramework
+    from paces.models import holstein
+    import paces_b200
+    assert paces.config.devices is paces_b200.config.devices is devices
+    assert issubclass(holstein.Hamiltonian, HamiltonianFramework)
+    assert issubclass(holstein.Observables, ObservablesFramework)
+    assert issubclass(holstein.TimeEvolution, TimeEvolutionFramework)
+    assert INIT_VERBOSITY_LEVEL == 0 and SEARCHSORTED_TIMING_LEVEL == 7
+    assert ExpmParams().m_star == 100 and TimeEvoParams(1, 1).shuffle_seed == 0
+    cso = CoeffSaveParams(save_every=3, save_first=True, save_last=True, max_i=7)
+    assert [cso.save_necessary(i) for i in range(8)] == [True, False, False, True, False, False, True, True]
+    assert holstein.Observables.calculate_n_exc.fname == "n_exc"
+    assert MelTriple._fields == ("inds", "vals", "mask")
+
+
+def test_framework_needs_configured_devices():
+    from paces_b200.config import DeviceConfig
+    d = DeviceConfig()
+    with pytest.raises(NotImplementedError):
+        d.configure(whoami_device_id=0, vector_device_id=1)
+    with pytest.raises(NotImplementedError):
+        d.configure(unified_memory_bytes=1 << 30)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _replica_worker(rank, world, port, out):
+    import torch.distributed as dist
+    import bench
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    ms = bench.max_over_ranks(10.0 + rank, dist, device="cpu")
+    out[rank] = ms
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_timing_takes_the_max_over_ranks():
+    import torch.multiprocessing as mp
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    port = _free_port()
+    mp.start_processes(_replica_worker, args=(2, port, out), nprocs=2, start_method="spawn")
+    assert dict(out) == {0: 11.0, 1: 11.0}
