@@ -19,8 +19,11 @@
 
 namespace paces {
 
-// Diagonal element from the row metadata (paces/models/holstein.py:280-287).
-__device__ __forceinline__ double diag_value(const ModelDev& m, uint32_t meta) {
+// Diagonal element from the row metadata (paces/models/holstein.py:280-287).  `P` is the
+// model (ModelDev) or a batched trajectory's parameters: any type with eps_sys,
+// hbar_omega, delta_eps, has_site_eps, site_eps[] and J.
+template <class P>
+__device__ __forceinline__ double diag_value(const P& m, uint32_t meta) {
     const int pos = int(meta & 0xffu);
     const uint32_t ntot = meta >> 16;
     double d = __dadd_rn(m.eps_sys, __dmul_rn(m.hbar_omega, double(ntot)));
@@ -34,7 +37,8 @@ __device__ __forceinline__ int4 load_nbr(const int* __restrict__ nbr, int64_t r)
 }
 
 // y = (H x)[r] in complex128.  sq[k] = sqrt(k) * g.
-__device__ __forceinline__ double2 h_row_c128(const ModelDev& m, const double* sq, int64_t r,
+template <class P>
+__device__ __forceinline__ double2 h_row_c128(const P& m, const double* sq, int64_t r,
                                               const int* __restrict__ nbr, uint32_t meta,
                                               const double2* __restrict__ x) {
     const int n = int((meta >> 8) & 0xffu);
@@ -65,7 +69,8 @@ __device__ __forceinline__ double2 h_row_c128(const ModelDev& m, const double* s
 }
 
 // y = (H x)[r] in complex64 with fp32 accumulation.  sq[k] = float(sqrt(k) * g).
-__device__ __forceinline__ float2 h_row_c64(const ModelDev& m, const float* sq, float J, int64_t r,
+template <class P>
+__device__ __forceinline__ float2 h_row_c64(const P& m, const float* sq, float J, int64_t r,
                                             const int* __restrict__ nbr, uint32_t meta,
                                             const float2* __restrict__ x) {
     const int n = int((meta >> 8) & 0xffu);

@@ -46,3 +46,43 @@ def csr_from_table(eng, basis, h, J, g):
         m.sort_indices()
         mats[term] = m
     return diag, mats, pos
+
+
+def initial_rows(nchain, dim=16, initpos=0):
+    """Reference row of the exciton on site `initpos` with the phonon vacuum."""
+    from paces_b200 import layout
+    raw = np.zeros((1, nchain + 1), dtype=np.uint32)
+    raw[0, 0] = initpos
+    return layout.pack_rows(raw, layout.bitwidths_for([nchain] + [dim] * nchain))
+
+
+def grown_trajectory(eng, nchain, maxstates, es=1, initpos=0, dim=16):
+    """A trajectory on grow_optimal_basis(fillfac=1) with the exciton on `initpos` in the
+    phonon vacuum, after its first (non-evolving) step
+    (paces/core/time_evolution.py:290-323, :325-363)."""
+    import torch
+    from paces_b200.engine import Trajectory
+    rows = initial_rows(nchain, dim, initpos)
+    tr = Trajectory(eng, maxstates, es)
+    b = eng.basis_from_ref(rows)
+    while True:
+        nxt = eng.expand(b)
+        if nxt.count() > maxstates or nxt.count() == 0:
+            break
+        b = nxt
+    keys, pos, n = eng.query_from_ref(rows)
+    idx = int(eng.lookup(b, keys, pos, n, must_exist=True)[0].item())
+    psi = torch.zeros(max(b.count(), 1), dtype=eng.cdtype, device=eng.device)
+    psi[idx] = 1.0
+    tr.set_state(b, psi)
+    first = tr.step(evolve=False)
+    return tr, first
+
+
+def observables_of(recs, nchain):
+    return {
+        "n_exc": np.array([list(r.n_exc)[:nchain] for r in recs]),
+        "n_pho": np.array([list(r.n_pho)[:nchain] for r in recs]),
+        "energy": np.array([r.energy_re for r in recs]),
+        "norm": np.array([r.norm for r in recs]),
+    }

@@ -1,0 +1,45 @@
+"""The complex64 form against the complex128 form (the plain method at the reference's
+precision) over t = 10/J: every observable stays within the stated bound.
+
+complex64 keeps amplitudes, the neighbour-table SpMV and the Taylor updates in fp32 (FMA,
+fp32 accumulation) and the stop test, norms, energies and site sums in fp64; the Taylor
+tolerance is 2^-24 instead of 2^-53.  The bounds asserted here are the measured maximum
+absolute differences over 200 steps of dt = 0.05 with about a 3x margin (measured:
+N=32, maxstates 2^18: n_exc 7.2e-7, n_pho 2.3e-6, energy 3.3e-6, norm 8.7e-7;
+N=32, maxstates 2^22: 1.7e-7, 5.6e-7, 1.3e-6, 5.6e-7; N=16, g=1, maxstates 2^16:
+4.0e-6, 7.0e-6, 1.4e-5, 2.3e-6)."""
+
+import numpy as np
+import pytest
+
+from tests import gpu_helpers
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # nchain, g, maxstates, bound
+    (32, 1.5, 1 << 18, 1e-5),
+    (32, 1.5, 1 << 22, 1e-5),
+    (16, 1.0, 1 << 16, 5e-5),
+]
+
+
+def _run(nchain, g, maxstates, precision, steps=200, dt=0.05):
+    eng = gpu_helpers.engine_for(nchain, 16, g, cap=1 << 16, precision=precision, periodic=True)
+    tr, first = gpu_helpers.grown_trajectory(eng, nchain, maxstates)
+    recs = [first] + [tr.step(evolve=True, dt=dt) for _ in range(steps)]
+    out = gpu_helpers.observables_of(recs, nchain)
+    eng.close()
+    return out
+
+
+@pytest.mark.parametrize("nchain,g,maxstates,bound", CASES, ids=lambda v: str(v))
+def test_complex64_observables_within_bound(nchain, g, maxstates, bound):
+    ref = _run(nchain, g, maxstates, "c128")
+    got = _run(nchain, g, maxstates, "c64")
+    errs = {k: float(np.max(np.abs(ref[k] - got[k]))) for k in ref}
+    print(f"N={nchain} g={g} maxstates={maxstates}: max |c64 - c128| over t=10: {errs}")
+    for k, e in errs.items():
+        assert e <= bound, (k, e)
+    # the forms stay close to the end, not just on average
+    assert np.all(np.isfinite(got["energy"]))
