@@ -236,6 +236,39 @@ int paces_step(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi, pa
                void *new_psi, paces_hmat *h, const paces_step_params *prm,
                paces_step_record *dev_rec, void *ws, size_t ws_bytes, paces_stream_t stream);
 
+/* ---- batched trajectories (no counterpart in the reference, which runs one trajectory
+ * per process) ------------------------------------------------------------------------
+ * paces_batch_step advances up to 128 independent trajectories -- each with its own
+ * context (model, key width, dt, maxstates), buffers and record -- by one time step.
+ * The per-trajectory truncation, enlargement, assembly, remap and observables are spread
+ * over the batch's own streams (forked from and joined back into `stream`, so the whole
+ * call can be captured into one CUDA graph); the Taylor series of every trajectory runs
+ * in ONE persistent cooperative launch.  Each trajectory's results are bit-identical to
+ * paces_step on the same inputs.  All contexts share one precision and device.  Item
+ * errors land in each record's status; a non-OK return names the item in
+ * paces_batch_last_error. */
+typedef struct paces_batch paces_batch;
+typedef struct paces_batch_item {
+    paces_ctx *ctx;
+    const paces_basis *old_basis;
+    const void *old_psi;
+    paces_basis *new_basis;
+    void *new_psi;
+    paces_hmat *h;
+    const paces_step_params *params;
+    paces_step_record *record;   /* device */
+    void *workspace;
+    size_t workspace_bytes;
+} paces_batch_item;
+/* max_items <= 128; n_streams in [1, 64] (allocates the Taylor scratch, a few KB). */
+int paces_batch_create(int32_t max_items, int32_t n_streams, paces_batch **out);
+int paces_batch_destroy(paces_batch *batch);
+int paces_batch_step(paces_batch *batch, const paces_batch_item *items, int32_t n,
+                     paces_stream_t stream);
+const char *paces_batch_last_error(const paces_batch *batch);
+/* Number of kernels paces_batch_step has enqueued on this batch so far. */
+unsigned long long paces_batch_kernel_launches(const paces_batch *batch);
+
 #ifdef __cplusplus
 }
 #endif

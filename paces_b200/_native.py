@@ -103,6 +103,23 @@ class ExpmInfo(ctypes.Structure):
                 ("c1_plus_c2", ctypes.c_double), ("term_ratio", ctypes.c_double)]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [
+        ("ctx", ctypes.c_void_p),
+        ("old_basis", ctypes.POINTER(Basis)),
+        ("old_psi", ctypes.c_void_p),
+        ("new_basis", ctypes.POINTER(Basis)),
+        ("new_psi", ctypes.c_void_p),
+        ("h", ctypes.POINTER(HMat)),
+        ("params", ctypes.POINTER(StepParams)),
+        ("record", ctypes.c_void_p),
+        ("workspace", ctypes.c_void_p),
+        ("workspace_bytes", ctypes.c_size_t),
+    ]
+
+
+MAX_BATCH = 128
+
 # entry point name -> (argtypes); every entry point returns int (status) unless listed in _RESTYPES
 _P = ctypes.c_void_p
 _SIGNATURES = {
@@ -136,8 +153,14 @@ _SIGNATURES = {
     "paces_set_profiling": [_P, ctypes.c_int32],
     "paces_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
     "paces_kernel_launches": [_P],
+    "paces_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)],
+    "paces_batch_destroy": [_P],
+    "paces_batch_step": [_P, ctypes.POINTER(BatchItem), ctypes.c_int32, _P],
+    "paces_batch_last_error": [_P],
+    "paces_batch_kernel_launches": [_P],
 }
-_RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_kernel_launches": ctypes.c_ulonglong}
+_RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_kernel_launches": ctypes.c_ulonglong,
+             "paces_batch_last_error": ctypes.c_char_p, "paces_batch_kernel_launches": ctypes.c_ulonglong}
 STAGES = ("truncate", "expand", "assemble", "remap", "diagnostics", "taylor", "observables")
 
 _lib = None

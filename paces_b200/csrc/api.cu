@@ -1,4 +1,5 @@
 // C ABI of libpaces_b200 (declared in include/paces_b200.h).
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -15,10 +16,28 @@ struct paces_ctx {
     int device;
     int num_sms;
     int taylor_grid;
-    int* d_status;  // device status word for the stage entry points
+    int* d_status;  // device status word for the stage entry points (start of the constants block)
+    double* d_site_eps;  // [kMaxSites] per-site energies, device copy (batched Taylor)
+    double* d_sq;        // [kSqrtTable] sqrt(k) * g
+    float* d_sqf;        // [kSqrtTable] the same rounded to fp32
     int profiling;  // record stage events in paces_step
     cudaEvent_t ev[8];
     unsigned long long launches;  // kernels launched by paces_step since creation
+    char err[512];
+};
+
+
+struct paces_batch {
+    int max_items;
+    int n_streams;
+    int device;
+    int num_sms;
+    cudaStream_t* streams;
+    cudaEvent_t fork;
+    cudaEvent_t* join;
+    void* d_ws;                   // TaylorBatchWs: barrier words + per-term maxima
+    TaylorBatch* desc;            // host staging of the launch descriptors
+    unsigned long long launches;  // kernels enqueued by paces_batch_step
     char err[512];
 };
 
@@ -193,6 +212,160 @@ __global__ void record_counts_kernel(paces_step_record* rec, const int* sel_blk,
     rec->n_states = new_blk[L];
 }
 
+// ---- the time step, in the pieces the single and the batched step share ---------------------
+struct StepPlan {
+    Layout l;
+    const paces_basis* old_b;
+    const void* old_psi;
+    paces_basis* new_b;
+    void* new_psi;
+    paces_hmat* h;
+    const paces_step_params* prm;
+    paces_step_record* rec;
+    void* ws;
+    paces_basis A, B;   // truncated basis, enlargement ping-pong
+    paces_basis* cur;   // the enlarged basis (A or B after enlarge_steps merges)
+    void* target;       // remapped amplitudes (the Taylor input when evolving)
+};
+
+int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces_basis* new_b, void* new_psi,
+              paces_hmat* h, const paces_step_params* prm, paces_step_record* rec, void* ws, size_t ws_bytes,
+              StepPlan* p) {
+    if (!c) return PACES_ERR_BADARG;
+    if (!valid_basis(old_b) || !valid_basis(new_b) || !old_psi || !new_psi || !h || !h->nbr || !h->meta ||
+        !prm || !rec || !ws)
+        return fail(c, PACES_ERR_BADARG, "paces_step: null argument");
+    if (prm->maxstates < 1 || prm->enlarge_steps < 0 || (prm->evolve && prm->m_star < 1))
+        return fail(c, PACES_ERR_BADARG, "paces_step: bad parameters");
+    p->l = fit_layout(c, ws_bytes);
+    const Layout& l = p->l;
+    if (old_b->cap > l.cap || new_b->cap > l.cap || h->cap > l.cap)
+        return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states; bases hold %lld/%lld", (long long)l.cap,
+                    (long long)old_b->cap, (long long)new_b->cap);
+    p->old_b = old_b;
+    p->old_psi = old_psi;
+    p->new_b = new_b;
+    p->new_psi = new_psi;
+    p->h = h;
+    p->prm = prm;
+    p->rec = rec;
+    p->ws = ws;
+    p->A = paces_basis{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap};
+    p->B = paces_basis{at<uint64_t>(ws, l.keysB), at<int32_t>(ws, l.blkB), l.cap};
+    p->cur = (prm->enlarge_steps & 1) ? &p->B : &p->A;
+    p->target = prm->evolve ? at<void>(ws, l.v_V) : new_psi;
+    return PACES_OK;
+}
+
+// Kernels one step enqueues (merge: 5, +1 with the neighbour table; truncation: 18, +14
+// with tie shuffling; remap 3; observables 2 or 3; Taylor 1; renormalisation 3; record 2).
+unsigned long long step_launches(const paces_step_params& prm, bool with_taylor) {
+    return 2 + (prm.shuffle ? 32 : 18) + 5ull * prm.enlarge_steps + 6 + 3 + (prm.diagnostics ? 2 : 0) +
+           (prm.evolve ? (with_taylor ? 1 : 0) + (prm.renormalize ? 3 : 0) : 0) + 3;
+}
+
+// Record, truncation, enlargement, new basis + H, remap, post-adaptation diagnostics.
+int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
+    const bool c64 = c->precision == PACES_C64;
+    const paces_step_params* prm = p.prm;
+    paces_step_record* rec = p.rec;
+    int* status = &rec->status;
+    void* ws = p.ws;
+    const Layout& l = p.l;
+    auto mark = [&](int i) {
+        if (marks && c->profiling) cudaEventRecord(c->ev[i], st);
+    };
+    record_init_kernel<<<1, 32, 0, st>>>(rec, prm->diagnostics);
+    mark(0);
+    // 1. truncation of the old state
+    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, prm->maxstates,
+                                          prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), p.A.keys,
+                                          p.A.blk, p.A.cap, &rec->n_tied, status, c->num_sms, st),
+                       "step/truncate");
+    mark(1);
+    // 2. enlargement (enlarge_steps times)
+    const MergeWs mws = merge_ws(l, ws);
+    paces_basis* cur = &p.A;
+    paces_basis* other = &p.B;
+    for (int e = 0; e < prm->enlarge_steps; ++e) {
+        MergeOut mo{};
+        mo.keys = other->keys;
+        mo.blk = other->blk;
+        mo.cap = other->cap;
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->m, cur->keys, cur->blk, mws, mo, nullptr, status,
+                                           c->num_sms, st),
+                           "step/expand");
+        paces_basis* t = cur;
+        cur = other;
+        other = t;
+    }
+    mark(2);
+    // 3. new basis + H
+    {
+        MergeOut mo{};
+        mo.keys = p.new_b->keys;
+        mo.blk = p.new_b->blk;
+        mo.cap = p.new_b->cap < p.h->cap ? p.new_b->cap : p.h->cap;
+        mo.meta = p.h->meta;
+        mo.nbr = p.h->nbr;
+        mo.nbr_cap = p.h->cap;
+        mo.maps = at<int>(ws, l.maps);
+        mo.map_cap = l.cap;
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->m, cur->keys, cur->blk, mws, mo, &rec->ceiling_hits,
+                                           status, c->num_sms, st),
+                           "step/assemble");
+    }
+    mark(3);
+    // 4. amplitudes into the new basis
+    PACES_CHECK_LAUNCH(c, launch_remap(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, p.new_b->keys,
+                                       p.new_b->blk, p.target, remap_ws(l, ws), status, c->num_sms, st),
+                       "step/remap");
+    mark(4);
+    // 5. post-adaptation diagnostics
+    if (prm->diagnostics) {
+        ObsTarget t{&rec->post_adapt_norm, &rec->post_adapt_energy_re, &rec->post_adapt_energy_im, nullptr, nullptr};
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
+                                                 p.h->meta, p.target, PACES_OBS_NORM | PACES_OBS_ENERGY,
+                                                 at<double>(ws, l.o_partials), t, c->num_sms, st),
+                           "step/diagnostics");
+    }
+    mark(5);
+    return PACES_OK;
+}
+
+// Renormalisation, observables of the new state, sizes into the record.
+int step_back(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
+    const bool c64 = c->precision == PACES_C64;
+    const paces_step_params* prm = p.prm;
+    paces_step_record* rec = p.rec;
+    double* opart = at<double>(p.ws, p.l.o_partials);
+    auto mark = [&](int i) {
+        if (marks && c->profiling) cudaEventRecord(c->ev[i], st);
+    };
+    if (prm->evolve && prm->renormalize) {
+        ObsTarget t{&rec->norm, nullptr, nullptr, nullptr, nullptr};
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
+                                                 p.h->meta, p.new_psi, PACES_OBS_NORM, opart, t, c->num_sms, st),
+                           "step/norm");
+        PACES_CHECK_LAUNCH(c, launch_scale(c64, c->m, p.new_b->blk, p.new_psi, &rec->norm, c->num_sms, st),
+                           "step/renormalize");
+    }
+    mark(6);
+    // 7. observables of the new state
+    {
+        ObsTarget t{&rec->norm, &rec->energy_re, &rec->energy_im, rec->n_exc, rec->n_pho};
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
+                                                 p.h->meta, p.new_psi,
+                                                 PACES_OBS_NORM | PACES_OBS_ENERGY | PACES_OBS_SITES, opart, t,
+                                                 c->num_sms, st),
+                           "step/observables");
+    }
+    record_counts_kernel<<<1, 32, 0, st>>>(rec, p.A.blk, p.cur->blk, p.new_b->blk, c->m.L);
+    mark(7);
+    if (cudaGetLastError() != cudaSuccess) return cuda_fail(c, "step/record");
+    return PACES_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -267,9 +440,32 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
         return PACES_ERR_CUDA;
     }
     c->taylor_grid = taylor_max_grid(c->precision == PACES_C64, c->num_sms);
-    if (cudaMalloc(&c->d_status, 64) != cudaSuccess || cudaMemset(c->d_status, 0, 64) != cudaSuccess) {
-        delete c;
-        return PACES_ERR_CUDA;
+    // constants block: status words, per-site energies and the sqrt(k) * g tables
+    {
+        const size_t o_eps = 64, o_sq = o_eps + kMaxSites * 8, o_sqf = o_sq + kSqrtTable * 8;
+        const size_t bytes = o_sqf + kSqrtTable * 4;
+        alignas(8) unsigned char host[o_sqf + kSqrtTable * 4];
+        std::memset(host, 0, sizeof(host));
+        double* eps = reinterpret_cast<double*>(host + o_eps);
+        double* sq = reinterpret_cast<double*>(host + o_sq);
+        float* sqf = reinterpret_cast<float*>(host + o_sqf);
+        for (int s = 0; s < L; ++s) eps[s] = m.site_eps[s];
+        // IEEE sqrt and product, rounded to nearest: the values the kernels compute themselves
+        for (int k = 0; k < kSqrtTable; ++k) {
+            sq[k] = std::sqrt(double(k)) * m.g;
+            sqf[k] = float(sq[k]);
+        }
+        void* d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess || cudaMemcpy(d, host, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            if (d) cudaFree(d);
+            delete c;
+            return PACES_ERR_CUDA;
+        }
+        unsigned char* base = static_cast<unsigned char*>(d);
+        c->d_status = reinterpret_cast<int*>(base);
+        c->d_site_eps = reinterpret_cast<double*>(base + o_eps);
+        c->d_sq = reinterpret_cast<double*>(base + o_sq);
+        c->d_sqf = reinterpret_cast<float*>(base + o_sqf);
     }
     *out = c;
     return PACES_OK;
@@ -500,112 +696,177 @@ int paces_lookup(paces_ctx* c, const paces_basis* pb, const uint64_t* q_keys, co
 int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces_basis* new_b, void* new_psi,
                paces_hmat* h, const paces_step_params* prm, paces_step_record* rec, void* ws, size_t ws_bytes,
                paces_stream_t stream) {
-    if (!c || !valid_basis(old_b) || !valid_basis(new_b) || !old_psi || !new_psi || !h || !h->nbr || !h->meta ||
-        !prm || !rec || !ws)
-        return fail(c, PACES_ERR_BADARG, "paces_step: null argument");
-    if (prm->maxstates < 1 || prm->enlarge_steps < 0 || (prm->evolve && prm->m_star < 1))
-        return fail(c, PACES_ERR_BADARG, "paces_step: bad parameters");
-    const Layout l = fit_layout(c, ws_bytes);
-    if (old_b->cap > l.cap || new_b->cap > l.cap || h->cap > l.cap)
-        return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states; bases hold %lld/%lld", (long long)l.cap,
-                    (long long)old_b->cap, (long long)new_b->cap);
+    StepPlan p;
+    const int rc = plan_step(c, old_b, old_psi, new_b, new_psi, h, prm, rec, ws, ws_bytes, &p);
+    if (rc != PACES_OK) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const bool c64 = c->precision == PACES_C64;
-    const int L = c->m.L;
-    int* status = &rec->status;
-    auto mark = [&](int i) {
-        if (c->profiling) cudaEventRecord(c->ev[i], st);
-    };
-    // kernels issued by this step (merge: 5, +1 with the neighbour table; truncation: 18,
-    // +14 with tie shuffling; remap 2; observables 2; Taylor 1; renormalisation 3; record 2)
-    c->launches += 2 + (prm->shuffle ? 32 : 18) + 5ull * prm->enlarge_steps + 6 + 3 + (prm->diagnostics ? 2 : 0) +
-                   (prm->evolve ? 1 + (prm->renormalize ? 3 : 0) : 0) + 3;
-    record_init_kernel<<<1, 32, 0, st>>>(rec, prm->diagnostics);
-    mark(0);
-
-    paces_basis A{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap};
-    paces_basis B{at<uint64_t>(ws, l.keysB), at<int32_t>(ws, l.blkB), l.cap};
-    // 1. truncation of the old state
-    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, old_b->keys, old_b->blk, old_psi, prm->maxstates,
-                                          prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), A.keys,
-                                          A.blk, A.cap, &rec->n_tied, status, c->num_sms, st),
-                       "step/truncate");
-    mark(1);
-    // 2. enlargement (enlarge_steps times)
-    const MergeWs mws = merge_ws(l, ws);
-    paces_basis* cur = &A;
-    paces_basis* other = &B;
-    for (int e = 0; e < prm->enlarge_steps; ++e) {
-        MergeOut mo{};
-        mo.keys = other->keys;
-        mo.blk = other->blk;
-        mo.cap = other->cap;
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->m, cur->keys, cur->blk, mws, mo, nullptr, status,
-                                           c->num_sms, st),
-                           "step/expand");
-        paces_basis* t = cur;
-        cur = other;
-        other = t;
-    }
-    mark(2);
-    // 3. new basis + H
-    {
-        MergeOut mo{};
-        mo.keys = new_b->keys;
-        mo.blk = new_b->blk;
-        mo.cap = new_b->cap < h->cap ? new_b->cap : h->cap;
-        mo.meta = h->meta;
-        mo.nbr = h->nbr;
-        mo.nbr_cap = h->cap;
-        mo.maps = at<int>(ws, l.maps);
-        mo.map_cap = l.cap;
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->m, cur->keys, cur->blk, mws, mo, &rec->ceiling_hits,
-                                           status, c->num_sms, st),
-                           "step/assemble");
-    }
-    mark(3);
-    // 4. amplitudes into the new basis
-    void* target = prm->evolve ? at<void>(ws, l.v_V) : new_psi;
-    PACES_CHECK_LAUNCH(c, launch_remap(c->nw, c64, c->m, old_b->keys, old_b->blk, old_psi, new_b->keys, new_b->blk,
-                                       target, remap_ws(l, ws), status, c->num_sms, st),
-                       "step/remap");
-    mark(4);
-    double* opart = at<double>(ws, l.o_partials);
-    // 5. post-adaptation diagnostics
-    if (prm->diagnostics) {
-        ObsTarget t{&rec->post_adapt_norm, &rec->post_adapt_energy_re, &rec->post_adapt_energy_im, nullptr, nullptr};
-        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, new_b->keys, new_b->blk, h->nbr, h->cap, h->meta,
-                                                 target, PACES_OBS_NORM | PACES_OBS_ENERGY, opart, t, c->num_sms, st),
-                           "step/diagnostics");
-    }
-    mark(5);
-    // 6. propagation
+    c->launches += step_launches(*prm, true);
+    int r = step_front(c, p, st, true);
+    if (r != PACES_OK) return r;
     if (prm->evolve) {
         TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
-        PACES_CHECK_LAUNCH(c, launch_taylor(c64, c->m, new_b->blk, h->nbr, h->cap, h->meta, target, new_psi, prm->dt,
-                                            prm->m_star, prm->tol, taylor_ws(l, ws), o, status, c->num_sms, st),
+        PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, new_b->blk, h->nbr, h->cap, h->meta,
+                                            p.target, new_psi, prm->dt, prm->m_star, prm->tol, taylor_ws(p.l, ws), o,
+                                            &rec->status, c->num_sms, st),
                            "step/taylor");
-        if (prm->renormalize) {
-            ObsTarget t{&rec->norm, nullptr, nullptr, nullptr, nullptr};
-            PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, new_b->keys, new_b->blk, h->nbr, h->cap, h->meta,
-                                                     new_psi, PACES_OBS_NORM, opart, t, c->num_sms, st),
-                               "step/norm");
-            PACES_CHECK_LAUNCH(c, launch_scale(c64, c->m, new_b->blk, new_psi, &rec->norm, c->num_sms, st),
-                               "step/renormalize");
+    }
+    return step_back(c, p, st, true);
+}
+
+
+// ---- batched trajectories ------------------------------------------------------------------
+int paces_batch_create(int32_t max_items, int32_t n_streams, paces_batch** out) {
+    if (!out) return PACES_ERR_BADARG;
+    *out = nullptr;
+    if (max_items < 1 || max_items > kMaxBatch || n_streams < 1 || n_streams > 64) return PACES_ERR_BADARG;
+    paces_batch* b = new paces_batch();
+    b->max_items = max_items;
+    b->n_streams = n_streams;
+    b->streams = new cudaStream_t[n_streams]();
+    b->join = new cudaEvent_t[n_streams]();
+    b->desc = new TaylorBatch();
+    bool ok = cudaGetDevice(&b->device) == cudaSuccess &&
+              cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaMalloc(&b->d_ws, kTaylorBatchWsBytes) == cudaSuccess;
+    for (int k = 0; ok && k < n_streams; ++k)
+        ok = cudaStreamCreateWithFlags(&b->streams[k], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        paces_batch_destroy(b);
+        return PACES_ERR_CUDA;
+    }
+    *out = b;
+    return PACES_OK;
+}
+
+int paces_batch_destroy(paces_batch* b) {
+    if (!b) return PACES_OK;
+    for (int k = 0; k < b->n_streams; ++k) {
+        if (b->streams && b->streams[k]) cudaStreamDestroy(b->streams[k]);
+        if (b->join && b->join[k]) cudaEventDestroy(b->join[k]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->d_ws) cudaFree(b->d_ws);
+    delete[] b->streams;
+    delete[] b->join;
+    delete b->desc;
+    delete b;
+    return PACES_OK;
+}
+
+const char* paces_batch_last_error(const paces_batch* b) { return b ? b->err : "no batch"; }
+
+unsigned long long paces_batch_kernel_launches(const paces_batch* b) { return b ? b->launches : 0ull; }
+
+int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, paces_stream_t stream) {
+    if (!b) return PACES_ERR_BADARG;
+    auto bfail = [&](int code, const char* fmt, ...) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(b->err, sizeof(b->err), fmt, ap);
+        va_end(ap);
+        return code;
+    };
+    if (!items || n < 1 || n > b->max_items) return bfail(PACES_ERR_BADARG, "paces_batch_step: %d items (max %d)", n, b->max_items);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int precision = items[0].ctx ? items[0].ctx->precision : -1;
+    StepPlan* plans = new StepPlan[n];
+    struct Cleanup {
+        StepPlan* p;
+        ~Cleanup() { delete[] p; }
+    } cleanup{plans};
+    unsigned long long launches = 0;
+    int n_evolve = 0;
+    for (int i = 0; i < n; ++i) {
+        const paces_batch_item& it = items[i];
+        if (!it.ctx) return bfail(PACES_ERR_BADARG, "item %d: no context", i);
+        if (it.ctx->precision != precision) return bfail(PACES_ERR_BADARG, "item %d: mixed precisions in one batch", i);
+        if (it.ctx->device != b->device) return bfail(PACES_ERR_BADARG, "item %d: context on another device", i);
+        const int rc = plan_step(it.ctx, it.old_basis, it.old_psi, it.new_basis, it.new_psi, it.h, it.params,
+                                 it.record, it.workspace, it.workspace_bytes, &plans[i]);
+        if (rc != PACES_OK) return bfail(rc, "item %d: %s", i, it.ctx->err);
+        launches += step_launches(*it.params, false);
+        n_evolve += it.params->evolve ? 1 : 0;
+    }
+    auto fork = [&]() -> bool {
+        if (cudaEventRecord(b->fork, st) != cudaSuccess) return false;
+        for (int k = 0; k < b->n_streams; ++k)
+            if (cudaStreamWaitEvent(b->streams[k], b->fork, 0) != cudaSuccess) return false;
+        return true;
+    };
+    auto join = [&]() -> bool {
+        for (int k = 0; k < b->n_streams; ++k)
+            if (cudaEventRecord(b->join[k], b->streams[k]) != cudaSuccess ||
+                cudaStreamWaitEvent(st, b->join[k], 0) != cudaSuccess)
+                return false;
+        return true;
+    };
+    // 1. every trajectory's truncation, enlargement, assembly, remap and diagnostics,
+    //    spread over the batch's streams
+    if (!fork()) return bfail(PACES_ERR_CUDA, "fork: %s", cudaGetErrorString(cudaGetLastError()));
+    for (int i = 0; i < n; ++i) {
+        const int rc = step_front(items[i].ctx, plans[i], b->streams[i % b->n_streams], false);
+        if (rc != PACES_OK) {
+            join();
+            return bfail(rc, "item %d: %s", i, items[i].ctx->err);
         }
     }
-    mark(6);
-    // 7. observables of the new state
-    {
-        ObsTarget t{&rec->norm, &rec->energy_re, &rec->energy_im, rec->n_exc, rec->n_pho};
-        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, new_b->keys, new_b->blk, h->nbr, h->cap, h->meta,
-                                                 new_psi, PACES_OBS_NORM | PACES_OBS_ENERGY | PACES_OBS_SITES, opart, t,
-                                                 c->num_sms, st),
-                           "step/observables");
+    if (!join()) return bfail(PACES_ERR_CUDA, "join: %s", cudaGetErrorString(cudaGetLastError()));
+    // 2. one persistent launch for every trajectory's Taylor series
+    if (n_evolve > 0) {
+        TaylorBatch& bt = *b->desc;
+        bt.n = 0;
+        bt.max_m_star = 0;
+        for (int i = 0; i < n; ++i) {
+            const paces_step_params* prm = items[i].params;
+            if (!prm->evolve) continue;
+            paces_ctx* c = items[i].ctx;
+            const StepPlan& p = plans[i];
+            const TaylorWs tw = taylor_ws(p.l, p.ws);
+            TaylorItem& ti = bt.items[bt.n++];
+            ti.blk = p.new_b->blk;
+            ti.nbr = p.h->nbr;
+            ti.meta = p.h->meta;
+            ti.v_in = p.target;
+            ti.res = p.new_psi;
+            ti.ta = tw.ta;
+            ti.tb = tw.tb;
+            ti.site_eps = c->d_site_eps;
+            ti.sq = c->d_sq;
+            ti.sqf = c->d_sqf;
+            ti.status = &p.rec->status;
+            ti.out = TaylorOut{&p.rec->converged, &p.rec->final_m, &p.rec->c1_plus_c2, &p.rec->term_ratio};
+            ti.dt = prm->dt;
+            ti.tol = prm->tol;
+            ti.eps_sys = c->m.eps_sys;
+            ti.hbar_omega = c->m.hbar_omega;
+            ti.delta_eps = c->m.delta_eps;
+            ti.J = c->m.J;
+            ti.L = c->m.L;
+            ti.has_site_eps = c->m.has_site_eps;
+            ti.m_star = prm->m_star;
+            ti.pad = 0;
+            if (prm->m_star > bt.max_m_star) bt.max_m_star = prm->m_star;
+        }
+        TaylorBatchWs tws;
+        tws.barrier = static_cast<unsigned*>(b->d_ws);
+        tws.maxima = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(b->d_ws) + 256);
+        if (launch_taylor_batch(precision == PACES_C64, bt, tws, b->num_sms, st) != PACES_OK)
+            return bfail(PACES_ERR_CUDA, "batched Taylor: %s", cudaGetErrorString(cudaGetLastError()));
+        launches += 1;
     }
-    record_counts_kernel<<<1, 32, 0, st>>>(rec, A.blk, cur->blk, new_b->blk, L);
-    mark(7);
-    if (cudaGetLastError() != cudaSuccess) return cuda_fail(c, "step/record");
+    // 3. renormalisation, observables and records, again spread over the streams
+    if (!fork()) return bfail(PACES_ERR_CUDA, "fork: %s", cudaGetErrorString(cudaGetLastError()));
+    for (int i = 0; i < n; ++i) {
+        const int rc = step_back(items[i].ctx, plans[i], b->streams[i % b->n_streams], false);
+        if (rc != PACES_OK) {
+            join();
+            return bfail(rc, "item %d: %s", i, items[i].ctx->err);
+        }
+    }
+    if (!join()) return bfail(PACES_ERR_CUDA, "join: %s", cudaGetErrorString(cudaGetLastError()));
+    b->launches += launches;
     return PACES_OK;
 }
 

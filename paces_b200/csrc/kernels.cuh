@@ -54,6 +54,42 @@ int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, i
                   double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
                   cudaStream_t st);
 
+// ---- batched Taylor: many trajectories in one persistent launch ---------------------------
+constexpr int kMaxBatch = 128;  // trajectories per launch (the descriptors travel as kernel parameters)
+constexpr int kSqrtTable = 260; // sqrt(k) * g for k < 260 (occupations up to 255, plus one)
+// One trajectory of a batched Taylor launch: its H (neighbour table + metadata), vectors,
+// model constants and where its results go.  Field names follow ModelDev so the row
+// helpers take either.
+struct TaylorItem {
+    const int* blk;            // [L+1]; blk[L] = rows
+    const int* nbr;            // [rows][4]
+    const uint32_t* meta;      // [rows]
+    const void* v_in;          // input state
+    void* res;                 // output state
+    void* ta;                  // term buffers [cap]
+    void* tb;
+    const double* site_eps;    // [L] device (read when has_site_eps)
+    const double* sq;          // [kSqrtTable] sqrt(k) * g, fp64
+    const float* sqf;          // [kSqrtTable] the same rounded to fp32
+    int* status;               // the trajectory's status word
+    TaylorOut out;
+    double dt, tol, eps_sys, hbar_omega, delta_eps, J;
+    int L, has_site_eps, m_star, pad;
+};
+struct TaylorBatch {
+    TaylorItem items[kMaxBatch];
+    int n;
+    int max_m_star;
+};
+struct TaylorBatchWs {
+    unsigned* barrier;             // [2]
+    unsigned long long* maxima;    // [3][kMaxBatch][4] per-term maxima (fp64 bit patterns)
+};
+constexpr size_t kTaylorBatchWsBytes = 256 + size_t(3) * kMaxBatch * 4 * 8;
+int taylor_batch_max_grid(bool c64, int num_sms);
+int launch_taylor_batch(bool c64, const TaylorBatch& bt, const TaylorBatchWs& ws, int num_sms,
+                        cudaStream_t st);
+
 // ---- observables --------------------------------------------------------------------------
 struct ObsTarget {
     double* norm;        // may be null

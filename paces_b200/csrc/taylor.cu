@@ -11,6 +11,7 @@
 // neighbour indices of consecutive rows are monotone (images of a sorted block are
 // sorted), so the four gathers stream through L2.  complex128 rounds every operation
 // like the reference; complex64 uses fp32 FMA with fp64 stop arithmetic.
+#include "grid.cuh"
 #include "hrow.cuh"
 #include "kernels.cuh"
 
@@ -20,36 +21,6 @@ namespace {
 
 constexpr int kTThreads = 256;
 constexpr int kTWarps = kTThreads / 32;
-
-// Bounded grid-wide barrier (all blocks are co-resident: cooperative launch).
-__device__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen, int* status) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        s_ok = 1;
-        __threadfence();
-        const unsigned arrived = atomicAdd(&bar[0], 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&bar[0], 0u);
-            __threadfence();
-            atomicAdd(&bar[1], 1u);
-        } else {
-            const uint64_t t0 = global_ns();
-            while (atomicAdd(&bar[1], 0u) == gen) {
-                if (global_ns() - t0 > kWaitLimitNs) {
-                    raise_status(status, PACES_ERR_TIMEOUT);
-                    s_ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        ++gen;
-        __threadfence();
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
 
 // max-reduce four values over the block; result in out[0..3] (shared), valid after return.
 __device__ void block_max4(double v[4], double (*red)[kTWarps], double* out) {
@@ -195,17 +166,19 @@ int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, i
     if (m_star < 1) return PACES_ERR_BADARG;
     if (cudaMemsetAsync(ws.barrier, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return PACES_ERR_CUDA;
     const int grid = taylor_max_grid(c64, num_sms);
-    ModelDev mm = m;
-    TaylorWs w = ws;
-    TaylorOut o = out;
-    int64_t cap = nbr_cap;
-    void* args[] = {&mm, (void*)&blk, (void*)&nbr, &cap, (void*)&meta, (void*)&v_in, &res, &w,
-                    &dt, &m_star, &tol, &o, &status};
-    cudaError_t e;
-    if (c64)
-        e = cudaLaunchCooperativeKernel((const void*)taylor_kernel<true>, dim3(grid), dim3(kTThreads), args, 0, st);
-    else
-        e = cudaLaunchCooperativeKernel((const void*)taylor_kernel<false>, dim3(grid), dim3(kTThreads), args, 0, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kTThreads);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int64_t cap = nbr_cap;
+    const cudaError_t e =
+        c64 ? cudaLaunchKernelEx(&cfg, taylor_kernel<true>, m, blk, nbr, cap, meta, v_in, res, ws, dt, m_star, tol, out, status)
+            : cudaLaunchKernelEx(&cfg, taylor_kernel<false>, m, blk, nbr, cap, meta, v_in, res, ws, dt, m_star, tol, out, status);
     return e == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 

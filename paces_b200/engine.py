@@ -302,10 +302,15 @@ class Trajectory:
     Two basis/amplitude slots alternate: a step reads the current slot and writes the
     other, so a capacity overflow leaves the state intact and the step is retried with
     larger buffers.
+
+    With `graph=True` the evolving steps replay CUDA graphs (one per slot parity and dt)
+    captured from `paces_step`, so a step costs one graph launch and one 2 KB record read.
+    Tie shuffling hashes the step index into the kernels' arguments and is stepped without
+    graphs.  Growing the buffers drops the graphs; the next step captures them again.
     """
 
     def __init__(self, eng: Engine, maxstates, enlarge_steps, m_star=100, diagnostics=True,
-                 shuffle_seed=None, renormalize=False, explosion_cutoff=2.0, cap=None):
+                 shuffle_seed=None, renormalize=False, explosion_cutoff=2.0, cap=None, graph=False):
         self.eng = eng
         self.maxstates = int(maxstates)
         self.enlarge_steps = int(enlarge_steps)
@@ -320,6 +325,8 @@ class Trajectory:
         self.cur = 0
         self.step_index = 0
         self.last = None
+        self.use_graph = bool(graph)
+        self._graphs = {}
 
     def _alloc(self):
         e = self.eng
@@ -330,6 +337,7 @@ class Trajectory:
     def _regrow(self, factor=1.6):
         """Grow every buffer, keeping the current state."""
         e = self.eng
+        self._graphs = {}
         old_b, old_psi = self.bases[self.cur], self.psis[self.cur]
         n = old_b.count()
         e._grow(int(e.cap * factor))
@@ -375,8 +383,40 @@ class Trajectory:
         p.explosion_cutoff = self.explosion_cutoff
         return p
 
+    def _capture(self, dt):
+        """CUDA graph of one evolving paces_step from the current slot into the other."""
+        nxt = 1 - self.cur
+        prm = self.params(True, dt)
+        dev = self.eng.device
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(dev)
+        torch.cuda.synchronize(dev)
+        with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+            self.eng.step(self.bases[self.cur], self.psis[self.cur], self.bases[nxt], self.psis[nxt], self.h, prm,
+                          sync=False)
+        return g, prm
+
+    def _graph_step(self, dt):
+        key = (self.cur, float(dt))
+        if key not in self._graphs:
+            self._graphs[key] = self._capture(dt)
+        self._graphs[key][0].replay()
+        rec = self.eng.read_record()
+        if rec.status == nat.ERR_CAPACITY:
+            return None
+        if rec.status != nat.PACES_OK:
+            raise nat.PacesError(rec.status, "paces_step")
+        self.cur = 1 - self.cur
+        self.step_index += 1
+        self.last = rec
+        return rec
+
     def step(self, evolve=True, dt=0.0):
         """One time step (first step: evolve=False).  Returns the step record."""
+        if self.use_graph and evolve and self.shuffle_seed is None:
+            rec = self._graph_step(dt)
+            if rec is not None:
+                return rec
         nxt = 1 - self.cur
         for _ in range(12):
             rec = self.eng.step(self.bases[self.cur], self.psis[self.cur], self.bases[nxt], self.psis[nxt],
@@ -391,3 +431,120 @@ class Trajectory:
         self.step_index += 1
         self.last = rec
         return rec
+
+
+class TrajectoryBatch:
+    """Independent trajectories (each its own Engine: model, key width, dt, maxstates)
+    advanced together by `paces_batch_step`: their stages run concurrently on the batch's
+    streams and all their Taylor series in one persistent launch.  With `graph=True` each
+    batch step replays a CUDA graph (one per slot parity and dt).  A capacity overflow in
+    any trajectory grows that trajectory's buffers and repeats the batch step (inputs are
+    read only, so the repeat is exact).
+    """
+
+    def __init__(self, trajs: list, n_streams=8, graph=False):
+        if not trajs or len(trajs) > nat.MAX_BATCH:
+            raise ValueError(f"a batch holds 1..{nat.MAX_BATCH} trajectories")
+        devs = {t.eng.device for t in trajs}
+        precs = {t.eng.c64 for t in trajs}
+        if len(devs) != 1 or len(precs) != 1:
+            raise ValueError("all trajectories of a batch share one device and one precision")
+        self.trajs = list(trajs)
+        self.device = trajs[0].eng.device
+        self.lib = nat.load()
+        self.use_graph = bool(graph)
+        self._graphs = {}
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            nat.check(self.lib.paces_batch_create(len(trajs), int(n_streams), ctypes.byref(h)), None, "batch_create")
+        self.handle = h
+        self.rec_host = torch.zeros((len(trajs), ctypes.sizeof(nat.StepRecord)), dtype=torch.uint8).pin_memory()
+
+    def _dts(self, dt):
+        if isinstance(dt, (int, float)):
+            return (float(dt),) * len(self.trajs)
+        dts = tuple(float(x) for x in dt)
+        if len(dts) != len(self.trajs):
+            raise ValueError("one dt per trajectory")
+        return dts
+
+    def _items(self, evolve, dts):
+        """C item array for the current slots; the ctypes objects it points to are kept."""
+        keep, arr = [], (nat.BatchItem * len(self.trajs))()
+        for i, t in enumerate(self.trajs):
+            nxt = 1 - t.cur
+            ob, nb, hm = t.bases[t.cur].c(), t.bases[nxt].c(), t.h.c()
+            prm = t.params(evolve, dts[i])
+            ws, nbytes = t.eng.workspace()
+            keep += [ob, nb, hm, prm]
+            arr[i] = nat.BatchItem(t.eng.ctx, ctypes.pointer(ob), _ptr(t.psis[t.cur]), ctypes.pointer(nb),
+                                   _ptr(t.psis[nxt]), ctypes.pointer(hm), ctypes.pointer(prm), _ptr(t.eng.rec_dev),
+                                   ws, nbytes)
+        return arr, keep
+
+    def _launch(self, evolve, dts):
+        arr, keep = self._items(evolve, dts)
+        rc = self.lib.paces_batch_step(self.handle, arr, len(self.trajs), _stream(self.device))
+        if rc != nat.PACES_OK:
+            raise nat.PacesError(rc, self.lib.paces_batch_last_error(self.handle).decode(errors="replace"))
+        return keep
+
+    def _capture(self, dts):
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(self.device)
+        torch.cuda.synchronize(self.device)
+        with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+            keep = self._launch(True, dts)
+        return g, keep
+
+    def read_records(self):
+        for i, t in enumerate(self.trajs):
+            self.rec_host[i].copy_(t.eng.rec_dev, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        raw = self.rec_host.numpy()
+        return [nat.StepRecord.from_buffer_copy(raw[i].tobytes()) for i in range(len(self.trajs))]
+
+    def kernel_launches(self):
+        return int(self.lib.paces_batch_kernel_launches(self.handle))
+
+    def step(self, evolve=True, dt=0.0):
+        """One time step of every trajectory (dt: one value, or one per trajectory);
+        returns their records."""
+        dts = self._dts(dt)
+        graphed = self.use_graph and evolve and all(t.shuffle_seed is None for t in self.trajs)
+        for _ in range(12):
+            if graphed:
+                key = (tuple(t.cur for t in self.trajs), dts)
+                if key not in self._graphs:
+                    self._graphs[key] = self._capture(dts)
+                self._graphs[key][0].replay()
+            else:
+                self._launch(evolve, dts)
+            recs = self.read_records()
+            grow = [i for i, r in enumerate(recs) if r.status == nat.ERR_CAPACITY]
+            if grow:
+                for i in grow:
+                    self.trajs[i]._regrow()
+                self._graphs = {}
+                continue
+            break
+        for i, r in enumerate(recs):
+            if r.status != nat.PACES_OK:
+                raise nat.PacesError(r.status, f"batch item {i}")
+        for t, r in zip(self.trajs, recs):
+            t.cur = 1 - t.cur
+            t.step_index += 1
+            t.last = r
+        return recs
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._graphs = {}
+            self.lib.paces_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -7,9 +7,10 @@ import scipy.sparse as sp
 from paces_b200.engine import Engine, ModelParams
 
 
-def engine_for(nchain, dim, g, cap=1 << 16, precision="c128", periodic=False, site_eps=None, J=1.0):
+def engine_for(nchain, dim, g, cap=1 << 16, precision="c128", periodic=False, site_eps=None, J=1.0,
+               hbar_omega=1.0):
     return Engine(ModelParams(nchain=nchain, max_ho_dims=[dim] * nchain, J=J, g=g, periodic=periodic,
-                              site_eps=site_eps, precision=precision), cap=cap)
+                              site_eps=site_eps, precision=precision, hbar_omega=hbar_omega), cap=cap)
 
 
 def ref_rows(eng, basis):
@@ -56,14 +57,14 @@ def initial_rows(nchain, dim=16, initpos=0):
     return layout.pack_rows(raw, layout.bitwidths_for([nchain] + [dim] * nchain))
 
 
-def grown_trajectory(eng, nchain, maxstates, es=1, initpos=0, dim=16):
+def grown_trajectory(eng, nchain, maxstates, es=1, initpos=0, dim=16, graph=False):
     """A trajectory on grow_optimal_basis(fillfac=1) with the exciton on `initpos` in the
     phonon vacuum, after its first (non-evolving) step
     (paces/core/time_evolution.py:290-323, :325-363)."""
     import torch
     from paces_b200.engine import Trajectory
     rows = initial_rows(nchain, dim, initpos)
-    tr = Trajectory(eng, maxstates, es)
+    tr = Trajectory(eng, maxstates, es, graph=graph)
     b = eng.basis_from_ref(rows)
     while True:
         nxt = eng.expand(b)
