@@ -52,6 +52,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
+                    help="plain: one N=32 chain at maxstates 2^22; batched: 64 trajectories drawn from --seed")
+    ap.add_argument("--no-graph", action="store_true", help="step without CUDA-graph replay")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--batch", type=int, default=64, help="trajectories of the batched workload")
+    ap.add_argument("--seed", type=int, default=0, help="seed of the batched workload's draws")
+    ap.add_argument("--streams", type=int, default=8, help="streams of the batched step")
     return ap.parse_args()
 
 
@@ -140,29 +147,32 @@ def initial_rows(nchain, initpos=0):
     return layout.pack_rows(raw, layout.bitwidths_for([nchain] + [16] * nchain))
 
 
-def prepare(a, eng, maxstates):
-    """Grow the basis (grow_optimal_basis, fillfac=1), first step, then propagate until the
-    truncation keeps exactly maxstates states; returns the saturated trajectory."""
+def start_trajectory(eng, nchain, maxstates, es, initpos=0, graph=False):
+    """grow_optimal_basis(fillfac=1) around the exciton on `initpos` in the phonon vacuum,
+    amplitude 1 on that state, then the first (non-evolving) step."""
     import torch
     from paces_b200.engine import Trajectory
-    tr = Trajectory(eng, maxstates, a.enlarge_steps)
-    b = eng.basis_from_ref(initial_rows(a.nchain))
-    prev = b
+    tr = Trajectory(eng, maxstates, es, graph=graph)
+    rows = initial_rows(nchain, initpos)
+    b = eng.basis_from_ref(rows)
     while True:
-        nxt = eng.expand(prev)
-        if nxt.count() > maxstates:
+        nxt = eng.expand(b)
+        if nxt.count() > maxstates or nxt.count() == 0:
             break
-        b, prev = nxt, nxt
-        if nxt.count() == 0:
-            break
-    init = eng.basis_from_ref(initial_rows(a.nchain))
-    keys, pos, n = eng.query_from_ref(initial_rows(a.nchain))
+        b = nxt
+    keys, pos, n = eng.query_from_ref(rows)
     idx = int(eng.lookup(b, keys, pos, n, must_exist=True)[0].item())
     psi = torch.zeros(max(b.count(), 1), dtype=eng.cdtype, device=eng.device)
     psi[idx] = 1.0
-    del init
     tr.set_state(b, psi)
-    rec = tr.step(evolve=False)
+    tr.step(evolve=False)
+    return tr
+
+
+def prepare(a, eng, maxstates):
+    """Grow the basis (grow_optimal_basis, fillfac=1), first step, then propagate until the
+    truncation keeps exactly maxstates states; returns the saturated trajectory."""
+    tr = start_trajectory(eng, a.nchain, maxstates, a.enlarge_steps, graph=not a.no_graph)
     nprep = 1
     while True:
         rec = tr.step(evolve=True, dt=a.dt)
@@ -299,9 +309,13 @@ def run_ours(a):
     eng = Engine(model_params(a, a.precision), device=f"cuda:{local}")
     cs = 8 if a.precision == "c64" else 16
     tr, nprep = prepare(a, eng, a.maxstates)
+    tuning = None
+    if not a.no_tune:
+        from paces_b200 import autotune
+        tuning = autotune.tune(tr, a.dt)
+        log(a, f"tuning: {tuning}")
     for _ in range(max(a.warmup, 0)):
         tr.step(evolve=True, dt=a.dt)
-    eng.set_profiling(True)
 
     def barrier():
         torch.cuda.synchronize()
@@ -309,9 +323,8 @@ def run_ours(a):
             dist.barrier()
         torch.cuda.synchronize()
 
-    stage_sum = {s: 0.0 for s in nat.STAGES}
+    # timed region: K steps, each replaying the step's CUDA graph and reading its record
     recs = []
-    launches0 = eng.kernel_launches()
     barrier()
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -319,15 +332,28 @@ def run_ours(a):
         ev0.record(stream)
         for _ in range(a.steps):
             recs.append(tr.step(evolve=True, dt=a.dt))
-            for k, v in eng.stage_times().items():
-                stage_sum[k] += v
         ev1.record(stream)
         ev1.synchronize()
-    launches = eng.kernel_launches() - launches0
     ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     clocks = clk.summary()
     barrier()
+
+    # stage split and the Taylor launch time: eager steps with CUDA events between stages
+    n_prof = max(3, min(a.steps, 10))
+    eng.set_profiling(True)
+    stage_sum = {s_: 0.0 for s_ in nat.STAGES}
+    prof_recs = []
+    launches0 = eng.kernel_launches()
+    use_graph, tr.use_graph = tr.use_graph, False
+    for _ in range(n_prof):
+        prof_recs.append(tr.step(evolve=True, dt=a.dt))
+        for k, v in eng.stage_times().items():
+            stage_sum[k] += v
+    tr.use_graph = use_graph
+    launches_per_step = (eng.kernel_launches() - launches0) / n_prof
+    launches = int(round(launches_per_step * a.steps))
     eng.set_profiling(False)
+    barrier()
 
     # e2e: the C ABI called with host buffers -- every step copies the state in from pinned
     # host memory, runs paces_step, and copies the new state and its record back out.
@@ -337,11 +363,10 @@ def run_ours(a):
 
     total_steps = a.steps * world
     value = total_steps / (ms / 1e3)
-    last = recs[-1]
-    taylor_ms = stage_sum["taylor"] / a.steps
+    taylor_ms = stage_sum["taylor"] / n_prof
     terms = statistics.mean(r.final_m + 1 for r in recs)
     S_mean = statistics.mean(r.n_states for r in recs)
-    taylor_alg = statistics.mean(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in recs)
+    taylor_alg = statistics.mean(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in prof_recs)
     achieved = taylor_alg / (taylor_ms / 1e3) / 1e9
     peak, peak_kind = read_peaks()
     per_row_term = read_profile_traffic(a.precision)
@@ -356,7 +381,9 @@ def run_ours(a):
                "dt": a.dt, "maxstates": a.maxstates, "enlarge_steps": a.enlarge_steps,
                "boundary": "open" if a.open_chain else "periodic", "precision": a.precision,
                "states_per_step": int(S_mean), "taylor_terms_per_step": terms, "prep_steps": nprep,
-               "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}"}
+               "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}",
+               "cuda_graph": not a.no_graph,
+               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")}}
         line = {
             "metric": "time-steps/s at 4M states", "value": value, "unit": "time-steps/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
@@ -366,7 +393,7 @@ def run_ours(a):
                          "algorithmic_bytes": taylor_alg, "launch_ms": taylor_ms},
             "step_roofline": {"achieved": step_alg / (ms / a.steps / 1e3) / 1e9, "unit": "GB/s",
                               "frac": step_alg / (ms / a.steps / 1e3) / 1e9 / peak},
-            "stage_ms": {k: v / a.steps for k, v in stage_sum.items()},
+            "stage_ms": {k: v / n_prof for k, v in stage_sum.items()}, "stage_steps": n_prof,
             "clocks": clocks, "gpu_launches": launches, "cpu_baseline": cpu, "e2e": e2e,
         }
         print(json.dumps(line), flush=True)
@@ -418,11 +445,158 @@ def run_e2e(a, eng, tr, barrier, dist):
             "h2d_bytes_per_step": h2d // a.steps, "d2h_bytes_per_step": d2h // a.steps,
             "api": "paces_step (C ABI) with the state in pinned host memory"}
 
+# --------------------------------------------------------------------------------------------
+# batched workload: independent trajectories advanced together
+# --------------------------------------------------------------------------------------------
+def batched_specs(seed, n):
+    """n Holstein rings drawn from numpy.random.default_rng(seed), one parameter at a time
+    in this order: g ~ U[0.5, 2], omega0 ~ U[0.5, 1.5], N uniform over {16, 24, 32},
+    maxstates = round(2^U[14, 20]) (log-uniform), exciton site uniform over the ring."""
+    rng = np.random.default_rng(seed)
+    g = rng.uniform(0.5, 2.0, n)
+    w0 = rng.uniform(0.5, 1.5, n)
+    N = rng.choice(np.array([16, 24, 32]), n)
+    M = np.round(2.0 ** rng.uniform(14.0, 20.0, n)).astype(np.int64)
+    site = rng.integers(0, N)
+    return [dict(g=float(g[i]), omega0=float(w0[i]), nchain=int(N[i]), maxstates=int(M[i]), site=int(site[i]))
+            for i in range(n)]
+
+
+def run_batched(a):
+    import torch
+    from paces_b200 import _native as nat
+    from paces_b200.engine import Engine, ModelParams, TrajectoryBatch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    cs = 8 if a.precision == "c64" else 16
+    # each rank runs its own draw of the batch (replicas: rank r uses seed + r)
+    specs = batched_specs(a.seed + rank, a.batch)
+    trajs = []
+    for sp in specs:
+        eng = Engine(ModelParams(nchain=sp["nchain"], max_ho_dims=[16] * sp["nchain"], J=1.0, g=sp["g"],
+                                 hbar_omega=sp["omega0"], periodic=True, precision=a.precision),
+                     device=f"cuda:{local}")
+        trajs.append(start_trajectory(eng, sp["nchain"], sp["maxstates"], a.enlarge_steps, sp["site"],
+                                      graph=not a.no_graph))
+    batch = TrajectoryBatch(trajs, n_streams=a.streams, graph=not a.no_graph)
+    nprep = 0
+    while True:
+        recs = batch.step(evolve=True, dt=a.dt)
+        nprep += 1
+        if all(r.n_select >= sp["maxstates"] for r, sp in zip(recs, specs)) or nprep >= 60:
+            break
+    tuning = None
+    if not a.no_tune:
+        from paces_b200 import autotune
+        tuning = autotune.tune_batch(batch, a.dt)
+    for _ in range(max(a.warmup, 0)):
+        batch.step(evolve=True, dt=a.dt)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    rounds = []
+    barrier()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            rounds.append(batch.step(evolve=True, dt=a.dt))
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
+    clocks = clk.summary()
+    barrier()
+
+    # phase split (eager batch steps with events) and the batched Taylor launch
+    n_prof = max(3, min(a.steps, 10))
+    batch.set_profiling(True)
+    batch.use_graph = False
+    phase = {k: 0.0 for k in nat.BATCH_STAGES}
+    prof = []
+    l0 = batch.kernel_launches()
+    for _ in range(n_prof):
+        prof.append(batch.step(evolve=True, dt=a.dt))
+        for k, v in batch.stage_times().items():
+            phase[k] += v
+    launches_per_step = (batch.kernel_launches() - l0) / n_prof
+    batch.set_profiling(False)
+    batch.use_graph = not a.no_graph
+    barrier()
+
+    # the same trajectories stepped one after another (paces_step each, graphs on)
+    seq_steps = 2
+    for t in trajs:
+        t.use_graph = not a.no_graph
+    for _ in range(2):  # captures each trajectory's graphs (both slot parities)
+        for t in trajs:
+            t.step(evolve=True, dt=a.dt)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(seq_steps):
+        for t in trajs:
+            t.step(evolve=True, dt=a.dt)
+    e1.record(stream)
+    e1.synchronize()
+    seq_ms = e0.elapsed_time(e1) / seq_steps
+
+    n = len(trajs)
+    value = n * a.steps * world / (ms / 1e3)
+    taylor_ms = phase["taylor"] / n_prof
+    taylor_alg = statistics.mean(sum(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in rr) for rr in prof)
+    achieved = taylor_alg / (taylor_ms / 1e3) / 1e9
+    peak, peak_kind = read_peaks()
+    states = statistics.mean(sum(r.n_states for r in rr) for rr in rounds)
+    if rank == 0:
+        cfg = {"workload": f"holstein_batched_{n}_seed{a.seed}_c64_dt{a.dt:g}_es{a.enlarge_steps}",
+               "trajectories": n, "nchain": "uniform {16,24,32}", "g": "U[0.5,2]", "omega0": "U[0.5,1.5]",
+               "maxstates": "log-uniform [2^14, 2^20]", "cutoff": 15, "J": 1.0, "dt": a.dt, "boundary": "periodic",
+               "precision": a.precision, "states_per_step_all": int(states), "prep_steps": nprep,
+               "streams": a.streams, "cuda_graph": not a.no_graph,
+               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")},
+               "l2": "inputs larger than L2 (all trajectories' states and H tables > 126 MB)",
+               "parallelism": f"replicas x{world}",
+               "maxstates_drawn": [sp["maxstates"] for sp in specs], "nchain_drawn": [sp["nchain"] for sp in specs]}
+        line = {
+            "metric": "trajectory time-steps/s (batched trajectories)", "value": value, "unit": "trajectory-steps/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": a.precision,
+            "data": "synthetic", "config": cfg,
+            "roofline": {"bound": "hbm", "kernel": "taylor_batch_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "algorithmic_bytes": taylor_alg, "launch_ms": taylor_ms},
+            "phase_ms": {k: v / n_prof for k, v in phase.items()},
+            "sequential_ms_per_step": seq_ms, "batched_speedup": seq_ms / (ms / a.steps),
+            "clocks": clocks, "gpu_launches": int(round(launches_per_step * a.steps)), "cpu_baseline": None,
+            "e2e": None,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
 
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "batched":
+        run_batched(a)
     else:
         run_ours(a)
 

@@ -9,7 +9,8 @@
  *     bounded wait that ran out) are written to the device-side status word of
  *     the step record / context and returned by the next call that reads it.
  *   - Device buffers are owned by the caller.  No entry point allocates device
- *     memory after paces_create (which allocates a few bytes of status words).
+ *     memory except paces_create (4 KB of status words and model constants) and
+ *     paces_batch_create (a few KB of Taylor scratch).
  *     Scratch comes from a caller-provided workspace sized by
  *     paces_workspace_bytes.
  *   - All work is enqueued on the caller's stream; nothing synchronises the
@@ -176,6 +177,21 @@ int paces_set_profiling(paces_ctx *ctx, int32_t on);
 int paces_stage_times(paces_ctx *ctx, float *ms);
 /* Number of kernels paces_step has enqueued on this context so far. */
 unsigned long long paces_kernel_launches(const paces_ctx *ctx);
+/* Launch shapes (no counterpart in the reference): the merge tiles' splitter stride
+ * (tile size = 13 * stride elements) and the Taylor kernel's blocks per SM.  Results do
+ * not depend on them; paces_b200.autotune picks them by timing the live workload.
+ * paces_get_tuning also reports the allowed ranges; paces_set_tuning rejects values
+ * outside them with PACES_ERR_BADARG. */
+typedef struct paces_tuning {
+    int32_t merge_stride;              /* multiple of 16 in [merge_stride_min, merge_stride_max] */
+    int32_t taylor_blocks_per_sm;      /* 0 = as many as fit, else 1..taylor_blocks_per_sm_max */
+    int32_t merge_stride_min;          /* read only */
+    int32_t merge_stride_max;          /* read only */
+    int32_t taylor_blocks_per_sm_max;  /* read only */
+    int32_t reserved[3];
+} paces_tuning;
+int paces_get_tuning(const paces_ctx *ctx, paces_tuning *t);
+int paces_set_tuning(paces_ctx *ctx, const paces_tuning *t);
 /* Workspace bytes for every entry point on bases of up to `cap` states. */
 int paces_workspace_bytes(const paces_ctx *ctx, int64_t cap, size_t *bytes);
 
@@ -268,6 +284,11 @@ int paces_batch_step(paces_batch *batch, const paces_batch_item *items, int32_t 
 const char *paces_batch_last_error(const paces_batch *batch);
 /* Number of kernels paces_batch_step has enqueued on this batch so far. */
 unsigned long long paces_batch_kernel_launches(const paces_batch *batch);
+/* With profiling on (not under stream capture), paces_batch_step records events around
+ * its three phases; paces_batch_stage_times waits for the last step and returns their
+ * durations in ms: per-trajectory front stages, the batched Taylor launch, back stages. */
+int paces_batch_set_profiling(paces_batch *batch, int32_t on);
+int paces_batch_stage_times(paces_batch *batch, float *ms);
 
 #ifdef __cplusplus
 }

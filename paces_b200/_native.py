@@ -103,6 +103,17 @@ class ExpmInfo(ctypes.Structure):
                 ("c1_plus_c2", ctypes.c_double), ("term_ratio", ctypes.c_double)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("merge_stride", ctypes.c_int32),
+        ("taylor_blocks_per_sm", ctypes.c_int32),
+        ("merge_stride_min", ctypes.c_int32),
+        ("merge_stride_max", ctypes.c_int32),
+        ("taylor_blocks_per_sm_max", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
+    ]
+
+
 class BatchItem(ctypes.Structure):
     _fields_ = [
         ("ctx", ctypes.c_void_p),
@@ -153,15 +164,20 @@ _SIGNATURES = {
     "paces_set_profiling": [_P, ctypes.c_int32],
     "paces_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
     "paces_kernel_launches": [_P],
+    "paces_get_tuning": [_P, ctypes.POINTER(Tuning)],
+    "paces_set_tuning": [_P, ctypes.POINTER(Tuning)],
     "paces_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)],
     "paces_batch_destroy": [_P],
     "paces_batch_step": [_P, ctypes.POINTER(BatchItem), ctypes.c_int32, _P],
     "paces_batch_last_error": [_P],
     "paces_batch_kernel_launches": [_P],
+    "paces_batch_set_profiling": [_P, ctypes.c_int32],
+    "paces_batch_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
 }
 _RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_kernel_launches": ctypes.c_ulonglong,
              "paces_batch_last_error": ctypes.c_char_p, "paces_batch_kernel_launches": ctypes.c_ulonglong}
 STAGES = ("truncate", "expand", "assemble", "remap", "diagnostics", "taylor", "observables")
+BATCH_STAGES = ("front", "taylor", "back")
 
 _lib = None
 

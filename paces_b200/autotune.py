@@ -1,0 +1,183 @@
+"""Autotuner for the launch shapes of the time step.
+
+Two shapes change the speed of a step but never its results (each trajectory's
+arithmetic and ordering are fixed by the data, not by the tiling):
+
+* the merge tiles' splitter stride (tile = 13 * stride elements): larger tiles spend less
+  on splitters and look-back, smaller ones fit more blocks per SM;
+* the persistent Taylor kernel's blocks per SM (its grid).
+
+`tune(trajectory, dt)` times candidates on the live workload -- eager steps with the
+library's stage events -- and keeps, shape by shape, the fastest (merge stride by the
+expand + assemble time, Taylor blocks by the Taylor time).  `tune_batch` does the same for
+a TrajectoryBatch with its phase times.  Choices are cached per (GPU name, key words,
+precision, log2 of the basis size) in memory and in a JSON file
+($PACES_TUNE_CACHE, default ~/.cache/paces_b200/tuning.json), so a later run of the same
+workload on the same GPU model skips the search.
+"""
+
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import torch
+
+from . import _native as nat
+
+CACHE_PATH = os.environ.get("PACES_TUNE_CACHE",
+                            os.path.join(os.path.expanduser("~"), ".cache", "paces_b200", "tuning.json"))
+_memory: dict = {}
+
+
+def get_tuning(eng) -> nat.Tuning:
+    t = nat.Tuning()
+    nat.check(eng.lib.paces_get_tuning(eng.ctx, t), eng.ctx, "get_tuning")
+    return t
+
+
+def set_tuning(eng, merge_stride=None, taylor_blocks_per_sm=None):
+    t = get_tuning(eng)
+    if merge_stride is not None:
+        t.merge_stride = int(merge_stride)
+    if taylor_blocks_per_sm is not None:
+        t.taylor_blocks_per_sm = int(taylor_blocks_per_sm)
+    nat.check(eng.lib.paces_set_tuning(eng.ctx, t), eng.ctx, "set_tuning")
+
+
+def stride_candidates(t: nat.Tuning):
+    grid = [64, 80, 96, 128, 160, 192, 240]
+    return [s for s in grid if t.merge_stride_min <= s <= t.merge_stride_max]
+
+
+def bps_candidates(t: nat.Tuning):
+    return [0] + list(range(1, t.taylor_blocks_per_sm_max))
+
+
+def _key(eng, states):
+    name = torch.cuda.get_device_name(eng.device)
+    return f"{name}|nw{eng.nw}|{'c64' if eng.c64 else 'c128'}|s{int(round(math.log2(max(states, 1))))}"
+
+
+def _load_file():
+    try:
+        with open(CACHE_PATH) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _save_file(key, choice):
+    try:
+        data = _load_file()
+        data[key] = choice
+        os.makedirs(os.path.dirname(CACHE_PATH), exist_ok=True)
+        tmp = CACHE_PATH + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, CACHE_PATH)
+    except OSError:
+        pass
+
+
+def _lookup(key, use_cache):
+    if not use_cache:
+        return None
+    if key in _memory:
+        return _memory[key]
+    return _load_file().get(key)
+
+
+def _search(apply, measure, strides, bpss, base_bps):
+    """Coordinate search: the stride by its stages' time, then the Taylor grid by its own."""
+    timings = {"merge_stride": {}, "taylor_blocks_per_sm": {}}
+    for s in strides:
+        apply(s, base_bps)
+        timings["merge_stride"][s] = measure()["merge"]
+    best_s = min(timings["merge_stride"], key=timings["merge_stride"].get)
+    for b in bpss:
+        apply(best_s, b)
+        timings["taylor_blocks_per_sm"][b] = measure()["taylor"]
+    best_b = min(timings["taylor_blocks_per_sm"], key=timings["taylor_blocks_per_sm"].get)
+    apply(best_s, best_b)
+    return {"merge_stride": best_s, "taylor_blocks_per_sm": best_b, "timings_ms": timings}
+
+
+def tune(tr, dt, steps=2, use_cache=True):
+    """Pick the shapes for trajectory `tr` (its engine keeps them).  The candidate steps
+    advance the trajectory like ordinary steps.  Returns the choice (and its timings when
+    it was searched)."""
+    eng = tr.eng
+    key = _key(eng, tr.basis.count())
+    hit = _lookup(key, use_cache)
+    if hit is not None:
+        set_tuning(eng, hit["merge_stride"], hit["taylor_blocks_per_sm"])
+        return dict(hit, cached=True)
+    t0 = get_tuning(eng)
+    use_graph, tr.use_graph = tr.use_graph, False
+    eng.set_profiling(True)
+
+    def measure():
+        tr.step(evolve=True, dt=dt)  # first step after a change: not timed
+        acc = {"merge": 0.0, "taylor": 0.0}
+        for _ in range(steps):
+            tr.step(evolve=True, dt=dt)
+            st = eng.stage_times()
+            acc["merge"] += st["expand"] + st["assemble"]
+            acc["taylor"] += st["taylor"]
+        return {k: v / steps for k, v in acc.items()}
+
+    try:
+        choice = _search(lambda s, b: set_tuning(eng, s, b), measure, stride_candidates(t0), bps_candidates(t0),
+                         t0.taylor_blocks_per_sm)
+    finally:
+        eng.set_profiling(False)
+        tr.use_graph = use_graph
+    tr._graphs = {}
+    _memory[key] = {k: choice[k] for k in ("merge_stride", "taylor_blocks_per_sm")}
+    _save_file(key, _memory[key])
+    return dict(choice, cached=False)
+
+
+def tune_batch(batch, dt, steps=2, use_cache=True):
+    """The same search for a TrajectoryBatch: one stride for every trajectory (timed by the
+    batch's front phase) and the Taylor grid of its one persistent launch."""
+    engs = [t.eng for t in batch.trajs]
+    total = sum(t.basis.count() for t in batch.trajs)
+    key = "batch|" + _key(engs[0], total) + f"|n{len(engs)}"
+    hit = _lookup(key, use_cache)
+
+    def apply(s, b):
+        for e in engs:
+            t = get_tuning(e)
+            set_tuning(e, min(max(s, t.merge_stride_min), t.merge_stride_max), b)
+
+    if hit is not None:
+        apply(hit["merge_stride"], hit["taylor_blocks_per_sm"])
+        return dict(hit, cached=True)
+    t0 = get_tuning(engs[0])
+    use_graph, batch.use_graph = batch.use_graph, False
+    batch.set_profiling(True)
+
+    def measure():
+        batch.step(evolve=True, dt=dt)
+        acc = {"merge": 0.0, "taylor": 0.0}
+        for _ in range(steps):
+            batch.step(evolve=True, dt=dt)
+            st = batch.stage_times()
+            acc["merge"] += st["front"]
+            acc["taylor"] += st["taylor"]
+        return {k: v / steps for k, v in acc.items()}
+
+    try:
+        choice = _search(apply, measure, stride_candidates(t0), bps_candidates(t0), t0.taylor_blocks_per_sm)
+    finally:
+        batch.set_profiling(False)
+        batch.use_graph = use_graph
+    batch._graphs = {}
+    for t in batch.trajs:
+        t._graphs = {}
+    _memory[key] = {k: choice[k] for k in ("merge_stride", "taylor_blocks_per_sm")}
+    _save_file(key, _memory[key])
+    return dict(choice, cached=False)

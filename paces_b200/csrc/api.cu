@@ -16,6 +16,8 @@ struct paces_ctx {
     int device;
     int num_sms;
     int taylor_grid;
+    int merge_stride;  // tuning: elements per splitter of the merge tiles
+    int taylor_bps;    // tuning: Taylor blocks per SM (0 = as many as fit)
     int* d_status;  // device status word for the stage entry points (start of the constants block)
     double* d_site_eps;  // [kMaxSites] per-site energies, device copy (batched Taylor)
     double* d_sq;        // [kSqrtTable] sqrt(k) * g
@@ -37,6 +39,8 @@ struct paces_batch {
     cudaEvent_t* join;
     void* d_ws;                   // TaylorBatchWs: barrier words + per-term maxima
     TaylorBatch* desc;            // host staging of the launch descriptors
+    int profiling;                // record events around the three phases of a batch step
+    cudaEvent_t ev[4];
     unsigned long long launches;  // kernels enqueued by paces_batch_step
     char err[512];
 };
@@ -292,7 +296,7 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.keys = other->keys;
         mo.blk = other->blk;
         mo.cap = other->cap;
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->m, cur->keys, cur->blk, mws, mo, nullptr, status,
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->merge_stride, c->m, cur->keys, cur->blk, mws, mo, nullptr, status,
                                            c->num_sms, st),
                            "step/expand");
         paces_basis* t = cur;
@@ -311,7 +315,7 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.nbr_cap = p.h->cap;
         mo.maps = at<int>(ws, l.maps);
         mo.map_cap = l.cap;
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->m, cur->keys, cur->blk, mws, mo, &rec->ceiling_hits,
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->merge_stride, c->m, cur->keys, cur->blk, mws, mo, &rec->ceiling_hits,
                                            status, c->num_sms, st),
                            "step/assemble");
     }
@@ -414,9 +418,14 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
     }
     c->nw = word + 1;
     m.nw = c->nw;
-    if (c->nw > 8) {
+    if (c->nw > kMaxKeyWords) {
         delete c;
         return PACES_ERR_BADARG;
+    }
+    m.max_bits = 0;
+    for (int s = 0; s < L; ++s) {
+        if (m.bits[s] > m.max_bits) m.max_bits = m.bits[s];
+        for (int b = 0; b < m.bits[s]; ++b) m.plane[m.word[s]][b] |= uint64_t(1) << (m.shift[s] + b);
     }
     // reference row layout: position field first, then the sites (hamiltonian.py:140-160)
     int pb = 0;
@@ -440,6 +449,8 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
         return PACES_ERR_CUDA;
     }
     c->taylor_grid = taylor_max_grid(c->precision == PACES_C64, c->num_sms);
+    c->merge_stride = merge_stride(c->nw);
+    c->taylor_bps = 0;
     // constants block: status words, per-site energies and the sqrt(k) * g tables
     {
         const size_t o_eps = 64, o_sq = o_eps + kMaxSites * 8, o_sqf = o_sq + kSqrtTable * 8;
@@ -519,6 +530,30 @@ int paces_key_layout(const paces_ctx* c, int32_t* word, int32_t* shift, int32_t*
     return PACES_OK;
 }
 
+int paces_get_tuning(const paces_ctx* c, paces_tuning* t) {
+    if (!c || !t) return PACES_ERR_BADARG;
+    std::memset(t, 0, sizeof(*t));
+    t->merge_stride = c->merge_stride;
+    t->merge_stride_max = merge_stride(c->nw);
+    t->merge_stride_min = kMinMergeStride;
+    t->taylor_blocks_per_sm = c->taylor_bps;
+    t->taylor_blocks_per_sm_max = c->taylor_grid / c->num_sms;
+    return PACES_OK;
+}
+
+int paces_set_tuning(paces_ctx* c, const paces_tuning* t) {
+    if (!c || !t) return PACES_ERR_BADARG;
+    if (t->merge_stride < kMinMergeStride || t->merge_stride > merge_stride(c->nw) || t->merge_stride % 16)
+        return fail(c, PACES_ERR_BADARG, "merge_stride %d: a multiple of 16 in [%d, %d]", t->merge_stride,
+                    kMinMergeStride, merge_stride(c->nw));
+    if (t->taylor_blocks_per_sm < 0 || t->taylor_blocks_per_sm > c->taylor_grid / c->num_sms)
+        return fail(c, PACES_ERR_BADARG, "taylor_blocks_per_sm %d: 0..%d", t->taylor_blocks_per_sm,
+                    c->taylor_grid / c->num_sms);
+    c->merge_stride = t->merge_stride;
+    c->taylor_bps = t->taylor_blocks_per_sm;
+    return PACES_OK;
+}
+
 int paces_workspace_bytes(const paces_ctx* c, int64_t cap, size_t* bytes) {
     if (!c || !bytes || cap < 0) return PACES_ERR_BADARG;
     *bytes = make_layout(c, cap).total;
@@ -563,7 +598,7 @@ int paces_expand(paces_ctx* c, const paces_basis* in, paces_basis* out, void* ws
     mo.keys = out->keys;
     mo.blk = out->blk;
     mo.cap = out->cap;
-    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->m, in->keys, in->blk, merge_ws(l, ws), mo, nullptr,
+    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->merge_stride, c->m, in->keys, in->blk, merge_ws(l, ws), mo, nullptr,
                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "expand");
     return PACES_OK;
@@ -584,7 +619,7 @@ int paces_assemble(paces_ctx* c, const paces_basis* in, paces_basis* out, paces_
     mo.maps = at<int>(ws, l.maps);
     mo.map_cap = l.cap;
     if (h->cap < out->cap) mo.cap = h->cap;
-    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->m, in->keys, in->blk, merge_ws(l, ws), mo, dev_ceiling_hits,
+    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->merge_stride, c->m, in->keys, in->blk, merge_ws(l, ws), mo, dev_ceiling_hits,
                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "assemble");
     return PACES_OK;
@@ -655,7 +690,7 @@ int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
     }
     PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->cap, h->meta, psi_in,
                                         psi_out, dt, m_star, tol, taylor_ws(l, ws), o, c->d_status, c->num_sms,
-                                        reinterpret_cast<cudaStream_t>(stream)),
+                                        c->taylor_bps, reinterpret_cast<cudaStream_t>(stream)),
                        "taylor");
     return PACES_OK;
 }
@@ -707,7 +742,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
         TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
         PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, new_b->blk, h->nbr, h->cap, h->meta,
                                             p.target, new_psi, prm->dt, prm->m_star, prm->tol, taylor_ws(p.l, ws), o,
-                                            &rec->status, c->num_sms, st),
+                                            &rec->status, c->num_sms, c->taylor_bps, st),
                            "step/taylor");
     }
     return step_back(c, p, st, true);
@@ -747,6 +782,7 @@ int paces_batch_destroy(paces_batch* b) {
         if (b->join && b->join[k]) cudaEventDestroy(b->join[k]);
     }
     if (b->fork) cudaEventDestroy(b->fork);
+    if (b->profiling) paces_batch_set_profiling(b, 0);
     if (b->d_ws) cudaFree(b->d_ws);
     delete[] b->streams;
     delete[] b->join;
@@ -756,6 +792,25 @@ int paces_batch_destroy(paces_batch* b) {
 }
 
 const char* paces_batch_last_error(const paces_batch* b) { return b ? b->err : "no batch"; }
+
+int paces_batch_set_profiling(paces_batch* b, int32_t on) {
+    if (!b) return PACES_ERR_BADARG;
+    if (on && !b->profiling)
+        for (int i = 0; i < 4; ++i)
+            if (cudaEventCreate(&b->ev[i]) != cudaSuccess) return PACES_ERR_CUDA;
+    if (!on && b->profiling)
+        for (int i = 0; i < 4; ++i) cudaEventDestroy(b->ev[i]);
+    b->profiling = on ? 1 : 0;
+    return PACES_OK;
+}
+
+int paces_batch_stage_times(paces_batch* b, float* ms) {
+    if (!b || !ms || !b->profiling) return PACES_ERR_BADARG;
+    if (cudaEventSynchronize(b->ev[3]) != cudaSuccess) return PACES_ERR_CUDA;
+    for (int i = 0; i < 3; ++i)
+        if (cudaEventElapsedTime(&ms[i], b->ev[i], b->ev[i + 1]) != cudaSuccess) return PACES_ERR_CUDA;
+    return PACES_OK;
+}
 
 unsigned long long paces_batch_kernel_launches(const paces_batch* b) { return b ? b->launches : 0ull; }
 
@@ -802,8 +857,12 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
                 return false;
         return true;
     };
+    auto mark = [&](int i) {
+        if (b->profiling) cudaEventRecord(b->ev[i], st);
+    };
     // 1. every trajectory's truncation, enlargement, assembly, remap and diagnostics,
     //    spread over the batch's streams
+    mark(0);
     if (!fork()) return bfail(PACES_ERR_CUDA, "fork: %s", cudaGetErrorString(cudaGetLastError()));
     for (int i = 0; i < n; ++i) {
         const int rc = step_front(items[i].ctx, plans[i], b->streams[i % b->n_streams], false);
@@ -813,6 +872,7 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
         }
     }
     if (!join()) return bfail(PACES_ERR_CUDA, "join: %s", cudaGetErrorString(cudaGetLastError()));
+    mark(1);
     // 2. one persistent launch for every trajectory's Taylor series
     if (n_evolve > 0) {
         TaylorBatch& bt = *b->desc;
@@ -852,10 +912,11 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
         TaylorBatchWs tws;
         tws.barrier = static_cast<unsigned*>(b->d_ws);
         tws.maxima = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(b->d_ws) + 256);
-        if (launch_taylor_batch(precision == PACES_C64, bt, tws, b->num_sms, st) != PACES_OK)
+        if (launch_taylor_batch(precision == PACES_C64, bt, tws, b->num_sms, items[0].ctx->taylor_bps, st) != PACES_OK)
             return bfail(PACES_ERR_CUDA, "batched Taylor: %s", cudaGetErrorString(cudaGetLastError()));
         launches += 1;
     }
+    mark(2);
     // 3. renormalisation, observables and records, again spread over the streams
     if (!fork()) return bfail(PACES_ERR_CUDA, "fork: %s", cudaGetErrorString(cudaGetLastError()));
     for (int i = 0; i < n; ++i) {
@@ -866,6 +927,7 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
         }
     }
     if (!join()) return bfail(PACES_ERR_CUDA, "join: %s", cudaGetErrorString(cudaGetLastError()));
+    mark(3);
     b->launches += launches;
     return PACES_OK;
 }

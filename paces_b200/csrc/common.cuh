@@ -10,6 +10,7 @@
 namespace paces {
 
 constexpr int kMaxSites = PACES_MAX_SITES;
+constexpr int kMaxKeyWords = 8;
 constexpr int kRuns = 5;  // candidate runs per exciton block: self, from-left, from-right, up, down
 enum Run : int { RUN_SELF = 0, RUN_FROM_LEFT = 1, RUN_FROM_RIGHT = 2, RUN_UP = 3, RUN_DOWN = 4 };
 // neighbour slots of the H table (paces_hmat.nbr)
@@ -27,6 +28,10 @@ struct ModelDev {
     uint8_t bits[kMaxSites];   // field width
     uint16_t maxd[kMaxSites];  // max_ho_dims[s]
     double site_eps[kMaxSites];
+    // plane[q][b]: the bits of word q that are bit b of some field (b < max_bits), so the
+    // total phonon count of a key is sum_{q,b} popc(w[q] & plane[q][b]) << b
+    int max_bits;
+    uint64_t plane[kMaxKeyWords][8];
 };
 
 template <int NW>
@@ -102,10 +107,15 @@ __device__ __forceinline__ void add_field(const ModelDev& m, Key<NW>& k, int s, 
         if (w == m.word[s]) k.w[w] = delta > 0 ? k.w[w] + one : k.w[w] - one;
 }
 
+// Sum of all occupation fields: one popcount per word and bit plane.
 template <int NW>
 __device__ __forceinline__ uint32_t total_phonons(const ModelDev& m, const Key<NW>& k) {
     uint32_t t = 0;
-    for (int s = 0; s < m.L; ++s) t += get_field(m, k, s);
+#pragma unroll
+    for (int q = 0; q < NW; ++q) {
+#pragma unroll 8
+        for (int b = 0; b < m.max_bits; ++b) t += uint32_t(__popcll(k.w[q] & m.plane[q][b])) << b;
+    }
     return t;
 }
 

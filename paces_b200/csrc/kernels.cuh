@@ -49,10 +49,11 @@ struct TaylorWs {
     unsigned* barrier;   // [2]
 };
 int taylor_max_grid(bool c64, int num_sms);
+// blocks_per_sm: 0 = as many as fit (the grid never exceeds taylor_max_grid)
 int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,
                   const uint32_t* meta, const void* v_in, void* res, double dt, int m_star,
                   double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
-                  cudaStream_t st);
+                  int blocks_per_sm, cudaStream_t st);
 
 // ---- batched Taylor: many trajectories in one persistent launch ---------------------------
 constexpr int kMaxBatch = 128;  // trajectories per launch (the descriptors travel as kernel parameters)
@@ -88,7 +89,7 @@ struct TaylorBatchWs {
 constexpr size_t kTaylorBatchWsBytes = 256 + size_t(3) * kMaxBatch * 4 * 8;
 int taylor_batch_max_grid(bool c64, int num_sms);
 int launch_taylor_batch(bool c64, const TaylorBatch& bt, const TaylorBatchWs& ws, int num_sms,
-                        cudaStream_t st);
+                        int blocks_per_sm, cudaStream_t st);
 
 // ---- observables --------------------------------------------------------------------------
 struct ObsTarget {

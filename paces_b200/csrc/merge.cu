@@ -610,23 +610,22 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
 }
 
 template <int NW>
-size_t tile_smem_bytes() {
-    const int tmax = merge_tmax(NW);
+size_t tile_smem_bytes(int tmax) {
     // keys, order flags, then three uint16 arrays (merged order, rank, running count)
     return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) + size_t(tmax) * 6;
 }
 
 template <int NW>
-int launch_merge_t(bool assemble, const ModelDev& m, const uint64_t* X, const int* x_blk,
+int launch_merge_t(bool assemble, int stride, const ModelDev& m, const uint64_t* X, const int* x_blk,
                    const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status, int num_sms,
                    cudaStream_t st) {
-    const int stride = merge_stride(NW);
-    const int tmax = merge_tmax(NW);
+    if (stride < kMinMergeStride || stride > merge_stride(NW) || stride % 16) return PACES_ERR_BADARG;
+    const int tmax = merge_tmax(stride);
     merge_plan_kernel<<<1, 1024, 0, st>>>(m, x_blk, ws, stride, status);
     const int g = num_sms * 8;
     merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, ws, stride);
     merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
-    const size_t smem = tile_smem_bytes<NW>();
+    const size_t smem = tile_smem_bytes<NW>(tmax);
     if (assemble) {
         auto kfn = merge_tile_kernel<NW, true>;
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -647,20 +646,23 @@ int launch_merge_t(bool assemble, const ModelDev& m, const uint64_t* X, const in
 
 }  // namespace
 
-int launch_merge(int nw, bool assemble, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+int launch_merge(int nw, bool assemble, int stride, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                  const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status, int num_sms,
                  cudaStream_t st) {
+#define PACES_MERGE_CASE(W) \
+    case W: return launch_merge_t<W>(assemble, stride, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
     switch (nw) {
-        case 1: return launch_merge_t<1>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
-        case 2: return launch_merge_t<2>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
-        case 3: return launch_merge_t<3>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
-        case 4: return launch_merge_t<4>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
-        case 5: return launch_merge_t<5>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
-        case 6: return launch_merge_t<6>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
-        case 7: return launch_merge_t<7>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
-        case 8: return launch_merge_t<8>(assemble, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+        PACES_MERGE_CASE(1)
+        PACES_MERGE_CASE(2)
+        PACES_MERGE_CASE(3)
+        PACES_MERGE_CASE(4)
+        PACES_MERGE_CASE(5)
+        PACES_MERGE_CASE(6)
+        PACES_MERGE_CASE(7)
+        PACES_MERGE_CASE(8)
         default: return PACES_ERR_BADARG;
     }
+#undef PACES_MERGE_CASE
 }
 
 }  // namespace paces

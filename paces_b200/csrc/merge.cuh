@@ -56,21 +56,26 @@ struct MergeOut {
     int64_t map_cap;
 };
 
-// Tiling constants by key width (shared memory of one tile stays below ~100 KB).
+// Tiling constants by key width.  merge_stride(nw) is the default and largest stride (the
+// tile's shared memory stays below ~100 KB); any multiple of 16 down to kMinMergeStride
+// works (paces_set_tuning), smaller tiles trading splitter work for more resident blocks.
 __host__ __device__ constexpr int merge_stride(int nw) { return nw <= 2 ? 240 : (nw <= 4 ? 128 : 64); }
+constexpr int kMinMergeStride = 64;
 constexpr int kMergeGroup = 8;
 // A tile holds the merged range of kMergeGroup consecutive splitters; every run contributes
 // fewer than (its splitters in the range + 1) * stride elements, so at most
 // (kMergeGroup + kRuns) * stride elements in total.
-__host__ __device__ constexpr int merge_tmax(int nw) { return (kMergeGroup + kRuns) * merge_stride(nw); }
+__host__ __device__ constexpr int merge_tmax(int stride) { return (kMergeGroup + kRuns) * stride; }
 
+// Splitter capacity for inputs of up to in_cap states at any stride >= kMinMergeStride.
 inline int64_t merge_split_cap(int64_t in_cap, int nw, int L) {
-    return kRuns * (in_cap / merge_stride(nw) + 1) * 1 + int64_t(kRuns) * L + 8;
+    (void)nw;
+    return kRuns * (in_cap / kMinMergeStride + 1) + int64_t(kRuns) * L + 8;
 }
 inline int64_t merge_tile_cap(int64_t split_cap, int L) { return split_cap / kMergeGroup + L + 8; }
 
-int launch_merge(int nw, bool assemble, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                 const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status,
+int launch_merge(int nw, bool assemble, int stride, const ModelDev& m, const uint64_t* x_keys,
+                 const int* x_blk, const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status,
                  int num_sms, cudaStream_t st);
 
 }  // namespace paces

@@ -162,10 +162,11 @@ int taylor_max_grid(bool c64, int num_sms) { return num_sms * (c64 ? occupancy<t
 int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,
                   const uint32_t* meta, const void* v_in, void* res, double dt, int m_star,
                   double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
-                  cudaStream_t st) {
+                  int blocks_per_sm, cudaStream_t st) {
     if (m_star < 1) return PACES_ERR_BADARG;
     if (cudaMemsetAsync(ws.barrier, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return PACES_ERR_CUDA;
-    const int grid = taylor_max_grid(c64, num_sms);
+    const int occ = c64 ? occupancy<true>() : occupancy<false>();
+    const int grid = num_sms * (blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kTThreads);

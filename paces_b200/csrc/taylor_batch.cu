@@ -250,11 +250,13 @@ int taylor_batch_max_grid(bool c64, int num_sms) {
     return num_sms * (c64 ? batch_occupancy<true>() : batch_occupancy<false>());
 }
 
-int launch_taylor_batch(bool c64, const TaylorBatch& bt, const TaylorBatchWs& ws, int num_sms, cudaStream_t st) {
+int launch_taylor_batch(bool c64, const TaylorBatch& bt, const TaylorBatchWs& ws, int num_sms, int blocks_per_sm,
+                        cudaStream_t st) {
     if (bt.n < 1 || bt.n > kMaxBatch || bt.max_m_star < 1) return PACES_ERR_BADARG;
     if (cudaMemsetAsync(ws.barrier, 0, kTaylorBatchWsBytes, st) != cudaSuccess) return PACES_ERR_CUDA;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(taylor_batch_max_grid(c64, num_sms));
+    const int occ = c64 ? batch_occupancy<true>() : batch_occupancy<false>();
+    cfg.gridDim = dim3(num_sms * (blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ));
     cfg.blockDim = dim3(kBThreads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;

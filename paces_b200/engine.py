@@ -507,6 +507,15 @@ class TrajectoryBatch:
     def kernel_launches(self):
         return int(self.lib.paces_batch_kernel_launches(self.handle))
 
+    def set_profiling(self, on=True):
+        nat.check(self.lib.paces_batch_set_profiling(self.handle, 1 if on else 0), None, "batch_set_profiling")
+
+    def stage_times(self):
+        """Device ms of the last eager batch step: front stages, batched Taylor, back stages."""
+        ms = (ctypes.c_float * 3)()
+        nat.check(self.lib.paces_batch_stage_times(self.handle, ms), None, "batch_stage_times")
+        return dict(zip(nat.BATCH_STAGES, [float(x) for x in ms]))
+
     def step(self, evolve=True, dt=0.0):
         """One time step of every trajectory (dt: one value, or one per trajectory);
         returns their records."""

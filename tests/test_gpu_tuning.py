@@ -1,0 +1,64 @@
+"""Launch shapes (merge stride, Taylor grid) change speed only: every shape the tuner may
+pick gives bit-identical trajectories, and the tuner returns one of them."""
+
+import numpy as np
+import pytest
+
+from tests import gpu_helpers
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(precision, stride=None, bps=None, steps=8):
+    from paces_b200 import autotune
+    eng = gpu_helpers.engine_for(16, 16, 1.0, cap=1 << 14, precision=precision, periodic=True)
+    if stride is not None or bps is not None:
+        autotune.set_tuning(eng, stride, bps)
+    tr, _ = gpu_helpers.grown_trajectory(eng, 16, 20000)
+    recs = [tr.step(evolve=True, dt=0.05) for _ in range(steps)]
+    n = tr.basis.count()
+    out = (recs, tr.basis.keys[:n].cpu().numpy(), tr.vector.cpu().numpy())
+    eng.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_results_do_not_depend_on_launch_shapes(precision):
+    ref = _run(precision)
+    for stride, bps in ((64, 1), (96, 2), (160, 0), (240, 1)):
+        got = _run(precision, stride, bps)
+        for a, b in zip(ref[0], got[0]):
+            assert (a.n_states, a.final_m, a.converged) == (b.n_states, b.final_m, b.converged)
+            assert list(a.n_exc) == list(b.n_exc) and list(a.n_pho) == list(b.n_pho)
+            assert a.energy_re == b.energy_re
+        assert np.array_equal(ref[1], got[1]) and np.array_equal(ref[2], got[2])
+
+
+def test_out_of_range_shapes_are_rejected():
+    from paces_b200 import _native as nat
+    from paces_b200 import autotune
+    eng = gpu_helpers.engine_for(8, 16, 1.0, cap=1 << 10)
+    t = autotune.get_tuning(eng)
+    assert t.merge_stride == t.merge_stride_max == 240 and t.merge_stride_min == 64
+    for bad in (48, 250, 72):
+        with pytest.raises(nat.PacesError):
+            autotune.set_tuning(eng, merge_stride=bad)
+    with pytest.raises(nat.PacesError):
+        autotune.set_tuning(eng, taylor_blocks_per_sm=t.taylor_blocks_per_sm_max + 1)
+    eng.close()
+
+
+def test_tuner_picks_an_allowed_shape(tmp_path, monkeypatch):
+    from paces_b200 import autotune
+    monkeypatch.setattr(autotune, "CACHE_PATH", str(tmp_path / "tuning.json"))
+    monkeypatch.setattr(autotune, "_memory", {})
+    eng = gpu_helpers.engine_for(16, 16, 1.0, cap=1 << 14, periodic=True)
+    tr, _ = gpu_helpers.grown_trajectory(eng, 16, 20000)
+    choice = autotune.tune(tr, 0.05, steps=1)
+    t = autotune.get_tuning(eng)
+    assert not choice["cached"]
+    assert t.merge_stride == choice["merge_stride"] and t.taylor_blocks_per_sm == choice["taylor_blocks_per_sm"]
+    assert set(choice["timings_ms"]["merge_stride"]) == set(autotune.stride_candidates(t))
+    again = autotune.tune(tr, 0.05, steps=1)
+    assert again["cached"] and again["merge_stride"] == choice["merge_stride"]
+    eng.close()
