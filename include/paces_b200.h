@@ -121,6 +121,12 @@ typedef struct paces_step_params {
     uint64_t shuffle_seed;
     uint64_t step_index;     /* mixes into the shuffle stream */
     double explosion_cutoff; /* ExpmParams.explosion_cutoff */
+    /* learned proposal (no counterpart in the reference): with proposal != 0 the first
+     * enlargement keeps only the images the MLP at proposal_params (paces_mlp_param_bytes
+     * bytes, device) scores above proposal_threshold */
+    int32_t proposal;
+    float proposal_threshold;
+    const void *proposal_params;
 } paces_step_params;
 
 /* Written on the device by paces_step; the caller copies it back (one transfer per step). */
@@ -133,6 +139,8 @@ typedef struct paces_step_record {
     int32_t final_m;         /* Taylor: index of the last term (j_ind) */
     int32_t ceiling_hits;    /* enlarged-basis states at the phonon ceiling */
     int32_t n_tied;          /* states tied with the truncation threshold */
+    int32_t n_candidates;    /* proposal: images scored (existing ones) */
+    int32_t n_candidates_kept; /* proposal: images kept */
     double c1_plus_c2;
     double term_ratio;
     double post_adapt_norm;  /* -1 when diagnostics are off */
@@ -251,6 +259,46 @@ int paces_lookup(paces_ctx *ctx, const paces_basis *phonebook, const uint64_t *q
 int paces_step(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi, paces_basis *new_b,
                void *new_psi, paces_hmat *h, const paces_step_params *prm,
                paces_step_record *dev_rec, void *ws, size_t ws_bytes, paces_stream_t stream);
+
+/* ---- learned proposal (no counterpart in the reference) ------------------------------
+ * Events of a basis X (nx states): e = (j-1)*nx + i, the image of state i under run j =
+ * 1 (exciton hops right), 2 (hops left), 3 (phonon created at the exciton site), 4
+ * (annihilated).  Features, network and keep rule are documented in
+ * paces_b200/csrc/proposal.cuh.  The MLP's packed inference parameters are
+ * paces_mlp_param_bytes() bytes of device memory; its fp32 master weights (and
+ * gradients, and Adam moments) paces_mlp_master_floats() floats. */
+size_t paces_mlp_param_bytes(void);
+int32_t paces_mlp_master_floats(void);
+/* The truncated basis of the last paces_step that used this workspace, its amplitudes
+ * |psi| (float, one per state) and the cut (one float: the smallest kept |psi|, 0 when the
+ * truncation dropped nothing); views into the workspace, valid until its next use. */
+int paces_selected_view(const paces_ctx *ctx, void *ws, size_t ws_bytes, paces_basis *sel, float **weights,
+                        float **cut);
+/* Score every event of X with the MLP on the tensor cores: keep[j*keep_cap + i] (j = 1..4)
+ * = logit > threshold (every existing image when *cut == 0), logits[e] (optional),
+ * counts[0..1] += existing / kept events (optional).  Any of keep, logits, counts may be
+ * NULL; weights and cut are device pointers. */
+int paces_proposal_score(paces_ctx *ctx, const paces_basis *x, const float *weights, const float *cut,
+                         const void *params, float threshold, uint8_t *keep, int64_t keep_cap, float *logits,
+                         int32_t *counts, paces_stream_t stream);
+/* Features of every event as bf16 [4*nx][16] and whether the image exists [4*nx]. */
+int paces_proposal_features(paces_ctx *ctx, const paces_basis *x, const float *weights, const float *cut,
+                            uint16_t *feats, uint8_t *valid, paces_stream_t stream);
+/* Training labels of X's events against the next truncated basis Y: 1 image in Y, 0 not,
+ * 255 image already in X (not a candidate), 254 image does not exist. */
+int paces_proposal_labels(paces_ctx *ctx, const paces_basis *x, const paces_basis *y, uint8_t *labels,
+                          paces_stream_t stream);
+/* fp32 master weights -> packed inference parameters. */
+int paces_mlp_pack(const float *master, void *params, paces_stream_t stream);
+/* logits of n feature rows (bf16 [n][16]) -- CUDA cores, the reference for the scorer. */
+int paces_mlp_forward(const void *params, const uint16_t *x, int64_t n, float *logits, paces_stream_t stream);
+/* grads += d/dw of inv_norm * sum_s sw[s] * BCE(logit_s, y[s]); loss += that loss (double). */
+int paces_mlp_backward(const void *params, const uint16_t *x, const float *y, const float *sw, int64_t n,
+                       float inv_norm, float *grads, double *loss, paces_stream_t stream);
+/* One Adam step (step t >= 1) on the master weights; writes the packed parameters and
+ * clears the gradients. */
+int paces_mlp_adam(float *master, float *m1, float *m2, float *grads, int32_t t, float lr, float beta1,
+                   float beta2, float eps, void *params, paces_stream_t stream);
 
 /* ---- batched trajectories (no counterpart in the reference, which runs one trajectory
  * per process) ------------------------------------------------------------------------

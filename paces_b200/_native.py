@@ -72,6 +72,9 @@ class StepParams(ctypes.Structure):
         ("shuffle_seed", ctypes.c_uint64),
         ("step_index", ctypes.c_uint64),
         ("explosion_cutoff", ctypes.c_double),
+        ("proposal", ctypes.c_int32),
+        ("proposal_threshold", ctypes.c_float),
+        ("proposal_params", ctypes.c_void_p),
     ]
 
 
@@ -85,6 +88,8 @@ class StepRecord(ctypes.Structure):
         ("final_m", ctypes.c_int32),
         ("ceiling_hits", ctypes.c_int32),
         ("n_tied", ctypes.c_int32),
+        ("n_candidates", ctypes.c_int32),
+        ("n_candidates_kept", ctypes.c_int32),
         ("c1_plus_c2", ctypes.c_double),
         ("term_ratio", ctypes.c_double),
         ("post_adapt_norm", ctypes.c_double),
@@ -166,6 +171,18 @@ _SIGNATURES = {
     "paces_kernel_launches": [_P],
     "paces_get_tuning": [_P, ctypes.POINTER(Tuning)],
     "paces_set_tuning": [_P, ctypes.POINTER(Tuning)],
+    "paces_mlp_param_bytes": [],
+    "paces_mlp_master_floats": [],
+    "paces_selected_view": [_P, _P, ctypes.c_size_t, ctypes.POINTER(Basis), ctypes.POINTER(ctypes.c_void_p),
+                            ctypes.POINTER(ctypes.c_void_p)],
+    "paces_proposal_score": [_P, ctypes.POINTER(Basis), _P, _P, _P, ctypes.c_float, _P, ctypes.c_int64, _P, _P, _P],
+    "paces_proposal_features": [_P, ctypes.POINTER(Basis), _P, _P, _P, _P, _P],
+    "paces_proposal_labels": [_P, ctypes.POINTER(Basis), ctypes.POINTER(Basis), _P, _P],
+    "paces_mlp_pack": [_P, _P, _P],
+    "paces_mlp_forward": [_P, _P, ctypes.c_int64, _P, _P],
+    "paces_mlp_backward": [_P, _P, _P, _P, ctypes.c_int64, ctypes.c_float, _P, _P, _P],
+    "paces_mlp_adam": [_P, _P, _P, _P, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                       _P, _P],
     "paces_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)],
     "paces_batch_destroy": [_P],
     "paces_batch_step": [_P, ctypes.POINTER(BatchItem), ctypes.c_int32, _P],
@@ -175,6 +192,7 @@ _SIGNATURES = {
     "paces_batch_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
 }
 _RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_kernel_launches": ctypes.c_ulonglong,
+             "paces_mlp_param_bytes": ctypes.c_size_t, "paces_mlp_master_floats": ctypes.c_int32,
              "paces_batch_last_error": ctypes.c_char_p, "paces_batch_kernel_launches": ctypes.c_ulonglong}
 STAGES = ("truncate", "expand", "assemble", "remap", "diagnostics", "taylor", "observables")
 BATCH_STAGES = ("front", "taylor", "back")

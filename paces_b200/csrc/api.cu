@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "kernels.cuh"
+#include "proposal.cuh"
 
 using namespace paces;
 
@@ -83,6 +84,7 @@ struct Layout {
     int r_tiles;
     size_t v_V, v_TA, v_TB, v_partials, v_bar;
     size_t o_partials, o_out;
+    size_t aw, keep;  // kept amplitudes of the truncation, proposal keep mask [kRuns][cap]
 };
 
 Layout make_layout(const paces_ctx* c, int64_t cap) {
@@ -131,6 +133,8 @@ Layout make_layout(const paces_ctx* c, int64_t cap) {
     l.v_bar = take(16);
     l.o_partials = take(size_t(obs_max_grid(c->num_sms)) * (4 + 2 * L) * 8);
     l.o_out = take(size_t(3 + 2 * L) * 8);
+    l.aw = take((ucap + 1) * 4);
+    l.keep = take(size_t(kRuns) * ucap);
     l.total = off;
     return l;
 }
@@ -163,6 +167,8 @@ MergeWs merge_ws(const Layout& l, void* ws) {
     w.tile_state = at<unsigned long long>(ws, l.m_tile_state);
     w.split_cap = int(l.split_cap);
     w.tile_cap = int(l.tile_cap);
+    w.keep = nullptr;
+    w.keep_cap = 0;
     return w;
 }
 
@@ -241,6 +247,8 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
         return fail(c, PACES_ERR_BADARG, "paces_step: null argument");
     if (prm->maxstates < 1 || prm->enlarge_steps < 0 || (prm->evolve && prm->m_star < 1))
         return fail(c, PACES_ERR_BADARG, "paces_step: bad parameters");
+    if (prm->proposal && !prm->proposal_params)
+        return fail(c, PACES_ERR_BADARG, "paces_step: proposal without MLP parameters");
     p->l = fit_layout(c, ws_bytes);
     const Layout& l = p->l;
     if (old_b->cap > l.cap || new_b->cap > l.cap || h->cap > l.cap)
@@ -264,7 +272,8 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
 // Kernels one step enqueues (merge: 5, +1 with the neighbour table; truncation: 18, +14
 // with tie shuffling; remap 3; observables 2 or 3; Taylor 1; renormalisation 3; record 2).
 unsigned long long step_launches(const paces_step_params& prm, bool with_taylor) {
-    return 2 + (prm.shuffle ? 32 : 18) + 5ull * prm.enlarge_steps + 6 + 3 + (prm.diagnostics ? 2 : 0) +
+    return 2 + (prm.shuffle ? 32 : 18) + (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 5ull * prm.enlarge_steps + 6 +
+           3 + (prm.diagnostics ? 2 : 0) +
            (prm.evolve ? (with_taylor ? 1 : 0) + (prm.renormalize ? 3 : 0) : 0) + 3;
 }
 
@@ -284,14 +293,30 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     // 1. truncation of the old state
     PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, prm->maxstates,
                                           prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), p.A.keys,
-                                          p.A.blk, p.A.cap, &rec->n_tied, status, c->num_sms, st),
+                                          p.A.blk, p.A.cap, at<float>(ws, l.aw), &rec->n_tied, status, c->num_sms, st),
                        "step/truncate");
+    // 1b. learned proposal: score the truncated basis' images
+    const bool propose = prm->proposal && prm->enlarge_steps > 0;
+    if (propose) {
+        ProposalOut po{};
+        po.keep = at<uint8_t>(ws, l.keep);
+        po.keep_cap = l.cap;
+        po.counts = &rec->n_candidates;
+        PACES_CHECK_LAUNCH(c, launch_proposal_score(c->nw, c->m, p.A.keys, p.A.blk, at<float>(ws, l.aw),
+                                                    at<float>(ws, l.aw) + l.cap, prm->proposal_params,
+                                                    prm->proposal_threshold, po, status, c->num_sms, st),
+                           "step/proposal");
+    }
     mark(1);
-    // 2. enlargement (enlarge_steps times)
-    const MergeWs mws = merge_ws(l, ws);
+    // 2. enlargement (enlarge_steps times; the first one filtered by the proposal)
     paces_basis* cur = &p.A;
     paces_basis* other = &p.B;
     for (int e = 0; e < prm->enlarge_steps; ++e) {
+        MergeWs mws = merge_ws(l, ws);
+        if (propose && e == 0) {
+            mws.keep = at<uint8_t>(ws, l.keep);
+            mws.keep_cap = l.cap;
+        }
         MergeOut mo{};
         mo.keys = other->keys;
         mo.blk = other->blk;
@@ -315,8 +340,8 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.nbr_cap = p.h->cap;
         mo.maps = at<int>(ws, l.maps);
         mo.map_cap = l.cap;
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->merge_stride, c->m, cur->keys, cur->blk, mws, mo, &rec->ceiling_hits,
-                                           status, c->num_sms, st),
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->merge_stride, c->m, cur->keys, cur->blk, merge_ws(l, ws), mo,
+                                           &rec->ceiling_hits, status, c->num_sms, st),
                            "step/assemble");
     }
     mark(3);
@@ -633,7 +658,7 @@ int paces_truncate(paces_ctx* c, const paces_basis* in, const void* psi, int64_t
     if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
     PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, psi, maxstates,
                                           shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys, out->blk,
-                                          out->cap, nullptr, c->d_status, c->num_sms,
+                                          out->cap, nullptr, nullptr, c->d_status, c->num_sms,
                                           reinterpret_cast<cudaStream_t>(stream)),
                        "truncate");
     return PACES_OK;
@@ -748,6 +773,86 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
     return step_back(c, p, st, true);
 }
 
+
+// ---- learned proposal ----------------------------------------------------------------------
+size_t paces_mlp_param_bytes(void) { return kMlpParamBytes; }
+
+int32_t paces_mlp_master_floats(void) { return kMlpMasterFloats; }
+
+int paces_selected_view(const paces_ctx* c, void* ws, size_t ws_bytes, paces_basis* sel, float** weights,
+                        float** cut) {
+    if (!c || !ws || !sel) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    *sel = paces_basis{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap};
+    if (weights) *weights = at<float>(ws, l.aw);
+    if (cut) *cut = at<float>(ws, l.aw) + l.cap;
+    return PACES_OK;
+}
+
+int paces_proposal_score(paces_ctx* c, const paces_basis* x, const float* weights, const float* cut, const void* params,
+                         float threshold, uint8_t* keep, int64_t keep_cap, float* logits, int32_t* counts,
+                         paces_stream_t stream) {
+    if (!c || !valid_basis(x) || !weights || !params || (keep && keep_cap < x->cap)) return PACES_ERR_BADARG;
+    ProposalOut po{keep, keep_cap, logits, counts};
+    PACES_CHECK_LAUNCH(c, launch_proposal_score(c->nw, c->m, x->keys, x->blk, weights, cut, params, threshold, po,
+                                                c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
+                       "proposal_score");
+    return PACES_OK;
+}
+
+int paces_proposal_features(paces_ctx* c, const paces_basis* x, const float* weights, const float* cut,
+                            uint16_t* feats, uint8_t* valid, paces_stream_t stream) {
+    if (!c || !valid_basis(x) || !weights || !feats || !valid) return PACES_ERR_BADARG;
+    PACES_CHECK_LAUNCH(c, launch_proposal_features(c->nw, c->m, x->keys, x->blk, weights, cut, feats, valid, c->num_sms,
+                                                   reinterpret_cast<cudaStream_t>(stream)),
+                       "proposal_features");
+    return PACES_OK;
+}
+
+int paces_proposal_labels(paces_ctx* c, const paces_basis* x, const paces_basis* y, uint8_t* labels,
+                          paces_stream_t stream) {
+    if (!c || !valid_basis(x) || !valid_basis(y) || !labels) return PACES_ERR_BADARG;
+    PACES_CHECK_LAUNCH(c, launch_proposal_labels(c->nw, c->m, x->keys, x->blk, y->keys, y->blk, labels, c->num_sms,
+                                                 reinterpret_cast<cudaStream_t>(stream)),
+                       "proposal_labels");
+    return PACES_OK;
+}
+
+namespace {
+int device_sms() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    return sms;
+}
+}  // namespace
+
+int paces_mlp_pack(const float* master, void* params, paces_stream_t stream) {
+    if (!master || !params) return PACES_ERR_BADARG;
+    return launch_mlp_pack(master, params, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int paces_mlp_forward(const void* params, const uint16_t* x, int64_t n, float* logits, paces_stream_t stream) {
+    if (!params || n < 0 || (n > 0 && (!x || !logits))) return PACES_ERR_BADARG;
+    const int sms = device_sms();
+    if (sms < 1) return PACES_ERR_CUDA;
+    return launch_mlp_forward(params, x, n, logits, sms, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int paces_mlp_backward(const void* params, const uint16_t* x, const float* y, const float* sw, int64_t n,
+                       float inv_norm, float* grads, double* loss, paces_stream_t stream) {
+    if (!params || !grads || n < 0 || (n > 0 && (!x || !y || !sw))) return PACES_ERR_BADARG;
+    const int sms = device_sms();
+    if (sms < 1) return PACES_ERR_CUDA;
+    return launch_mlp_backward(params, x, y, sw, n, inv_norm, grads, loss, sms, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int paces_mlp_adam(float* master, float* m1, float* m2, float* grads, int32_t t, float lr, float beta1, float beta2,
+                   float eps, void* params, paces_stream_t stream) {
+    if (!master || !m1 || !m2 || !grads || !params || t < 1) return PACES_ERR_BADARG;
+    return launch_mlp_adam(master, m1, m2, grads, t, lr, beta1, beta2, eps, params,
+                           reinterpret_cast<cudaStream_t>(stream));
+}
 
 // ---- batched trajectories ------------------------------------------------------------------
 int paces_batch_create(int32_t max_items, int32_t n_streams, paces_batch** out) {

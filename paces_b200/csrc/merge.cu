@@ -20,10 +20,11 @@ __device__ __forceinline__ int run_source(const ModelDev& m, int p, int j) {
 // Element `src` of X as it appears in run j of block p: key and order flag
 // (0 = floor hole, 1 = real, 2 = ceiling hole).
 template <int NW>
-__device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __restrict__ X, int p,
-                                         int j, int64_t src, Key<NW>& k, int& flag) {
+__device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __restrict__ X, const MergeWs& ws,
+                                         int p, int j, int64_t src, Key<NW>& k, int& flag) {
     k = load_key<NW>(X, src);
     flag = 1;
+    if (ws.keep && j != RUN_SELF && src < ws.keep_cap && !__ldg(ws.keep + j * ws.keep_cap + src)) flag = 2;
     if (j == RUN_UP || j == RUN_DOWN) {
         const int w = m.word[p];
         const int sh = m.shift[p];
@@ -64,14 +65,14 @@ __device__ __forceinline__ int cmp_kf(const Key<NW>& a, int fa, const Key<NW>& b
 // Elements of run (p, j) that precede (key, flag): strictly smaller, or not larger when
 // `upper` (the element's own run index is larger than j).
 template <int NW>
-__device__ int run_bound(const ModelDev& m, const uint64_t* __restrict__ X, int p, int j, int lo,
-                         int len, const Key<NW>& key, int flag, bool upper) {
+__device__ int run_bound(const ModelDev& m, const uint64_t* __restrict__ X, const MergeWs& ws, int p, int j,
+                         int lo, int len, const Key<NW>& key, int flag, bool upper) {
     int a = 0, b = len;
     while (a < b) {
         const int mid = (a + b) >> 1;
         Key<NW> k2;
         int f2;
-        run_elem<NW>(m, X, p, j, lo + mid, k2, f2);
+        run_elem<NW>(m, X, ws, p, j, lo + mid, k2, f2);
         const int c = cmp_kf(k2, f2, key, flag);
         if (upper ? (c <= 0) : (c < 0)) a = mid + 1; else b = mid;
     }
@@ -201,13 +202,13 @@ __global__ void __launch_bounds__(256) merge_split_kernel(ModelDev m, const uint
         const int i = (s - ws.split_off[r]) * stride;
         Key<NW> k;
         int f;
-        run_elem<NW>(m, X, p, j, ws.run_lo[r] + i, k, f);
+        run_elem<NW>(m, X, ws, p, j, ws.run_lo[r] + i, k, f);
         int rank = 0;
 #pragma unroll 1
         for (int jj = 0; jj < kRuns; ++jj) {
             int co;
             if (jj == j) co = i;
-            else co = run_bound<NW>(m, X, p, jj, ws.run_lo[p * kRuns + jj], ws.run_len[p * kRuns + jj],
+            else co = run_bound<NW>(m, X, ws, p, jj, ws.run_lo[p * kRuns + jj], ws.run_len[p * kRuns + jj],
                                     k, f, jj < j);
             ws.split_co[int64_t(s) * kRuns + jj] = co;
             rank += co;
@@ -335,7 +336,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             if (st > 0) {
                 Key<NW> k;
                 int f;
-                run_elem<NW>(m, X, p, j, int64_t(lo) + st - 1, k, f);
+                run_elem<NW>(m, X, ws, p, j, int64_t(lo) + st - 1, k, f);
                 s_pk[j] = k;
                 s_pf[j] = f;
                 s_pv[j] = 1;
@@ -394,7 +395,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
             Key<NW> k;
             int f;
-            run_elem<NW>(m, X, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
+            run_elem<NW>(m, X, ws, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
             s_key.set(e, k);
             s_flag[e] = uint8_t(f);
             s_perm[e] = 0xffff;  // every rank must be claimed below

@@ -13,6 +13,8 @@
 //   FROM_RIGHT X_{p+1}                  (left hops)
 //   UP         X_p with n_p + 1         (b^dagger at the exciton site; ceiling n_p = maxd-1 is a hole)
 //   DOWN       X_p with n_p - 1         (b at the exciton site; floor n_p = 0 is a hole)
+// An expansion may also take a keep mask over the images (the learned proposal): a
+// dropped image keeps its key and sorts like a ceiling hole, so it is never emitted.
 // A hole keeps a placeholder key that preserves the run's order (DOWN: fields after p
 // cleared; UP: all bits below field p set) and a flag that sorts it before (DOWN) or
 // after (UP) real keys with the same words, so holes never produce output.
@@ -42,6 +44,11 @@ struct MergeWs {
     unsigned long long* tile_state;  // [tile_cap] look-back words
     int split_cap;
     int tile_cap;
+    // optional candidate filter (expansion only): keep[j * keep_cap + src] == 0 drops the
+    // image of source element src under run j (j = 1..4); dropped images sort like
+    // ceiling holes (after real elements with the same key) and are never emitted
+    const uint8_t* keep;
+    int64_t keep_cap;
 };
 
 struct MergeOut {

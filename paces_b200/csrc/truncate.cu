@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
                                                           uint64_t seed, uint64_t step,
                                                           uint64_t* __restrict__ out_keys,
                                                           int* __restrict__ out_blk, int64_t out_cap,
-                                                          int* status) {
+                                                          float* __restrict__ out_w, int* status) {
     __shared__ unsigned long long s_k[kTruncTile];
     __shared__ int s_blk[kMaxSites + 1];
     __shared__ int s_w[8][3];
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t i0 = int64_t(t) * kTruncTile;
         const int n = int(min(int64_t(kTruncTile), S - i0));
-        if (!all)
+        if (!all || out_w)
             for (int e = tid; e < n; e += 256) s_k[e] = weight_bits<C64>(psi, i0 + e, status);
         __syncthreads();
         // per-thread chunk [q0, q1): counts of above / tied / hash-kept tied states
@@ -414,6 +414,7 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
                     uint64_t* dst = out_keys + out * NW;
 #pragma unroll
                     for (int w = 0; w < NW; ++w) dst[w] = src[w];
+                    if (out_w) out_w[out] = float(__longlong_as_double((long long)s_k[q]));
                 } else {
                     raise_status(status, PACES_ERR_CAPACITY);
                 }
@@ -425,8 +426,10 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
 
 __global__ void trunc_finalize_kernel(ModelDev m, const int* __restrict__ x_blk, int64_t maxstates,
                                       TruncWs ws, int* out_blk, int64_t out_cap, int* n_tied_out,
-                                      int* status) {
+                                      float* cut_out, int* status) {
     if (threadIdx.x != 0) return;
+    // the cut: |psi| of the smallest kept state when states were dropped, else 0
+    if (cut_out) *cut_out = ws.sel[SEL_ALL] ? 0.f : float(__longlong_as_double(ws.sel[SEL_W + 0]));
     const int L = m.L;
     const long long S = ws.sel[SEL_S];
     long long total = ws.sel[SEL_ALL] ? S : maxstates;
@@ -444,8 +447,8 @@ __global__ void trunc_finalize_kernel(ModelDev m, const int* __restrict__ x_blk,
 template <int NW, bool C64>
 int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_blk, const void* psi,
                       int64_t maxstates, int shuffle, uint64_t seed, uint64_t step, const TruncWs& ws,
-                      uint64_t* out_keys, int* out_blk, int64_t out_cap, int* n_tied_out, int* status,
-                      int num_sms, cudaStream_t st) {
+                      uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w, int* n_tied_out,
+                      int* status, int num_sms, cudaStream_t st) {
     const int g = num_sms * 4;
     trunc_init_kernel<<<1, 1024, 0, st>>>(m, x_blk, maxstates, ws);
     trunc_hist_all_kernel<C64><<<g, 256, 0, st>>>(psi, ws, status);
@@ -466,33 +469,34 @@ int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_bl
     trunc_count_kernel<C64><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
     trunc_scan_kernel<<<1, 1024, 0, st>>>(ws);
     trunc_write_kernel<NW, C64><<<g, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
-                                                   out_blk, out_cap, status);
-    trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out, status);
+                                                   out_blk, out_cap, out_w, status);
+    trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out,
+                                            out_w ? out_w + out_cap : nullptr, status);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
 template <int NW>
 int dispatch_prec(bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                   const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
-                  const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
+                  const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
                   int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
     if (c64)
         return launch_truncate_t<NW, true>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
-                                           out_keys, out_blk, out_cap, n_tied_out, status, num_sms, st);
+                                           out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
     return launch_truncate_t<NW, false>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
-                                        out_keys, out_blk, out_cap, n_tied_out, status, num_sms, st);
+                                        out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
 }
 
 }  // namespace
 
 int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                     const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
-                    const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
+                    const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
                     int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
 #define PACES_TRUNC_CASE(N)                                                                       \
     case N:                                                                                       \
         return dispatch_prec<N>(c64, m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,   \
-                                out_keys, out_blk, out_cap, n_tied_out, status, num_sms, st);
+                                out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
     switch (nw) {
         PACES_TRUNC_CASE(1)
         PACES_TRUNC_CASE(2)

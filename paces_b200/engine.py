@@ -58,6 +58,20 @@ class DevBasis:
     def count(self) -> int:
         return int(self.blk[self.eng.L].item())
 
+    @classmethod
+    def wrap(cls, eng: "Engine", keys, blk, cap):
+        """A basis over existing device tensors (no copy)."""
+        b = cls.__new__(cls)
+        b.eng, b.cap, b.keys, b.blk = eng, int(cap), keys, blk
+        return b
+
+    def clone(self) -> "DevBasis":
+        n = self.count()
+        b = DevBasis(self.eng, max(n, 1))
+        b.keys[:n] = self.keys[:n]
+        b.blk.copy_(self.blk)
+        return b
+
 
 class DevHMat:
     """Neighbour table [cap, 4] (left, right, down, up; -1 = absent) and row metadata [cap]."""
@@ -270,6 +284,52 @@ class Engine:
     def set_profiling(self, on=True):
         nat.check(self.lib.paces_set_profiling(self.ctx, 1 if on else 0), self.ctx, "set_profiling")
 
+    # ---- learned proposal ---------------------------------------------------------------------
+    def selected(self):
+        """(basis, |psi| float32 per state, cut float32 [1]) of the last paces_step's
+        truncation -- views into the workspace, valid until the next call that uses it."""
+        sel, wp, cp = nat.Basis(), ctypes.c_void_p(), ctypes.c_void_p()
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_selected_view(self.ctx, ws, nb, ctypes.byref(sel), ctypes.byref(wp), ctypes.byref(cp)),
+                  self.ctx, "selected_view")
+        base = self.ws.data_ptr()
+        cap = int(sel.cap)
+        ok, obk, ow, oc = sel.keys - base, sel.blk - base, wp.value - base, cp.value - base
+        keys = self.ws[ok:ok + cap * self.nw * 8].view(torch.int64).view(cap, self.nw)
+        blk = self.ws[obk:obk + (self.L + 1) * 4].view(torch.int32)
+        w = self.ws[ow:ow + cap * 4].view(torch.float32)
+        cut = self.ws[oc:oc + 4].view(torch.float32)
+        return DevBasis.wrap(self, keys, blk, cap), w, cut
+
+    def proposal_features(self, x: DevBasis, w, cut):
+        n = x.count()
+        feats = torch.empty((max(4 * n, 1), 16), dtype=torch.bfloat16, device=self.device)
+        valid = torch.empty(max(4 * n, 1), dtype=torch.uint8, device=self.device)
+        nat.check(self.lib.paces_proposal_features(self.ctx, ctypes.byref(x.c()), _ptr(w), _ptr(cut), _ptr(feats),
+                                                   _ptr(valid), _stream(self.device)), self.ctx, "proposal_features")
+        return feats[:4 * n], valid[:4 * n]
+
+    def proposal_labels(self, x: DevBasis, y: DevBasis):
+        n = x.count()
+        lab = torch.empty(max(4 * n, 1), dtype=torch.uint8, device=self.device)
+        nat.check(self.lib.paces_proposal_labels(self.ctx, ctypes.byref(x.c()), ctypes.byref(y.c()), _ptr(lab),
+                                                 _stream(self.device)), self.ctx, "proposal_labels")
+        return lab[:4 * n]
+
+    def proposal_score(self, x: DevBasis, w, cut, params, threshold=0.0, keep=None):
+        """Logits of every event of x (tensor cores); keep (optional, uint8 [5][cap]) gets the
+        keep mask.  Returns (logits, (existing, kept))."""
+        n = x.count()
+        logits = torch.empty(max(4 * n, 1), dtype=torch.float32, device=self.device)
+        counts = torch.zeros(2, dtype=torch.int32, device=self.device)
+        kcap = keep.shape[1] if keep is not None else 0
+        nat.check(self.lib.paces_proposal_score(self.ctx, ctypes.byref(x.c()), _ptr(w), _ptr(cut), _ptr(params),
+                                                float(threshold), _ptr(keep), int(kcap), _ptr(logits), _ptr(counts),
+                                                _stream(self.device)), self.ctx, "proposal_score")
+        self.raise_status("proposal_score")
+        c = counts.cpu().tolist()
+        return logits[:4 * n], (c[0], c[1])
+
     def stage_times(self):
         """Per-stage device milliseconds of the last profiled step."""
         ms = (ctypes.c_float * 7)()
@@ -327,6 +387,7 @@ class Trajectory:
         self.last = None
         self.use_graph = bool(graph)
         self._graphs = {}
+        self.proposal = None  # (packed MLP parameters on the device, threshold) or None
 
     def _alloc(self):
         e = self.eng
@@ -381,6 +442,10 @@ class Trajectory:
         p.shuffle_seed = 0 if self.shuffle_seed is None else int(self.shuffle_seed) & 0xFFFFFFFFFFFFFFFF
         p.step_index = self.step_index
         p.explosion_cutoff = self.explosion_cutoff
+        if self.proposal is not None:
+            p.proposal = 1
+            p.proposal_threshold = float(self.proposal[1])
+            p.proposal_params = self.proposal[0].data_ptr()
         return p
 
     def _capture(self, dt):
@@ -397,7 +462,8 @@ class Trajectory:
         return g, prm
 
     def _graph_step(self, dt):
-        key = (self.cur, float(dt))
+        key = (self.cur, float(dt),
+               None if self.proposal is None else (self.proposal[0].data_ptr(), float(self.proposal[1])))
         if key not in self._graphs:
             self._graphs[key] = self._capture(dt)
         self._graphs[key][0].replay()
@@ -454,6 +520,7 @@ class TrajectoryBatch:
         self.lib = nat.load()
         self.use_graph = bool(graph)
         self._graphs = {}
+        self.proposal = None  # (packed MLP parameters on the device, threshold) or None
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             nat.check(self.lib.paces_batch_create(len(trajs), int(n_streams), ctypes.byref(h)), None, "batch_create")
