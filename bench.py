@@ -42,7 +42,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="c128", choices=["c128", "c64"])
+    ap.add_argument("--precision", default="c64", choices=["c128", "c64"],
+                    help="c64: the FP32 form, checked against a complex128 run of the same trajectory; "
+                         "c128: the plain FP64 form alone")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="c64: skip the complex128 comparison run over t = 10/J")
     ap.add_argument("--maxstates", type=int, default=1 << 22)
     ap.add_argument("--nchain", type=int, default=32)
     ap.add_argument("--g", type=float, default=1.5)
@@ -52,8 +56,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verbose", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
-                    help="plain: one N=32 chain at maxstates 2^22; batched: 64 trajectories drawn from --seed")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "learned"],
+                    help="plain: one N=32 chain at maxstates 2^22; batched: 64 trajectories drawn from --seed; "
+                         "learned: the learned proposal + complex64 against the plain complex128 run")
+    ap.add_argument("--recall", type=float, default=0.999, help="learned: target recall of the keep threshold")
+    ap.add_argument("--train-seeds", type=int, default=8, help="learned: plain training runs (shuffle seeds 0..n-1)")
+    ap.add_argument("--learn-from", type=int, default=50, help="learned: plain steps before the proposal is used")
+    ap.add_argument("--total-steps", type=int, default=200, help="learned: steps of the compared trajectories")
     ap.add_argument("--no-graph", action="store_true", help="step without CUDA-graph replay")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--batch", type=int, default=64, help="trajectories of the batched workload")
@@ -280,7 +289,8 @@ def run_reference(a):
     value, desc, _, _ = oracle_sample(a, 1 << 16, steps, max(0, a.warmup))
     cfg = {"workload": workload_name(a), "nchain": a.nchain, "maxstates": a.maxstates, "g": a.g,
            "enlarge_steps": a.enlarge_steps, "precision": "c128", "bench_sample": "bounded, see cpu_baseline"}
-    line = {"impl": "reference", "metric": "time-steps/s at 4M states", "value": value, "unit": "time-steps/s",
+    line = {"impl": "reference", "metric": "time-steps/s at 4M states: learned+FP32 vs plain FP64, observable err <=1e-5",
+            "value": value, "unit": "time-steps/s",
             "n_gpus": a.gpus, "steps": steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": "time-steps/s", "cores": 1, "kind": "port", "sample": desc},
@@ -361,6 +371,10 @@ def run_ours(a):
     if not a.no_e2e:
         e2e = run_e2e(a, eng, tr, barrier, dist)
 
+    compare = None
+    if a.precision == "c64" and not a.no_compare:
+        compare = compare_precisions(a, f"cuda:{local}", dist)
+
     total_steps = a.steps * world
     value = total_steps / (ms / 1e3)
     taylor_ms = stage_sum["taylor"] / n_prof
@@ -383,9 +397,13 @@ def run_ours(a):
                "states_per_step": int(S_mean), "taylor_terms_per_step": terms, "prep_steps": nprep,
                "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}",
                "cuda_graph": not a.no_graph,
-               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")}}
+               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")},
+               "form": ("complex64 amplitudes and SpMV, fp64 norms / stop test / sums; learned proposal off "
+                        "(--workload learned measures it)") if a.precision == "c64" else "complex128 plain"}
         line = {
-            "metric": "time-steps/s at 4M states", "value": value, "unit": "time-steps/s", "n_gpus": world,
+            "metric": "time-steps/s at 4M states: learned+FP32 vs plain FP64, observable err <=1e-5"
+                      if a.precision == "c64" else "time-steps/s at 4M states (plain FP64)",
+            "value": value, "unit": "time-steps/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "kernel": "taylor_kernel", "achieved": achieved, "peak": peak,
@@ -396,10 +414,45 @@ def run_ours(a):
             "stage_ms": {k: v / n_prof for k, v in stage_sum.items()}, "stage_steps": n_prof,
             "clocks": clocks, "gpu_launches": launches, "cpu_baseline": cpu, "e2e": e2e,
         }
+        if compare is not None:
+            line.update(compare)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def compare_precisions(a, dev, dist, total=200, window_from=50):
+    """The same trajectory (t = 0 .. total * dt) in complex128 -- the FP64 plain oracle --
+    and in complex64: time-steps/s of both over steps window_from..total and the largest
+    difference of every observable over the whole run."""
+    import torch
+    from paces_b200.engine import Engine
+    stream = torch.cuda.current_stream()
+    obs, rate = {}, {}
+    for prec in ("c128", "c64"):
+        eng = Engine(model_params(a, prec), device=dev)
+        tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
+        recs = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(window_from)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        recs += [tr.step(evolve=True, dt=a.dt) for _ in range(total - window_from)]
+        e1.record(stream)
+        e1.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), dist)
+        rate[prec] = (total - window_from) / (ms / 1e3)
+        L = a.nchain
+        obs[prec] = {"n_exc": np.array([list(r.n_exc)[:L] for r in recs]),
+                     "n_pho": np.array([list(r.n_pho)[:L] for r in recs]),
+                     "energy": np.array([r.energy_re for r in recs]), "norm": np.array([r.norm for r in recs])}
+        eng.close()
+    err = {k: float(np.max(np.abs(obs["c128"][k] - obs["c64"][k]))) for k in obs["c128"]}
+    return {"plain_c128": {"value": rate["c128"], "unit": "time-steps/s",
+                           "window": f"steps {window_from + 1}..{total} of a fresh run"},
+            "c64_same_window": {"value": rate["c64"], "unit": "time-steps/s"},
+            "speedup_c64_vs_c128": rate["c64"] / rate["c128"],
+            "observable_error": {"c64_vs_c128": err, "t_end": total * a.dt, "bound": 1e-5,
+                                 "within_bound": all(v <= 1e-5 for v in err.values())}}
 
 
 def run_e2e(a, eng, tr, barrier, dist):
@@ -591,12 +644,160 @@ def run_batched(a):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------------------------
+# learned workload: the proposal + complex64 against the plain complex128 run
+# --------------------------------------------------------------------------------------------
+def run_learned(a):
+    import torch
+    from paces_b200 import _native as nat
+    from paces_b200.engine import Engine
+    from paces_b200.proposal import LearnedTrajectory, ProposalMLP, collect, threshold_for_recall
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = f"cuda:{local}"
+    steps, lf = a.total_steps, a.learn_from
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    def observables(recs):
+        L = a.nchain
+        return {"n_exc": np.array([list(r.n_exc)[:L] for r in recs]), "n_pho": np.array([list(r.n_pho)[:L] for r in recs]),
+                "energy": np.array([r.energy_re for r in recs]), "norm": np.array([r.norm for r in recs])}
+
+    def plain(precision):
+        eng = Engine(model_params(a, precision), device=dev)
+        tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
+        recs = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(lf)]
+        window, ms = timed(lambda: [tr.step(evolve=True, dt=a.dt) for _ in range(steps - lf)])
+        eng.close()
+        return recs + window, ms
+
+    # 1. the plain complex128 run (the oracle of the comparison) and the plain complex64 run
+    ref, ms128 = plain("c128")
+    r64, ms64 = plain("c64")
+    # 2. training data: the first learn_from steps of plain complex64 runs at shuffle seeds 0..n-1
+    xs, ys, sws, hold = [], [], [], None
+    t0 = time.perf_counter()
+    for seed in range(a.train_seeds):
+        eng = Engine(model_params(a, "c64"), device=dev)
+        tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps)
+        tr.shuffle_seed = seed
+        ds, h = collect(tr, lf, a.dt, neg_per_pos=4, max_pos=25_000, seed=seed, held_out=lf - 5)
+        xs.append(ds.x)
+        ys.append(ds.y)
+        sws.append(ds.sw)
+        hold = hold or h
+        eng.close()
+    collect_s = time.perf_counter() - t0
+    x, y, sw = torch.cat(xs), torch.cat(ys), torch.cat(sws)
+    mlp = ProposalMLP(dev, seed=0)
+    t0 = time.perf_counter()
+    losses = mlp.fit(x, y, sw, epochs=2, batch=8192, lr=2e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    thr0 = threshold_for_recall(mlp.forward(hold[0]), hold[1], a.recall)
+    # 3. the learned run: plain complex64 for learn_from steps, then the proposal
+    eng = Engine(model_params(a, "c64"), device=dev)
+    tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
+    recs = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(lf)]
+    lt = LearnedTrajectory(tr, mlp, thr0, judge_every=10, target_recall=a.recall)
+    with ClockSampler(local) as clk:
+        window, ms = timed(lambda: [lt.step(a.dt) for _ in range(steps - lf)])
+    clocks = clk.summary()
+    recs += window
+    # stage split of proposal (non-judge) steps
+    eng.set_profiling(True)
+    use_graph, tr.use_graph = tr.use_graph, False
+    stage = {k: 0.0 for k in nat.STAGES}
+    nprof = 0
+    l0 = eng.kernel_launches()
+    for _ in range(12):
+        judge = lt.k % lt.judge_every == 0
+        lt.step(a.dt)
+        if not judge:
+            for k, v in eng.stage_times().items():
+                stage[k] += v
+            nprof += 1
+    launches_per_step = (eng.kernel_launches() - l0) / 12
+    tr.use_graph = use_graph
+    eng.set_profiling(False)
+    eng.close()
+    ms = max_over_ranks(ms, dist)
+
+    A, B, C = observables(ref), observables(recs), observables(r64)
+    err = {k: float(np.max(np.abs(A[k] - B[k]))) for k in A}
+    err64 = {k: float(np.max(np.abs(A[k] - C[k]))) for k in A}
+    nwin = steps - lf
+    value = nwin * world / (ms / 1e3)
+    cs = 8
+    taylor_ms = stage["taylor"] / max(nprof, 1)
+    win = recs[lf + 1:]
+    taylor_alg = statistics.mean(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in win)
+    peak, peak_kind = read_peaks()
+    achieved = taylor_alg / (taylor_ms / 1e3) / 1e9 if taylor_ms > 0 else None
+    if rank == 0:
+        cfg = {"workload": f"holstein_periodic_n{a.nchain}_cutoff15_g{a.g:g}_maxstates{a.maxstates}_dt{a.dt:g}"
+                           f"_es{a.enlarge_steps}_learned_c64",
+               "nchain": a.nchain, "g": a.g, "omega0": 1.0, "J": 1.0, "dt": a.dt, "maxstates": a.maxstates,
+               "enlarge_steps": a.enlarge_steps, "precision": "c64 (fp64 norms, stop test and sums)",
+               "timed_steps": f"{lf + 1}..{steps} (proposal steps and every 10th a full-expansion judge step)",
+               "training": {"runs": a.train_seeds, "steps_per_run": lf, "samples": int(x.shape[0]),
+                            "positives": int(y.sum().item()), "epochs": 2, "loss": losses, "collect_s": collect_s,
+                            "train_s": train_s},
+               "target_recall": a.recall, "threshold_start": thr0, "threshold_end": lt.threshold,
+               "states_per_step_learned": statistics.mean(r.n_states for r in win),
+               "states_per_step_plain": statistics.mean(r.n_states for r in ref[lf + 1:]),
+               "enlarged_learned": statistics.mean(r.n_enlarged for r in win),
+               "enlarged_plain": statistics.mean(r.n_enlarged for r in ref[lf + 1:]),
+               "judges": [[j.step, j.recall, j.candidates, j.kept] for j in lt.judges],
+               "l2": "inputs larger than L2", "parallelism": f"replicas x{world}", "cuda_graph": not a.no_graph}
+        line = {
+            "metric": "time-steps/s at 4M states: learned+FP32 vs plain FP64, observable err <=1e-5",
+            "value": value, "unit": "time-steps/s", "n_gpus": world, "steps": nwin, "warmup": lf,
+            "ms_per_step": ms / nwin, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64", "data": "synthetic", "config": cfg,
+            "plain_c128": {"value": nwin / (ms128 / 1e3), "unit": "time-steps/s", "ms_per_step": ms128 / nwin},
+            "plain_c64": {"value": nwin / (ms64 / 1e3), "unit": "time-steps/s", "ms_per_step": ms64 / nwin},
+            "speedup_vs_plain_c128": ms128 / ms,
+            "observable_error": {"learned_c64": err, "plain_c64": err64, "bound": 1e-5,
+                                 "within_bound": all(v <= 1e-5 for v in err.values())},
+            "roofline": {"bound": "hbm", "kernel": "taylor_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": None if achieved is None else achieved / peak,
+                         "traffic": None, "launch_ms": taylor_ms},
+            "stage_ms": {k: v / max(nprof, 1) for k, v in stage.items()},
+            "clocks": clocks, "gpu_launches": int(round(launches_per_step * nwin)), "cpu_baseline": None, "e2e": None,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
     elif a.workload == "batched":
         run_batched(a)
+    elif a.workload == "learned":
+        a.precision = "c64"
+        run_learned(a)
     else:
         run_ours(a)
 

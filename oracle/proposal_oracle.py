@@ -99,7 +99,7 @@ def features(model, rows, weights, cut=0.0):
         else:
             inside = (s >= 0) & (s < L)
             s = np.clip(s, 0, L - 1)
-        v = cocc[r, s].astype(np.float32) / (maxd[s] - 1).astype(np.float32)
+        v = cocc[r, s].astype(np.float32) * (np.float32(1) / (maxd[s] - 1).astype(np.float32))
         f[:, d + 4] = np.where(inside, v, np.float32(0))
     f[:, 9] = cocc.sum(axis=1).astype(np.float32) * np.float32(1.0 / 16.0)
     w = np.asarray(weights, dtype=np.float32)[i]

@@ -53,18 +53,50 @@ __device__ __forceinline__ bool image_of(const ModelDev& m, const Key<NW>& k, in
     return true;
 }
 
+// Per-site constants of the features, staged in shared memory by each kernel: where the
+// field lives (word, shift, mask) and 1 / (max_ho_dim - 1) rounded to fp32.
+struct SiteTab {
+    uint8_t word[kMaxSites];
+    uint8_t shift[kMaxSites];
+    uint16_t mask[kMaxSites];
+    float inv[kMaxSites];
+};
+
+__device__ __forceinline__ void load_site_tab(const ModelDev& m, SiteTab& t) {
+    for (int s = threadIdx.x; s < m.L; s += blockDim.x) {
+        t.word[s] = m.word[s];
+        t.shift[s] = m.shift[s];
+        t.mask[s] = uint16_t((1u << m.bits[s]) - 1u);
+        t.inv[s] = 1.0f / float(m.maxd[s] - 1);
+    }
+}
+
 template <int NW>
-__device__ __forceinline__ void event_features(const ModelDev& m, const Key<NW>& c, int cpos, int j, float w,
-                                               float log_cut, float f[kMlpIn]) {
+__device__ __forceinline__ uint32_t tab_field(const SiteTab& t, const Key<NW>& k, int s) {
+    uint64_t word = 0;
+    const int w = t.word[s];
+#pragma unroll
+    for (int q = 0; q < NW; ++q)
+        if (q == w) word = k.w[q];
+    return uint32_t(word >> t.shift[s]) & t.mask[s];
+}
+
+template <int NW>
+__device__ __forceinline__ void event_features(const ModelDev& m, const SiteTab& tab, const Key<NW>& c, int cpos,
+                                               int j, float w, float log_cut, float f[kMlpIn]) {
 #pragma unroll
     for (int d = -4; d <= 4; ++d) {
         int s = cpos + d;
         float v = 0.f;
         if (m.periodic) {
-            s = ((s % m.L) + m.L) % m.L;
-            v = float(get_field(m, c, s)) / float(m.maxd[s] - 1);
+            // s is in [-4, L+3] and L >= 3: at most two wraps either way
+            s += s < 0 ? m.L : 0;
+            s += s < 0 ? m.L : 0;
+            s -= s >= m.L ? m.L : 0;
+            s -= s >= m.L ? m.L : 0;
+            v = float(tab_field<NW>(tab, c, s)) * tab.inv[s];
         } else if (s >= 0 && s < m.L) {
-            v = float(get_field(m, c, s)) / float(m.maxd[s] - 1);
+            v = float(tab_field<NW>(tab, c, s)) * tab.inv[s];
         }
         f[d + 4] = v;
     }
@@ -78,7 +110,7 @@ __device__ __forceinline__ void event_features(const ModelDev& m, const Key<NW>&
     if (j == RUN_FROM_LEFT || j == RUN_FROM_RIGHT) {
         elem = float(m.J);
     } else {
-        const float nc = float(get_field(m, c, cpos));
+        const float nc = float(tab_field<NW>(tab, c, cpos));
         elem = float(m.g) * sqrtf(j == RUN_UP ? nc : nc + 1.f);
     }
     f[14] = logf(fmaxf(fabsf(elem), 1e-30f)) * 0.25f;
@@ -109,10 +141,12 @@ __device__ __forceinline__ bool contains(const uint64_t* __restrict__ keys, int 
 // ---- tensor-core inference --------------------------------------------------------------
 constexpr int kSThreads = 128;  // one thread per row of the 128-row MMA tile
 constexpr uint32_t kSOffW1 = 0, kSOffW2 = 2048, kSOffA1 = 10240, kSOffA2 = 14336;
-// 50 KB of dynamic shared memory keeps at most 4 CTAs on an SM, so their 4 x 128 tensor-memory
-// columns always fit the SM's 512 and no allocation waits.
-constexpr size_t kScoreSmem = 50 * 1024;
-constexpr uint32_t kTmemCols = 128;  // D1 in columns [0, 64), D2 in [64, 128)
+// Both layers accumulate into the same 64 tensor-memory columns (D1 is read out before the
+// second MMA is issued).  The 30 KB of operands per CTA let at most 7 CTAs share an SM, so
+// their 7 x 64 columns always fit the SM's 512 and no allocation waits.
+constexpr size_t kScoreSmem = 30 * 1024;
+constexpr uint32_t kTmemCols = 64;
+constexpr int kScoreCtasPerSm = 7;
 
 template <int NW>
 __global__ void __launch_bounds__(kSThreads, 1)
@@ -127,9 +161,11 @@ proposal_score_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* 
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
     __shared__ int s_cnt[2];
+    __shared__ SiteTab s_tab;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int L = m.L;
     for (int i = tid; i <= L; i += kSThreads) s_blk[i] = blk[i];
+    load_site_tab(m, s_tab);
     // weights into the canonical K-major layout (16-byte chunks of 8 bf16)
     for (int c = tid; c < kMlpHid * 2; c += kSThreads) {
         const int n = c >> 1, kc = c & 1;
@@ -187,7 +223,7 @@ proposal_score_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* 
         if (e < nev) {
             Key<NW> child;
             valid = event_image<NW>(m, keys, s_blk, nx, e, j, i, child, cpos);
-            if (valid) event_features<NW>(m, child, cpos, j, __ldg(wts + i), log_cut, f);
+            if (valid) event_features<NW>(m, s_tab, child, cpos, j, __ldg(wts + i), log_cut, f);
         }
         {
             uint32_t pk[8];
@@ -233,7 +269,7 @@ proposal_score_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* 
             tc::fence_after_sync();
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk)
-                tc::mma_bf16(tmem + 64, tc::smem_desc(a2 + kk * 256, 128, 1024), tc::smem_desc(w2 + kk * 256, 128, 1024),
+                tc::mma_bf16(tmem, tc::smem_desc(a2 + kk * 256, 128, 1024), tc::smem_desc(w2 + kk * 256, 128, 1024),
                              idesc, kk > 0 ? 1u : 0u);
             tc::commit(mbar);
         }
@@ -244,7 +280,7 @@ proposal_score_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* 
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             uint32_t v[16];
-            tc::ld16(tmem + row_lane + 64u + uint32_t(c * 16), v);
+            tc::ld16(tmem + row_lane + uint32_t(c * 16), v);
             tc::wait_ld();
 #pragma unroll
             for (int q = 0; q < 16; ++q)
@@ -298,7 +334,9 @@ proposal_features_kernel(ModelDev m, const uint64_t* __restrict__ keys, const in
                          const float* __restrict__ wts, const float* __restrict__ cut, uint16_t* __restrict__ feats,
                          uint8_t* __restrict__ valid) {
     __shared__ int s_blk[kMaxSites + 1];
+    __shared__ SiteTab s_tab;
     for (int i = threadIdx.x; i <= m.L; i += blockDim.x) s_blk[i] = blk[i];
+    load_site_tab(m, s_tab);
     __syncthreads();
     const float log_cut = logf(fmaxf(cut ? __ldg(cut) : 0.f, 1e-30f));
     const int64_t nx = s_blk[m.L], nev = 4 * nx;
@@ -310,7 +348,7 @@ proposal_features_kernel(ModelDev m, const uint64_t* __restrict__ keys, const in
 #pragma unroll
         for (int q = 0; q < kMlpIn; ++q) f[q] = 0.f;
         const bool ok = event_image<NW>(m, keys, s_blk, nx, e, j, i, child, cpos);
-        if (ok) event_features<NW>(m, child, cpos, j, wts[i], log_cut, f);
+        if (ok) event_features<NW>(m, s_tab, child, cpos, j, wts[i], log_cut, f);
         uint32_t pk[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) pk[q] = uint32_t(bf16_bits(f[2 * q])) | (uint32_t(bf16_bits(f[2 * q + 1])) << 16);
@@ -569,7 +607,7 @@ int score_t(const ModelDev& m, const uint64_t* keys, const int* blk, const float
     auto kfn = proposal_score_kernel<NW>;
     if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kScoreSmem)) != cudaSuccess)
         return PACES_ERR_CUDA;
-    kfn<<<num_sms * 4, kSThreads, kScoreSmem, st>>>(m, keys, blk, w, cut, static_cast<const uint8_t*>(params), thr,
+    kfn<<<num_sms * kScoreCtasPerSm, kSThreads, kScoreSmem, st>>>(m, keys, blk, w, cut, static_cast<const uint8_t*>(params), thr,
                                                     out, status);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }

@@ -9,8 +9,8 @@
 // exist (open-chain end, occupation ceiling, floor).
 //
 // Features (16, rounded to bf16) of event (j, i) with image state (p', n'):
-//   f[0..8]  n'_{p'+d} / (max_ho_dim_{p'+d} - 1), d = -4..4 (ring: wrapped; open chain: 0
-//            outside the chain)
+//   f[0..8]  n'_{p'+d} * fp32(1 / (max_ho_dim_{p'+d} - 1)), d = -4..4 (ring: wrapped; open
+//            chain: 0 outside the chain)
 //   f[9]     sum_s n'_s / 16
 //   f[10]    (log max(|psi_i|, 1e-30) - log max(cut, 1e-30)) / 16: the source state's
 //            amplitude relative to the cut of the truncation that kept it (the smallest

@@ -117,7 +117,7 @@ class Dataset:
     negatives: int
 
 
-def collect(tr: Trajectory, steps, dt, neg_per_pos=8, max_neg=200_000, seed=0, held_out=None):
+def collect(tr: Trajectory, steps, dt, neg_per_pos=8, max_neg=200_000, max_pos=100_000, seed=0, held_out=None):
     """Run `steps` plain steps of `tr` and gather labelled events of every step but the last
     (steps whose truncation dropped nothing -- the basis still growing -- have no cut and
     give no samples).
@@ -132,7 +132,16 @@ def collect(tr: Trajectory, steps, dt, neg_per_pos=8, max_neg=200_000, seed=0, h
     prev = None
     hold = None
     for k in range(steps):
-        tr.step(evolve=True, dt=dt)
+        try:
+            tr.step(evolve=True, dt=dt)
+        except nat.PacesError as err:
+            # a tie shuffle over nearly every state (the reference raises there too): take
+            # that step with the deterministic tie rule
+            if err.code != nat.ERR_SHUFFLE:
+                raise
+            seed_, tr.shuffle_seed = tr.shuffle_seed, None
+            tr.step(evolve=True, dt=dt)
+            tr.shuffle_seed = seed_
         sel, w, cut = eng.selected()
         cur = sel.clone()
         saturated = float(cut.item()) > 0.0
@@ -143,6 +152,8 @@ def collect(tr: Trajectory, steps, dt, neg_per_pos=8, max_neg=200_000, seed=0, h
                 hold = (pf, lab.clone())
             pos = torch.nonzero(lab == 1).flatten()
             neg = torch.nonzero(lab == 0).flatten()
+            if pos.numel() > max_pos:
+                pos = pos[torch.randperm(pos.numel(), device=eng.device, generator=gen)[:max_pos]]
             keep_neg = min(int(neg.numel()), max(neg_per_pos * int(pos.numel()), 1), max_neg)
             if keep_neg < neg.numel():
                 neg = neg[torch.randperm(neg.numel(), device=eng.device, generator=gen)[:keep_neg]]
@@ -185,17 +196,43 @@ class JudgeRecord:
 
 class LearnedTrajectory:
     """A trajectory whose expansions keep only the images the MLP scores above the
-    threshold; every judge_every-th step runs the full expansion and re-checks recall."""
+    threshold.  Every judge_every-th step runs the full expansion instead; its candidates
+    are scored and, once the next step has truncated, labelled: the recall the threshold
+    had on them is recorded, the network is fine-tuned on them (online_epochs passes of
+    Adam over a class-balanced sample, 0 to switch off) and the threshold is re-set to keep
+    target_recall of their positives (up or down)."""
 
-    def __init__(self, tr: Trajectory, mlp: ProposalMLP, threshold, judge_every=10, target_recall=0.999):
+    def __init__(self, tr: Trajectory, mlp: ProposalMLP, threshold, judge_every=10, target_recall=0.999,
+                 online_epochs=1, online_lr=1e-3, max_pos=10_000, neg_per_pos=4):
         self.tr = tr
         self.mlp = mlp
         self.threshold = float(threshold)
         self.judge_every = int(judge_every)
         self.target_recall = float(target_recall)
+        self.online_epochs = int(online_epochs)
+        self.online_lr = float(online_lr)
+        self.max_pos = int(max_pos)
+        self.neg_per_pos = int(neg_per_pos)
         self.k = 0
         self._pending = None
         self.judges: list[JudgeRecord] = []
+        self._gen = torch.Generator(device=tr.eng.device)
+        self._gen.manual_seed(0)
+
+    def _learn(self, feats, lab):
+        dev = feats.device
+        pos = torch.nonzero(lab == 1).flatten()
+        neg = torch.nonzero(lab == 0).flatten()
+        if pos.numel() == 0 or neg.numel() == 0:
+            return
+        if pos.numel() > self.max_pos:
+            pos = pos[torch.randint(0, pos.numel(), (self.max_pos,), device=dev, generator=self._gen)]
+        kn = min(int(neg.numel()), self.neg_per_pos * int(pos.numel()))
+        neg = neg[torch.randint(0, neg.numel(), (kn,), device=dev, generator=self._gen)]
+        x = torch.cat([feats[pos], feats[neg]])
+        y = torch.cat([torch.ones(pos.numel(), device=dev), torch.zeros(neg.numel(), device=dev)])
+        sw = torch.where(y > 0, 0.5 / pos.numel(), 0.5 / neg.numel()).float() * float(x.shape[0])
+        self.mlp.fit(x, y, sw, epochs=self.online_epochs, lr=self.online_lr, seed=self.k)
 
     def step(self, dt):
         tr, eng = self.tr, self.tr.eng
@@ -204,22 +241,32 @@ class LearnedTrajectory:
         rec = tr.step(evolve=True, dt=dt)
         sel, w, cut = eng.selected()
         if self._pending is not None:
-            px, logits, thr_before = self._pending
+            px, feats, logits, thr_before = self._pending
             lab = eng.proposal_labels(px, sel)
             pos = lab == 1
             npos = int(pos.sum().item())
             recall = float(((logits > thr_before) & pos).sum().item()) / max(npos, 1)
+            cand_mask = (lab == 0) | (lab == 1)
+            cand = int(cand_mask.sum().item())
+            kept = int((cand_mask & (logits > thr_before)).sum().item())
             thr = self.threshold
-            if recall < self.target_recall:
-                thr = min(thr, threshold_for_recall(logits, lab, self.target_recall))
-            cand = int(((lab == 0) | (lab == 1)).sum().item())
-            kept = int((((lab == 0) | (lab == 1)) & (logits > thr_before)).sum().item())
+            if npos:
+                if self.online_epochs > 0:
+                    self._learn(feats, lab)
+                    # the threshold needs the positives' logits only
+                    pidx = torch.nonzero(pos).flatten()
+                    logits = torch.full_like(logits, float("-inf"))
+                    logits[pidx] = self.mlp.forward(feats[pidx].contiguous())
+                thr = threshold_for_recall(logits, lab, self.target_recall)
             self.judges.append(JudgeRecord(self.k - 1, recall, thr_before, thr, cand, kept))
             self.threshold = thr
             self._pending = None
-        if judge:
+        if judge and float(cut.item()) > 0.0:
             x = sel.clone()
-            logits, _ = eng.proposal_score(x, w[:x.count()].clone(), cut.clone(), self.mlp.params, self.threshold)
-            self._pending = (x, logits.clone(), self.threshold)
+            n = x.count()
+            ww, cc = w[:n].clone(), cut.clone()
+            logits, _ = eng.proposal_score(x, ww, cc, self.mlp.params, self.threshold)
+            feats = eng.proposal_features(x, ww, cc)[0] if self.online_epochs > 0 else None
+            self._pending = (x, feats, logits.clone(), self.threshold)
         self.k += 1
         return rec
