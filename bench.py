@@ -56,13 +56,17 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verbose", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "learned"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "learned", "longchain"],
                     help="plain: one N=32 chain at maxstates 2^22; batched: 64 trajectories drawn from --seed; "
                          "learned: the learned proposal + complex64 against the plain complex128 run")
     ap.add_argument("--recall", type=float, default=0.999, help="learned: target recall of the keep threshold")
     ap.add_argument("--train-seeds", type=int, default=8, help="learned: plain training runs (shuffle seeds 0..n-1)")
     ap.add_argument("--learn-from", type=int, default=50, help="learned: plain steps before the proposal is used")
     ap.add_argument("--total-steps", type=int, default=200, help="learned: steps of the compared trajectories")
+    ap.add_argument("--realizations", type=int, default=4, help="longchain: disorder realizations batched")
+    ap.add_argument("--sigma", type=float, default=0.5, help="longchain: site-energy disorder (Gaussian sigma)")
+    ap.add_argument("--compare-steps", type=int, default=0,
+                    help="longchain: steps of realization 0 compared against a complex128 run (0: none)")
     ap.add_argument("--no-graph", action="store_true", help="step without CUDA-graph replay")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--batch", type=int, default=64, help="trajectories of the batched workload")
@@ -789,6 +793,145 @@ def run_learned(a):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------------------------
+# long chain: N=64 rings with site-energy disorder, realizations batched in one launch
+# --------------------------------------------------------------------------------------------
+def longchain_site_eps(seed, nchain, sigma):
+    """Site energies of disorder realization `seed`: numpy.random.default_rng(seed).normal(0, sigma, N)."""
+    return np.random.default_rng(seed).normal(0.0, sigma, nchain)
+
+
+def run_longchain(a):
+    import torch
+    from paces_b200 import _native as nat
+    from paces_b200.engine import Engine, ModelParams, TrajectoryBatch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = f"cuda:{local}"
+    cs = 8 if a.precision == "c64" else 16
+
+    def params(seed, precision):
+        return ModelParams(nchain=a.nchain, max_ho_dims=[16] * a.nchain, J=1.0, g=a.g, hbar_omega=1.0,
+                           periodic=True, site_eps=list(longchain_site_eps(seed, a.nchain, a.sigma)),
+                           precision=precision)
+
+    seeds = [a.seed + rank * a.realizations + r for r in range(a.realizations)]
+    trajs = []
+    for sd in seeds:
+        eng = Engine(params(sd, a.precision), device=dev)
+        trajs.append(start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph))
+    batch = TrajectoryBatch(trajs, n_streams=min(4, a.realizations), graph=not a.no_graph)
+    nprep = 0
+    while True:
+        recs = batch.step(evolve=True, dt=a.dt)
+        nprep += 1
+        log(a, f"prep {nprep}: " + " ".join(f"{r.n_select}/{r.n_states}" for r in recs))
+        if all(r.n_select >= a.maxstates for r in recs) or nprep >= 80:
+            break
+    tuning = None
+    if not a.no_tune:
+        from paces_b200 import autotune
+        tuning = autotune.tune_batch(batch, a.dt, steps=1)
+    for _ in range(max(a.warmup, 0)):
+        batch.step(evolve=True, dt=a.dt)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    rounds = []
+    barrier()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            rounds.append(batch.step(evolve=True, dt=a.dt))
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
+    clocks = clk.summary()
+    barrier()
+    n_prof = 3
+    batch.set_profiling(True)
+    batch.use_graph = False
+    phase = {k: 0.0 for k in nat.BATCH_STAGES}
+    prof = []
+    l0 = batch.kernel_launches()
+    for _ in range(n_prof):
+        prof.append(batch.step(evolve=True, dt=a.dt))
+        for k, v in batch.stage_times().items():
+            phase[k] += v
+    launches_per_step = (batch.kernel_launches() - l0) / n_prof
+    batch.set_profiling(False)
+    batch.close()
+    for t in trajs:
+        t.eng.close()
+    del trajs, batch
+    torch.cuda.empty_cache()
+
+    compare = None
+    if a.compare_steps > 0:
+        obs = {}
+        for prec in ("c128", a.precision):
+            eng = Engine(params(seeds[0], prec), device=dev)
+            tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
+            rr = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(a.compare_steps)]
+            L = a.nchain
+            obs[prec] = {"n_exc": np.array([list(r.n_exc)[:L] for r in rr]),
+                         "n_pho": np.array([list(r.n_pho)[:L] for r in rr]),
+                         "energy": np.array([r.energy_re for r in rr]), "norm": np.array([r.norm for r in rr])}
+            eng.close()
+            torch.cuda.empty_cache()
+        err = {k: float(np.max(np.abs(obs["c128"][k] - obs[a.precision][k]))) for k in obs["c128"]}
+        compare = {"realization": seeds[0], "steps": a.compare_steps, "t_end": a.compare_steps * a.dt,
+                   "max_abs_error_vs_c128": err}
+
+    n = len(seeds)
+    value = n * a.steps * world / (ms / 1e3)
+    taylor_ms = phase["taylor"] / n_prof
+    taylor_alg = statistics.mean(sum(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in rr) for rr in prof)
+    achieved = taylor_alg / (taylor_ms / 1e3) / 1e9
+    peak, peak_kind = read_peaks()
+    if rank == 0:
+        cfg = {"workload": f"holstein_periodic_n{a.nchain}_cutoff15_g{a.g:g}_disorder{a.sigma:g}_maxstates{a.maxstates}"
+                           f"_dt{a.dt:g}_x{n}",
+               "nchain": a.nchain, "g": a.g, "omega0": 1.0, "J": 1.0, "dt": a.dt, "maxstates": a.maxstates,
+               "site_energy_sigma": a.sigma, "realization_seeds": seeds, "precision": a.precision,
+               "key_words": 4 if a.nchain == 64 else None, "enlarge_steps": a.enlarge_steps,
+               "states_per_step": [int(statistics.mean(rr[i].n_states for rr in rounds)) for i in range(n)],
+               "prep_steps": nprep, "cuda_graph": not a.no_graph,
+               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")},
+               "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"}
+        line = {
+            "metric": "trajectory time-steps/s (N=64 disorder realizations batched)", "value": value,
+            "unit": "trajectory-steps/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": a.precision, "data": "synthetic", "config": cfg,
+            "roofline": {"bound": "hbm", "kernel": "taylor_batch_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "launch_ms": taylor_ms},
+            "phase_ms": {k: v / n_prof for k, v in phase.items()}, "compare": compare,
+            "clocks": clocks, "gpu_launches": int(round(launches_per_step * a.steps)), "cpu_baseline": None,
+            "e2e": None,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -798,6 +941,14 @@ def main():
     elif a.workload == "learned":
         a.precision = "c64"
         run_learned(a)
+    elif a.workload == "longchain":
+        # the long-chain configuration unless overridden: N=64, g=2, maxstates 2^24, dt 0.025
+        given = {x.split("=")[0] for x in sys.argv[1:] if x.startswith("--")}
+        for flag, attr, val in (("--nchain", "nchain", 64), ("--g", "g", 2.0), ("--maxstates", "maxstates", 1 << 24),
+                                ("--dt", "dt", 0.025), ("--steps", "steps", 10)):
+            if flag not in given:
+                setattr(a, attr, val)
+        run_longchain(a)
     else:
         run_ours(a)
 
