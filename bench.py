@@ -199,6 +199,11 @@ def prepare(a, eng, maxstates):
     return tr, nprep
 
 
+def autotune_shapes():
+    from paces_b200 import autotune
+    return autotune.SHAPES
+
+
 def max_over_ranks(value, dist, device="cuda"):
     """Largest value over all ranks (the timed region's duration); the value itself when
     there is no process group."""
@@ -401,7 +406,7 @@ def run_ours(a):
                "states_per_step": int(S_mean), "taylor_terms_per_step": terms, "prep_steps": nprep,
                "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}",
                "cuda_graph": not a.no_graph,
-               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")},
+               "tuning": None if tuning is None else {k: tuning[k] for k in autotune_shapes()},
                "form": ("complex64 amplitudes and SpMV, fp64 norms / stop test / sums; learned proposal off "
                         "(--workload learned measures it)") if a.precision == "c64" else "complex128 plain"}
         line = {
@@ -624,7 +629,7 @@ def run_batched(a):
                "maxstates": "log-uniform [2^14, 2^20]", "cutoff": 15, "J": 1.0, "dt": a.dt, "boundary": "periodic",
                "precision": a.precision, "states_per_step_all": int(states), "prep_steps": nprep,
                "streams": a.streams, "cuda_graph": not a.no_graph,
-               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")},
+               "tuning": None if tuning is None else {k: tuning.get(k) for k in autotune_shapes()},
                "l2": "inputs larger than L2 (all trajectories' states and H tables > 126 MB)",
                "parallelism": f"replicas x{world}",
                "maxstates_drawn": [sp["maxstates"] for sp in specs], "nchain_drawn": [sp["nchain"] for sp in specs]}
@@ -912,7 +917,7 @@ def run_longchain(a):
                "key_words": 4 if a.nchain == 64 else None, "enlarge_steps": a.enlarge_steps,
                "states_per_step": [int(statistics.mean(rr[i].n_states for rr in rounds)) for i in range(n)],
                "prep_steps": nprep, "cuda_graph": not a.no_graph,
-               "tuning": None if tuning is None else {k: tuning[k] for k in ("merge_stride", "taylor_blocks_per_sm")},
+               "tuning": None if tuning is None else {k: tuning.get(k) for k in autotune_shapes()},
                "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"}
         line = {
             "metric": "trajectory time-steps/s (N=64 disorder realizations batched)", "value": value,

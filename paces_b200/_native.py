@@ -115,7 +115,8 @@ class Tuning(ctypes.Structure):
         ("merge_stride_min", ctypes.c_int32),
         ("merge_stride_max", ctypes.c_int32),
         ("taylor_blocks_per_sm_max", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("taylor_variant", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 

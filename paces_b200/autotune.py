@@ -1,11 +1,12 @@
 """Autotuner for the launch shapes of the time step.
 
-Two shapes change the speed of a step but never its results (each trajectory's
+These shapes change the speed of a step but never its results (each trajectory's
 arithmetic and ordering are fixed by the data, not by the tiling):
 
 * the merge tiles' splitter stride (tile = 13 * stride elements): larger tiles spend less
   on splitters and look-back, smaller ones fit more blocks per SM;
-* the persistent Taylor kernel's blocks per SM (its grid).
+* the persistent Taylor kernel's blocks per SM (its grid) and its row schedule (rows read
+  directly, or 512-row chunks prefetched into shared memory by bulk TMA copies).
 
 `tune(trajectory, dt)` times candidates on the live workload -- eager steps with the
 library's stage events -- and keeps, shape by shape, the fastest (merge stride by the
@@ -29,6 +30,8 @@ from . import _native as nat
 CACHE_PATH = os.environ.get("PACES_TUNE_CACHE",
                             os.path.join(os.path.expanduser("~"), ".cache", "paces_b200", "tuning.json"))
 _memory: dict = {}
+VARIANTS = [0, 1]  # Taylor row schedules: direct, bulk-prefetched
+SHAPES = ("merge_stride", "taylor_blocks_per_sm", "taylor_variant")
 
 
 def get_tuning(eng) -> nat.Tuning:
@@ -37,12 +40,14 @@ def get_tuning(eng) -> nat.Tuning:
     return t
 
 
-def set_tuning(eng, merge_stride=None, taylor_blocks_per_sm=None):
+def set_tuning(eng, merge_stride=None, taylor_blocks_per_sm=None, taylor_variant=None):
     t = get_tuning(eng)
     if merge_stride is not None:
         t.merge_stride = int(merge_stride)
     if taylor_blocks_per_sm is not None:
         t.taylor_blocks_per_sm = int(taylor_blocks_per_sm)
+    if taylor_variant is not None:
+        t.taylor_variant = int(taylor_variant)
     nat.check(eng.lib.paces_set_tuning(eng.ctx, t), eng.ctx, "set_tuning")
 
 
@@ -89,19 +94,22 @@ def _lookup(key, use_cache):
     return _load_file().get(key)
 
 
-def _search(apply, measure, strides, bpss, base_bps):
-    """Coordinate search: the stride by its stages' time, then the Taylor grid by its own."""
-    timings = {"merge_stride": {}, "taylor_blocks_per_sm": {}}
+def _search(apply, measure, strides, bpss, variants):
+    """Coordinate search: the stride by its stages' time, then the Taylor schedule and grid
+    by the Taylor time."""
+    timings = {"merge_stride": {}, "taylor": {}}
     for s in strides:
-        apply(s, base_bps)
+        apply(s, 0, variants[0])
         timings["merge_stride"][s] = measure()["merge"]
     best_s = min(timings["merge_stride"], key=timings["merge_stride"].get)
-    for b in bpss:
-        apply(best_s, b)
-        timings["taylor_blocks_per_sm"][b] = measure()["taylor"]
-    best_b = min(timings["taylor_blocks_per_sm"], key=timings["taylor_blocks_per_sm"].get)
-    apply(best_s, best_b)
-    return {"merge_stride": best_s, "taylor_blocks_per_sm": best_b, "timings_ms": timings}
+    for v in variants:
+        for b in bpss:
+            apply(best_s, b, v)
+            timings["taylor"][(v, b)] = measure()["taylor"]
+    best_v, best_b = min(timings["taylor"], key=timings["taylor"].get)
+    apply(best_s, best_b, best_v)
+    timings["taylor"] = {f"variant{v}_bps{b}": ms for (v, b), ms in timings["taylor"].items()}
+    return {"merge_stride": best_s, "taylor_blocks_per_sm": best_b, "taylor_variant": best_v, "timings_ms": timings}
 
 
 def tune(tr, dt, steps=2, use_cache=True):
@@ -112,7 +120,7 @@ def tune(tr, dt, steps=2, use_cache=True):
     key = _key(eng, tr.basis.count())
     hit = _lookup(key, use_cache)
     if hit is not None:
-        set_tuning(eng, hit["merge_stride"], hit["taylor_blocks_per_sm"])
+        set_tuning(eng, hit["merge_stride"], hit["taylor_blocks_per_sm"], hit.get("taylor_variant"))
         return dict(hit, cached=True)
     t0 = get_tuning(eng)
     use_graph, tr.use_graph = tr.use_graph, False
@@ -129,13 +137,13 @@ def tune(tr, dt, steps=2, use_cache=True):
         return {k: v / steps for k, v in acc.items()}
 
     try:
-        choice = _search(lambda s, b: set_tuning(eng, s, b), measure, stride_candidates(t0), bps_candidates(t0),
-                         t0.taylor_blocks_per_sm)
+        choice = _search(lambda s, b, v: set_tuning(eng, s, b, v), measure, stride_candidates(t0), bps_candidates(t0),
+                         VARIANTS)
     finally:
         eng.set_profiling(False)
         tr.use_graph = use_graph
     tr._graphs = {}
-    _memory[key] = {k: choice[k] for k in ("merge_stride", "taylor_blocks_per_sm")}
+    _memory[key] = {k: choice[k] for k in SHAPES}
     _save_file(key, _memory[key])
     return dict(choice, cached=False)
 
@@ -148,10 +156,10 @@ def tune_batch(batch, dt, steps=2, use_cache=True):
     key = "batch|" + _key(engs[0], total) + f"|n{len(engs)}"
     hit = _lookup(key, use_cache)
 
-    def apply(s, b):
+    def apply(s, b, v=None):
         for e in engs:
             t = get_tuning(e)
-            set_tuning(e, min(max(s, t.merge_stride_min), t.merge_stride_max), b)
+            set_tuning(e, min(max(s, t.merge_stride_min), t.merge_stride_max), b, v)
 
     if hit is not None:
         apply(hit["merge_stride"], hit["taylor_blocks_per_sm"])
@@ -171,13 +179,14 @@ def tune_batch(batch, dt, steps=2, use_cache=True):
         return {k: v / steps for k, v in acc.items()}
 
     try:
-        choice = _search(apply, measure, stride_candidates(t0), bps_candidates(t0), t0.taylor_blocks_per_sm)
+        # the batched Taylor launch has one schedule; its grid is tuned, the variant is not
+        choice = _search(apply, measure, stride_candidates(t0), bps_candidates(t0), [t0.taylor_variant])
     finally:
         batch.set_profiling(False)
         batch.use_graph = use_graph
     batch._graphs = {}
     for t in batch.trajs:
         t._graphs = {}
-    _memory[key] = {k: choice[k] for k in ("merge_stride", "taylor_blocks_per_sm")}
+    _memory[key] = {k: choice[k] for k in SHAPES}
     _save_file(key, _memory[key])
     return dict(choice, cached=False)

@@ -19,6 +19,7 @@ struct paces_ctx {
     int taylor_grid;
     int merge_stride;  // tuning: elements per splitter of the merge tiles
     int taylor_bps;    // tuning: Taylor blocks per SM (0 = as many as fit)
+    int taylor_variant;  // tuning: 0 direct rows, 1 bulk-prefetched chunks
     int* d_status;  // device status word for the stage entry points (start of the constants block)
     double* d_site_eps;  // [kMaxSites] per-site energies, device copy (batched Taylor)
     double* d_sq;        // [kSqrtTable] sqrt(k) * g
@@ -476,6 +477,7 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
     c->taylor_grid = taylor_max_grid(c->precision == PACES_C64, c->num_sms);
     c->merge_stride = merge_stride(c->nw);
     c->taylor_bps = 0;
+    c->taylor_variant = 1;
     // constants block: status words, per-site energies and the sqrt(k) * g tables
     {
         const size_t o_eps = 64, o_sq = o_eps + kMaxSites * 8, o_sqf = o_sq + kSqrtTable * 8;
@@ -563,6 +565,7 @@ int paces_get_tuning(const paces_ctx* c, paces_tuning* t) {
     t->merge_stride_min = kMinMergeStride;
     t->taylor_blocks_per_sm = c->taylor_bps;
     t->taylor_blocks_per_sm_max = c->taylor_grid / c->num_sms;
+    t->taylor_variant = c->taylor_variant;
     return PACES_OK;
 }
 
@@ -574,8 +577,11 @@ int paces_set_tuning(paces_ctx* c, const paces_tuning* t) {
     if (t->taylor_blocks_per_sm < 0 || t->taylor_blocks_per_sm > c->taylor_grid / c->num_sms)
         return fail(c, PACES_ERR_BADARG, "taylor_blocks_per_sm %d: 0..%d", t->taylor_blocks_per_sm,
                     c->taylor_grid / c->num_sms);
+    if (t->taylor_variant < 0 || t->taylor_variant > 1)
+        return fail(c, PACES_ERR_BADARG, "taylor_variant %d: 0 or 1", t->taylor_variant);
     c->merge_stride = t->merge_stride;
     c->taylor_bps = t->taylor_blocks_per_sm;
+    c->taylor_variant = t->taylor_variant;
     return PACES_OK;
 }
 
@@ -715,7 +721,7 @@ int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
     }
     PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->cap, h->meta, psi_in,
                                         psi_out, dt, m_star, tol, taylor_ws(l, ws), o, c->d_status, c->num_sms,
-                                        c->taylor_bps, reinterpret_cast<cudaStream_t>(stream)),
+                                        c->taylor_bps, c->taylor_variant, reinterpret_cast<cudaStream_t>(stream)),
                        "taylor");
     return PACES_OK;
 }
@@ -767,7 +773,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
         TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
         PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, new_b->blk, h->nbr, h->cap, h->meta,
                                             p.target, new_psi, prm->dt, prm->m_star, prm->tol, taylor_ws(p.l, ws), o,
-                                            &rec->status, c->num_sms, c->taylor_bps, st),
+                                            &rec->status, c->num_sms, c->taylor_bps, c->taylor_variant, st),
                            "step/taylor");
     }
     return step_back(c, p, st, true);

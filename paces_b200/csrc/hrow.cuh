@@ -36,18 +36,16 @@ __device__ __forceinline__ int4 load_nbr(const int* __restrict__ nbr, int64_t r)
     return __ldg(reinterpret_cast<const int4*>(nbr) + r);
 }
 
-// y = (H x)[r] in complex128.  sq[k] = sqrt(k) * g.
+// y = (H x)[r] in complex128 from the row's neighbour entry nb and its own element xr.
+// sq[k] = sqrt(k) * g.
 template <class P>
-__device__ __forceinline__ double2 h_row_c128(const P& m, const double* sq, int64_t r,
-                                              const int* __restrict__ nbr, uint32_t meta,
-                                              const double2* __restrict__ x) {
+__device__ __forceinline__ double2 h_row_c128_nb(const P& m, const double* sq, int64_t r, int4 nb, uint32_t meta,
+                                                 double2 xr, const double2* __restrict__ x) {
     const int n = int((meta >> 8) & 0xffu);
-    const int4 nb = load_nbr(nbr, r);
     // hopping columns in increasing order (a <= b), as the CSR row sum visits them
     const bool swap = nb.y >= 0 && (nb.x < 0 || nb.y < nb.x);
     const int a = swap ? nb.y : nb.x, b = swap ? nb.x : nb.y;
     const bool ha = a >= 0, hb = b >= 0, hd = nb.z >= 0, hu = nb.w >= 0;
-    const double2 xr = __ldcg(x + r);
     const double2 xa = __ldcg(x + (ha ? a : r));
     const double2 xb = __ldcg(x + (hb ? b : r));
     const double2 xd = __ldcg(x + (hd ? nb.z : r));
@@ -68,14 +66,18 @@ __device__ __forceinline__ double2 h_row_c128(const P& m, const double* sq, int6
     return y;
 }
 
+template <class P>
+__device__ __forceinline__ double2 h_row_c128(const P& m, const double* sq, int64_t r,
+                                              const int* __restrict__ nbr, uint32_t meta,
+                                              const double2* __restrict__ x) {
+    return h_row_c128_nb(m, sq, r, load_nbr(nbr, r), meta, __ldcg(x + r), x);
+}
+
 // y = (H x)[r] in complex64 with fp32 accumulation.  sq[k] = float(sqrt(k) * g).
 template <class P>
-__device__ __forceinline__ float2 h_row_c64(const P& m, const float* sq, float J, int64_t r,
-                                            const int* __restrict__ nbr, uint32_t meta,
-                                            const float2* __restrict__ x) {
+__device__ __forceinline__ float2 h_row_c64_nb(const P& m, const float* sq, float J, int64_t r, int4 nb,
+                                               uint32_t meta, float2 xr, const float2* __restrict__ x) {
     const int n = int((meta >> 8) & 0xffu);
-    const int4 nb = load_nbr(nbr, r);
-    const float2 xr = __ldcg(x + r);
     const float2 xa = __ldcg(x + (nb.x >= 0 ? nb.x : r));
     const float2 xb = __ldcg(x + (nb.y >= 0 ? nb.y : r));
     const float2 xd = __ldcg(x + (nb.z >= 0 ? nb.z : r));
@@ -93,6 +95,13 @@ __device__ __forceinline__ float2 h_row_c64(const P& m, const float* sq, float J
     y.x = fmaf(cu, xu.x, y.x);
     y.y = fmaf(cu, xu.y, y.y);
     return y;
+}
+
+template <class P>
+__device__ __forceinline__ float2 h_row_c64(const P& m, const float* sq, float J, int64_t r,
+                                            const int* __restrict__ nbr, uint32_t meta,
+                                            const float2* __restrict__ x) {
+    return h_row_c64_nb(m, sq, J, r, load_nbr(nbr, r), meta, __ldcg(x + r), x);
 }
 
 }  // namespace paces

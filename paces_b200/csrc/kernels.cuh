@@ -49,11 +49,12 @@ struct TaylorWs {
     unsigned* barrier;   // [2]
 };
 int taylor_max_grid(bool c64, int num_sms);
-// blocks_per_sm: 0 = as many as fit (the grid never exceeds taylor_max_grid)
+// blocks_per_sm: 0 = as many as fit (the grid never exceeds taylor_max_grid);
+// variant: 0 = direct grid-stride rows, 1 = chunks prefetched by bulk TMA copies
 int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,
                   const uint32_t* meta, const void* v_in, void* res, double dt, int m_star,
                   double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
-                  int blocks_per_sm, cudaStream_t st);
+                  int blocks_per_sm, int variant, cudaStream_t st);
 
 // ---- batched Taylor: many trajectories in one persistent launch ---------------------------
 constexpr int kMaxBatch = 128;  // trajectories per launch (the descriptors travel as kernel parameters)

@@ -11,9 +11,19 @@
 // neighbour indices of consecutive rows are monotone (images of a sorted block are
 // sorted), so the four gathers stream through L2.  complex128 rounds every operation
 // like the reference; complex64 uses fp32 FMA with fp64 stop arithmetic.
+//
+// Two row schedules (a tuning choice; the results are identical because every row's
+// arithmetic is the same and the maxima are exact):
+//  * direct: grid-stride, two rows per thread per pass, all loads from global memory;
+//  * bulk:   each block owns 512-row chunks; while it computes one chunk, one thread has
+//            the next chunk's neighbour rows, metadata, result and own term elements
+//            brought into the other half of a shared-memory double buffer by bulk TMA
+//            copies (cp.async.bulk, completion on an mbarrier), so the streaming reads are
+//            in flight while the gathers of the current chunk wait on L2.
 #include "grid.cuh"
 #include "hrow.cuh"
 #include "kernels.cuh"
+#include "tc.cuh"
 
 namespace paces {
 
@@ -40,18 +50,36 @@ __device__ void block_max4(double v[4], double (*red)[kTWarps], double* out) {
     __syncthreads();
 }
 
+constexpr int kChunk = 2 * kTThreads;  // rows per block pass of the bulk schedule
 template <bool C64>
+constexpr uint32_t chunk_bytes() {  // neighbour rows, metadata, result, own term element
+    return uint32_t(kChunk) * (16 + 4 + 2 * (C64 ? 8 : 16));
+}
+
+template <bool C64, bool BULK>
 __global__ void __launch_bounds__(kTThreads, C64 ? 4 : 3)
 taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nbr, int64_t cap,
               const uint32_t* __restrict__ meta, const void* v_in, void* res_out, TaylorWs ws,
               double dt, int m_star, double tol, TaylorOut out, int* status) {
     using C = typename std::conditional<C64, float2, double2>::type;
     using R = typename std::conditional<C64, float, double>::type;
+    extern __shared__ __align__(128) unsigned char t_smem[];  // bulk: 2 x chunk_bytes
     __shared__ R s_sq[260];
     __shared__ double s_red[4][kTWarps];
     __shared__ double s_fin[4];
+    __shared__ __align__(8) uint64_t s_mbar[2];
+    __shared__ int s_abort;
     for (int k = threadIdx.x; k < 260; k += kTThreads) s_sq[k] = R(__dmul_rn(sqrt(double(k)), m.g));
+    if constexpr (BULK) {
+        if (threadIdx.x == 0) {
+            tc::mbar_init(tc::smem_addr(&s_mbar[0]), 1);
+            tc::mbar_init(tc::smem_addr(&s_mbar[1]), 1);
+            s_abort = 0;
+        }
+    }
     __syncthreads();
+    uint32_t parity = 0;    // bulk: phase parity of each buffer's mbarrier (bit b)
+    uint32_t pending = 0;   // bulk, thread 0: buffers with copies issued and not yet consumed
 
     const int64_t S = blk[m.L];
     const unsigned nblocks = gridDim.x;
@@ -95,16 +123,84 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
             dst[r] = t;
             res[r] = rr;
         };
-        // two rows per thread per pass: all loads of both rows precede the stores
-        const int64_t stride = int64_t(gridDim.x) * kTThreads;
-        int64_t r = int64_t(blockIdx.x) * kTThreads + threadIdx.x;
-        for (; r + stride < S; r += 2 * stride) {
-            const C y0 = hrow(r), y1 = hrow(r + stride);
-            const C a0 = rin[r], a1 = rin[r + stride];
-            finish(r, y0, a0);
-            finish(r + stride, y1, a1);
+        if constexpr (!BULK) {
+            // two rows per thread per pass: all loads of both rows precede the stores
+            const int64_t stride = int64_t(gridDim.x) * kTThreads;
+            int64_t r = int64_t(blockIdx.x) * kTThreads + threadIdx.x;
+            for (; r + stride < S; r += 2 * stride) {
+                const C y0 = hrow(r), y1 = hrow(r + stride);
+                const C a0 = rin[r], a1 = rin[r + stride];
+                finish(r, y0, a0);
+                finish(r + stride, y1, a1);
+            }
+            if (r < S) finish(r, hrow(r), rin[r]);
+        } else {
+            constexpr uint32_t kCB = chunk_bytes<C64>();
+            constexpr uint32_t kOffMeta = kChunk * 16, kOffRin = kOffMeta + kChunk * 4,
+                               kOffSelf = kOffRin + kChunk * sizeof(C);
+            const int64_t nch = (S + kChunk - 1) / kChunk;
+            auto full = [&](int64_t c) { return (c + 1) * kChunk <= S; };
+            auto issue = [&](int64_t c, int b) {  // thread 0
+                const int64_t r0 = c * kChunk;
+                const uint32_t base = tc::smem_addr(t_smem + b * kCB);
+                const uint32_t mb = tc::smem_addr(&s_mbar[b]);
+                tc::mbar_expect_tx(mb, kCB);
+                tc::bulk_g2s(base, nbr + r0 * 4, kChunk * 16, mb);
+                tc::bulk_g2s(base + kOffMeta, meta + r0, kChunk * 4, mb);
+                tc::bulk_g2s(base + kOffRin, rin + r0, kChunk * sizeof(C), mb);
+                tc::bulk_g2s(base + kOffSelf, src + r0, kChunk * sizeof(C), mb);
+                pending |= 1u << b;
+            };
+            int64_t c = blockIdx.x;
+            if (threadIdx.x == 0 && c < nch) {
+                // the previous term's stores (every block's, ordered by the grid barrier) before
+                // this term's bulk reads of them
+                tc::fence_proxy_async_global();
+                if (full(c)) issue(c, 0);
+            }
+            for (int k = 0; c < nch; c += gridDim.x, ++k) {
+                const int b = k & 1;
+                const int64_t cn = c + gridDim.x;
+                if (threadIdx.x == 0 && cn < nch && full(cn)) issue(cn, b ^ 1);
+                const int64_t r0 = c * kChunk;
+                const int t0 = threadIdx.x, t1 = threadIdx.x + kTThreads;
+                if (full(c)) {
+                    if (!tc::mbar_wait(tc::smem_addr(&s_mbar[b]), (parity >> b) & 1u)) s_abort = 1;
+                    parity ^= 1u << b;
+                    if (threadIdx.x == 0) pending &= ~(1u << b);
+                    const unsigned char* base = t_smem + b * kCB;
+                    const int4* snb = reinterpret_cast<const int4*>(base);
+                    const uint32_t* smeta = reinterpret_cast<const uint32_t*>(base + kOffMeta);
+                    const C* srin = reinterpret_cast<const C*>(base + kOffRin);
+                    const C* sself = reinterpret_cast<const C*>(base + kOffSelf);
+                    C y0, y1;
+                    if constexpr (C64) {
+                        y0 = h_row_c64_nb(m, s_sq, J, r0 + t0, snb[t0], smeta[t0], sself[t0], src);
+                        y1 = h_row_c64_nb(m, s_sq, J, r0 + t1, snb[t1], smeta[t1], sself[t1], src);
+                    } else {
+                        y0 = h_row_c128_nb(m, s_sq, r0 + t0, snb[t0], smeta[t0], sself[t0], src);
+                        y1 = h_row_c128_nb(m, s_sq, r0 + t1, snb[t1], smeta[t1], sself[t1], src);
+                    }
+                    finish(r0 + t0, y0, srin[t0]);
+                    finish(r0 + t1, y1, srin[t1]);
+                } else {
+                    // the last, partial chunk: direct loads
+                    if (r0 + t0 < S) finish(r0 + t0, hrow(r0 + t0), rin[r0 + t0]);
+                    if (r0 + t1 < S) finish(r0 + t1, hrow(r0 + t1), rin[r0 + t1]);
+                }
+                __syncthreads();  // the buffer is free for the copy issued next iteration
+                if (s_abort) break;
+            }
+            if (s_abort) {
+                // a copy that never completed: wait (bounded) for what is still in flight
+                if (threadIdx.x == 0)
+                    for (int bb = 0; bb < 2; ++bb)
+                        if (pending & (1u << bb)) tc::mbar_wait(tc::smem_addr(&s_mbar[bb]), (parity >> bb) & 1u);
+                if (threadIdx.x == 0) raise_status(status, PACES_ERR_TIMEOUT);
+                fin_j = j;
+                break;
+            }
         }
-        if (r < S) finish(r, hrow(r), rin[r]);
         block_max4(mx, s_red, s_fin);
         if (threadIdx.x == 0) {
             double* pp = ws.partials + (size_t((j & 1) * nblocks) + blockIdx.x) * 4;
@@ -148,28 +244,56 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
     }
 }
 
-template <bool C64>
+template <bool C64, bool BULK>
+size_t dyn_smem() {
+    return BULK ? size_t(2) * chunk_bytes<C64>() : 0;
+}
+
+template <bool C64, bool BULK>
 int occupancy() {
+    static int cached = 0;  // per process: the kernels' resources do not change
+    if (cached) return cached;
+    auto kfn = taylor_kernel<C64, BULK>;
+    if (BULK) cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn_smem<C64, BULK>()));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, taylor_kernel<C64>, kTThreads, 0);
-    return per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTThreads, dyn_smem<C64, BULK>());
+    cached = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+    return cached;
+}
+
+template <bool C64>
+int occupancy_any(int variant) {
+    return variant == 1 ? occupancy<C64, true>() : occupancy<C64, false>();
 }
 
 }  // namespace
 
-int taylor_max_grid(bool c64, int num_sms) { return num_sms * (c64 ? occupancy<true>() : occupancy<false>()); }
+int taylor_max_grid(bool c64, int num_sms) {
+    const int a = c64 ? occupancy<true, false>() : occupancy<false, false>();
+    const int b = c64 ? occupancy<true, true>() : occupancy<false, true>();
+    return num_sms * (a > b ? a : b);
+}
 
 int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,
                   const uint32_t* meta, const void* v_in, void* res, double dt, int m_star,
                   double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
-                  int blocks_per_sm, cudaStream_t st) {
-    if (m_star < 1) return PACES_ERR_BADARG;
+                  int blocks_per_sm, int variant, cudaStream_t st) {
+    if (m_star < 1 || variant < 0 || variant > 1) return PACES_ERR_BADARG;
     if (cudaMemsetAsync(ws.barrier, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return PACES_ERR_CUDA;
-    const int occ = c64 ? occupancy<true>() : occupancy<false>();
+    const int occ = c64 ? occupancy_any<true>(variant) : occupancy_any<false>(variant);
     const int grid = num_sms * (blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ);
+    if (variant == 1) {  // the attribute belongs to the current device: set it on every launch
+        const cudaError_t a =
+            c64 ? cudaFuncSetAttribute(taylor_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(dyn_smem<true, true>()))
+                : cudaFuncSetAttribute(taylor_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(dyn_smem<false, true>()));
+        if (a != cudaSuccess) return PACES_ERR_CUDA;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kTThreads);
+    cfg.dynamicSmemBytes = variant == 1 ? (c64 ? dyn_smem<true, true>() : dyn_smem<false, true>()) : 0;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -177,9 +301,17 @@ int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, i
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const int64_t cap = nbr_cap;
-    const cudaError_t e =
-        c64 ? cudaLaunchKernelEx(&cfg, taylor_kernel<true>, m, blk, nbr, cap, meta, v_in, res, ws, dt, m_star, tol, out, status)
-            : cudaLaunchKernelEx(&cfg, taylor_kernel<false>, m, blk, nbr, cap, meta, v_in, res, ws, dt, m_star, tol, out, status);
+    cudaError_t e;
+    if (c64)
+        e = variant == 1 ? cudaLaunchKernelEx(&cfg, taylor_kernel<true, true>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
+                                              m_star, tol, out, status)
+                         : cudaLaunchKernelEx(&cfg, taylor_kernel<true, false>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
+                                              m_star, tol, out, status);
+    else
+        e = variant == 1 ? cudaLaunchKernelEx(&cfg, taylor_kernel<false, true>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
+                                              m_star, tol, out, status)
+                         : cudaLaunchKernelEx(&cfg, taylor_kernel<false, false>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
+                                              m_star, tol, out, status);
     return e == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 

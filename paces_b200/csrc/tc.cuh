@@ -106,5 +106,23 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     }
 }
 
+// ---- bulk (non-tensor) TMA copies: global -> this CTA's shared memory --------------------
+// One thread arms the mbarrier with the byte count it expects, then issues the copies; the
+// phase completes when every byte has landed.  Addresses 16-byte aligned, sizes multiples
+// of 16.  No multicast: each CTA fetches its own rows from this GPU's memory.
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+// order this thread's earlier generic-proxy global accesses (and those it synchronised
+// with) before its later async-proxy (bulk copy) accesses
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 }  // namespace tc
 }  // namespace paces

@@ -9,11 +9,11 @@ from tests import gpu_helpers
 pytestmark = pytest.mark.gpu
 
 
-def _run(precision, stride=None, bps=None, steps=8):
+def _run(precision, stride=None, bps=None, variant=None, steps=8):
     from paces_b200 import autotune
     eng = gpu_helpers.engine_for(16, 16, 1.0, cap=1 << 14, precision=precision, periodic=True)
-    if stride is not None or bps is not None:
-        autotune.set_tuning(eng, stride, bps)
+    if stride is not None or bps is not None or variant is not None:
+        autotune.set_tuning(eng, stride, bps, variant)
     tr, _ = gpu_helpers.grown_trajectory(eng, 16, 20000)
     recs = [tr.step(evolve=True, dt=0.05) for _ in range(steps)]
     n = tr.basis.count()
@@ -24,9 +24,9 @@ def _run(precision, stride=None, bps=None, steps=8):
 
 @pytest.mark.parametrize("precision", ["c128", "c64"])
 def test_results_do_not_depend_on_launch_shapes(precision):
-    ref = _run(precision)
-    for stride, bps in ((64, 1), (96, 2), (160, 0), (240, 1)):
-        got = _run(precision, stride, bps)
+    ref = _run(precision, variant=0)
+    for stride, bps, variant in ((64, 1, 0), (96, 2, 1), (160, 0, 1), (240, 1, 1), (128, 0, 0)):
+        got = _run(precision, stride, bps, variant)
         for a, b in zip(ref[0], got[0]):
             assert (a.n_states, a.final_m, a.converged) == (b.n_states, b.final_m, b.converged)
             assert list(a.n_exc) == list(b.n_exc) and list(a.n_pho) == list(b.n_pho)
@@ -45,6 +45,8 @@ def test_out_of_range_shapes_are_rejected():
             autotune.set_tuning(eng, merge_stride=bad)
     with pytest.raises(nat.PacesError):
         autotune.set_tuning(eng, taylor_blocks_per_sm=t.taylor_blocks_per_sm_max + 1)
+    with pytest.raises(nat.PacesError):
+        autotune.set_tuning(eng, taylor_variant=2)
     eng.close()
 
 
@@ -59,6 +61,7 @@ def test_tuner_picks_an_allowed_shape(tmp_path, monkeypatch):
     assert not choice["cached"]
     assert t.merge_stride == choice["merge_stride"] and t.taylor_blocks_per_sm == choice["taylor_blocks_per_sm"]
     assert set(choice["timings_ms"]["merge_stride"]) == set(autotune.stride_candidates(t))
+    assert t.taylor_variant == choice["taylor_variant"] in (0, 1)
     again = autotune.tune(tr, 0.05, steps=1)
     assert again["cached"] and again["merge_stride"] == choice["merge_stride"]
     eng.close()
