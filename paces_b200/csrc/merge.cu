@@ -111,15 +111,18 @@ struct SKeys {
     }
 };
 
-// (key, flag) of tile element x strictly below that of element y.
+// (key, flag) of tile element x strictly below that of element y.  Branch-free: every word
+// is read and the comparison folds from the least significant end, so a warp's lanes never
+// diverge on where their keys first differ.
 template <int NW>
 __device__ __forceinline__ bool tile_less(const SKeys<NW>& keys, const uint8_t* flags, int x, int y) {
+    bool lt = flags[x] < flags[y];
 #pragma unroll
-    for (int q = 0; q < NW; ++q) {
+    for (int q = NW - 1; q >= 0; --q) {
         const uint64_t a = keys.w[q * keys.stride + x], b = keys.w[q * keys.stride + y];
-        if (a != b) return a < b;
+        lt = (a < b) | ((a == b) & lt);
     }
-    return flags[x] < flags[y];
+    return lt;
 }
 
 // Output positions [d0, d1) of the merge of two sorted sequences of tile elements, A
@@ -134,16 +137,17 @@ __device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t
         if (!tile_less<NW>(keys, flags, B(d0 - 1 - mid), A(mid))) lo = mid + 1; else hi = mid;
     }
     int i = lo, j = d0 - lo;
-    int ea = i < na ? A(i) : 0, eb = j < nb ? B(j) : 0;
+    // branch-free merge steps: both heads are re-read every step (indices clamped into their
+    // sequences; an exhausted sequence's head is never taken)
     for (int d = d0; d < d1; ++d) {
-        const bool take_a = j >= nb || (i < na && !tile_less<NW>(keys, flags, eb, ea));
-        if (take_a) {
-            out[d] = uint16_t(ea);
-            if (++i < na) ea = A(i);
-        } else {
-            out[d] = uint16_t(eb);
-            if (++j < nb) eb = B(j);
-        }
+        const int ia = min(i, na - 1), jb = min(j, nb - 1);
+        const int ea = ia >= 0 ? A(ia) : 0;
+        const int eb = jb >= 0 ? B(jb) : 0;
+        const bool a_left = i < na, b_left = j < nb;
+        const bool take_a = a_left & (!b_left | !tile_less<NW>(keys, flags, eb, ea));
+        out[d] = uint16_t(take_a ? ea : eb);
+        i += take_a ? 1 : 0;
+        j += take_a ? 0 : 1;
     }
 }
 
