@@ -125,29 +125,67 @@ __device__ __forceinline__ bool tile_less(const SKeys<NW>& keys, const uint8_t* 
     return lt;
 }
 
-// Output positions [d0, d1) of the merge of two sorted sequences of tile elements, A
-// (na elements, A(i) = element index) and B; an element of A precedes an equal element of
-// B (A always holds the lower run indices).  Merge-path split, then a sequential merge.
-template <int NW, typename FA, typename FB>
-__device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t* flags, FA A, int na, FB B,
-                                            int nb, int d0, int d1, uint16_t* out) {
-    int lo = max(0, d0 - nb), hi = min(d0, na);
+// A sorted sequence of tile elements: element k is ptr[k] (a merged level) or base + k
+// (a run segment, ptr == nullptr).
+struct Seq {
+    const uint16_t* ptr;
+    int base;
+    int n;
+    __device__ __forceinline__ int at(int k) const { return ptr ? int(ptr[k]) : base + k; }
+};
+
+// (key, flag) pairs held in registers: a strictly below b.  Branch-free fold from the least
+// significant word.
+template <int NW>
+__device__ __forceinline__ bool reg_less(const Key<NW>& a, int fa, const Key<NW>& b, int fb) {
+    bool lt = fa < fb;
+#pragma unroll
+    for (int q = NW - 1; q >= 0; --q) lt = (a.w[q] < b.w[q]) | ((a.w[q] == b.w[q]) & lt);
+    return lt;
+}
+
+// Output positions [d0, d1) of the merge of two sorted sequences of tile elements, A and B;
+// an element of A precedes an equal element of B (A always holds the lower run indices).
+// Merge-path split, then a sequential merge that keeps both heads' keys in registers and
+// per step reads only the next element of the side it took, without branches.
+template <int NW>
+__device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t* flags, Seq A, Seq B, int d0,
+                                            int d1, uint16_t* out) {
+    int lo = max(0, d0 - B.n), hi = min(d0, A.n);
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (!tile_less<NW>(keys, flags, B(d0 - 1 - mid), A(mid))) lo = mid + 1; else hi = mid;
+        if (!tile_less<NW>(keys, flags, B.at(d0 - 1 - mid), A.at(mid))) lo = mid + 1; else hi = mid;
     }
     int i = lo, j = d0 - lo;
-    // branch-free merge steps: both heads are re-read every step (indices clamped into their
-    // sequences; an exhausted sequence's head is never taken)
+    int ea = i < A.n ? A.at(i) : -1;
+    int eb = j < B.n ? B.at(j) : -1;
+    Key<NW> ka, kb;
+    int fa = 0, fb = 0;
+    ka = keys.get(ea >= 0 ? ea : 0);
+    fa = flags[ea >= 0 ? ea : 0];
+    kb = keys.get(eb >= 0 ? eb : 0);
+    fb = flags[eb >= 0 ? eb : 0];
     for (int d = d0; d < d1; ++d) {
-        const int ia = min(i, na - 1), jb = min(j, nb - 1);
-        const int ea = ia >= 0 ? A(ia) : 0;
-        const int eb = jb >= 0 ? B(jb) : 0;
-        const bool a_left = i < na, b_left = j < nb;
-        const bool take_a = a_left & (!b_left | !tile_less<NW>(keys, flags, eb, ea));
+        const bool take_a = (ea >= 0) & ((eb < 0) | !reg_less<NW>(kb, fb, ka, fa));
         out[d] = uint16_t(take_a ? ea : eb);
-        i += take_a ? 1 : 0;
-        j += take_a ? 0 : 1;
+        // the next head of the side taken
+        const int k = take_a ? ++i : ++j;
+        const uint16_t* sp = take_a ? A.ptr : B.ptr;
+        const int sb = take_a ? A.base : B.base, sn = take_a ? A.n : B.n;
+        int en = -1;
+        if (k < sn) en = sp ? int(sp[k]) : sb + k;
+        const int el = en >= 0 ? en : 0;
+        const Key<NW> kn = keys.get(el);
+        const int fn = flags[el];
+        if (take_a) {
+            ea = en;
+            ka = kn;
+            fa = fn;
+        } else {
+            eb = en;
+            kb = kn;
+            fb = fn;
+        }
     }
 }
 
@@ -414,24 +452,24 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             uint16_t* lv2 = s_cnt;
             const int o1 = s_off[1], o2 = s_off[2], o3 = s_off[3], o4 = s_off[4];
             const int n01 = o2, n0123 = o4;
-            auto ident = [](int base) { return [base](int i) { return base + i; }; };
-            auto arr = [](const uint16_t* a) { return [a](int i) { return int(a[i]); }; };
+            auto ident = [](int base, int n) { return Seq{nullptr, base, n}; };
+            auto arr = [](const uint16_t* a, int n) { return Seq{a, 0, n}; };
             int per = (n0123 + kTileThreads - 1) / kTileThreads;
             int d0 = min(tid * per, n0123), d1 = min(d0 + per, n0123);
             if (d0 < n01)
-                merge_range<NW>(s_key, s_flag, ident(0), o1, ident(o1), o2 - o1, d0, min(d1, n01), lv1);
+                merge_range<NW>(s_key, s_flag, ident(0, o1), ident(o1, o2 - o1), d0, min(d1, n01), lv1);
             if (d1 > n01)
-                merge_range<NW>(s_key, s_flag, ident(o2), o3 - o2, ident(o3), o4 - o3, max(d0, n01) - n01,
+                merge_range<NW>(s_key, s_flag, ident(o2, o3 - o2), ident(o3, o4 - o3), max(d0, n01) - n01,
                                 d1 - n01, lv1 + n01);
             __syncthreads();
             d0 = min(tid * per, n0123);
             d1 = min(d0 + per, n0123);
-            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv1), n01, arr(lv1 + n01), n0123 - n01, d0, d1, lv2);
+            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv1, n01), arr(lv1 + n01, n0123 - n01), d0, d1, lv2);
             __syncthreads();
             per = (n + kTileThreads - 1) / kTileThreads;
             d0 = min(tid * per, n);
             d1 = min(d0 + per, n);
-            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv2), n0123, ident(o4), n - o4, d0, d1, s_perm);
+            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv2, n0123), ident(o4, n - o4), d0, d1, s_perm);
             __syncthreads();
             for (int q = tid; q < n; q += kTileThreads) {
                 const int e = s_perm[q];
