@@ -112,7 +112,8 @@ class ObservablesFramework:
         whoami = self.teobj.whoami
         occs = self.hamobj.get_n_at_site(whoami, site).to(torch.int64)
         ok = occs + n < int(self.hamobj.max_dims_v[site])
-        plus = whoami[ok].clone()
+        # boolean indexing of uint32 tensors is not available on the GPU: select on an int32 view
+        plus = whoami.view(torch.int32)[ok].clone().view(torch.uint32)
         self.hamobj.add_n_at_site(plus, n, site)
         idx = self.hamobj.searchsorted(whoami, plus, allow_escapes=True)
         res = torch.zeros_like(vector)

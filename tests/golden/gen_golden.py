@@ -252,6 +252,46 @@ def gen_traj(paces, name, cfg, workdir):
         config=np.array([nchain, dim, g, maxstates, es, steps, initpos], dtype=np.float64))
 
 
+def gen_obs_extra(paces, workdir):
+    """The remaining Holstein observables on an open chain of odd length (N=7, dim 8, g=1.2,
+    maxstates 3000, enlarge_steps 1, 30 steps of dt 0.05, exciton starting on site 1 -- off
+    the chain's mirror axis, so no two states tie exactly at the truncation cut and the
+    amplitudes themselves can be compared): hopping energy per bond and
+    <mu(t) mu(0)> at every step (paces/models/holstein.py:325-357, :366-377), and for the
+    last state the vibronic coupling energy per site (holstein.py:360-364, computed with the
+    term's real key "vib_coupling": the reference method reads a key "coupling" that its
+    matrices dictionary does not have) and the reduced density matrices of sites 0 and 3
+    (paces/core/observables.py:126-163)."""
+    from paces.models import holstein
+    from paces.core.time_evolution import CoeffSaveParams, ExpmParams, TimeEvoParams
+    from paces.config import devices
+    nchain, dim, g = 7, 8, 1.2
+    with devices.vector_dev:
+        ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain, use_terms=terms(g), debug_verb=0)
+        te = holstein.TimeEvolution(ham, holstein.Observables, ["n_exc", "hopping", "mu_to_0"], workdir,
+                                    TimeEvoParams(maxstates=3000, enlarge_steps=1, shuffle_seed=None),
+                                    ExpmParams(), os.path.join(workdir, "params.log"))
+        te.create_nonuniform_basis([1] * nchain, minpos=1, maxpos=2)
+        te.create_initial_vector([1.0], [[1] + [0] * nchain])
+        te.generate_timeline(np.arange(31) * 0.05, CoeffSaveParams())
+        obs = te.obsobj
+        vec = te.vector
+        allvals = vec.conj() * te.sparse_mats_dict["vib_coupling"].dot(vec)
+        coupling = np.asarray(obs._calculate_partitioned_sum(allvals))
+        rdm0 = np.asarray(obs.calculate_rdm(0, vec))
+        rdm3 = np.asarray(obs.calculate_rdm(3, vec))
+    od = os.path.join(workdir, "observables")
+    np.savez_compressed(os.path.join(HERE, "obs_extra_n7c8.npz"),
+                        hop_re=np.loadtxt(os.path.join(od, "V_hop.real")),
+                        hop_im=np.loadtxt(os.path.join(od, "V_hop.imag")),
+                        mu_re=np.loadtxt(os.path.join(od, "mu_to_0.real")),
+                        mu_im=np.loadtxt(os.path.join(od, "mu_to_0.imag")),
+                        n_exc=np.loadtxt(os.path.join(od, "n_exc.real")),
+                        coupling=coupling, rdm0=rdm0, rdm3=rdm3, vector=np.asarray(vec),
+                        whoami=np.asarray(te.whoami),
+                        config=np.array([nchain, dim, g, 3000, 1, 30, 1], dtype=np.float64))
+
+
 def gen_ed(paces, workdir):
     """N=4, max_ho_dims=4, J=g=omega=1: the full space (1024 states) fits, so paces == exact."""
     ham, te = make_objects(paces, 4, 4, 1.0, 100000, 1, 0, workdir)
@@ -286,6 +326,7 @@ def main():
     for name, cfg in TRAJ_RUNS.items():
         jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))
     jobs.append(("ed_n4", lambda: gen_ed(paces, fresh())))
+    jobs.append(("obs_extra_n7c8", lambda: gen_obs_extra(paces, fresh())))
     if args.long:
         for name, cfg in LONG_TRAJ_RUNS.items():
             jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))
