@@ -244,6 +244,25 @@ int paces_taylor(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, cons
 int paces_observables(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi,
                       int32_t what, double *dev_out, void *ws, size_t ws_bytes,
                       paces_stream_t stream);
+/* Norms for the scaling-and-squaring propagation: dev_out[0] = trace of H, dev_out[1] =
+ * the largest row 1-norm of H - (*dev_shift) I (0 when dev_shift is NULL), dev_out[2] =
+ * trace / n (three doubles, device).  Reference: _trace and _exact_1_norm,
+ * paces/aux/_scipy/_expm_multiply.py:23-40, applied to 1j * H in expm_multiply_simple
+ * (:106-160); H is symmetric, so its column and row 1-norms agree. */
+int paces_hnorms(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const double *dev_shift,
+                 double *dev_out, void *ws, size_t ws_bytes, paces_stream_t stream);
+/* psi_out = exp(t A) psi_in with A = 1j * (H - shift I), by `stages` stages of at most
+ * m_star Taylor terms each, stopping a stage by the inf-norm test at tol, and multiplying
+ * by eta = eta_re + 1j eta_im (exp(t mu / stages) for the removed mean mu = 1j * shift)
+ * after every stage.  dev_info gets converged, final_m (terms over all stages), the last
+ * c1 + c2 and term ratio.  Reference: _expm_multiply_simple_core,
+ * paces/aux/_scipy/_expm_multiply.py:163-202, called with 1j * H and t = dt by
+ * paces/core/time_evolution.py:579-581.  The host picks stages and m_star
+ * (paces_b200.expm). */
+int paces_expm_scaled(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi_in,
+                      void *psi_out, double t, double shift, int32_t m_star, int32_t stages, double tol,
+                      double eta_re, double eta_im, paces_expm_info *dev_info, void *ws, size_t ws_bytes,
+                      paces_stream_t stream);
 /* y = H x on a basis (x and y distinct).  Reference: TimeEvolutionFramework.total_ham,
  * paces/core/time_evolution.py:382-400. */
 int paces_apply_h(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *x, void *y,

@@ -440,6 +440,75 @@ def taylor(asm: Assembly, v, dt, m_star=100, tol=TAYLOR_TOL_F64):
     return res, [converged, j_ind, c1_plus_c2, term_ratio]
 
 
+# theta_m of Al-Mohy and Higham (2011), table 3.1 (m <= 30: Higham, Functions of
+# Matrices, table A.3) -- the bounds paces/aux/_scipy/_expm_multiply.py:205-245 tabulates.
+_THETA = {
+    1: 2.29e-16, 2: 2.58e-8, 3: 1.39e-5, 4: 3.40e-4, 5: 2.40e-3, 6: 9.07e-3, 7: 2.38e-2, 8: 5.00e-2,
+    9: 8.96e-2, 10: 1.44e-1, 11: 2.14e-1, 12: 3.00e-1, 13: 4.00e-1, 14: 5.14e-1, 15: 6.41e-1,
+    16: 7.81e-1, 17: 9.31e-1, 18: 1.09, 19: 1.26, 20: 1.44, 21: 1.62, 22: 1.82, 23: 2.01, 24: 2.22,
+    25: 2.43, 26: 2.64, 27: 2.86, 28: 3.08, 29: 3.31, 30: 3.54, 35: 4.7, 40: 6.0, 45: 7.2, 50: 8.5,
+    55: 9.9,
+}
+
+
+def total_matrix(asm: Assembly):
+    """diags(diag) + sum of the term matrices.  paces/core/time_evolution.py:375-379."""
+    h = sp.diags(asm.diag).tocsr()
+    for m in asm.mats.values():
+        h = h + m
+    return h
+
+
+def expm_scaled(asm: Assembly, v, t, tol=TAYLOR_TOL_F64):
+    """exp(t * 1j H) v by scaling and squaring: expm_multiply_simple(1j * H, v, t) as
+    paces/core/time_evolution.py:579-581 calls it (paces/aux/_scipy/_expm_multiply.py:
+    106-202).  Only the branch of fragment 3.1 that condition (3.13) selects is restated
+    (the one the reference takes for t ||A - mu I||_1 below about 63).
+
+    Returns (F, [converged, final_m, c1_plus_c2, term_ratio])."""
+    A = (1j * total_matrix(asm)).tocsr()
+    n = A.shape[0]
+    mu = A.diagonal().sum() / float(n)
+    A = (A - mu * sp.identity(n, format="csr")).tocsr()
+    a1 = abs(A).sum(axis=0).max()
+    if t * a1 == 0:
+        m_star, s = 0, 1
+    else:
+        m_max, ell = 55, 2
+        p = int(math.floor(math.sqrt(m_max)))
+        while (p + 1) * p <= m_max + 1:
+            p += 1
+        if t * a1 > 2 * ell * p * (p + 3) * _THETA[m_max] / float(m_max):
+            raise NotImplementedError("1-norm estimation of matrix powers (equation 3.11) is not restated")
+        m_star = s = None
+        for m, theta in _THETA.items():
+            ss = int(math.ceil(t * a1 / theta))
+            if m_star is None or m * ss < m_star * s:
+                m_star, s = m, ss
+    B = np.asarray(v, dtype=np.complex128)
+    F = B
+    eta = np.exp(t * mu / float(s))
+    converged, final_m, c1_plus_c2, term_ratio = False, 0, 0.0, 0.0
+    for _ in range(s):
+        c1 = np.linalg.norm(B, np.inf)
+        for j in range(m_star):
+            final_m += 1
+            coeff = t / float(s * (j + 1))
+            B = coeff * A.dot(B)
+            c2 = np.linalg.norm(B, np.inf)
+            F = F + B
+            c1_plus_c2 = c1 + c2
+            term_ratio = c1_plus_c2 / np.linalg.norm(F, np.inf)
+            if term_ratio <= tol:
+                converged = True
+                break
+            c1 = c2
+        if eta != 1:
+            F = eta * F
+        B = F
+    return F, [converged, final_m, c1_plus_c2, term_ratio]
+
+
 def n_exc(model, whoami, vector):
     """Sum |psi|^2 per exciton position.  paces/models/holstein.py:311-314, :380-396."""
     pos = get_pos(model, whoami)
@@ -506,7 +575,7 @@ class Trajectory:
 
     def __init__(self, model, whoami, vector, maxstates, enlarge_steps, m_star=100,
                  tol=TAYLOR_TOL_F64, diagnostics=True, shuffle_rng=None, renormalize=False,
-                 explosion_cutoff=2.0):
+                 explosion_cutoff=2.0, use_scaling=False):
         self.model = model
         self.whoami = whoami
         self.vector = np.asarray(vector, dtype=np.complex128)
@@ -518,6 +587,7 @@ class Trajectory:
         self.rng = shuffle_rng
         self.renormalize = renormalize
         self.explosion_cutoff = explosion_cutoff
+        self.use_scaling = use_scaling
         self.asm = None
         self.records = []
 
@@ -554,7 +624,10 @@ class Trajectory:
     def step(self, t, dt):
         """paces/core/time_evolution.py:552-613."""
         pan, pae = self._new_space()
-        self.vector, dbg = taylor(self.asm, self.vector, dt, self.m_star, self.tol)
+        if self.use_scaling:
+            self.vector, dbg = expm_scaled(self.asm, self.vector, dt)
+        else:
+            self.vector, dbg = taylor(self.asm, self.vector, dt, self.m_star, self.tol)
         nrm = np.linalg.norm(self.vector)
         if self.renormalize:
             self.vector /= nrm

@@ -46,8 +46,9 @@ class CoeffSaveParams:
 class ExpmParams:
     """Matrix-exponential parameters (paces/core/time_evolution.py:57-82).
 
-    The device runs the truncated Taylor series; use_scaling=True (scaling and squaring)
-    and lanczos_order > 0 are not implemented and raise when a timeline starts.
+    The device runs the truncated Taylor series, or with use_scaling=True the scaling-and-
+    squaring series of paces_b200.expm; lanczos_order > 0 is not implemented and raises
+    when a timeline starts.
     """
     m_star: int = 100
     explosion_cutoff: float = 2.0
@@ -358,8 +359,6 @@ class TimeEvolutionFramework:
             print("Setting up generate_timeline function...")
         self.write_current_params_to_file(inspect.currentframe(), time.time())
         ep, tp = self.expm_params, self.te_params
-        if ep.use_scaling:
-            raise NotImplementedError("scaling-and-squaring propagation (use_scaling=True) is not implemented")
         if ep.lanczos_order > 0:
             raise NotImplementedError("Lanczos propagation (lanczos_order > 0) is not implemented")
         if tp.tau != 0:
@@ -386,7 +385,10 @@ class TimeEvolutionFramework:
                 rec = self._traj.step(evolve=False)
                 expm_dbg = [0, 0, 0, 0]
             else:
-                rec = self._traj.step(evolve=True, dt=float(t_curr - t_array[i - 1]))
+                if ep.use_scaling:
+                    rec = self._traj.step_scaled(float(t_curr - t_array[i - 1]))
+                else:
+                    rec = self._traj.step(evolve=True, dt=float(t_curr - t_array[i - 1]))
                 expm_dbg = [bool(rec.converged), int(rec.final_m), float(rec.c1_plus_c2), float(rec.term_ratio)]
                 if not ep.renormalize and rec.norm > ep.explosion_cutoff:
                     raise RuntimeError(f"Norm has exceeded preset explosion cutoff value ({ep.explosion_cutoff})!")

@@ -726,6 +726,40 @@ int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
     return PACES_OK;
 }
 
+int paces_hnorms(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const double* dev_shift, double* dev_out,
+                 void* ws, size_t ws_bytes, paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !dev_out || !ws) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    const int nparts = c->num_sms * 2;  // the observables' partials hold far more than 2 * nparts doubles
+    PACES_CHECK_LAUNCH(c, launch_hnorms(c->m, b->blk, h->nbr, h->meta, dev_shift, at<double>(ws, l.o_partials), nparts,
+                                        dev_out, reinterpret_cast<cudaStream_t>(stream)),
+                       "hnorms");
+    return PACES_OK;
+}
+
+int paces_expm_scaled(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi_in, void* psi_out,
+                      double t, double shift, int32_t m_star, int32_t stages, double tol, double eta_re, double eta_im,
+                      paces_expm_info* dev_info, void* ws, size_t ws_bytes, paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !psi_in || !psi_out || psi_in == psi_out || !ws ||
+        m_star < 0 || stages < 1)
+        return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    if (h->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states", (long long)l.cap);
+    TaylorOut o{};
+    if (dev_info) {
+        o.converged = &dev_info->converged;
+        o.final_m = &dev_info->final_m;
+        o.c1_plus_c2 = &dev_info->c1_plus_c2;
+        o.term_ratio = &dev_info->term_ratio;
+    }
+    PACES_CHECK_LAUNCH(c, launch_expm_scaled(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->meta, psi_in, psi_out,
+                                             t, shift, m_star, stages, tol, eta_re, eta_im, taylor_ws(l, ws), o,
+                                             c->d_status, c->num_sms, c->taylor_grid,
+                                             reinterpret_cast<cudaStream_t>(stream)),
+                       "expm_scaled");
+    return PACES_OK;
+}
+
 int paces_observables(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi, int32_t what,
                       double* dev_out, void* ws, size_t ws_bytes, paces_stream_t stream) {
     if (!c || !valid_basis(b) || !h || !psi || !dev_out || !ws) return PACES_ERR_BADARG;

@@ -56,6 +56,16 @@ int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, i
                   double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
                   int blocks_per_sm, int variant, cudaStream_t st);
 
+// ---- scaling and squaring (expm.cu) ---------------------------------------------------------
+// out[0] = trace(H), out[1] = max row 1-norm of H - *shift I (0 when shift is null),
+// out[2] = trace / n; part holds 2 * nparts doubles.
+int launch_hnorms(const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta, const double* shift,
+                  double* part, int nparts, double* out, cudaStream_t st);
+int launch_expm_scaled(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
+                       const void* v_in, void* res, double t, double shift, int m_star, int stages, double tol,
+                       double eta_re, double eta_im, const TaylorWs& ws, const TaylorOut& out, int* status,
+                       int num_sms, int max_grid, cudaStream_t st);
+
 // ---- batched Taylor: many trajectories in one persistent launch ---------------------------
 constexpr int kMaxBatch = 128;  // trajectories per launch (the descriptors travel as kernel parameters)
 constexpr int kSqrtTable = 260; // sqrt(k) * g for k < 260 (occupations up to 255, plus one)

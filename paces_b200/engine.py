@@ -254,6 +254,29 @@ class Engine:
         return {"norm": o[0], "energy": complex(o[1], o[2]), "n_exc": o[3:3 + self.L],
                 "n_pho": o[3 + self.L:3 + 2 * self.L]}
 
+    def hnorms(self, b: DevBasis, h: DevHMat, shift=None):
+        """(trace of H, largest row 1-norm of H - shift I, trace / n) on the device."""
+        out = torch.zeros(3, dtype=torch.float64, device=self.device)
+        sh = None if shift is None else torch.tensor([float(shift)], dtype=torch.float64, device=self.device)
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_hnorms(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(sh), _ptr(out), ws, nb,
+                                        _stream(self.device)), self.ctx, "hnorms")
+        return [float(x) for x in out.cpu().tolist()]
+
+    def expm_scaled(self, b: DevBasis, h: DevHMat, psi_in, psi_out, t, shift, m_star, stages, eta, tol=None):
+        """psi_out = exp(t * 1j (H - shift I)) psi_in in `stages` stages of at most m_star terms,
+        times eta after each stage.  Returns [converged, final_m, c1 + c2, term ratio]."""
+        info = torch.zeros(ctypes.sizeof(nat.ExpmInfo), dtype=torch.uint8, device=self.device)
+        ws, nb = self.workspace()
+        eta = complex(eta)
+        nat.check(self.lib.paces_expm_scaled(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(psi_in),
+                                             _ptr(psi_out), float(t), float(shift), int(m_star), int(stages),
+                                             float(self.tol if tol is None else tol), eta.real, eta.imag, _ptr(info),
+                                             ws, nb, _stream(self.device)), self.ctx, "expm_scaled")
+        self.raise_status("expm_scaled")
+        e = nat.ExpmInfo.from_buffer_copy(info.cpu().numpy().tobytes())
+        return [bool(e.converged), int(e.final_m), float(e.c1_plus_c2), float(e.term_ratio)]
+
     def apply_h(self, b: DevBasis, h: DevHMat, x, y=None):
         """y = H x (total_ham)."""
         y = torch.empty_like(x) if y is None else y
@@ -474,6 +497,42 @@ class Trajectory:
             raise nat.PacesError(rec.status, "paces_step")
         self.cur = 1 - self.cur
         self.step_index += 1
+        self.last = rec
+        return rec
+
+    def step_scaled(self, dt):
+        """One time step propagated by scaling and squaring, as the reference does with
+        ExpmParams(use_scaling=True): exp(dt * 1j H) applied with expm_multiply_simple
+        (paces/core/time_evolution.py:579-581) -- note the sign: the reference's call
+        propagates with +1j H where its plain Taylor path uses -1j H.  The new space is
+        built by a non-evolving paces_step; the norms, stage count and order come from
+        paces_b200.expm; the observables of the propagated state are measured again.
+        Returns the step record."""
+        from . import expm
+        rec = self.step(evolve=False)
+        e, b, h = self.eng, self.basis, self.h
+        psi = self.psis[self.cur]
+        _, _, dbar = e.hnorms(b, h)
+        _, a1, _ = e.hnorms(b, h, shift=dbar)
+        m, s = expm.choose(dt * a1)
+        eta = np.exp(dt * 1j * dbar / s)
+        out = self.psis[1 - self.cur]
+        dbg = e.expm_scaled(b, h, psi, out, dt, dbar, m, s, eta, tol=expm.TOL if not e.c64 else e.tol)
+        psi.copy_(out)
+        n = b.count()
+        if self.renormalize:
+            nrm = torch.linalg.vector_norm(psi[:n].to(torch.complex128)).item()
+            psi[:n] /= nrm
+        o = e.observables(b, h, psi)
+        rec.converged, rec.final_m = int(dbg[0]), int(dbg[1])
+        rec.c1_plus_c2, rec.term_ratio = dbg[2], dbg[3]
+        rec.norm = float(o["norm"])
+        rec.energy_re, rec.energy_im = o["energy"].real, o["energy"].imag
+        for i in range(e.L):
+            rec.n_exc[i] = float(o["n_exc"][i])
+            rec.n_pho[i] = float(o["n_pho"][i])
+        if not self.renormalize and rec.norm > self.explosion_cutoff:
+            raise RuntimeError(f"Norm has exceeded preset explosion cutoff value ({self.explosion_cutoff})!")
         self.last = rec
         return rec
 

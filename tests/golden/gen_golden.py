@@ -16,6 +16,8 @@ Fixtures written:
                       remap output, Taylor output and diagnostics, observables
   traj_<name>.npz     observables and diagnostics of every step of a trajectory
   ed_n4.npz           exact-diagonalisation known answer (full Hilbert space)
+  obs_extra_n7c8.npz  hopping, mu_to_0, coupling and reduced density matrices
+  scaled_n8c16.npz    a trajectory propagated with ExpmParams(use_scaling=True)
 """
 
 import argparse
@@ -292,6 +294,33 @@ def gen_obs_extra(paces, workdir):
                         config=np.array([nchain, dim, g, 3000, 1, 30, 1], dtype=np.float64))
 
 
+def gen_traj_scaled(paces, workdir):
+    """The scaling-and-squaring propagation (ExpmParams(use_scaling=True): the reference's
+    expm_multiply_simple on 1j * the total Hamiltonian, paces/core/time_evolution.py:579-581
+    and paces/aux/_scipy/_expm_multiply.py:106-202) on an open chain, N=8, dim 16, g=1,
+    maxstates 2000, 30 steps of dt 0.05, exciton starting on site 2 (off the mirror axis)."""
+    from paces.models import holstein
+    from paces.core.time_evolution import CoeffSaveParams, ExpmParams, TimeEvoParams
+    from paces.config import devices
+    nchain, dim, g = 8, 16, 1.0
+    with devices.vector_dev:
+        ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain, use_terms=terms(g), debug_verb=0)
+        te = holstein.TimeEvolution(ham, holstein.Observables, ["n_exc", "n_pho"], workdir,
+                                    TimeEvoParams(maxstates=2000, enlarge_steps=1, shuffle_seed=None),
+                                    ExpmParams(use_scaling=True), os.path.join(workdir, "params.log"))
+        te.create_nonuniform_basis([1] * nchain, minpos=2, maxpos=3)
+        te.create_initial_vector([1.0], [[2] + [0] * nchain])
+        te.generate_timeline(np.arange(31) * 0.05, CoeffSaveParams())
+        vec, who = np.asarray(te.vector), np.asarray(te.whoami)
+    od = os.path.join(workdir, "observables")
+    np.savez_compressed(os.path.join(HERE, "scaled_n8c16.npz"),
+                        n_exc=np.loadtxt(os.path.join(od, "n_exc.real")),
+                        n_pho=np.loadtxt(os.path.join(od, "n_pho.real")),
+                        diagnostics=np.loadtxt(os.path.join(od, "diagnostics.log")),
+                        vector=vec, whoami=who,
+                        config=np.array([nchain, dim, g, 2000, 1, 30, 2], dtype=np.float64))
+
+
 def gen_ed(paces, workdir):
     """N=4, max_ho_dims=4, J=g=omega=1: the full space (1024 states) fits, so paces == exact."""
     ham, te = make_objects(paces, 4, 4, 1.0, 100000, 1, 0, workdir)
@@ -327,6 +356,7 @@ def main():
         jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))
     jobs.append(("ed_n4", lambda: gen_ed(paces, fresh())))
     jobs.append(("obs_extra_n7c8", lambda: gen_obs_extra(paces, fresh())))
+    jobs.append(("scaled_n8c16", lambda: gen_traj_scaled(paces, fresh())))
     if args.long:
         for name, cfg in LONG_TRAJ_RUNS.items():
             jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))

@@ -173,3 +173,20 @@ def test_site_disorder_extension_is_exact():
     tr = po.Trajectory(m, po.initial_basis(m, 2), np.array([1.0 + 0j]), 100000, 1)
     recs = tr.run(t)
     np.testing.assert_allclose(np.array([r.n_exc for r in recs]), exact, atol=1e-12)
+
+
+def test_scaling_and_squaring_matches_the_reference():
+    """The oracle's expm_scaled inside a trajectory against the reference run with
+    ExpmParams(use_scaling=True) (tests/golden/scaled_n8c16.npz)."""
+    f = np.load(os.path.join(GOLDEN, "scaled_n8c16.npz"))
+    nchain, dim, g, maxstates, es, steps, initpos = [int(x) if i != 2 else float(x) for i, x in enumerate(f["config"])]
+    m = po.Model(nchain, [dim] * nchain, g=g)
+    tr = po.Trajectory(m, po.initial_basis(m, initpos), np.array([1.0 + 0j]), maxstates, es, use_scaling=True)
+    recs = tr.run(np.arange(steps + 1) * 0.05)
+    ne = np.array([r.n_exc for r in recs])
+    np.testing.assert_allclose(ne, f["n_exc"][:, 2:], rtol=1e-10, atol=1e-13)
+    diag = f["diagnostics"]
+    assert [r.numstates for r in recs] == diag[:, 9].astype(int).tolist()
+    assert [int(r.expm_dbg[1]) for r in recs[1:]] == diag[1:, 6].astype(int).tolist()
+    assert np.array_equal(tr.whoami, f["whoami"])
+    np.testing.assert_allclose(tr.vector, f["vector"], rtol=0, atol=1e-13)
