@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--sigma", type=float, default=0.5, help="longchain: site-energy disorder (Gaussian sigma)")
     ap.add_argument("--compare-steps", type=int, default=0,
                     help="longchain: steps of realization 0 compared against a complex128 run (0: none)")
+    ap.add_argument("--weighting", default="none", choices=["none", "coherence", "norm"],
+                    help="plain: rank the truncation by the look-ahead weights (TimeEvoParams.weighting_name)")
+    ap.add_argument("--tau", type=float, default=0.2, help="plain: look-ahead time of --weighting")
     ap.add_argument("--no-graph", action="store_true", help="step without CUDA-graph replay")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--batch", type=int, default=64, help="trajectories of the batched workload")
@@ -160,12 +163,14 @@ def initial_rows(nchain, initpos=0):
     return layout.pack_rows(raw, layout.bitwidths_for([nchain] + [16] * nchain))
 
 
-def start_trajectory(eng, nchain, maxstates, es, initpos=0, graph=False):
+def start_trajectory(eng, nchain, maxstates, es, initpos=0, graph=False, weighting="none", tau=0.0):
     """grow_optimal_basis(fillfac=1) around the exciton on `initpos` in the phonon vacuum,
     amplitude 1 on that state, then the first (non-evolving) step."""
     import torch
+    from paces_b200 import _native as nat
     from paces_b200.engine import Trajectory
-    tr = Trajectory(eng, maxstates, es, graph=graph)
+    kind = {"none": nat.WEIGHT_NONE, "coherence": nat.WEIGHT_COHERENCE, "norm": nat.WEIGHT_NORM}[weighting]
+    tr = Trajectory(eng, maxstates, es, graph=graph, weighting=kind, tau=tau if kind else 0.0)
     rows = initial_rows(nchain, initpos)
     b = eng.basis_from_ref(rows)
     while True:
@@ -185,7 +190,8 @@ def start_trajectory(eng, nchain, maxstates, es, initpos=0, graph=False):
 def prepare(a, eng, maxstates):
     """Grow the basis (grow_optimal_basis, fillfac=1), first step, then propagate until the
     truncation keeps exactly maxstates states; returns the saturated trajectory."""
-    tr = start_trajectory(eng, a.nchain, maxstates, a.enlarge_steps, graph=not a.no_graph)
+    tr = start_trajectory(eng, a.nchain, maxstates, a.enlarge_steps, graph=not a.no_graph,
+                          weighting=getattr(a, "weighting", "none"), tau=getattr(a, "tau", 0.0))
     nprep = 1
     while True:
         rec = tr.step(evolve=True, dt=a.dt)
@@ -381,7 +387,7 @@ def run_ours(a):
         e2e = run_e2e(a, eng, tr, barrier, dist)
 
     compare = None
-    if a.precision == "c64" and not a.no_compare:
+    if a.precision == "c64" and not a.no_compare and a.weighting == "none":
         compare = compare_precisions(a, f"cuda:{local}", dist)
 
     total_steps = a.steps * world
@@ -406,6 +412,7 @@ def run_ours(a):
                "states_per_step": int(S_mean), "taylor_terms_per_step": terms, "prep_steps": nprep,
                "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}",
                "cuda_graph": not a.no_graph,
+               "weighting": None if a.weighting == "none" else {"name": a.weighting, "tau": a.tau},
                "tuning": None if tuning is None else {k: tuning[k] for k in autotune_shapes()},
                "form": ("complex64 amplitudes and SpMV, fp64 norms / stop test / sums; learned proposal off "
                         "(--workload learned measures it)") if a.precision == "c64" else "complex128 plain"}
@@ -472,11 +479,19 @@ def run_e2e(a, eng, tr, barrier, dist):
     hk = [torch.empty((cap, e.nw), dtype=torch.int64).pin_memory() for _ in range(2)]
     hb = [torch.empty(e.L + 1, dtype=torch.int32).pin_memory() for _ in range(2)]
     hp = [torch.empty(cap, dtype=e.cdtype).pin_memory() for _ in range(2)]
+    # with the look-ahead weighting the state includes the basis' neighbour table
+    table = bool(tr.weighting)
+    if table:
+        hn = [torch.empty((cap, 4), dtype=torch.int32).pin_memory() for _ in range(2)]
+        hm = [torch.empty(cap, dtype=torch.int32).pin_memory() for _ in range(2)]
     b, v = tr.basis, tr.psis[tr.cur]
     n = b.count()
     hk[0][:n].copy_(b.keys[:n])
     hb[0].copy_(b.blk)
     hp[0][:n].copy_(v[:n])
+    if table:
+        hn[0][:n].copy_(tr.h.nbr[:n])
+        hm[0][:n].copy_(tr.h.meta[:n])
     cur = 0
     h2d = d2h = 0
     barrier()
@@ -489,6 +504,10 @@ def run_e2e(a, eng, tr, barrier, dist):
         db.blk.copy_(hb[cur], non_blocking=True)
         dv[:n].copy_(hp[cur][:n], non_blocking=True)
         h2d += n * (e.nw * 8 + cs) + (e.L + 1) * 4
+        if table:
+            tr.h.nbr[:n].copy_(hn[cur][:n], non_blocking=True)
+            tr.h.meta[:n].copy_(hm[cur][:n], non_blocking=True)
+            h2d += n * 20
         rec = tr.step(evolve=True, dt=a.dt)
         n = rec.n_states
         nb, nv = tr.basis, tr.psis[tr.cur]
@@ -497,6 +516,10 @@ def run_e2e(a, eng, tr, barrier, dist):
         hb[nxt].copy_(nb.blk, non_blocking=True)
         hp[nxt][:n].copy_(nv[:n], non_blocking=True)
         d2h += n * (e.nw * 8 + cs) + (e.L + 1) * 4 + ctypes.sizeof(type(rec))
+        if table:
+            hn[nxt][:n].copy_(tr.h.nbr[:n], non_blocking=True)
+            hm[nxt][:n].copy_(tr.h.meta[:n], non_blocking=True)
+            d2h += n * 20
         torch.cuda.current_stream().synchronize()
         cur = nxt
     ev1.record(stream)

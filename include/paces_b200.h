@@ -33,6 +33,9 @@
  *   paces_assemble     HamiltonianFramework.generate_mel       paces/core/hamiltonian.py:383-547
  *                      + TimeEvolutionFramework.create_matrices paces/core/time_evolution.py:365-372
  *   paces_truncate     _determine_select_whoami                paces/core/time_evolution.py:833-910
+ *   paces_truncate_weighted  the same with use_weight_function     paces/core/time_evolution.py:854-857
+ *   paces_lookahead_weights  coherence_weighting_func / norm_weighting_func / total_ham_ones
+ *                                                             paces/core/time_evolution.py:464-476, :403-420
  *   paces_remap        vector remap in _generate_new_hilbert_space_cupy
  *                                                             paces/core/time_evolution.py:781-797
  *   paces_taylor       _simple_taylor + total_ham              paces/core/time_evolution.py:482-512, :382-400
@@ -127,6 +130,17 @@ typedef struct paces_step_params {
     int32_t proposal;
     float proposal_threshold;
     const void *proposal_params;
+    /* look-ahead weighting (TimeEvoParams.weighting_name / tau; the reference applies it
+     * from the second time step on, time_evolution.py:560): weighting = PACES_WEIGHT_NONE
+     * ranks the states by |psi|, PACES_WEIGHT_COHERENCE / PACES_WEIGHT_NORM by the weights
+     * paces_lookahead_weights computes with tau (non-zero) and old_h, the neighbour table of
+     * old_basis (what the previous step wrote into its h).  old_h may be h itself: the step
+     * reads it before it writes h, but then a step that fails leaves no table to retry from.
+     * Not combined with the learned proposal. */
+    int32_t weighting;
+    int32_t reserved0;
+    double tau;
+    const paces_hmat *old_h;
 } paces_step_params;
 
 /* Written on the device by paces_step; the caller copies it back (one transfer per step). */
@@ -164,6 +178,12 @@ typedef struct paces_expm_info {
 /* Observables (device output of paces_observables): [0] norm, [1] energy re, [2] energy im,
  * [3 .. 3+L) n_exc, [3+L .. 3+2L) n_pho.  `what` is a bit set of PACES_OBS_*. */
 enum { PACES_OBS_NORM = 1, PACES_OBS_ENERGY = 2, PACES_OBS_SITES = 4 };
+
+/* Truncation weights (paces_lookahead_weights, paces_step_params.weighting):
+ *   COHERENCE  |psi|^2 + tau^2 |psi|^2 (H 1)^2   coherence_weighting_func  time_evolution.py:464-469
+ *   NORM       |psi - 1j tau H psi|              norm_weighting_func       time_evolution.py:472-476
+ *   HAM_ONES   H 1 (signed; not a ranking)       total_ham_ones            time_evolution.py:403-420 */
+enum { PACES_WEIGHT_NONE = 0, PACES_WEIGHT_COHERENCE = 1, PACES_WEIGHT_NORM = 2, PACES_WEIGHT_HAM_ONES = 3 };
 
 /* ---- context ----------------------------------------------------------------------- */
 int paces_create(const paces_model_desc *desc, paces_ctx **out);
@@ -222,6 +242,16 @@ int paces_assemble(paces_ctx *ctx, const paces_basis *in, paces_basis *out, pace
 int paces_truncate(paces_ctx *ctx, const paces_basis *in, const void *psi, int64_t maxstates,
                    int32_t shuffle, uint64_t shuffle_seed, uint64_t step_index,
                    paces_basis *out, void *ws, size_t ws_bytes, paces_stream_t stream);
+/* The look-ahead weights of the states of b (dev_weights: one double per state) from psi
+ * and b's neighbour table h; `weighting` is a PACES_WEIGHT_* other than NONE. */
+int paces_lookahead_weights(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi,
+                            double tau, int32_t weighting, double *dev_weights, paces_stream_t stream);
+/* paces_truncate ranking by dev_weights (non-negative, one per state of `in`) instead of
+ * |psi|: _determine_select_whoami with use_weight_function (time_evolution.py:854-857). */
+int paces_truncate_weighted(paces_ctx *ctx, const paces_basis *in, const double *dev_weights,
+                            int64_t maxstates, int32_t shuffle, uint64_t shuffle_seed,
+                            uint64_t step_index, paces_basis *out, void *ws, size_t ws_bytes,
+                            paces_stream_t stream);
 int paces_remap(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi,
                 const paces_basis *new_b, void *new_psi, void *ws, size_t ws_bytes,
                 paces_stream_t stream);

@@ -369,7 +369,7 @@ def generate_mel(model: Model, select, enlarge_steps):
 # --------------------------------------------------------------------------------------------
 
 
-def truncate(whoami, vector, maxstates, rng=None):
+def truncate(whoami, vector, maxstates, rng=None, weights=None):
     """Keep the `maxstates` largest |psi| states, lexicographically sorted.
 
     paces/core/time_evolution.py:833-910.  Stable ascending argsort of |psi| and
@@ -377,8 +377,9 @@ def truncate(whoami, vector, maxstates, rng=None):
     original indices are kept (shuffle_seed=None).  With `rng` the tied states
     at the cut are drawn at random instead (the reference's shuffle, whose
     cuRAND stream cannot be reproduced: parity unpinned for that branch).
+    `weights` (the look-ahead weights, :854-857) replace |psi| as the ranking.
     """
-    w = np.abs(vector)
+    w = np.abs(vector) if weights is None else np.asarray(weights)
     order = np.argsort(w, kind="stable")
     ms = int(maxstates)
     if rng is None or len(vector) < ms or w[order[-ms - 1]] < w[order[-ms]]:
@@ -395,6 +396,29 @@ def truncate(whoami, vector, maxstates, rng=None):
         sel = np.concatenate([rng.permutation(tied)[: ms - back], order[last:]])
     sel = np.sort(sel)          # whoami is sorted, so index order == lexicographic order
     return whoami[sel]
+
+
+def ham_ones(asm: Assembly):
+    """H applied to a vector of ones: diag + each term matrix's row sums, added in the
+    terms' order.  total_ham_ones, paces/core/time_evolution.py:403-420."""
+    res = asm.diag.copy()
+    for m in asm.mats.values():
+        res += np.asarray(m.sum(axis=1)).ravel()
+    return res
+
+
+def lookahead_weights(asm: Assembly, vector, tau, weighting):
+    """The truncation weights with look-ahead time tau.
+
+    coherence: |psi|^2 + tau^2 |psi|^2 (H 1)^2   (time_evolution.py:464-469)
+    norm:      |psi - 1j tau H psi|              (time_evolution.py:472-476)
+    """
+    if weighting == "coherence":
+        psi_sq = np.abs(vector) ** 2
+        return psi_sq + (tau ** 2) * psi_sq * np.power(ham_ones(asm), 2)
+    if weighting == "norm":
+        return np.abs(vector - 1j * tau * apply_h(asm, vector))
+    raise ValueError(f"unknown weighting {weighting!r}")
 
 
 def remap(old_whoami, vector, new_inds):
@@ -575,7 +599,7 @@ class Trajectory:
 
     def __init__(self, model, whoami, vector, maxstates, enlarge_steps, m_star=100,
                  tol=TAYLOR_TOL_F64, diagnostics=True, shuffle_rng=None, renormalize=False,
-                 explosion_cutoff=2.0, use_scaling=False):
+                 explosion_cutoff=2.0, use_scaling=False, tau=0.0, weighting="coherence"):
         self.model = model
         self.whoami = whoami
         self.vector = np.asarray(vector, dtype=np.complex128)
@@ -588,12 +612,18 @@ class Trajectory:
         self.renormalize = renormalize
         self.explosion_cutoff = explosion_cutoff
         self.use_scaling = use_scaling
+        self.tau = tau
+        self.weighting = weighting
         self.asm = None
         self.records = []
 
-    def _new_space(self):
-        """paces/core/time_evolution.py:735-807."""
-        select = truncate(self.whoami, self.vector, self.maxstates, self.rng)
+    def _new_space(self, weighted=False):
+        """paces/core/time_evolution.py:735-807; `weighted` ranks by the look-ahead weights
+        computed with the current basis' Hamiltonian (every step but the first, :560)."""
+        w = None
+        if weighted and self.tau != 0:
+            w = lookahead_weights(self.asm, self.vector, self.tau, self.weighting)
+        select = truncate(self.whoami, self.vector, self.maxstates, self.rng, weights=w)
         asm = generate_mel(self.model, select, self.enlarge_steps)
         self.vector = remap(self.whoami, self.vector, asm.new_inds)
         self.whoami = asm.new_inds
@@ -623,7 +653,7 @@ class Trajectory:
 
     def step(self, t, dt):
         """paces/core/time_evolution.py:552-613."""
-        pan, pae = self._new_space()
+        pan, pae = self._new_space(weighted=True)
         if self.use_scaling:
             self.vector, dbg = expm_scaled(self.asm, self.vector, dt)
         else:

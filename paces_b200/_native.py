@@ -32,6 +32,7 @@ C128 = 0
 C64 = 1
 MAX_SITES = 128
 OBS_NORM, OBS_ENERGY, OBS_SITES = 1, 2, 4
+WEIGHT_NONE, WEIGHT_COHERENCE, WEIGHT_NORM, WEIGHT_HAM_ONES = 0, 1, 2, 3
 
 
 class ModelDesc(ctypes.Structure):
@@ -75,6 +76,10 @@ class StepParams(ctypes.Structure):
         ("proposal", ctypes.c_int32),
         ("proposal_threshold", ctypes.c_float),
         ("proposal_params", ctypes.c_void_p),
+        ("weighting", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
+        ("tau", ctypes.c_double),
+        ("old_h", ctypes.c_void_p),
     ]
 
 
@@ -156,6 +161,10 @@ _SIGNATURES = {
                        ctypes.c_size_t, _P],
     "paces_truncate": [_P, ctypes.POINTER(Basis), _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64,
                        ctypes.c_uint64, ctypes.POINTER(Basis), _P, ctypes.c_size_t, _P],
+    "paces_truncate_weighted": [_P, ctypes.POINTER(Basis), _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64,
+                                ctypes.c_uint64, ctypes.POINTER(Basis), _P, ctypes.c_size_t, _P],
+    "paces_lookahead_weights": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, ctypes.c_double, ctypes.c_int32,
+                                _P, _P],
     "paces_remap": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P, ctypes.c_size_t, _P],
     "paces_remap_noalloc": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P],
     "paces_taylor": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, ctypes.c_double, ctypes.c_int32,

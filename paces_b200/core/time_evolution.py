@@ -159,10 +159,15 @@ class TimeEvolutionFramework:
     def _trajectory(self):
         if self._traj is None:
             from ..engine import Trajectory
+            from .. import _native as nat
             tp, ep = self.te_params, self.expm_params
+            weighting = nat.WEIGHT_NONE
+            if tp.tau != 0:
+                weighting = {"coherence": nat.WEIGHT_COHERENCE, "norm": nat.WEIGHT_NORM}[tp.weighting_name]
             self._traj = Trajectory(self.engine, tp.maxstates, tp.enlarge_steps, m_star=ep.m_star,
                                     diagnostics=tp.diagnostics, shuffle_seed=tp.shuffle_seed,
-                                    renormalize=ep.renormalize, explosion_cutoff=ep.explosion_cutoff)
+                                    renormalize=ep.renormalize, explosion_cutoff=ep.explosion_cutoff,
+                                    weighting=weighting, tau=tp.tau)
         return self._traj
 
     def _commit_state(self):
@@ -315,18 +320,32 @@ class TimeEvolutionFramework:
         x = torch.as_tensor(vector).to(self.engine.device, self.engine.cdtype).contiguous()
         return self.engine.apply_h(self._traj.basis, self._traj.h, x)
 
+    def _weights(self, vector, tau, weighting):
+        """Per-state weights of `vector` on the current basis, computed by the device."""
+        n = self.numstates
+        x = torch.zeros(max(self._traj.basis.cap, 1), dtype=self.engine.cdtype, device=self.engine.device)
+        if vector is not None:
+            x[:n] = torch.as_tensor(vector).to(self.engine.device, self.engine.cdtype)[:n]
+        return self.engine.lookahead_weights(self._traj.basis, self._traj.h, x, tau, weighting)
+
     def total_ham_ones(self, use_ham_mat=False):
-        ones = torch.ones(self.numstates, dtype=self.engine.cdtype, device=self.engine.device)
-        return self.total_ham(ones, use_ham_mat).real
+        """H applied to a vector of ones: diag + the row sums of every term matrix
+        (paces/core/time_evolution.py:403-420), float64 on the GPU.  (The reference adds the
+        row sums into its diag_vals array in place; here the diagonal is left unchanged.)"""
+        from .. import _native as nat
+        if use_ham_mat:
+            raise NotImplementedError("use_ham_mat=True (explicit total Hamiltonian) is not implemented")
+        return self._weights(None, 0.0, nat.WEIGHT_HAM_ONES)
 
     def coherence_weighting_func(self, vector, tau):
-        """|psi|^2 (1 + tau^2 (H 1)^2) (paces/core/time_evolution.py:464-469)."""
-        psi_sq = torch.abs(vector) ** 2
-        return psi_sq + (tau ** 2) * psi_sq * torch.pow(self.total_ham_ones(), 2)
+        """|psi|^2 + tau^2 |psi|^2 (H 1)^2 per state (paces/core/time_evolution.py:464-469)."""
+        from .. import _native as nat
+        return self._weights(vector, tau, nat.WEIGHT_COHERENCE)
 
     def norm_weighting_func(self, vector, tau):
-        """|psi - i tau H psi| (paces/core/time_evolution.py:472-476)."""
-        return torch.abs(vector - 1j * tau * self.total_ham(vector))
+        """|psi - 1j tau H psi| per state (paces/core/time_evolution.py:472-476)."""
+        from .. import _native as nat
+        return self._weights(vector, tau, nat.WEIGHT_NORM)
 
     # ---- propagation on the current basis --------------------------------------------------
     def _simple_taylor(self, delta_t):
@@ -361,8 +380,6 @@ class TimeEvolutionFramework:
         ep, tp = self.expm_params, self.te_params
         if ep.lanczos_order > 0:
             raise NotImplementedError("Lanczos propagation (lanczos_order > 0) is not implemented")
-        if tp.tau != 0:
-            raise NotImplementedError("look-ahead weighting (tau != 0) is not implemented")
         if tp.garbage_tol >= 0:
             raise NotImplementedError("garbage_tol is not implemented")
         if tp.use_two_streams:
@@ -393,7 +410,10 @@ class TimeEvolutionFramework:
                 if not ep.renormalize and rec.norm > ep.explosion_cutoff:
                     raise RuntimeError(f"Norm has exceeded preset explosion cutoff value ({ep.explosion_cutoff})!")
             self._whoami_cache = None
-            if tp.diagnostics and rec.post_adapt_energy_im > 1e-12:
+            # the reference's threshold is for complex128; complex64 amplitudes carry ~1e-7
+            # relative rounding into <psi|H|psi>
+            imag_tol = 1e-6 if self.engine.c64 else 1e-12
+            if tp.diagnostics and rec.post_adapt_energy_im > imag_tol:
                 raise RuntimeError(f"Energy has non-zero imaginary part: {rec.post_adapt_energy_im}.")
             L = self.engine.L
             self._obs_cache = {"n_exc": numpy.array(rec.n_exc[:L]), "n_pho": numpy.array(rec.n_pho[:L]),

@@ -250,6 +250,16 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
         return fail(c, PACES_ERR_BADARG, "paces_step: bad parameters");
     if (prm->proposal && !prm->proposal_params)
         return fail(c, PACES_ERR_BADARG, "paces_step: proposal without MLP parameters");
+    if (prm->weighting) {
+        if (prm->weighting != PACES_WEIGHT_COHERENCE && prm->weighting != PACES_WEIGHT_NORM)
+            return fail(c, PACES_ERR_BADARG, "paces_step: unknown weighting %d", int(prm->weighting));
+        if (!(prm->tau != 0.0 && std::isfinite(prm->tau)))
+            return fail(c, PACES_ERR_BADARG, "paces_step: the look-ahead weighting needs a non-zero finite tau");
+        if (!prm->old_h || !prm->old_h->nbr || !prm->old_h->meta || prm->old_h->cap < old_b->cap)
+            return fail(c, PACES_ERR_BADARG, "paces_step: the look-ahead weighting needs the old basis' table");
+        if (prm->proposal)
+            return fail(c, PACES_ERR_BADARG, "paces_step: the look-ahead weighting and the proposal exclude each other");
+    }
     p->l = fit_layout(c, ws_bytes);
     const Layout& l = p->l;
     if (old_b->cap > l.cap || new_b->cap > l.cap || h->cap > l.cap)
@@ -271,9 +281,10 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
 }
 
 // Kernels one step enqueues (merge: 5, +1 with the neighbour table; truncation: 18, +14
-// with tie shuffling; remap 3; observables 2 or 3; Taylor 1; renormalisation 3; record 2).
+// with tie shuffling, +1 with look-ahead weights; remap 3; observables 2 or 3; Taylor 1; renormalisation 3; record 2).
 unsigned long long step_launches(const paces_step_params& prm, bool with_taylor) {
-    return 2 + (prm.shuffle ? 32 : 18) + (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 5ull * prm.enlarge_steps + 6 +
+    return 2 + (prm.weighting ? 1 : 0) + (prm.shuffle ? 32 : 18) + (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) +
+           5ull * prm.enlarge_steps + 6 +
            3 + (prm.diagnostics ? 2 : 0) +
            (prm.evolve ? (with_taylor ? 1 : 0) + (prm.renormalize ? 3 : 0) : 0) + 3;
 }
@@ -291,8 +302,17 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     };
     record_init_kernel<<<1, 32, 0, st>>>(rec, prm->diagnostics);
     mark(0);
-    // 1. truncation of the old state
-    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, prm->maxstates,
+    // 1. truncation of the old state (ranked by the look-ahead weights, in the Taylor term
+    //    buffer, which is free until the propagation)
+    const double* weights = nullptr;
+    if (prm->weighting) {
+        double* w = at<double>(ws, l.v_TA);
+        PACES_CHECK_LAUNCH(c, launch_lookahead(c64, c->m, p.old_b->blk, prm->old_h->nbr, prm->old_h->meta, p.old_psi,
+                                               prm->tau, prm->weighting, w, status, c->num_sms, st),
+                           "step/weights");
+        weights = w;
+    }
+    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, weights, prm->maxstates,
                                           prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), p.A.keys,
                                           p.A.blk, p.A.cap, at<float>(ws, l.aw), &rec->n_tied, status, c->num_sms, st),
                        "step/truncate");
@@ -662,11 +682,37 @@ int paces_truncate(paces_ctx* c, const paces_basis* in, const void* psi, int64_t
     if (!c || !valid_basis(in) || !valid_basis(out) || !psi || !ws || maxstates < 1) return PACES_ERR_BADARG;
     const Layout l = fit_layout(c, ws_bytes);
     if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
-    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, psi, maxstates,
-                                          shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys, out->blk,
-                                          out->cap, nullptr, nullptr, c->d_status, c->num_sms,
+    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, psi, nullptr,
+                                          maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
+                                          out->blk, out->cap, nullptr, nullptr, c->d_status, c->num_sms,
                                           reinterpret_cast<cudaStream_t>(stream)),
                        "truncate");
+    return PACES_OK;
+}
+
+int paces_truncate_weighted(paces_ctx* c, const paces_basis* in, const double* weights, int64_t maxstates,
+                            int32_t shuffle, uint64_t shuffle_seed, uint64_t step_index, paces_basis* out, void* ws,
+                            size_t ws_bytes, paces_stream_t stream) {
+    if (!c || !valid_basis(in) || !valid_basis(out) || !weights || !ws || maxstates < 1) return PACES_ERR_BADARG;
+    const Layout l = fit_layout(c, ws_bytes);
+    if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
+    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, nullptr, weights,
+                                          maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
+                                          out->blk, out->cap, nullptr, nullptr, c->d_status, c->num_sms,
+                                          reinterpret_cast<cudaStream_t>(stream)),
+                       "truncate_weighted");
+    return PACES_OK;
+}
+
+int paces_lookahead_weights(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi, double tau,
+                            int32_t weighting, double* w, paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !psi || !w || h->cap < b->cap) return PACES_ERR_BADARG;
+    if (weighting != PACES_WEIGHT_COHERENCE && weighting != PACES_WEIGHT_NORM && weighting != PACES_WEIGHT_HAM_ONES)
+        return fail(c, PACES_ERR_BADARG, "paces_lookahead_weights: unknown weighting %d", int(weighting));
+    if (!std::isfinite(tau)) return fail(c, PACES_ERR_BADARG, "paces_lookahead_weights: tau is not finite");
+    PACES_CHECK_LAUNCH(c, launch_lookahead(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->meta, psi, tau, weighting,
+                                           w, c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
+                       "lookahead_weights");
     return PACES_OK;
 }
 

@@ -66,6 +66,12 @@ int launch_expm_scaled(bool c64, const ModelDev& m, const int* blk, const int* n
                        double eta_re, double eta_im, const TaylorWs& ws, const TaylorOut& out, int* status,
                        int num_sms, int max_grid, cudaStream_t st);
 
+// ---- look-ahead truncation weights (lookahead.cu) -------------------------------------------
+// w[r] for every row of the basis (blk[L] rows): kind is PACES_WEIGHT_COHERENCE, _NORM or
+// _HAM_ONES.
+int launch_lookahead(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
+                     const void* psi, double tau, int kind, double* w, int* status, int num_sms, cudaStream_t st);
+
 // ---- batched Taylor: many trajectories in one persistent launch ---------------------------
 constexpr int kMaxBatch = 128;  // trajectories per launch (the descriptors travel as kernel parameters)
 constexpr int kSqrtTable = 260; // sqrt(k) * g for k < 260 (occupations up to 255, plus one)

@@ -21,15 +21,20 @@ constexpr int kRounds = 6;
 __host__ __device__ constexpr int round_shift(int r) { return r < 5 ? 52 - 12 * r : 0; }
 __host__ __device__ constexpr int round_bits(int r) { return r < 5 ? 12 : 4; }
 
-template <bool C64>
+// The ranked weight of state i: WK 0 = |psi| of complex128 amplitudes, 1 = |psi| of
+// complex64 amplitudes, 2 = precomputed non-negative fp64 weights (the look-ahead
+// weighting).  Non-negative doubles order like their bit patterns.
+template <int WK>
 __device__ __forceinline__ unsigned long long weight_bits(const void* psi, int64_t i, int* status) {
     double w;
-    if constexpr (C64) {
+    if constexpr (WK == 1) {
         const float2 z = reinterpret_cast<const float2*>(psi)[i];
         w = double(hypotf(z.x, z.y));
-    } else {
+    } else if constexpr (WK == 0) {
         const double2 z = reinterpret_cast<const double2*>(psi)[i];
         w = hypot(z.x, z.y);
+    } else {
+        w = reinterpret_cast<const double*>(psi)[i];
     }
     if (!(w <= 1.7976931348623157e308)) raise_status(status, PACES_ERR_NONFINITE);
     return (unsigned long long)__double_as_longlong(w);
@@ -59,7 +64,7 @@ __global__ void trunc_init_kernel(ModelDev m, const int* __restrict__ x_blk, int
     }
 }
 
-template <bool C64>
+template <int WK>
 __global__ void __launch_bounds__(256) trunc_hist_all_kernel(const void* __restrict__ psi, TruncWs ws,
                                                              int* status) {
     __shared__ unsigned h[4096];
@@ -68,7 +73,7 @@ __global__ void __launch_bounds__(256) trunc_hist_all_kernel(const void* __restr
     __syncthreads();
     const int64_t S = ws.sel[SEL_S];
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < S; i += int64_t(gridDim.x) * blockDim.x) {
-        const unsigned long long k = weight_bits<C64>(psi, i, status);
+        const unsigned long long k = weight_bits<WK>(psi, i, status);
         atomicAdd(&h[(k >> 52) & 4095], 1u);
     }
     __syncthreads();
@@ -132,7 +137,7 @@ __global__ void __launch_bounds__(1024) trunc_select_kernel(TruncWs ws, int base
     for (int b = tid; b < 4096; b += blockDim.x) ws.hist[b] = 0;
 }
 
-template <bool C64>
+template <int WK>
 __global__ void __launch_bounds__(256) trunc_collect_kernel(const void* __restrict__ psi, TruncWs ws,
                                                             int* status) {
     if (!ws.sel[SEL_W + 3]) return;
@@ -145,7 +150,7 @@ __global__ void __launch_bounds__(256) trunc_collect_kernel(const void* __restri
         unsigned long long k = 0;
         bool take = false;
         if (i < S) {
-            k = weight_bits<C64>(psi, i, status);
+            k = weight_bits<WK>(psi, i, status);
             take = (k & msk) == pre;
         }
         const unsigned ballot = __ballot_sync(0xffffffffu, take);
@@ -198,7 +203,7 @@ __global__ void trunc_shuffle_prep_kernel(TruncWs ws, int* status) {
     ws.sel[SEL_CAND] = 0;
 }
 
-template <bool C64>
+template <int WK>
 __global__ void __launch_bounds__(256) trunc_collect_ties_kernel(const void* __restrict__ psi, TruncWs ws,
                                                                  uint64_t seed, uint64_t step, int* status) {
     if (!ws.sel[SEL_H + 3]) return;
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(256) trunc_collect_ties_kernel(const void* __r
     for (int64_t i0 = blockIdx.x * int64_t(blockDim.x); i0 < S; i0 += int64_t(gridDim.x) * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
         bool take = false;
-        if (i < S) take = weight_bits<C64>(psi, i, status) == vstar;
+        if (i < S) take = weight_bits<WK>(psi, i, status) == vstar;
         const unsigned ballot = __ballot_sync(0xffffffffu, take);
         if (!ballot) continue;
         int basei = 0;
@@ -226,7 +231,7 @@ __global__ void __launch_bounds__(256) trunc_collect_ties_kernel(const void* __r
 }
 
 // Per tile: states above the threshold, tied states, tied states kept by the hash rule.
-template <bool C64>
+template <int WK>
 __global__ void __launch_bounds__(256) trunc_count_kernel(const void* __restrict__ psi, TruncWs ws,
                                                           uint64_t seed, uint64_t step, int* status) {
     __shared__ int s_c[3];
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(256) trunc_count_kernel(const void* __restrict
         int a = 0, ti = 0, hk = 0;
         const int64_t i1 = min(S, int64_t(t + 1) * kTruncTile);
         for (int64_t i = int64_t(t) * kTruncTile + threadIdx.x; i < i1; i += blockDim.x) {
-            const unsigned long long k = weight_bits<C64>(psi, i, status);
+            const unsigned long long k = weight_bits<WK>(psi, i, status);
             a += k > vstar;
             if (k == vstar) {
                 ++ti;
@@ -306,7 +311,7 @@ __global__ void __launch_bounds__(1024) trunc_scan_kernel(TruncWs ws) {
         }
 }
 
-template <int NW, bool C64>
+template <int NW, int WK>
 __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint64_t* __restrict__ x_keys,
                                                           const int* __restrict__ x_blk,
                                                           const void* __restrict__ psi, TruncWs ws,
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
         const int64_t i0 = int64_t(t) * kTruncTile;
         const int n = int(min(int64_t(kTruncTile), S - i0));
         if (!all || out_w)
-            for (int e = tid; e < n; e += 256) s_k[e] = weight_bits<C64>(psi, i0 + e, status);
+            for (int e = tid; e < n; e += 256) s_k[e] = weight_bits<WK>(psi, i0 + e, status);
         __syncthreads();
         // per-thread chunk [q0, q1): counts of above / tied / hash-kept tied states
         const int q0 = min(tid * kPer, n), q1 = min(q0 + kPer, n);
@@ -444,31 +449,31 @@ __global__ void trunc_finalize_kernel(ModelDev m, const int* __restrict__ x_blk,
     if (n_tied_out) *n_tied_out = int(ws.sel[SEL_ALL] ? 0 : ws.sel[SEL_TIES]);
 }
 
-template <int NW, bool C64>
+template <int NW, int WK>
 int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_blk, const void* psi,
                       int64_t maxstates, int shuffle, uint64_t seed, uint64_t step, const TruncWs& ws,
                       uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w, int* n_tied_out,
                       int* status, int num_sms, cudaStream_t st) {
     const int g = num_sms * 4;
     trunc_init_kernel<<<1, 1024, 0, st>>>(m, x_blk, maxstates, ws);
-    trunc_hist_all_kernel<C64><<<g, 256, 0, st>>>(psi, ws, status);
+    trunc_hist_all_kernel<WK><<<g, 256, 0, st>>>(psi, ws, status);
     trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, 0, 1);
-    trunc_collect_kernel<C64><<<g, 256, 0, st>>>(psi, ws, status);
+    trunc_collect_kernel<WK><<<g, 256, 0, st>>>(psi, ws, status);
     for (int r = 1; r < kRounds; ++r) {
         trunc_hist_cand_kernel<<<g, 256, 0, st>>>(ws, SEL_W, r);
         trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, r, 1);
     }
     if (shuffle) {
         trunc_shuffle_prep_kernel<<<1, 32, 0, st>>>(ws, status);
-        trunc_collect_ties_kernel<C64><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
+        trunc_collect_ties_kernel<WK><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
         for (int r = 0; r < kRounds; ++r) {
             trunc_hist_cand_kernel<<<g, 256, 0, st>>>(ws, SEL_H, r);
             trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_H, r, 0);
         }
     }
-    trunc_count_kernel<C64><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
+    trunc_count_kernel<WK><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
     trunc_scan_kernel<<<1, 1024, 0, st>>>(ws);
-    trunc_write_kernel<NW, C64><<<g, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
+    trunc_write_kernel<NW, WK><<<g, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
                                                    out_blk, out_cap, out_w, status);
     trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out,
                                             out_w ? out_w + out_cap : nullptr, status);
@@ -477,25 +482,28 @@ int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_bl
 
 template <int NW>
 int dispatch_prec(bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                  const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
-                  const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
-                  int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
-    if (c64)
-        return launch_truncate_t<NW, true>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
-                                           out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
-    return launch_truncate_t<NW, false>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
+                  const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed,
+                  uint64_t step, const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
+                  float* out_w, int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
+    if (weights)
+        return launch_truncate_t<NW, 2>(m, x_keys, x_blk, weights, maxstates, shuffle, seed, step, ws,
                                         out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
+    if (c64)
+        return launch_truncate_t<NW, 1>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
+                                        out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
+    return launch_truncate_t<NW, 0>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
+                                    out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
 }
 
 }  // namespace
 
 int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                    const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
+                    const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
                     const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
                     int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
 #define PACES_TRUNC_CASE(N)                                                                       \
     case N:                                                                                       \
-        return dispatch_prec<N>(c64, m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,   \
+        return dispatch_prec<N>(c64, m, x_keys, x_blk, psi, weights, maxstates, shuffle, seed, step, ws,   \
                                 out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
     switch (nw) {
         PACES_TRUNC_CASE(1)

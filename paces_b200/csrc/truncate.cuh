@@ -35,11 +35,13 @@ constexpr int kTruncTile = 4096;
 
 inline int trunc_tiles_cap(int64_t cap) { return int(cap / kTruncTile + 2); }
 
-// out_w (optional, out_cap + 1 floats): |psi| of every kept state in the new basis' order,
-// and at out_w[out_cap] the cut -- |psi| of the smallest kept state, 0 when nothing was
-// dropped.
+// weights (optional, one non-negative double per state): rank by these instead of |psi|
+// (the look-ahead weighting, lookahead.cu).
+// out_w (optional, out_cap + 1 floats): the ranked weight (|psi|) of every kept state in the
+// new basis' order, and at out_w[out_cap] the cut -- the weight of the smallest kept state, 0
+// when nothing was dropped.
 int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                    const void* psi, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
+                    const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
                     const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
                     int* n_tied_out, int* status, int num_sms, cudaStream_t st);
 

@@ -224,6 +224,29 @@ class Engine:
         self.raise_status("truncate")
         return out
 
+    def truncate_weighted(self, b: DevBasis, weights, maxstates, shuffle=False, seed=0, step=0, out=None) -> DevBasis:
+        """`truncate` ranking the states by `weights` (float64, one per state) instead of |psi|."""
+        out = out or self.new_basis()
+        ws, nb = self.workspace()
+        if weights.dtype != torch.float64 or weights.device != self.device or weights.numel() < b.count():
+            raise ValueError("weights: one float64 per state, on the engine's device")
+        nat.check(self.lib.paces_truncate_weighted(self.ctx, ctypes.byref(b.c()), _ptr(weights), int(maxstates),
+                                                   int(bool(shuffle)), int(seed), int(step), ctypes.byref(out.c()),
+                                                   ws, nb, _stream(self.device)), self.ctx, "truncate_weighted")
+        self.raise_status("truncate_weighted")
+        return out
+
+    def lookahead_weights(self, b: DevBasis, h: DevHMat, psi, tau, weighting, out=None):
+        """Look-ahead weights (weighting = nat.WEIGHT_COHERENCE / WEIGHT_NORM) or H 1
+        (nat.WEIGHT_HAM_ONES) of every state of b, as float64 on the device."""
+        n = b.count()
+        out = torch.empty(max(n, 1), dtype=torch.float64, device=self.device) if out is None else out
+        nat.check(self.lib.paces_lookahead_weights(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(psi),
+                                                   float(tau), int(weighting), _ptr(out), _stream(self.device)),
+                  self.ctx, "lookahead_weights")
+        self.raise_status("lookahead_weights")
+        return out[:n]
+
     def remap(self, old: DevBasis, old_psi, new: DevBasis, new_psi=None):
         new_psi = self.new_vector(new.cap) if new_psi is None else new_psi
         ws, nb = self.workspace()
@@ -393,7 +416,14 @@ class Trajectory:
     """
 
     def __init__(self, eng: Engine, maxstates, enlarge_steps, m_star=100, diagnostics=True,
-                 shuffle_seed=None, renormalize=False, explosion_cutoff=2.0, cap=None, graph=False):
+                 shuffle_seed=None, renormalize=False, explosion_cutoff=2.0, cap=None, graph=False,
+                 weighting=nat.WEIGHT_NONE, tau=0.0):
+        if weighting not in (nat.WEIGHT_NONE, nat.WEIGHT_COHERENCE, nat.WEIGHT_NORM):
+            raise ValueError(f"unknown weighting {weighting}")
+        if weighting != nat.WEIGHT_NONE and tau == 0:
+            raise ValueError("Specify a non-zero tau for this function to use U-weighting.")
+        self.weighting = int(weighting)
+        self.tau = float(tau)
         self.eng = eng
         self.maxstates = int(maxstates)
         self.enlarge_steps = int(enlarge_steps)
@@ -416,23 +446,39 @@ class Trajectory:
         e = self.eng
         self.bases = [e.new_basis(), e.new_basis()]
         self.psis = [e.new_vector(), e.new_vector()]
-        self.h = e.new_hmat()
+        # with the look-ahead weighting a step reads the current basis' table while it writes
+        # the next one: two tables, swapped with the bases (one shared table otherwise)
+        h = e.new_hmat()
+        self.hs = [h, e.new_hmat() if self.weighting else h]
+        self._h_valid = False   # hs[cur] holds the table of bases[cur]
+
+    @property
+    def h(self) -> DevHMat:
+        """The neighbour table of the current basis (written by the last step)."""
+        return self.hs[self.cur]
 
     def _regrow(self, factor=1.6):
-        """Grow every buffer, keeping the current state."""
+        """Grow every buffer, keeping the current state (and its table)."""
         e = self.eng
         self._graphs = {}
-        old_b, old_psi = self.bases[self.cur], self.psis[self.cur]
+        old_b, old_psi, old_h = self.bases[self.cur], self.psis[self.cur], self.hs[self.cur]
         n = old_b.count()
         e._grow(int(e.cap * factor))
         keep_keys, keep_blk, keep_psi = old_b.keys[:n].clone(), old_b.blk.clone(), old_psi[:n].clone()
+        keep_h = (old_h.nbr[:n].clone(), old_h.meta[:n].clone()) if self._h_valid and self.weighting else None
+        valid = self._h_valid
         self._alloc()
         b = self.bases[self.cur]
         b.keys[:n] = keep_keys
         b.blk.copy_(keep_blk)
         self.psis[self.cur][:n] = keep_psi
+        if keep_h is not None:
+            self.hs[self.cur].nbr[:n] = keep_h[0]
+            self.hs[self.cur].meta[:n] = keep_h[1]
+        self._h_valid = valid and keep_h is not None
 
     def set_state(self, basis: DevBasis, psi):
+        self._h_valid = False
         n = basis.count()
         while n > self.eng.cap:
             self._regrow()
@@ -451,7 +497,9 @@ class Trajectory:
     def vector(self):
         return self.psis[self.cur][: self.basis.count()]
 
-    def params(self, evolve, dt):
+    def params(self, evolve, dt, weighted=None):
+        """Step parameters; `weighted` (default: evolve) applies the look-ahead weighting,
+        which the reference uses on every step but the first (time_evolution.py:560)."""
         p = nat.StepParams()
         p.maxstates = self.maxstates
         p.enlarge_steps = self.enlarge_steps
@@ -469,6 +517,14 @@ class Trajectory:
             p.proposal = 1
             p.proposal_threshold = float(self.proposal[1])
             p.proposal_params = self.proposal[0].data_ptr()
+        if self.weighting and (evolve if weighted is None else weighted):
+            if not self._h_valid:
+                raise RuntimeError("the look-ahead weighting needs the neighbour table of the current basis: "
+                                   "take a first (non-evolving) step after setting the state")
+            self._old_h_c = self.hs[self.cur].c()
+            p.weighting = self.weighting
+            p.tau = self.tau
+            p.old_h = ctypes.addressof(self._old_h_c)
         return p
 
     def _capture(self, dt):
@@ -480,8 +536,8 @@ class Trajectory:
         s = torch.cuda.Stream(dev)
         torch.cuda.synchronize(dev)
         with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
-            self.eng.step(self.bases[self.cur], self.psis[self.cur], self.bases[nxt], self.psis[nxt], self.h, prm,
-                          sync=False)
+            self.eng.step(self.bases[self.cur], self.psis[self.cur], self.bases[nxt], self.psis[nxt], self.hs[nxt],
+                          prm, sync=False)
         return g, prm
 
     def _graph_step(self, dt):
@@ -497,6 +553,7 @@ class Trajectory:
             raise nat.PacesError(rec.status, "paces_step")
         self.cur = 1 - self.cur
         self.step_index += 1
+        self._h_valid = True
         self.last = rec
         return rec
 
@@ -509,7 +566,7 @@ class Trajectory:
         paces_b200.expm; the observables of the propagated state are measured again.
         Returns the step record."""
         from . import expm
-        rec = self.step(evolve=False)
+        rec = self.step(evolve=False, weighted=True)
         e, b, h = self.eng, self.basis, self.h
         psi = self.psis[self.cur]
         _, _, dbar = e.hnorms(b, h)
@@ -536,16 +593,19 @@ class Trajectory:
         self.last = rec
         return rec
 
-    def step(self, evolve=True, dt=0.0):
-        """One time step (first step: evolve=False).  Returns the step record."""
-        if self.use_graph and evolve and self.shuffle_seed is None:
+    def step(self, evolve=True, dt=0.0, weighted=None):
+        """One time step (first step: evolve=False).  Returns the step record.  `weighted`
+        (default: evolve) ranks the truncation by the look-ahead weights when the
+        trajectory has a weighting."""
+        w = evolve if weighted is None else weighted
+        if self.use_graph and evolve and w == evolve and self.shuffle_seed is None:
             rec = self._graph_step(dt)
             if rec is not None:
                 return rec
         nxt = 1 - self.cur
         for _ in range(12):
             rec = self.eng.step(self.bases[self.cur], self.psis[self.cur], self.bases[nxt], self.psis[nxt],
-                                self.h, self.params(evolve, dt))
+                                self.hs[nxt], self.params(evolve, dt, w))
             if rec.status == nat.ERR_CAPACITY:
                 self._regrow()
                 continue
@@ -554,6 +614,7 @@ class Trajectory:
             raise nat.PacesError(rec.status, "paces_step")
         self.cur = nxt
         self.step_index += 1
+        self._h_valid = True
         self.last = rec
         return rec
 
@@ -599,7 +660,7 @@ class TrajectoryBatch:
         keep, arr = [], (nat.BatchItem * len(self.trajs))()
         for i, t in enumerate(self.trajs):
             nxt = 1 - t.cur
-            ob, nb, hm = t.bases[t.cur].c(), t.bases[nxt].c(), t.h.c()
+            ob, nb, hm = t.bases[t.cur].c(), t.bases[nxt].c(), t.hs[nxt].c()
             prm = t.params(evolve, dts[i])
             ws, nbytes = t.eng.workspace()
             keep += [ob, nb, hm, prm]
@@ -669,6 +730,7 @@ class TrajectoryBatch:
         for t, r in zip(self.trajs, recs):
             t.cur = 1 - t.cur
             t.step_index += 1
+            t._h_valid = True
             t.last = r
         return recs
 

@@ -18,6 +18,7 @@ Fixtures written:
   ed_n4.npz           exact-diagonalisation known answer (full Hilbert space)
   obs_extra_n7c8.npz  hopping, mu_to_0, coupling and reduced density matrices
   scaled_n8c16.npz    a trajectory propagated with ExpmParams(use_scaling=True)
+  tau_<weighting>_n8c16.npz  trajectories truncated by the look-ahead weights (tau=0.2)
 """
 
 import argparse
@@ -321,6 +322,43 @@ def gen_traj_scaled(paces, workdir):
                         config=np.array([nchain, dim, g, 2000, 1, 30, 2], dtype=np.float64))
 
 
+TAU_RUNS = {
+    # name: weighting_name -- N=8, dim 16, g=1, maxstates 1500, 30 steps of dt 0.05, tau 0.2
+    "tau_coherence_n8c16": "coherence",
+    "tau_norm_n8c16": "norm",
+}
+
+
+def gen_traj_tau(paces, name, weighting, workdir):
+    """The look-ahead weighting (TimeEvoParams(tau=0.2, weighting_name=...): the truncation
+    ranks by coherence_weighting_func or norm_weighting_func from the second step on,
+    paces/core/time_evolution.py:464-476, :560, :854-857) on an open chain, N=8, dim 16,
+    g=1, maxstates 1500, 30 steps of dt 0.05, exciton starting on site 2 (off the mirror
+    axis).  Stores the observables of every step and the last state."""
+    from paces.models import holstein
+    from paces.core.time_evolution import CoeffSaveParams, ExpmParams, TimeEvoParams
+    from paces.config import devices
+    nchain, dim, g, ms, tau = 8, 16, 1.0, 1500, 0.2
+    with devices.vector_dev:
+        ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain, use_terms=terms(g), debug_verb=0)
+        te = holstein.TimeEvolution(ham, holstein.Observables, ["n_exc", "n_pho", "total_energy"], workdir,
+                                    TimeEvoParams(maxstates=ms, enlarge_steps=1, shuffle_seed=None, tau=tau,
+                                                  weighting_name=weighting),
+                                    ExpmParams(), os.path.join(workdir, "params.log"))
+        te.create_nonuniform_basis([1] * nchain, minpos=2, maxpos=3)
+        te.create_initial_vector([1.0], [[2] + [0] * nchain])
+        te.generate_timeline(np.arange(31) * 0.05, CoeffSaveParams())
+        vec, who = np.asarray(te.vector), np.asarray(te.whoami)
+    od = os.path.join(workdir, "observables")
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"),
+                        n_exc=np.loadtxt(os.path.join(od, "n_exc.real")),
+                        n_pho=np.loadtxt(os.path.join(od, "n_pho.real")),
+                        energy=np.loadtxt(os.path.join(od, "total_energy.real")),
+                        diagnostics=np.loadtxt(os.path.join(od, "diagnostics.log")),
+                        vector=vec, whoami=who,
+                        config=np.array([nchain, dim, g, ms, 1, 30, 2, tau], dtype=np.float64))
+
+
 def gen_ed(paces, workdir):
     """N=4, max_ho_dims=4, J=g=omega=1: the full space (1024 states) fits, so paces == exact."""
     ham, te = make_objects(paces, 4, 4, 1.0, 100000, 1, 0, workdir)
@@ -357,6 +395,8 @@ def main():
     jobs.append(("ed_n4", lambda: gen_ed(paces, fresh())))
     jobs.append(("obs_extra_n7c8", lambda: gen_obs_extra(paces, fresh())))
     jobs.append(("scaled_n8c16", lambda: gen_traj_scaled(paces, fresh())))
+    for name, weighting in TAU_RUNS.items():
+        jobs.append((name, lambda name=name, w=weighting: gen_traj_tau(paces, name, w, fresh())))
     if args.long:
         for name, cfg in LONG_TRAJ_RUNS.items():
             jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))

@@ -57,14 +57,14 @@ def initial_rows(nchain, dim=16, initpos=0):
     return layout.pack_rows(raw, layout.bitwidths_for([nchain] + [dim] * nchain))
 
 
-def grown_trajectory(eng, nchain, maxstates, es=1, initpos=0, dim=16, graph=False):
+def grown_trajectory(eng, nchain, maxstates, es=1, initpos=0, dim=16, graph=False, **traj_kw):
     """A trajectory on grow_optimal_basis(fillfac=1) with the exciton on `initpos` in the
     phonon vacuum, after its first (non-evolving) step
     (paces/core/time_evolution.py:290-323, :325-363)."""
     import torch
     from paces_b200.engine import Trajectory
     rows = initial_rows(nchain, dim, initpos)
-    tr = Trajectory(eng, maxstates, es, graph=graph)
+    tr = Trajectory(eng, maxstates, es, graph=graph, **traj_kw)
     b = eng.basis_from_ref(rows)
     while True:
         nxt = eng.expand(b)

@@ -190,3 +190,27 @@ def test_scaling_and_squaring_matches_the_reference():
     assert [int(r.expm_dbg[1]) for r in recs[1:]] == diag[1:, 6].astype(int).tolist()
     assert np.array_equal(tr.whoami, f["whoami"])
     np.testing.assert_allclose(tr.vector, f["vector"], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("weighting", ["coherence", "norm"])
+def test_lookahead_weighting_matches_the_reference(weighting):
+    """The oracle's look-ahead weighting (coherence_weighting_func / norm_weighting_func
+    ranking the truncation from the second step on) against the reference's runs with
+    TimeEvoParams(tau=0.2) (tests/golden/tau_<weighting>_n8c16.npz), and the fixture
+    discriminates: ranking by |psi| alone ends in another basis."""
+    f = np.load(os.path.join(GOLDEN, f"tau_{weighting}_n8c16.npz"))
+    nchain, dim, g, maxstates, es, steps, initpos, tau = f["config"]
+    nchain, dim, maxstates, es, steps, initpos = (int(x) for x in (nchain, dim, maxstates, es, steps, initpos))
+    m = po.Model(nchain, [dim] * nchain, g=float(g))
+    runs = {}
+    for t in (float(tau), 0.0):
+        tr = po.Trajectory(m, po.initial_basis(m, initpos), np.array([1.0 + 0j]), maxstates, es, tau=t,
+                           weighting=weighting)
+        runs[t] = (tr, tr.run(np.arange(steps + 1) * 0.05))
+    tr, recs = runs[float(tau)]
+    np.testing.assert_allclose(np.array([r.n_exc for r in recs]), f["n_exc"][:, 2:], rtol=1e-10, atol=1e-14)
+    assert [r.numstates for r in recs] == f["diagnostics"][:, 9].astype(int).tolist()
+    assert np.array_equal(tr.whoami, f["whoami"])
+    np.testing.assert_allclose(tr.vector, f["vector"], rtol=0, atol=1e-14)
+    plain = runs[0.0][0]
+    assert plain.whoami.shape != f["whoami"].shape or not np.array_equal(plain.whoami, f["whoami"])
