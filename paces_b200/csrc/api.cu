@@ -280,11 +280,13 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
     return PACES_OK;
 }
 
-// Kernels one step enqueues (merge: 5, +1 with the neighbour table; truncation: 18, +14
-// with tie shuffling, +1 with look-ahead weights; remap 3; observables 2 or 3; Taylor 1; renormalisation 3; record 2).
-unsigned long long step_launches(const paces_step_params& prm, bool with_taylor) {
-    return 2 + (prm.weighting ? 1 : 0) + (prm.shuffle ? 32 : 18) + (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) +
-           5ull * prm.enlarge_steps + 6 +
+// Kernels one step enqueues (merge: 5, +1 with the neighbour table; truncation: see
+// trunc_launches, +1 with look-ahead weights; remap 3; observables 2 or 3; Taylor 1;
+// renormalisation 3; record 2).
+unsigned long long step_launches(const paces_step_params& prm, bool c64, bool with_taylor) {
+    const int wk = prm.weighting ? 2 : (c64 ? 1 : 0);
+    return 2 + (prm.weighting ? 1 : 0) + trunc_launches(wk, prm.shuffle != 0) +
+           (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 5ull * prm.enlarge_steps + 6 +
            3 + (prm.diagnostics ? 2 : 0) +
            (prm.evolve ? (with_taylor ? 1 : 0) + (prm.renormalize ? 3 : 0) : 0) + 3;
 }
@@ -846,7 +848,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
     const int rc = plan_step(c, old_b, old_psi, new_b, new_psi, h, prm, rec, ws, ws_bytes, &p);
     if (rc != PACES_OK) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    c->launches += step_launches(*prm, true);
+    c->launches += step_launches(*prm, c->precision == PACES_C64, true);
     int r = step_front(c, p, st, true);
     if (r != PACES_OK) return r;
     if (prm->evolve) {
@@ -1032,7 +1034,7 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
         const int rc = plan_step(it.ctx, it.old_basis, it.old_psi, it.new_basis, it.new_psi, it.h, it.params,
                                  it.record, it.workspace, it.workspace_bytes, &plans[i]);
         if (rc != PACES_OK) return bfail(rc, "item %d: %s", i, it.ctx->err);
-        launches += step_launches(*it.params, false);
+        launches += step_launches(*it.params, it.ctx->precision == PACES_C64, false);
         n_evolve += it.params->evolve ? 1 : 0;
     }
     auto fork = [&]() -> bool {

@@ -40,24 +40,34 @@ obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict
     const C* x = reinterpret_cast<const C*>(psi);
     const R J = R(m.J);
     double norm2 = 0.0, er = 0.0, ei = 0.0;
-    for (int64_t r = int64_t(blockIdx.x) * kOThreads + threadIdx.x; r < S; r += int64_t(gridDim.x) * kOThreads) {
-        const C z = x[r];
-        const double zr = double(z.x), zi = double(z.y);
+    auto row = [&](int64_t r) {
         const uint32_t mm = __ldg(meta + r);
+        const int4 nb = load_nbr(nbr, r);
+        const C z = __ldcg(x + r);
+        const double zr = double(z.x), zi = double(z.y);
         double yr, yi;
         if constexpr (C64) {
-            const float2 y = h_row_c64(m, s_sq, J, r, nbr, mm, x);
+            const float2 y = h_row_c64_nb(m, s_sq, J, r, nb, mm, z, x);
             yr = y.x;
             yi = y.y;
         } else {
-            const double2 y = h_row_c128(m, s_sq, r, nbr, mm, x);
+            const double2 y = h_row_c128_nb(m, s_sq, r, nb, mm, z, x);
             yr = y.x;
             yi = y.y;
         }
         norm2 += zr * zr + zi * zi;
         er += zr * yr + zi * yi;
         ei += zr * yi - zi * yr;
+    };
+    // two rows a grid stride apart per iteration: their loads are independent and in flight
+    // together
+    const int64_t gs = int64_t(gridDim.x) * kOThreads;
+    int64_t r = int64_t(blockIdx.x) * kOThreads + threadIdx.x;
+    for (; r + gs < S; r += 2 * gs) {
+        row(r);
+        row(r + gs);
     }
+    if (r < S) row(r);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         norm2 += __shfl_xor_sync(0xffffffffu, norm2, o);
@@ -80,7 +90,7 @@ obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict
 // `uniform`: every field is `ub` bits wide and word q holds sites q*fpw .. q*fpw+fpw-1
 // MSB-first (NW <= 4), so thread-private register accumulators cover all sites.
 template <int NW, bool C64>
-__global__ void __launch_bounds__(kOThreads)
+__global__ void __launch_bounds__(kOThreads, NW <= 2 ? 2 : 1)
 obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict__ blk,
                  const uint32_t* __restrict__ meta, const void* __restrict__ psi, double* __restrict__ part,
                  int uniform_in, int ub, int fpw) {
@@ -103,21 +113,42 @@ obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __res
     const int64_t S = blk[L];
     const C* x = reinterpret_cast<const C*>(psi);
     double norm2 = 0.0;
-    for (int64_t base = (int64_t(blockIdx.x) * kOWarps + wid) * 32; base < S;
-         base += int64_t(gridDim.x) * kOWarps * 32) {
+    // the loads of the next 32 rows are issued before the current rows are summed (the
+    // accumulators hold the occupancy at two blocks per SM, so the memory parallelism has
+    // to come from within each thread)
+    const int64_t gstride = int64_t(gridDim.x) * kOWarps * 32;
+    int64_t base = (int64_t(blockIdx.x) * kOWarps + wid) * 32;
+    C zn{};
+    uint32_t mn = 0;
+    Key<NW> kn;
+#pragma unroll
+    for (int q = 0; q < NW; ++q) kn.w[q] = 0;
+    if (base + lane < S) {
+        zn = __ldcs(x + base + lane);
+        mn = __ldcs(meta + base + lane);
+        kn = load_key<NW>(keys, base + lane);
+    }
+    for (; base < S; base += gstride) {
         const int64_t r = base + lane;
         const bool valid = r < S;
+        const C z = zn;
+        const uint32_t mm = valid ? mn : 0u;
+        Key<NW> k = kn;
+        {
+            const int64_t rn = r + gstride;
+            if (rn < S) {
+                zn = __ldcs(x + rn);
+                mn = __ldcs(meta + rn);
+                kn = load_key<NW>(keys, rn);
+            }
+        }
         double w = 0.0;
-        uint32_t mm = 0;
-        Key<NW> k;
-#pragma unroll
-        for (int q = 0; q < NW; ++q) k.w[q] = 0;
         if (valid) {
-            const C z = x[r];
             const double zr = double(z.x), zi = double(z.y);
             w = zr * zr + zi * zi;
-            mm = __ldg(meta + r);
-            k = load_key<NW>(keys, r);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NW; ++q) k.w[q] = 0;
         }
         norm2 += w;
         if (uniform) {

@@ -64,24 +64,8 @@ __global__ void trunc_init_kernel(ModelDev m, const int* __restrict__ x_blk, int
     }
 }
 
-template <int WK>
-__global__ void __launch_bounds__(256) trunc_hist_all_kernel(const void* __restrict__ psi, TruncWs ws,
-                                                             int* status) {
-    __shared__ unsigned h[4096];
-    if (!ws.sel[SEL_W + 3]) return;
-    for (int b = threadIdx.x; b < 4096; b += blockDim.x) h[b] = 0;
-    __syncthreads();
-    const int64_t S = ws.sel[SEL_S];
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < S; i += int64_t(gridDim.x) * blockDim.x) {
-        const unsigned long long k = weight_bits<WK>(psi, i, status);
-        atomicAdd(&h[(k >> 52) & 4095], 1u);
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < 4096; b += blockDim.x)
-        if (h[b]) atomicAdd(&ws.hist[b], h[b]);
-}
-
-// One radix round: find the digit holding the need-th largest key, narrow the prefix.
+// One radix round: find the digit holding the need-th largest key, narrow the prefix;
+// on the final round (record_ties) the chosen bin's count is the number of tied states.
 __global__ void __launch_bounds__(1024) trunc_select_kernel(TruncWs ws, int base, int round,
                                                             int record_ties) {
     __shared__ long long s_warp[32];
@@ -131,42 +115,46 @@ __global__ void __launch_bounds__(1024) trunc_select_kernel(TruncWs ws, int base
         ws.sel[base + 2] = need - s_above;
         ws.sel[base + 0] |= (long long)((unsigned long long)b << shift);
         ws.sel[base + 1] |= (long long)((unsigned long long)(nb - 1) << shift);
-        if (record_ties && round == kRounds - 1) ws.sel[SEL_TIES] = ws.hist[b];
+        if (record_ties) ws.sel[SEL_TIES] = ws.hist[b];
     }
     __syncthreads();
     for (int b = tid; b < 4096; b += blockDim.x) ws.hist[b] = 0;
 }
 
+// One radix round over all states: histogram of the round's digit among the states whose
+// higher digits equal the prefix chosen so far (round 0: every state).  A full streaming
+// pass per round -- no candidate list, so no global counter and no scattered writes.  Lanes
+// with the same digit add to the shared histogram once (warp-aggregated: in round 0 most
+// states share a few binades).
 template <int WK>
-__global__ void __launch_bounds__(256) trunc_collect_kernel(const void* __restrict__ psi, TruncWs ws,
-                                                            int* status) {
+__global__ void __launch_bounds__(256) trunc_hist_pass_kernel(const void* __restrict__ psi, TruncWs ws, int round,
+                                                              int* status) {
+    __shared__ unsigned h[4096];
     if (!ws.sel[SEL_W + 3]) return;
+    const int bits = round_bits(round), shift = round_shift(round);
+    const unsigned long long dm = (1ull << bits) - 1;
+    for (int b = threadIdx.x; b < (1 << bits); b += blockDim.x) h[b] = 0;
+    __syncthreads();
     const int64_t S = ws.sel[SEL_S];
     const unsigned long long pre = (unsigned long long)ws.sel[SEL_W + 0];
     const unsigned long long msk = (unsigned long long)ws.sel[SEL_W + 1];
     const int lane = threadIdx.x & 31;
-    for (int64_t i0 = blockIdx.x * int64_t(blockDim.x); i0 < S; i0 += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t i = i0 + threadIdx.x;
-        unsigned long long k = 0;
-        bool take = false;
+    for (int64_t i0 = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x - lane); i0 < S;
+         i0 += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = i0 + lane;
+        bool match = false;
+        unsigned bin = 0xffffffffu;
         if (i < S) {
-            k = weight_bits<WK>(psi, i, status);
-            take = (k & msk) == pre;
+            const unsigned long long k = weight_bits<WK>(psi, i, status);
+            match = (k & msk) == pre;
+            if (match) bin = unsigned((k >> shift) & dm);
         }
-        const unsigned ballot = __ballot_sync(0xffffffffu, take);
-        if (!ballot) continue;
-        int basei = 0;
-        if (lane == 0) basei = int(atomicAdd(reinterpret_cast<unsigned long long*>(&ws.sel[SEL_CAND]),
-                                            (unsigned long long)__popc(ballot)));
-        basei = __shfl_sync(0xffffffffu, basei, 0);
-        if (take) {
-            const int slot = basei + __popc(ballot & ((1u << lane) - 1));
-            if (slot < ws.cap) {
-                ws.cand[slot] = k;
-                ws.cand_idx[slot] = int(i);
-            }
-        }
+        const unsigned peers = __match_any_sync(0xffffffffu, bin);
+        if (match && lane == __ffs(peers) - 1) atomicAdd(&h[bin], unsigned(__popc(peers)));
     }
+    __syncthreads();
+    for (int b = threadIdx.x; b < (1 << bits); b += blockDim.x)
+        if (h[b]) atomicAdd(&ws.hist[b], h[b]);
 }
 
 __global__ void __launch_bounds__(256) trunc_hist_cand_kernel(TruncWs ws, int base, int round) {
@@ -311,6 +299,11 @@ __global__ void __launch_bounds__(1024) trunc_scan_kernel(TruncWs ws) {
         }
 }
 
+// The compaction: every warp owns kTruncTile / 8 consecutive states of the tile.  Pass 1
+// counts, per warp, the states above the threshold, the tied ones and the tied ones the
+// hash keeps (ballots); pass 2 walks the same states 32 at a time and places every kept
+// state at its rank among the kept ones (ballot prefixes).  Lanes read consecutive keys
+// and the kept ones write consecutive outputs, so both sides coalesce.
 template <int NW, int WK>
 __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint64_t* __restrict__ x_keys,
                                                           const int* __restrict__ x_blk,
@@ -319,9 +312,11 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
                                                           uint64_t* __restrict__ out_keys,
                                                           int* __restrict__ out_blk, int64_t out_cap,
                                                           float* __restrict__ out_w, int* status) {
+    constexpr int kWarps = 8;
+    constexpr int kSeg = kTruncTile / kWarps;
     __shared__ unsigned long long s_k[kTruncTile];
     __shared__ int s_blk[kMaxSites + 1];
-    __shared__ int s_w[8][3];
+    __shared__ int s_w[kWarps][3];
     const int L = m.L;
     for (int i = threadIdx.x; i <= L; i += blockDim.x) s_blk[i] = x_blk[i];
     const int64_t S = ws.sel[SEL_S];
@@ -330,44 +325,39 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
     const unsigned long long vstar = (unsigned long long)ws.sel[SEL_W + 0];
     const long long need = ws.sel[SEL_W + 2];
     const long long ties = ws.sel[SEL_TIES];
+    const long long skip_ties = ties - need;  // tied states dropped (the lowest indices)
     const bool shuf = ws.sel[SEL_SHUFFLE] != 0;
     const unsigned long long hstar = (unsigned long long)ws.sel[SEL_H + 0];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    constexpr int kPer = kTruncTile / 256;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
     __syncthreads();
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t i0 = int64_t(t) * kTruncTile;
         const int n = int(min(int64_t(kTruncTile), S - i0));
-        if (!all || out_w)
-            for (int e = tid; e < n; e += 256) s_k[e] = weight_bits<WK>(psi, i0 + e, status);
-        __syncthreads();
-        // per-thread chunk [q0, q1): counts of above / tied / hash-kept tied states
-        const int q0 = min(tid * kPer, n), q1 = min(q0 + kPer, n);
+        const int q_lo = min(wid * kSeg, n), q_hi = min(q_lo + kSeg, n);
+        // pass 1: weights into shared memory, per-warp counts
         int ca = 0, ct = 0, ch = 0;
-        if (!all)
-            for (int q = q0; q < q1; ++q) {
-                ca += s_k[q] > vstar;
-                if (s_k[q] == vstar) {
-                    ++ct;
-                    if (shuf) ch += tie_hash(seed, step, i0 + q) >= hstar;
+        if (!all || out_w) {
+            for (int q0 = q_lo; q0 < q_hi; q0 += 32) {
+                const int q = q0 + lane;
+                const bool v = q < q_hi;
+                unsigned long long k = 0;
+                if (v) {
+                    k = weight_bits<WK>(psi, i0 + q, status);
+                    s_k[q] = k;
+                }
+                if (!all) {
+                    const bool tie = v && k == vstar;
+                    ca += __popc(__ballot_sync(0xffffffffu, v && k > vstar));
+                    ct += __popc(__ballot_sync(0xffffffffu, tie));
+                    if (shuf) ch += __popc(__ballot_sync(0xffffffffu, tie && tie_hash(seed, step, i0 + q) >= hstar));
                 }
             }
-        int ia = ca, it = ct, ih = ch;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int va = __shfl_up_sync(0xffffffffu, ia, o);
-            const int vt = __shfl_up_sync(0xffffffffu, it, o);
-            const int vh = __shfl_up_sync(0xffffffffu, ih, o);
-            if (lane >= o) {
-                ia += va;
-                it += vt;
-                ih += vh;
-            }
         }
-        if (lane == 31) {
-            s_w[wid][0] = ia;
-            s_w[wid][1] = it;
-            s_w[wid][2] = ih;
+        if (lane == 0) {
+            s_w[wid][0] = ca;
+            s_w[wid][1] = ct;
+            s_w[wid][2] = ch;
         }
         __syncthreads();
         long long A = 0, T = 0, H = 0;
@@ -375,44 +365,46 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
             A = ws.tile_pre[t * 3 + 0];
             T = ws.tile_pre[t * 3 + 1];
             H = ws.tile_pre[t * 3 + 2];
+            for (int w = 0; w < wid; ++w) {
+                A += s_w[w][0];
+                T += s_w[w][1];
+                H += s_w[w][2];
+            }
         }
-        for (int w = 0; w < wid; ++w) {
-            A += s_w[w][0];
-            T += s_w[w][1];
-            H += s_w[w][2];
-        }
-        A += ia - ca;
-        T += it - ct;
-        H += ih - ch;
-        for (int q = q0; q < q1; ++q) {
+        // pass 2: ranks among the kept states, block starts, copies
+        for (int q0 = q_lo; q0 < q_hi; q0 += 32) {
+            const int q = q0 + lane;
+            const bool v = q < q_hi;
             const int64_t i = i0 + q;
             bool keep;
             long long out;
             if (all) {
-                keep = true;
+                keep = v;
                 out = i;
             } else {
-                const unsigned long long k = s_k[q];
-                const long long kept_ties = shuf ? H : max(0ll, T - (ties - need));
-                out = A + kept_ties;
-                if (k > vstar) {
-                    keep = true;
-                    ++A;
-                } else if (k == vstar) {
-                    if (shuf) {
-                        keep = tie_hash(seed, step, i) >= hstar;
-                        H += keep;
-                    } else {
-                        keep = T >= ties - need;
-                    }
-                    ++T;
-                } else {
-                    keep = false;
-                }
+                const unsigned long long k = v ? s_k[q] : 0ull;
+                const bool above = v && k > vstar;
+                const bool tie = v && k == vstar;
+                const bool hk = shuf && tie && tie_hash(seed, step, i) >= hstar;
+                const unsigned ba = __ballot_sync(0xffffffffu, above);
+                const unsigned bt = __ballot_sync(0xffffffffu, tie);
+                const unsigned bh = __ballot_sync(0xffffffffu, hk);
+                const long long a_l = A + __popc(ba & lt_mask);
+                const long long t_l = T + __popc(bt & lt_mask);
+                const long long h_l = H + __popc(bh & lt_mask);
+                out = a_l + (shuf ? h_l : max(0ll, t_l - skip_ties));
+                keep = above || (tie && (shuf ? hk : t_l >= skip_ties));
+                A += __popc(ba);
+                T += __popc(bt);
+                H += __popc(bh);
             }
-            // block starts: number of kept states before the first state of the block
-            int p = block_of(s_blk, L, i);
-            if (s_blk[p] == i) out_blk[p] = int(out);
+            // block starts among these 32 states: the number of kept states before them
+            for (int p0 = 0; p0 < L; p0 += 32) {
+                const int p = p0 + lane;
+                const int e = p < L ? int(int64_t(s_blk[p]) - (i0 + q0)) : -1;
+                const long long o = __shfl_sync(0xffffffffu, out, (e >= 0 && e < 32) ? e : 0);
+                if (p < L && e >= 0 && e < 32 && q0 + e < q_hi && s_blk[p] < s_blk[p + 1]) out_blk[p] = int(o);
+            }
             if (keep) {
                 if (out < out_cap) {
                     const uint64_t* src = x_keys + i * NW;
@@ -455,13 +447,11 @@ int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_bl
                       uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w, int* n_tied_out,
                       int* status, int num_sms, cudaStream_t st) {
     const int g = num_sms * 4;
+    const int rounds = weight_rounds(WK);
     trunc_init_kernel<<<1, 1024, 0, st>>>(m, x_blk, maxstates, ws);
-    trunc_hist_all_kernel<WK><<<g, 256, 0, st>>>(psi, ws, status);
-    trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, 0, 1);
-    trunc_collect_kernel<WK><<<g, 256, 0, st>>>(psi, ws, status);
-    for (int r = 1; r < kRounds; ++r) {
-        trunc_hist_cand_kernel<<<g, 256, 0, st>>>(ws, SEL_W, r);
-        trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, r, 1);
+    for (int r = 0; r < rounds; ++r) {
+        trunc_hist_pass_kernel<WK><<<g, 256, 0, st>>>(psi, ws, r, status);
+        trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, r, r == rounds - 1);
     }
     if (shuffle) {
         trunc_shuffle_prep_kernel<<<1, 32, 0, st>>>(ws, status);

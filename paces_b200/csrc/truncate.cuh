@@ -35,6 +35,14 @@ constexpr int kTruncTile = 4096;
 
 inline int trunc_tiles_cap(int64_t cap) { return int(cap / kTruncTile + 2); }
 
+// Radix rounds (12-bit digits from the top) of the weight selection for a weight kind (0
+// complex128 |psi|, 1 complex64 |psi|, 2 precomputed fp64 weights): a complex64 weight is
+// an fp32 value widened to a double, so its bits 28..0 are zero and rounds 0-2 (bits
+// 63..28) decide it.
+inline int weight_rounds(int wk) { return wk == 1 ? 3 : 6; }
+// Kernels one truncation enqueues.
+inline int trunc_launches(int wk, bool shuffle) { return 5 + 2 * weight_rounds(wk) + (shuffle ? 14 : 0); }
+
 // weights (optional, one non-negative double per state): rank by these instead of |psi|
 // (the look-ahead weighting, lookahead.cu).
 // out_w (optional, out_cap + 1 floats): the ranked weight (|psi|) of every kept state in the
