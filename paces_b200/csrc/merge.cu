@@ -606,7 +606,11 @@ __global__ void merge_finalize_kernel(ModelDev m, MergeWs ws, MergeOut out, int*
     if (ceiling_out) *ceiling_out = ws.counters[3];
 }
 
-// H neighbour table from the per-source index maps (assemble only).
+// H neighbour table from the per-source index maps (assemble only).  Source i of the
+// enlarged basis landed at row q; its four images (when coupled) at s_k.  Row q is exactly
+// (s_left, s_right, s_down, s_up): one 16-byte store, q ascending with i.  Each image row
+// gets the reverse entry (a 4-byte store); where an image row is itself a source row, both
+// writers store the same value.
 __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __restrict__ x_blk,
                                                        MergeOut out) {
     __shared__ int s_blk[kMaxSites + 1];
@@ -619,36 +623,27 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
     int* nb = out.nbr;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
         const int p = block_of(s_blk, L, i);
-        const int q = map[0 * mc + i];
+        const int q = __ldcs(map + i);
         if (q < 0 || q >= nc) continue;
-        if (p + 1 < L || m.periodic) {
-            const int s = map[int64_t(RUN_FROM_LEFT) * mc + i];
-            if (s >= 0 && s < nc) {
-                nb[4 * int64_t(q) + NB_RIGHT] = s;
-                nb[4 * int64_t(s) + NB_LEFT] = q;
-            }
-        }
-        if (p > 0 || m.periodic) {
-            const int s = map[int64_t(RUN_FROM_RIGHT) * mc + i];
-            if (s >= 0 && s < nc) {
-                nb[4 * int64_t(q) + NB_LEFT] = s;
-                nb[4 * int64_t(s) + NB_RIGHT] = q;
-            }
-        }
-        {
-            const int s = map[int64_t(RUN_UP) * mc + i];
-            if (s >= 0 && s < nc) {
-                nb[4 * int64_t(q) + NB_UP] = s;
-                nb[4 * int64_t(s) + NB_DOWN] = q;
-            }
-        }
-        {
-            const int s = map[int64_t(RUN_DOWN) * mc + i];
-            if (s >= 0 && s < nc) {
-                nb[4 * int64_t(q) + NB_DOWN] = s;
-                nb[4 * int64_t(s) + NB_UP] = q;
-            }
-        }
+        auto ok = [&](int s) { return s >= 0 && s < nc; };
+        int sr = (p + 1 < L || m.periodic) ? __ldcs(map + int64_t(RUN_FROM_LEFT) * mc + i) : -1;
+        int sl = (p > 0 || m.periodic) ? __ldcs(map + int64_t(RUN_FROM_RIGHT) * mc + i) : -1;
+        int su = __ldcs(map + int64_t(RUN_UP) * mc + i);
+        int sd = __ldcs(map + int64_t(RUN_DOWN) * mc + i);
+        sr = ok(sr) ? sr : -1;
+        sl = ok(sl) ? sl : -1;
+        su = ok(su) ? su : -1;
+        sd = ok(sd) ? sd : -1;
+        int4 row;
+        row.x = sl;  // NB_LEFT
+        row.y = sr;  // NB_RIGHT
+        row.z = sd;  // NB_DOWN
+        row.w = su;  // NB_UP
+        reinterpret_cast<int4*>(nb)[q] = row;
+        if (sr >= 0) nb[4 * int64_t(sr) + NB_LEFT] = q;
+        if (sl >= 0) nb[4 * int64_t(sl) + NB_RIGHT] = q;
+        if (su >= 0) nb[4 * int64_t(su) + NB_DOWN] = q;
+        if (sd >= 0) nb[4 * int64_t(sd) + NB_UP] = q;
     }
 }
 

@@ -94,12 +94,31 @@ __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint6
         __syncthreads();
         const int b0 = d0 - a0, b1 = d1 - a1;
         const int nold = a1 - a0;
-        for (int x = b0 + threadIdx.x; x < b1; x += blockDim.x) {
+        // every thread resolves a run of consecutive new keys: the first by a binary search,
+        // the next ones by stepping forward from the previous bound (new keys ascend, and
+        // few old keys lie between two of them), falling back to a binary search of the rest
+        const int per = (b1 - b0 + int(blockDim.x) - 1) / int(blockDim.x);
+        const int x0 = min(b0 + int(threadIdx.x) * per, b1), x1 = min(x0 + per, b1);
+        int lo = 0;  // upper bound among s_old[h .. h+nold) of the previous key
+        for (int x = x0; x < x1; ++x) {
             const Key<NW> k = load_key<NW>(N, x);
-            int lo = 0, hi = nold;  // upper bound among s_old[h .. h+nold)
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (key_cmp(s_old[h + mid], k) <= 0) lo = mid + 1; else hi = mid;
+            int hi = nold;
+            if (x == x0) {
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (key_cmp(s_old[h + mid], k) <= 0) lo = mid + 1; else hi = mid;
+                }
+            } else {
+                int steps = 0;
+                while (lo < nold && steps < 8 && key_cmp(s_old[h + lo], k) <= 0) {
+                    ++lo;
+                    ++steps;
+                }
+                if (steps == 8)
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (key_cmp(s_old[h + mid], k) <= 0) lo = mid + 1; else hi = mid;
+                    }
             }
             const int aa = a0 + lo;  // old elements before k in merged order
             C v;
