@@ -67,8 +67,10 @@ __global__ void __launch_bounds__(256) remap_split_kernel(ModelDev m, const uint
     }
 }
 
+constexpr int kRThreads = 256;
+
 template <int NW, bool C64>
-__global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint64_t* __restrict__ old_keys,
+__global__ void __launch_bounds__(kRThreads) remap_tile_kernel(ModelDev m, const uint64_t* __restrict__ old_keys,
                                                          const int* __restrict__ ob,
                                                          const void* __restrict__ old_psi,
                                                          const uint64_t* __restrict__ new_keys,
@@ -76,6 +78,7 @@ __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint6
                                                          RemapWs ws) {
     using C = typename std::conditional<C64, float2, double2>::type;
     constexpr int kTile = remap_tile(NW);
+    constexpr int kPer = kTile / kRThreads;  // new keys per thread at most
     __shared__ Key<NW> s_old[kTile + 1];
     const int ntiles = ws.counters[0];
     const C* op = reinterpret_cast<const C*>(old_psi);
@@ -90,6 +93,7 @@ __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint6
         const int d0 = tl * kTile, d1 = min(d0 + kTile, no + nn);
         const int a0 = ws.split[2 * t], a1 = ws.split[2 * t + 1];
         const int h = a0 > 0 ? 1 : 0;  // halo: the old element before the tile
+#pragma unroll 4
         for (int e = threadIdx.x; e < a1 - a0 + h; e += blockDim.x) s_old[e] = load_key<NW>(O, a0 - h + e);
         __syncthreads();
         const int b0 = d0 - a0, b1 = d1 - a1;
@@ -97,13 +101,23 @@ __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint6
         // every thread resolves a run of consecutive new keys: the first by a binary search,
         // the next ones by stepping forward from the previous bound (new keys ascend, and
         // few old keys lie between two of them), falling back to a binary search of the rest
-        const int per = (b1 - b0 + int(blockDim.x) - 1) / int(blockDim.x);
+        const int per = (b1 - b0 + kRThreads - 1) / kRThreads;  // <= kPer
         const int x0 = min(b0 + int(threadIdx.x) * per, b1), x1 = min(x0 + per, b1);
+        // 1. the old index of every new key of the run (-1: not in the old basis); the next
+        //    key's load is issued before the current key is searched
+        int found[kPer];
         int lo = 0;  // upper bound among s_old[h .. h+nold) of the previous key
-        for (int x = x0; x < x1; ++x) {
-            const Key<NW> k = load_key<NW>(N, x);
+        Key<NW> kn;
+        if (x0 < x1) kn = load_key<NW>(N, x0);
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            found[u] = -1;
+            const int x = x0 + u;
+            if (x >= x1) continue;
+            const Key<NW> k = kn;
+            if (x + 1 < x1) kn = load_key<NW>(N, x + 1);
             int hi = nold;
-            if (x == x0) {
+            if (u == 0) {
                 while (lo < hi) {
                     const int mid = (lo + hi) >> 1;
                     if (key_cmp(s_old[h + mid], k) <= 0) lo = mid + 1; else hi = mid;
@@ -121,12 +135,19 @@ __global__ void __launch_bounds__(256) remap_tile_kernel(ModelDev m, const uint6
                     }
             }
             const int aa = a0 + lo;  // old elements before k in merged order
-            C v;
-            v.x = 0;
-            v.y = 0;
-            if (aa > 0 && key_eq(s_old[h + lo - 1], k)) v = op[int64_t(o0) + aa - 1];
-            np[int64_t(n0) + x] = v;
+            if (aa > 0 && key_eq(s_old[h + lo - 1], k)) found[u] = o0 + aa - 1;
         }
+        // 2. the amplitudes: all gathers of the run in flight together
+        C v[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            v[u].x = 0;
+            v[u].y = 0;
+            if (found[u] >= 0) v[u] = op[found[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u)
+            if (x0 + u < x1) np[int64_t(n0) + x0 + u] = v[u];
         __syncthreads();
     }
 }
@@ -137,7 +158,7 @@ int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const v
                    int num_sms, cudaStream_t st) {
     remap_plan_kernel<<<1, 32, 0, st>>>(m, ob, nb, ws, remap_tile(NW), status);
     remap_split_kernel<NW><<<num_sms * 2, 256, 0, st>>>(m, ok, ob, nk, nb, ws, remap_tile(NW));
-    remap_tile_kernel<NW, C64><<<num_sms * 4, 256, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi, ws);
+    remap_tile_kernel<NW, C64><<<num_sms * 4, kRThreads, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi, ws);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 

@@ -1,4 +1,6 @@
 // Amplitude-ranked truncation (see truncate.cuh).
+#include <type_traits>
+
 #include "truncate.cuh"
 
 namespace paces {
@@ -23,21 +25,29 @@ __host__ __device__ constexpr int round_bits(int r) { return r < 5 ? 12 : 4; }
 
 // The ranked weight of state i: WK 0 = |psi| of complex128 amplitudes, 1 = |psi| of
 // complex64 amplitudes, 2 = precomputed non-negative fp64 weights (the look-ahead
-// weighting).  Non-negative doubles order like their bit patterns.
+// weighting).  Non-negative doubles order like their bit patterns.  The load and the
+// conversion are separate so that loops can issue several loads before the first use.
 template <int WK>
-__device__ __forceinline__ unsigned long long weight_bits(const void* psi, int64_t i, int* status) {
+using RawW = typename std::conditional<WK == 0, double2, typename std::conditional<WK == 1, float2, double>::type>::type;
+
+template <int WK>
+__device__ __forceinline__ RawW<WK> load_raw(const void* psi, int64_t i) {
+    return __ldcs(reinterpret_cast<const RawW<WK>*>(psi) + i);
+}
+
+template <int WK>
+__device__ __forceinline__ unsigned long long raw_bits(const RawW<WK>& z, int* status) {
     double w;
-    if constexpr (WK == 1) {
-        const float2 z = reinterpret_cast<const float2*>(psi)[i];
-        w = double(hypotf(z.x, z.y));
-    } else if constexpr (WK == 0) {
-        const double2 z = reinterpret_cast<const double2*>(psi)[i];
-        w = hypot(z.x, z.y);
-    } else {
-        w = reinterpret_cast<const double*>(psi)[i];
-    }
+    if constexpr (WK == 1) w = double(hypotf(z.x, z.y));
+    else if constexpr (WK == 0) w = hypot(z.x, z.y);
+    else w = z;
     if (!(w <= 1.7976931348623157e308)) raise_status(status, PACES_ERR_NONFINITE);
     return (unsigned long long)__double_as_longlong(w);
+}
+
+template <int WK>
+__device__ __forceinline__ unsigned long long weight_bits(const void* psi, int64_t i, int* status) {
+    return raw_bits<WK>(load_raw<WK>(psi, i), status);
 }
 
 // splitmix64 finaliser applied to (index + stream offset): a bijection of the index, so
@@ -139,18 +149,29 @@ __global__ void __launch_bounds__(256) trunc_hist_pass_kernel(const void* __rest
     const unsigned long long pre = (unsigned long long)ws.sel[SEL_W + 0];
     const unsigned long long msk = (unsigned long long)ws.sel[SEL_W + 1];
     const int lane = threadIdx.x & 31;
-    for (int64_t i0 = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x - lane); i0 < S;
-         i0 += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t i = i0 + lane;
-        bool match = false;
-        unsigned bin = 0xffffffffu;
-        if (i < S) {
-            const unsigned long long k = weight_bits<WK>(psi, i, status);
-            match = (k & msk) == pre;
-            if (match) bin = unsigned((k >> shift) & dm);
+    // warp chunks of 4 x 32 states: the four loads of a lane are in flight together
+    constexpr int kU = 4;
+    const int64_t nwarps = int64_t(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t c = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); c * 32 * kU < S; c += nwarps) {
+        RawW<WK> z[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int64_t i = (c * kU + u) * 32 + lane;
+            if (i < S) z[u] = load_raw<WK>(psi, i);
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, bin);
-        if (match && lane == __ffs(peers) - 1) atomicAdd(&h[bin], unsigned(__popc(peers)));
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int64_t i = (c * kU + u) * 32 + lane;
+            bool match = false;
+            unsigned bin = 0xffffffffu;
+            if (i < S) {
+                const unsigned long long k = raw_bits<WK>(z[u], status);
+                match = (k & msk) == pre;
+                if (match) bin = unsigned((k >> shift) & dm);
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, bin);
+            if (match && lane == __ffs(peers) - 1) atomicAdd(&h[bin], unsigned(__popc(peers)));
+        }
     }
     __syncthreads();
     for (int b = threadIdx.x; b < (1 << bits); b += blockDim.x)
@@ -234,12 +255,22 @@ __global__ void __launch_bounds__(256) trunc_count_kernel(const void* __restrict
         __syncthreads();
         int a = 0, ti = 0, hk = 0;
         const int64_t i1 = min(S, int64_t(t + 1) * kTruncTile);
-        for (int64_t i = int64_t(t) * kTruncTile + threadIdx.x; i < i1; i += blockDim.x) {
-            const unsigned long long k = weight_bits<WK>(psi, i, status);
-            a += k > vstar;
-            if (k == vstar) {
-                ++ti;
-                if (shuf) hk += tie_hash(seed, step, i) >= hstar;
+        constexpr int kU = 4;  // loads in flight per thread
+        for (int64_t i0 = int64_t(t) * kTruncTile + threadIdx.x; i0 < i1; i0 += kU * int64_t(blockDim.x)) {
+            RawW<WK> z[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (i0 + u * int64_t(blockDim.x) < i1) z[u] = load_raw<WK>(psi, i0 + u * int64_t(blockDim.x));
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int64_t i = i0 + u * int64_t(blockDim.x);
+                if (i >= i1) break;
+                const unsigned long long k = raw_bits<WK>(z[u], status);
+                a += k > vstar;
+                if (k == vstar) {
+                    ++ti;
+                    if (shuf) hk += tie_hash(seed, step, i) >= hstar;
+                }
             }
         }
 #pragma unroll
@@ -338,21 +369,31 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
         // pass 1: weights into shared memory, per-warp counts
         int ca = 0, ct = 0, ch = 0;
         if (!all || out_w) {
-            for (int q0 = q_lo; q0 < q_hi; q0 += 32) {
-                const int q = q0 + lane;
-                const bool v = q < q_hi;
-                unsigned long long k = 0;
-                if (v) {
-                    k = weight_bits<WK>(psi, i0 + q, status);
-                    s_k[q] = k;
+            constexpr int kU = 4;  // loads in flight per lane
+            for (int q0 = q_lo; q0 < q_hi; q0 += 32 * kU) {
+                RawW<WK> z[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int q = q0 + 32 * u + lane;
+                    if (q < q_hi) z[u] = load_raw<WK>(psi, i0 + q);
                 }
-                if (!all) {
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int q = q0 + 32 * u + lane;
+                    if (q < q_hi) s_k[q] = raw_bits<WK>(z[u], status);
+                }
+            }
+            __syncwarp();
+            if (!all)
+                for (int q0 = q_lo; q0 < q_hi; q0 += 32) {
+                    const int q = q0 + lane;
+                    const bool v = q < q_hi;
+                    const unsigned long long k = v ? s_k[q] : 0ull;
                     const bool tie = v && k == vstar;
                     ca += __popc(__ballot_sync(0xffffffffu, v && k > vstar));
                     ct += __popc(__ballot_sync(0xffffffffu, tie));
                     if (shuf) ch += __popc(__ballot_sync(0xffffffffu, tie && tie_hash(seed, step, i0 + q) >= hstar));
                 }
-            }
         }
         if (lane == 0) {
             s_w[wid][0] = ca;
@@ -371,47 +412,56 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
                 H += s_w[w][2];
             }
         }
-        // pass 2: ranks among the kept states, block starts, copies
-        for (int q0 = q_lo; q0 < q_hi; q0 += 32) {
-            const int q = q0 + lane;
-            const bool v = q < q_hi;
-            const int64_t i = i0 + q;
-            bool keep;
-            long long out;
-            if (all) {
-                keep = v;
-                out = i;
-            } else {
-                const unsigned long long k = v ? s_k[q] : 0ull;
-                const bool above = v && k > vstar;
-                const bool tie = v && k == vstar;
-                const bool hk = shuf && tie && tie_hash(seed, step, i) >= hstar;
-                const unsigned ba = __ballot_sync(0xffffffffu, above);
-                const unsigned bt = __ballot_sync(0xffffffffu, tie);
-                const unsigned bh = __ballot_sync(0xffffffffu, hk);
-                const long long a_l = A + __popc(ba & lt_mask);
-                const long long t_l = T + __popc(bt & lt_mask);
-                const long long h_l = H + __popc(bh & lt_mask);
-                out = a_l + (shuf ? h_l : max(0ll, t_l - skip_ties));
-                keep = above || (tie && (shuf ? hk : t_l >= skip_ties));
-                A += __popc(ba);
-                T += __popc(bt);
-                H += __popc(bh);
-            }
-            // block starts among these 32 states: the number of kept states before them
-            for (int p0 = 0; p0 < L; p0 += 32) {
-                const int p = p0 + lane;
-                const int e = p < L ? int(int64_t(s_blk[p]) - (i0 + q0)) : -1;
-                const long long o = __shfl_sync(0xffffffffu, out, (e >= 0 && e < 32) ? e : 0);
-                if (p < L && e >= 0 && e < 32 && q0 + e < q_hi && s_blk[p] < s_blk[p + 1]) out_blk[p] = int(o);
-            }
-            if (keep) {
-                if (out < out_cap) {
-                    const uint64_t* src = x_keys + i * NW;
-                    uint64_t* dst = out_keys + out * NW;
+        // pass 2: ranks among the kept states, block starts, copies; four slices of 32 per
+        // round, their key loads in flight together
+        constexpr int kU = 4;
+        for (int qb = q_lo; qb < q_hi; qb += 32 * kU) {
+            bool keep[kU];
+            long long out[kU];
 #pragma unroll
-                    for (int w = 0; w < NW; ++w) dst[w] = src[w];
-                    if (out_w) out_w[out] = float(__longlong_as_double((long long)s_k[q]));
+            for (int u = 0; u < kU; ++u) {
+                const int q0 = qb + 32 * u;
+                const int q = q0 + lane;
+                const bool v = q < q_hi;
+                const int64_t i = i0 + q;
+                if (all) {
+                    keep[u] = v;
+                    out[u] = i;
+                } else {
+                    const unsigned long long k = v ? s_k[q] : 0ull;
+                    const bool above = v && k > vstar;
+                    const bool tie = v && k == vstar;
+                    const bool hk = shuf && tie && tie_hash(seed, step, i) >= hstar;
+                    const unsigned ba = __ballot_sync(0xffffffffu, above);
+                    const unsigned bt = __ballot_sync(0xffffffffu, tie);
+                    const unsigned bh = __ballot_sync(0xffffffffu, hk);
+                    const long long a_l = A + __popc(ba & lt_mask);
+                    const long long t_l = T + __popc(bt & lt_mask);
+                    const long long h_l = H + __popc(bh & lt_mask);
+                    out[u] = a_l + (shuf ? h_l : max(0ll, t_l - skip_ties));
+                    keep[u] = above || (tie && (shuf ? hk : t_l >= skip_ties));
+                    A += __popc(ba);
+                    T += __popc(bt);
+                    H += __popc(bh);
+                }
+                // block starts among these 32 states: the number of kept states before them
+                for (int p0 = 0; p0 < L; p0 += 32) {
+                    const int p = p0 + lane;
+                    const int e = p < L ? int(int64_t(s_blk[p]) - (i0 + q0)) : -1;
+                    const long long o = __shfl_sync(0xffffffffu, out[u], (e >= 0 && e < 32) ? e : 0);
+                    if (p < L && e >= 0 && e < 32 && q0 + e < q_hi && s_blk[p] < s_blk[p + 1]) out_blk[p] = int(o);
+                }
+            }
+            Key<NW> kk[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (keep[u] && out[u] < out_cap) kk[u] = load_key<NW>(x_keys, i0 + qb + 32 * u + lane);
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                if (!keep[u]) continue;
+                if (out[u] < out_cap) {
+                    store_key<NW>(out_keys, out[u], kk[u]);
+                    if (out_w) out_w[out[u]] = float(__longlong_as_double((long long)s_k[qb + 32 * u + lane]));
                 } else {
                     raise_status(status, PACES_ERR_CAPACITY);
                 }
