@@ -86,6 +86,7 @@ struct Layout {
     size_t v_V, v_TA, v_TB, v_partials, v_bar;
     size_t o_partials, o_out;
     size_t aw, keep;  // kept amplitudes of the truncation, proposal keep mask [kRuns][cap]
+    size_t maps_e, keysN, blkN, n2b;  // split expansion: its maps, the new part, new part -> output
 };
 
 Layout make_layout(const paces_ctx* c, int64_t cap) {
@@ -136,6 +137,10 @@ Layout make_layout(const paces_ctx* c, int64_t cap) {
     l.o_out = take(size_t(3 + 2 * L) * 8);
     l.aw = take((ucap + 1) * 4);
     l.keep = take(size_t(kRuns) * ucap);
+    l.maps_e = take(size_t(kRuns) * ucap * 4);
+    l.keysN = take(ucap * nw * 8);
+    l.blkN = take(size_t(L + 1) * 4);
+    l.n2b = take(ucap * 4);
     l.total = off;
     return l;
 }
@@ -331,21 +336,36 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
                            "step/proposal");
     }
     mark(1);
-    // 2. enlargement (enlarge_steps times; the first one filtered by the proposal)
+    // 2. enlargement (enlarge_steps times; the first one filtered by the proposal).  Without
+    //    the proposal the last enlargement B = P + images(P) is split: it also records where
+    //    P's images landed and which states of B are new (N = B \ P), so the assembly merges
+    //    B with the images of N only -- the images of P are in B already.
+    const bool split = prm->enlarge_steps > 0 && !propose;
     paces_basis* cur = &p.A;
     paces_basis* other = &p.B;
+    paces_basis nbasis{at<uint64_t>(ws, l.keysN), at<int32_t>(ws, l.blkN), l.cap};
     for (int e = 0; e < prm->enlarge_steps; ++e) {
         MergeWs mws = merge_ws(l, ws);
         if (propose && e == 0) {
             mws.keep = at<uint8_t>(ws, l.keep);
             mws.keep_cap = l.cap;
         }
+        const bool last_split = split && e == prm->enlarge_steps - 1;
         MergeOut mo{};
         mo.keys = other->keys;
         mo.blk = other->blk;
         mo.cap = other->cap;
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->merge_stride, c->m, cur->keys, cur->blk, mws, mo, nullptr, status,
-                                           c->num_sms, st),
+        if (last_split) {
+            mo.maps = at<int>(ws, l.maps_e);
+            mo.map_cap = l.cap;
+            mo.new_keys = nbasis.keys;
+            mo.new_blk = nbasis.blk;
+            mo.new_to_out = at<int>(ws, l.n2b);
+            mo.new_cap = nbasis.cap;
+        }
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, last_split ? MERGE_EXPAND_SPLIT : MERGE_EXPAND, c->merge_stride, c->m,
+                                           cur->keys, cur->blk, nullptr, nullptr, mws, mo,
+                                           last_split ? &rec->ceiling_hits : nullptr, 0, status, c->num_sms, st),
                            "step/expand");
         paces_basis* t = cur;
         cur = other;
@@ -363,9 +383,15 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.nbr_cap = p.h->cap;
         mo.maps = at<int>(ws, l.maps);
         mo.map_cap = l.cap;
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->merge_stride, c->m, cur->keys, cur->blk, merge_ws(l, ws), mo,
-                                           &rec->ceiling_hits, status, c->num_sms, st),
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, cur->keys, cur->blk,
+                                           split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(l, ws),
+                                           mo, &rec->ceiling_hits, split ? 1 : 0, status, c->num_sms, st),
                            "step/assemble");
+        if (split)
+            PACES_CHECK_LAUNCH(c, launch_nbr_fill_split(c->m, other->blk, nbasis.blk, at<int>(ws, l.maps_e),
+                                                        at<int>(ws, l.maps), at<int>(ws, l.n2b), l.cap, p.h->nbr,
+                                                        p.h->cap, c->num_sms, st),
+                               "step/neighbours");
     }
     mark(3);
     // 4. amplitudes into the new basis
@@ -651,7 +677,8 @@ int paces_expand(paces_ctx* c, const paces_basis* in, paces_basis* out, void* ws
     mo.keys = out->keys;
     mo.blk = out->blk;
     mo.cap = out->cap;
-    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, false, c->merge_stride, c->m, in->keys, in->blk, merge_ws(l, ws), mo, nullptr,
+    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_EXPAND, c->merge_stride, c->m, in->keys, in->blk, nullptr, nullptr,
+                                       merge_ws(l, ws), mo, nullptr, 0,
                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "expand");
     return PACES_OK;
@@ -672,7 +699,8 @@ int paces_assemble(paces_ctx* c, const paces_basis* in, paces_basis* out, paces_
     mo.maps = at<int>(ws, l.maps);
     mo.map_cap = l.cap;
     if (h->cap < out->cap) mo.cap = h->cap;
-    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, true, c->merge_stride, c->m, in->keys, in->blk, merge_ws(l, ws), mo, dev_ceiling_hits,
+    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, in->keys, in->blk, nullptr, nullptr,
+                                       merge_ws(l, ws), mo, dev_ceiling_hits, 0,
                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "assemble");
     return PACES_OK;

@@ -20,9 +20,10 @@ __device__ __forceinline__ int run_source(const ModelDev& m, int p, int j) {
 // Element `src` of X as it appears in run j of block p: key and order flag
 // (0 = floor hole, 1 = real, 2 = ceiling hole).
 template <int NW>
-__device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __restrict__ X, const MergeWs& ws,
-                                         int p, int j, int64_t src, Key<NW>& k, int& flag) {
-    k = load_key<NW>(X, src);
+__device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __restrict__ X,
+                                         const uint64_t* __restrict__ Y, const MergeWs& ws, int p, int j,
+                                         int64_t src, Key<NW>& k, int& flag) {
+    k = load_key<NW>(j == RUN_SELF ? X : Y, src);
     flag = 1;
     if (ws.keep && j != RUN_SELF && src < ws.keep_cap && !__ldg(ws.keep + j * ws.keep_cap + src)) flag = 2;
     if (j == RUN_UP || j == RUN_DOWN) {
@@ -65,14 +66,14 @@ __device__ __forceinline__ int cmp_kf(const Key<NW>& a, int fa, const Key<NW>& b
 // Elements of run (p, j) that precede (key, flag): strictly smaller, or not larger when
 // `upper` (the element's own run index is larger than j).
 template <int NW>
-__device__ int run_bound(const ModelDev& m, const uint64_t* __restrict__ X, const MergeWs& ws, int p, int j,
-                         int lo, int len, const Key<NW>& key, int flag, bool upper) {
+__device__ int run_bound(const ModelDev& m, const uint64_t* __restrict__ X, const uint64_t* __restrict__ Y,
+                         const MergeWs& ws, int p, int j, int lo, int len, const Key<NW>& key, int flag, bool upper) {
     int a = 0, b = len;
     while (a < b) {
         const int mid = (a + b) >> 1;
         Key<NW> k2;
         int f2;
-        run_elem<NW>(m, X, ws, p, j, lo + mid, k2, f2);
+        run_elem<NW>(m, X, Y, ws, p, j, lo + mid, k2, f2);
         const int c = cmp_kf(k2, f2, key, flag);
         if (upper ? (c <= 0) : (c < 0)) a = mid + 1; else b = mid;
     }
@@ -189,18 +190,19 @@ __device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t
     }
 }
 
-__global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, MergeWs ws, int stride,
-                                  int* status) {
+__global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, const int* __restrict__ y_blk,
+                                  MergeWs ws, int stride, int* status) {
     __shared__ int s_len[kMaxSites * kRuns];
     __shared__ int s_tiles;
     const int L = m.L;
     for (int idx = threadIdx.x; idx < L * kRuns; idx += blockDim.x) {
         const int p = idx / kRuns, j = idx % kRuns;
         const int src = run_source(m, p, j);
+        const int* sb = j == RUN_SELF ? x_blk : y_blk;
         int lo = 0, len = 0;
         if (src >= 0) {
-            lo = x_blk[src];
-            len = x_blk[src + 1] - lo;
+            lo = sb[src];
+            len = sb[src + 1] - lo;
         }
         ws.run_lo[idx] = lo;
         ws.run_len[idx] = len;
@@ -235,7 +237,7 @@ __global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, Mer
 
 template <int NW>
 __global__ void __launch_bounds__(256) merge_split_kernel(ModelDev m, const uint64_t* __restrict__ X,
-                                                          MergeWs ws, int stride) {
+                                                          const uint64_t* __restrict__ Y, MergeWs ws, int stride) {
     const int total = ws.counters[0];
     const int nr = m.L * kRuns;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
@@ -244,13 +246,13 @@ __global__ void __launch_bounds__(256) merge_split_kernel(ModelDev m, const uint
         const int i = (s - ws.split_off[r]) * stride;
         Key<NW> k;
         int f;
-        run_elem<NW>(m, X, ws, p, j, ws.run_lo[r] + i, k, f);
+        run_elem<NW>(m, X, Y, ws, p, j, ws.run_lo[r] + i, k, f);
         int rank = 0;
 #pragma unroll 1
         for (int jj = 0; jj < kRuns; ++jj) {
             int co;
             if (jj == j) co = i;
-            else co = run_bound<NW>(m, X, ws, p, jj, ws.run_lo[p * kRuns + jj], ws.run_len[p * kRuns + jj],
+            else co = run_bound<NW>(m, X, Y, ws, p, jj, ws.run_lo[p * kRuns + jj], ws.run_len[p * kRuns + jj],
                                     k, f, jj < j);
             ws.split_co[int64_t(s) * kRuns + jj] = co;
             rank += co;
@@ -287,7 +289,11 @@ __global__ void __launch_bounds__(256) merge_order_kernel(ModelDev m, MergeWs ws
 
 // Exclusive prefix of `count` over tiles taken in ticket order: decoupled look-back by one
 // warp, 32 predecessors per probe.  Called by all lanes of one warp; returns the prefix.
-__device__ int lookback_warp(unsigned long long* state, int t, int count, int* status) {
+// A count packs two 31-bit counters (output states | new-part states << 31), which add
+// without carrying into each other.
+constexpr int kPackShift = 31;
+constexpr long long kPackLow = (1ll << kPackShift) - 1;
+__device__ long long lookback_warp(unsigned long long* state, int t, long long count, int* status) {
     const int lane = threadIdx.x & 31;
     if (t == 0) {
         if (lane == 0) atomicExch(&state[0], kLbInc | (unsigned long long)count);
@@ -324,21 +330,26 @@ __device__ int lookback_warp(unsigned long long* state, int t, int count, int* s
         __threadfence();
         atomicExch(&state[t], kLbInc | (unsigned long long)(excl + count));
     }
-    return int(excl);
+    return excl;
 }
 
-template <int NW, bool ASM>
+template <int NW, int MODE>
 __global__ void __launch_bounds__(kTileThreads)
-merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tmax, MergeOut out,
-                  int* status) {
+merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __restrict__ Y, MergeWs ws,
+                  int tmax, MergeOut out, int* status) {
+    constexpr bool ASM = MODE == MERGE_ASSEMBLE;
+    constexpr bool SPLIT = MODE == MERGE_EXPAND_SPLIT;
+    constexpr bool MAPS = ASM || SPLIT;
     extern __shared__ __align__(16) unsigned char smem[];
     const SKeys<NW> s_key{reinterpret_cast<uint64_t*>(smem), tmax};
     uint8_t* s_flag = smem + size_t(tmax) * NW * 8;
     uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_flag + ((tmax + 15) & ~15));  // merged pos -> element
     uint16_t* s_rank = s_perm + tmax;                                                // element -> merged pos
     uint16_t* s_cnt = s_rank + tmax;  // inclusive count of first occurrences per merged pos
-
-    __shared__ int s_t, s_p, s_tl, s_n, s_base, s_total;
+    uint16_t* s_cntn = s_cnt + tmax;  // split: the same for first occurrences of the new part
+    __shared__ int s_t, s_p, s_tl, s_n;
+    __shared__ long long s_base, s_total;
+    __shared__ int s_warpn[kTileThreads / 32];
     __shared__ int s_start[kRuns], s_off[kRuns + 1], s_lo[kRuns];
     __shared__ Key<NW> s_pred;
     __shared__ int s_pred_flag, s_has_pred;
@@ -378,7 +389,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             if (st > 0) {
                 Key<NW> k;
                 int f;
-                run_elem<NW>(m, X, ws, p, j, int64_t(lo) + st - 1, k, f);
+                run_elem<NW>(m, X, Y, ws, p, j, int64_t(lo) + st - 1, k, f);
                 s_pk[j] = k;
                 s_pf[j] = f;
                 s_pv[j] = 1;
@@ -437,7 +448,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
             Key<NW> k;
             int f;
-            run_elem<NW>(m, X, ws, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
+            run_elem<NW>(m, X, Y, ws, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
             s_key.set(e, k);
             s_flag[e] = uint8_t(f);
             s_perm[e] = 0xffff;  // every rank must be claimed below
@@ -479,11 +490,14 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
         }
         __syncthreads();
 
-        // 3. first-occurrence flags over a contiguous chunk per thread, then a block scan
+        // 3. first-occurrence flags over a contiguous chunk per thread, then a block scan (split:
+        //    also of the first occurrences that start a group without a self-run element --
+        //    the self run sorts first among equal keys, so that is a group's first element)
         const int per = (n + kTileThreads - 1) / kTileThreads;
         const int q0 = min(tid * per, n);
         const int q1 = min(q0 + per, n);
-        int cnt = 0;
+        const int o1 = s_off[1];
+        int cnt = 0, cntn = 0;
         for (int q = q0; q < q1; ++q) {
             const int e = s_perm[q];
             int first = 0;
@@ -499,47 +513,70 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
             }
             s_cnt[q] = uint16_t(first);  // turned into an inclusive count below
             cnt += first;
+            if constexpr (SPLIT) {
+                const int fn = first && e >= o1;
+                s_cntn[q] = uint16_t(fn);
+                cntn += fn;
+            }
         }
-        // block exclusive scan of cnt
+        // block exclusive scan of cnt (and cntn)
         const int lane = tid & 31, wid = tid >> 5;
-        int incl = cnt;
+        int incl = cnt, incln = cntn;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
+            const int vn = __shfl_up_sync(0xffffffffu, incln, o);
+            if (lane >= o) {
+                incl += v;
+                incln += vn;
+            }
         }
-        if (lane == 31) s_warp[wid] = incl;
+        if (lane == 31) {
+            s_warp[wid] = incl;
+            s_warpn[wid] = incln;
+        }
         __syncthreads();
         if (tid == 0) {
-            int acc = 0;
+            int acc = 0, accn = 0;
             for (int w = 0; w < kTileThreads / 32; ++w) {
-                const int v = s_warp[w];
+                const int v = s_warp[w], vn = s_warpn[w];
                 s_warp[w] = acc;
+                s_warpn[w] = accn;
                 acc += v;
+                accn += vn;
             }
-            s_total = acc;
+            s_total = (long long)acc | ((long long)accn << kPackShift);
         }
         __syncthreads();
         if (wid == 0) {
-            const int b = lookback_warp(ws.tile_state, t, s_total, status);
+            const long long b = lookback_warp(ws.tile_state, t, s_total, status);
             if (lane == 0) {
                 s_base = b;
-                if (s_tl == 0) out.blk[p] = b;
+                if (s_tl == 0) {
+                    out.blk[p] = int(b & kPackLow);
+                    if constexpr (SPLIT) out.new_blk[p] = int(b >> kPackShift);
+                }
             }
         }
         __syncthreads();
-        const int base = s_base;
+        const int base = int(s_base & kPackLow);
+        const int basen = int(s_base >> kPackShift);
         {
             // inclusive count of firsts at every merged position (for strided writes)
             int run = s_warp[wid] + incl - cnt;
+            int runn = s_warpn[wid] + incln - cntn;
             for (int q = q0; q < q1; ++q) {
                 run += s_cnt[q];
                 s_cnt[q] = uint16_t(run);
+                if constexpr (SPLIT) {
+                    runn += s_cntn[q];
+                    s_cntn[q] = uint16_t(runn);
+                }
             }
         }
         __syncthreads();
 
-        // 4a. new keys (and H rows), consecutive threads -> consecutive outputs
+        // 4a. new keys (and H rows, or the new part), consecutive threads -> consecutive outputs
         for (int q = tid; q < n; q += kTileThreads) {
             if (s_cnt[q] == (q > 0 ? s_cnt[q - 1] : 0)) continue;  // not a first occurrence
             const int e = s_perm[q];
@@ -555,13 +592,24 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                         reinterpret_cast<int4*>(out.nbr)[u] = make_int4(-1, -1, -1, -1);
                     }
                 }
+                if constexpr (SPLIT) {
+                    if (s_cntn[q] != (q > 0 ? s_cntn[q - 1] : 0)) {
+                        const int64_t v = int64_t(basen) + s_cntn[q] - 1;
+                        if (v < out.new_cap) {
+                            store_key<NW>(out.new_keys, v, k);
+                            out.new_to_out[v] = int(u);
+                        } else {
+                            raise_status(status, PACES_ERR_CAPACITY);
+                        }
+                    }
+                }
             } else {
                 raise_status(status, PACES_ERR_CAPACITY);
             }
         }
         // 4b. index maps in run order: consecutive threads -> consecutive source indices
         int ceil_local = 0;
-        if constexpr (ASM) {
+        if constexpr (MAPS) {
             for (int e = tid; e < n; e += kTileThreads) {
                 int j = 0;
 #pragma unroll
@@ -573,8 +621,6 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
                 ceil_local += (f == 2);
                 if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = u;
             }
-        }
-        if constexpr (ASM) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) ceil_local += __shfl_xor_sync(0xffffffffu, ceil_local, o);
             if (lane == 0 && ceil_local) atomicAdd(&s_ceil, ceil_local);
@@ -585,14 +631,16 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, MergeWs ws, int tm
     }
 }
 
-// Output block offsets for blocks without tiles, the output count, capacity check.
-__global__ void merge_finalize_kernel(ModelDev m, MergeWs ws, MergeOut out, int* ceiling_out,
-                                      int* status) {
+// Output block offsets for blocks without tiles, the output count, capacity check (split:
+// the same for the new part).
+__global__ void merge_finalize_kernel(ModelDev m, MergeWs ws, MergeOut out, int* ceiling_out, int ceiling_add,
+                                      int split, int* status) {
     if (threadIdx.x != 0) return;
     const int L = m.L;
     const int ntiles = ws.counters[1];
-    long long total = 0;
-    if (ntiles > 0) total = (long long)(ws.tile_state[ntiles - 1] & kLbMask);
+    long long packed = 0;
+    if (ntiles > 0) packed = (long long)(ws.tile_state[ntiles - 1] & kLbMask);
+    long long total = packed & kPackLow, total_n = packed >> kPackShift;
     if (total > out.cap) {
         raise_status(status, PACES_ERR_CAPACITY);
         total = out.cap;
@@ -602,8 +650,19 @@ __global__ void merge_finalize_kernel(ModelDev m, MergeWs ws, MergeOut out, int*
         if (ntiles == 0 || ws.tile_off[p] == ws.tile_off[p + 1]) out.blk[p] = out.blk[p + 1];
         if (out.blk[p] > total) out.blk[p] = int(total);
     }
+    if (split) {
+        if (total_n > out.new_cap) {
+            raise_status(status, PACES_ERR_CAPACITY);
+            total_n = out.new_cap;
+        }
+        out.new_blk[L] = int(total_n);
+        for (int p = L - 1; p >= 0; --p) {
+            if (ntiles == 0 || ws.tile_off[p] == ws.tile_off[p + 1]) out.new_blk[p] = out.new_blk[p + 1];
+            if (out.new_blk[p] > total_n) out.new_blk[p] = int(total_n);
+        }
+    }
     ws.counters[4] = int(total);
-    if (ceiling_out) *ceiling_out = ws.counters[3];
+    if (ceiling_out) *ceiling_out = (ceiling_add ? *ceiling_out : 0) + ws.counters[3];
 }
 
 // H neighbour table from the per-source index maps (assemble only).  Source i of the
@@ -648,47 +707,121 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
 }
 
 template <int NW>
-size_t tile_smem_bytes(int tmax) {
-    // keys, order flags, then three uint16 arrays (merged order, rank, running count)
-    return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) + size_t(tmax) * 6;
+size_t tile_smem_bytes(int tmax, int mode) {
+    // keys, order flags, then three uint16 arrays (merged order, rank, running count), a
+    // fourth for the new part's running count of a split expansion
+    return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) +
+           size_t(tmax) * (mode == MERGE_EXPAND_SPLIT ? 8 : 6);
+}
+
+template <int NW, int MODE>
+void launch_tile(int tmax, const ModelDev& m, const uint64_t* X, const uint64_t* Y, const MergeWs& ws,
+                 const MergeOut& out, int* status, int num_sms, cudaStream_t st) {
+    const size_t smem = tile_smem_bytes<NW>(tmax, MODE);
+    auto kfn = merge_tile_kernel<NW, MODE>;
+    cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTileThreads, smem);
+    kfn<<<num_sms * max(per_sm, 1), kTileThreads, smem, st>>>(m, X, Y, ws, tmax, out, status);
 }
 
 template <int NW>
-int launch_merge_t(bool assemble, int stride, const ModelDev& m, const uint64_t* X, const int* x_blk,
-                   const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status, int num_sms,
-                   cudaStream_t st) {
+int launch_merge_t(int mode, int stride, const ModelDev& m, const uint64_t* X, const int* x_blk, const uint64_t* Y,
+                   const int* y_blk, const MergeWs& ws, const MergeOut& out, int* ceiling_out, int ceiling_add,
+                   int* status, int num_sms, cudaStream_t st) {
     if (stride < kMinMergeStride || stride > merge_stride(NW) || stride % 16) return PACES_ERR_BADARG;
-    const int tmax = merge_tmax(stride);
-    merge_plan_kernel<<<1, 1024, 0, st>>>(m, x_blk, ws, stride, status);
-    const int g = num_sms * 8;
-    merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, ws, stride);
-    merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
-    const size_t smem = tile_smem_bytes<NW>(tmax);
-    if (assemble) {
-        auto kfn = merge_tile_kernel<NW, true>;
-        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTileThreads, smem);
-        kfn<<<num_sms * max(per_sm, 1), kTileThreads, smem, st>>>(m, X, ws, tmax, out, status);
-    } else {
-        auto kfn = merge_tile_kernel<NW, false>;
-        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTileThreads, smem);
-        kfn<<<num_sms * max(per_sm, 1), kTileThreads, smem, st>>>(m, X, ws, tmax, out, status);
+    if (mode < MERGE_EXPAND || mode > MERGE_EXPAND_SPLIT) return PACES_ERR_BADARG;
+    if (mode == MERGE_EXPAND_SPLIT && (!out.maps || !out.new_keys || !out.new_blk || !out.new_to_out))
+        return PACES_ERR_BADARG;
+    const bool split_input = Y != nullptr && Y != X;
+    if (!Y) {
+        Y = X;
+        y_blk = x_blk;
     }
-    merge_finalize_kernel<<<1, 32, 0, st>>>(m, ws, out, ceiling_out, status);
-    if (assemble) nbr_fill_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, out);
+    const int tmax = merge_tmax(stride);
+    merge_plan_kernel<<<1, 1024, 0, st>>>(m, x_blk, y_blk, ws, stride, status);
+    const int g = num_sms * 8;
+    merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, ws, stride);
+    merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
+    if (mode == MERGE_ASSEMBLE) launch_tile<NW, MERGE_ASSEMBLE>(tmax, m, X, Y, ws, out, status, num_sms, st);
+    else if (mode == MERGE_EXPAND_SPLIT) launch_tile<NW, MERGE_EXPAND_SPLIT>(tmax, m, X, Y, ws, out, status, num_sms, st);
+    else launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, out, status, num_sms, st);
+    merge_finalize_kernel<<<1, 32, 0, st>>>(m, ws, out, ceiling_out, ceiling_add, mode == MERGE_EXPAND_SPLIT ? 1 : 0,
+                                            status);
+    if (mode == MERGE_ASSEMBLE && !split_input) nbr_fill_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, out);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
+}
+
+// Neighbour table after a split expansion: sources are the expansion's input P (images
+// through the expansion's maps into its output B, then through the assembly's self map into
+// S) and the new part N (images through the assembly's maps).  Same row and reverse stores
+// as nbr_fill_kernel.
+__global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const int* __restrict__ p_blk,
+                                                             const int* __restrict__ n_blk,
+                                                             const int* __restrict__ maps_e,
+                                                             const int* __restrict__ maps_s,
+                                                             const int* __restrict__ new_to_out, int64_t mc,
+                                                             int* __restrict__ nb, int64_t nc) {
+    __shared__ int s_pb[kMaxSites + 1], s_nb[kMaxSites + 1];
+    const int L = m.L;
+    for (int i = threadIdx.x; i <= L; i += blockDim.x) {
+        s_pb[i] = p_blk[i];
+        s_nb[i] = n_blk[i];
+    }
+    __syncthreads();
+    const int np_ = s_pb[L], nn = s_nb[L];
+    for (int64_t x = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; x < int64_t(np_) + nn;
+         x += int64_t(gridDim.x) * blockDim.x) {
+        const bool from_p = x < np_;
+        const int i = int(from_p ? x : x - np_);
+        const int p = from_p ? block_of(s_pb, L, i) : block_of(s_nb, L, i);
+        // the S index of a map entry of run j for this source (-1: no coupling)
+        auto img = [&](int j) -> int {
+            if (from_p) {
+                const int b = __ldcs(maps_e + int64_t(j) * mc + i);
+                return (b >= 0 && b < mc) ? __ldg(maps_s + b) : -1;
+            }
+            return __ldcs(maps_s + int64_t(j) * mc + i);
+        };
+        int q;
+        if (from_p) {
+            q = img(RUN_SELF);
+        } else {
+            const int b = __ldcs(new_to_out + i);
+            q = (b >= 0 && b < mc) ? __ldg(maps_s + b) : -1;
+        }
+        if (q < 0 || q >= nc) continue;
+        auto ok = [&](int s) { return s >= 0 && s < nc; };
+        int sr = (p + 1 < L || m.periodic) ? img(RUN_FROM_LEFT) : -1;
+        int sl = (p > 0 || m.periodic) ? img(RUN_FROM_RIGHT) : -1;
+        int su = img(RUN_UP);
+        int sd = img(RUN_DOWN);
+        sr = ok(sr) ? sr : -1;
+        sl = ok(sl) ? sl : -1;
+        su = ok(su) ? su : -1;
+        sd = ok(sd) ? sd : -1;
+        int4 row;
+        row.x = sl;  // NB_LEFT
+        row.y = sr;  // NB_RIGHT
+        row.z = sd;  // NB_DOWN
+        row.w = su;  // NB_UP
+        reinterpret_cast<int4*>(nb)[q] = row;
+        if (sr >= 0) nb[4 * int64_t(sr) + NB_LEFT] = q;
+        if (sl >= 0) nb[4 * int64_t(sl) + NB_RIGHT] = q;
+        if (su >= 0) nb[4 * int64_t(su) + NB_DOWN] = q;
+        if (sd >= 0) nb[4 * int64_t(sd) + NB_UP] = q;
+    }
 }
 
 }  // namespace
 
-int launch_merge(int nw, bool assemble, int stride, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                 const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status, int num_sms,
-                 cudaStream_t st) {
-#define PACES_MERGE_CASE(W) \
-    case W: return launch_merge_t<W>(assemble, stride, m, x_keys, x_blk, ws, out, ceiling_out, status, num_sms, st);
+int launch_merge(int nw, int mode, int stride, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+                 const uint64_t* y_keys, const int* y_blk, const MergeWs& ws, const MergeOut& out,
+                 int* ceiling_out, int ceiling_add, int* status, int num_sms, cudaStream_t st) {
+#define PACES_MERGE_CASE(W)                                                                                    \
+    case W:                                                                                                    \
+        return launch_merge_t<W>(mode, stride, m, x_keys, x_blk, y_keys, y_blk, ws, out, ceiling_out, ceiling_add, \
+                                 status, num_sms, st);
     switch (nw) {
         PACES_MERGE_CASE(1)
         PACES_MERGE_CASE(2)
@@ -701,6 +834,14 @@ int launch_merge(int nw, bool assemble, int stride, const ModelDev& m, const uin
         default: return PACES_ERR_BADARG;
     }
 #undef PACES_MERGE_CASE
+}
+
+int launch_nbr_fill_split(const ModelDev& m, const int* p_blk, const int* n_blk, const int* maps_e,
+                          const int* maps_s, const int* new_to_out, int64_t map_cap, int* nbr, int64_t nbr_cap,
+                          int num_sms, cudaStream_t st) {
+    nbr_fill_split_kernel<<<num_sms * 8, 256, 0, st>>>(m, p_blk, n_blk, maps_e, maps_s, new_to_out, map_cap, nbr,
+                                                       nbr_cap);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
 }  // namespace paces

@@ -59,9 +59,24 @@ struct MergeOut {
     uint32_t* meta;
     int* nbr;        // [4][nbr_cap]
     int64_t nbr_cap;
-    int* maps;       // [kRuns][map_cap], indexed by source index in X
+    // assemble and split expansion: output index of every run element, -1 for holes;
+    // [kRuns][map_cap], indexed by the element's source index (in X for the self run, in Y
+    // for the image runs)
+    int* maps;
     int64_t map_cap;
+    // split expansion only: the "new part" -- output states whose group holds no element
+    // of the self run -- as a sorted, blocked basis, and each one's output index
+    uint64_t* new_keys;
+    int* new_blk;
+    int* new_to_out;
+    int64_t new_cap;
 };
+
+// Merge modes.  EXPAND: keys only.  ASSEMBLE: keys, the H rows' metadata and neighbour
+// table (through the maps).  EXPAND_SPLIT: an expansion that also writes the maps and the
+// new part, so that the following assembly needs the images of the new part only
+// (the images of the rest are already in this expansion's output).
+enum MergeMode : int { MERGE_EXPAND = 0, MERGE_ASSEMBLE = 1, MERGE_EXPAND_SPLIT = 2 };
 
 // Tiling constants by key width.  merge_stride(nw) is the default and largest stride (the
 // tile's shared memory stays below ~100 KB); any multiple of 16 down to kMinMergeStride
@@ -81,8 +96,18 @@ inline int64_t merge_split_cap(int64_t in_cap, int nw, int L) {
 }
 inline int64_t merge_tile_cap(int64_t split_cap, int L) { return split_cap / kMergeGroup + L + 8; }
 
-int launch_merge(int nw, bool assemble, int stride, const ModelDev& m, const uint64_t* x_keys,
-                 const int* x_blk, const MergeWs& ws, const MergeOut& out, int* ceiling_out, int* status,
-                 int num_sms, cudaStream_t st);
+// X feeds the self run, Y (null: X) the four image runs.  ceiling_out (optional) receives the
+// number of ceiling holes of the up run, or has it added (ceiling_add).  An assembly with
+// Y != X leaves the neighbour table to launch_nbr_fill_split.
+int launch_merge(int nw, int mode, int stride, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
+                 const uint64_t* y_keys, const int* y_blk, const MergeWs& ws, const MergeOut& out,
+                 int* ceiling_out, int ceiling_add, int* status, int num_sms, cudaStream_t st);
+
+// Neighbour table after a split expansion (maps_e, new part N with new_to_out) and the
+// assembly of its output with the images of N (maps_s): every state of the expansion's
+// input P and of N is a source.  p_blk / n_blk: block offsets of P and N.
+int launch_nbr_fill_split(const ModelDev& m, const int* p_blk, const int* n_blk, const int* maps_e,
+                          const int* maps_s, const int* new_to_out, int64_t map_cap, int* nbr, int64_t nbr_cap,
+                          int num_sms, cudaStream_t st);
 
 }  // namespace paces
