@@ -344,9 +344,10 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     const SKeys<NW> s_key{reinterpret_cast<uint64_t*>(smem), tmax};
     uint8_t* s_flag = smem + size_t(tmax) * NW * 8;
     uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_flag + ((tmax + 15) & ~15));  // merged pos -> element
-    uint16_t* s_rank = s_perm + tmax;                                                // element -> merged pos
-    uint16_t* s_cnt = s_rank + tmax;  // inclusive count of first occurrences per merged pos
-    uint16_t* s_cntn = s_cnt + tmax;  // split: the same for first occurrences of the new part
+    uint16_t* s_lv1 = s_perm + tmax;  // first merge level; then (split) s_cntn
+    uint16_t* s_cnt = s_lv1 + tmax;   // second merge level; then the inclusive count of first
+                                      // occurrences per merged pos
+    uint16_t* s_cntn = s_lv1;         // split: the same for first occurrences of the new part
     __shared__ int s_t, s_p, s_tl, s_n;
     __shared__ long long s_base, s_total;
     __shared__ int s_warpn[kTileThreads / 32];
@@ -457,9 +458,9 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
 
         // 2. merged order: pairwise merge tree (runs 0+1, 2+3) -> (0123) -> (01234) in shared
         //    memory; every thread merges a contiguous output range after a merge-path split.
-        //    The level buffers alias s_rank / s_cnt, which are filled only afterwards.
+        //    The level buffers alias s_cntn / s_cnt, which are filled only afterwards.
         {
-            uint16_t* lv1 = s_rank;
+            uint16_t* lv1 = s_lv1;
             uint16_t* lv2 = s_cnt;
             const int o1 = s_off[1], o2 = s_off[2], o3 = s_off[3], o4 = s_off[4];
             const int n01 = o2, n0123 = o4;
@@ -481,12 +482,6 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
             d0 = min(tid * per, n);
             d1 = min(d0 + per, n);
             if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv2, n0123), ident(o4, n - o4), d0, d1, s_perm);
-            __syncthreads();
-            for (int q = tid; q < n; q += kTileThreads) {
-                const int e = s_perm[q];
-                if (e < n) s_rank[e] = uint16_t(q);
-                else raise_status(status, PACES_ERR_BADARG);
-            }
         }
         __syncthreads();
 
@@ -607,17 +602,20 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
                 raise_status(status, PACES_ERR_CAPACITY);
             }
         }
-        // 4b. index maps in run order: consecutive threads -> consecutive source indices
+        // 4b. index maps in merged order: an element's output is its group's, the running
+        //    count at its merged position (five interleaved streams of ascending sources)
         int ceil_local = 0;
         if constexpr (MAPS) {
-            for (int e = tid; e < n; e += kTileThreads) {
+            for (int q = tid; q < n; q += kTileThreads) {
+                const int e = s_perm[q];
+                if (e >= n) continue;  // flagged in 3
                 int j = 0;
 #pragma unroll
                 for (int qq = 1; qq < kRuns; ++qq) j += (e >= s_off[qq]);
                 const int64_t src = int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]);
                 const int f = s_flag[e];
                 int u = -1;
-                if (f == 1) u = base + s_cnt[s_rank[e]] - 1;
+                if (f == 1) u = base + s_cnt[q] - 1;
                 ceil_local += (f == 2);
                 if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = u;
             }
@@ -708,10 +706,10 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
 
 template <int NW>
 size_t tile_smem_bytes(int tmax, int mode) {
-    // keys, order flags, then three uint16 arrays (merged order, rank, running count), a
-    // fourth for the new part's running count of a split expansion
-    return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) +
-           size_t(tmax) * (mode == MERGE_EXPAND_SPLIT ? 8 : 6);
+    // keys, order flags, then three uint16 arrays (merged order and two merge levels, which
+    // become the running counts)
+    (void)mode;
+    return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) + size_t(tmax) * 6;
 }
 
 template <int NW, int MODE>
@@ -770,8 +768,8 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
     }
     __syncthreads();
     const int np_ = s_pb[L], nn = s_nb[L];
-    for (int64_t x = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; x < int64_t(np_) + nn;
-         x += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t total = int64_t(np_) + nn;
+    auto fill = [&](int64_t x) {
         const bool from_p = x < np_;
         const int i = int(from_p ? x : x - np_);
         const int p = from_p ? block_of(s_pb, L, i) : block_of(s_nb, L, i);
@@ -790,12 +788,12 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
             const int b = __ldcs(new_to_out + i);
             q = (b >= 0 && b < mc) ? __ldg(maps_s + b) : -1;
         }
-        if (q < 0 || q >= nc) continue;
         auto ok = [&](int s) { return s >= 0 && s < nc; };
         int sr = (p + 1 < L || m.periodic) ? img(RUN_FROM_LEFT) : -1;
         int sl = (p > 0 || m.periodic) ? img(RUN_FROM_RIGHT) : -1;
         int su = img(RUN_UP);
         int sd = img(RUN_DOWN);
+        if (q < 0 || q >= nc) return;
         sr = ok(sr) ? sr : -1;
         sl = ok(sl) ? sl : -1;
         su = ok(su) ? su : -1;
@@ -810,7 +808,15 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
         if (sl >= 0) nb[4 * int64_t(sl) + NB_RIGHT] = q;
         if (su >= 0) nb[4 * int64_t(su) + NB_DOWN] = q;
         if (sd >= 0) nb[4 * int64_t(sd) + NB_UP] = q;
+    };
+    // two sources a grid stride apart per iteration: their map reads are in flight together
+    const int64_t gs = int64_t(gridDim.x) * blockDim.x;
+    int64_t x = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    for (; x + gs < total; x += 2 * gs) {
+        fill(x);
+        fill(x + gs);
     }
+    if (x < total) fill(x);
 }
 
 }  // namespace
