@@ -53,6 +53,8 @@ class Model:
     delta_eps: float = 0.0
     periodic: bool = False
     site_eps: np.ndarray | None = None
+    geo_dim: int = 1             # holstein.py:24, :48-51 (lattice_l ** geo_dim == nchain)
+    J2: float | None = None      # the "hopping2" term (next-nearest neighbours), holstein.py:234-240
 
     def __post_init__(self):
         self.max_ho_dims = [int(x) for x in self.max_ho_dims]
@@ -60,6 +62,13 @@ class Model:
             raise ValueError("nchain should match the number of QHOs.")
         if self.periodic and self.nchain < 3:
             raise ValueError("periodic hopping needs at least 3 sites")
+        self.lattice_l = int(np.round(self.nchain ** (1 / self.geo_dim)))
+        if self.lattice_l ** self.geo_dim != self.nchain:
+            raise ValueError(f"Number of sites {self.nchain} is incompatible with dimension {self.geo_dim}.")
+        if self.periodic and (self.geo_dim != 1 or self.J2 is not None):
+            raise NotImplementedError("Periodic hopping not yet implemented.")  # holstein.py:183-184
+        if self.J2 is not None and self.lattice_l - 1 < 2:
+            raise ValueError("Invalid value for base_order of hopping operator.")  # holstein.py:177-178
         max_dims = np.array([self.nchain] + self.max_ho_dims, dtype=np.float64)
         # hamiltonian.py:155 bitwidths = ceil(log2(max_dims))
         self.bitwidths = np.ceil(np.log2(max_dims)).astype(np.int64)
@@ -238,12 +247,24 @@ def lookup_with_mask(phonebook, findme):
 # --------------------------------------------------------------------------------------------
 
 
-def hopping_images(model: Model, basis):
-    """Right/left hop images and their masks.  paces/models/holstein.py:151-207 (order 1, 1D).
+def hop_channels(model: Model):
+    """The hopping channels in the reference's order: (term, J, base_order, cur_dim) for the
+    "hopping" term (order 1) and then the "hopping2" term (order 2), each over the lattice
+    dimensions (holstein.py:210-240, _hopping_dim_wrapper)."""
+    out = [("hopping", float(model.J), 1, d) for d in range(model.geo_dim)]
+    if model.J2 is not None:
+        out += [("hopping2", float(model.J2), 2, d) for d in range(model.geo_dim)]
+    return out
 
-    Returns (plus_inds, plus_mask, minus_inds_all, minus_mask): plus_inds are
-    the images of basis[plus_mask]; minus_inds_all[i] is the image of basis[i]
-    (only meaningful where minus_mask).
+
+def channel_images(model: Model, basis, base_order=1, cur_dim=0):
+    """Plus / minus hop images of one channel and their masks.  paces/models/holstein.py:151-207:
+    the exciton moves by base_order * l**cur_dim; with open boundaries it stays inside its
+    row of the l**(cur_dim+1) block.
+
+    Returns (plus_inds, plus_mask, minus_inds_all, minus_mask): plus_inds are the images of
+    basis[plus_mask]; minus_inds_all[i] is the image of basis[i] (only meaningful where
+    minus_mask).
     """
     L = model.nchain
     pos = get_pos(model, basis)
@@ -255,13 +276,24 @@ def hopping_images(model: Model, basis):
         set_field(model, plus, (pos + 1) % L, 0)
         set_field(model, minus, (pos - 1) % L, 0)
         return plus, plus_mask, minus, minus_mask
-    plus_mask = pos < (L - 1)
+    block = model.lattice_l ** (cur_dim + 1)
+    order = base_order * model.lattice_l ** cur_dim
+    excpos_mod = pos % block
+    plus_mask = excpos_mod < (block - order)
     plus = basis[plus_mask].copy()
-    add_field(model, plus, 1, 0)
+    add_field(model, plus, order, 0)
     minus = basis.copy()
-    add_field(model, minus, -1, 0)
-    minus_mask = pos > 0
-    return plus, plus_mask, minus, minus_mask
+    ok = excpos_mod > order - 1
+    sub = minus[ok]
+    add_field(model, sub, -order, 0)
+    minus[ok] = sub
+    return plus, plus_mask, minus, ok
+
+
+def hopping_images(model: Model, basis):
+    """Nearest-neighbour hop images along the first lattice dimension (the chain's only
+    channel); see channel_images."""
+    return channel_images(model, basis, 1, 0)
 
 
 def vib_images(model: Model, basis):
@@ -285,9 +317,12 @@ def vib_images(model: Model, basis):
 
 def enlarge(model: Model, basis):
     """basis U all raw images, unique.  paces/core/hamiltonian.py:550-577."""
-    hp, _, hm, hmm = hopping_images(model, basis)
+    parts = [basis]
+    for _, _, order, dim in hop_channels(model):
+        hp, _, hm, hmm = channel_images(model, basis, order, dim)
+        parts += [hp, hm[hmm]]
     vp, _, vm, vmm, _ = vib_images(model, basis)
-    allk = np.concatenate([basis, hp, hm[hmm], vp, vm[vmm]])
+    allk = np.concatenate(parts + [vp, vm[vmm]])
     return unique_rows(allk)
 
 
@@ -326,28 +361,37 @@ def generate_mel(model: Model, select, enlarge_steps):
     for _ in range(enlarge_steps):
         basis = enlarge(model, basis)
     n = basis.shape[0]
-    hp, hpm, hm_all, hmm = hopping_images(model, basis)
-    hmm = hmm & o_star_mask(basis, hp)
-    hm = hm_all[hmm]
+    hop = {}  # term -> [(plus, plus_mask, minus, minus_mask)] per channel, o-star applied
+    for term, _, order, dim in hop_channels(model):
+        hp, hpm, hm_all, hmm = channel_images(model, basis, order, dim)
+        hmm = hmm & o_star_mask(basis, hp)
+        hop.setdefault(term, []).append((hp, hpm, hm_all[hmm], hmm))
     vp, vpm, vm_all, vmm, occ = vib_images(model, basis)
     ceiling_hits = int(n - vpm.sum())
     vmm = vmm & o_star_mask(basis, vp)
     vm = vm_all[vmm]
-    new_inds = unique_rows(np.concatenate([basis, hp, hm, vp, vm]))
+    parts = [basis]
+    for chans in hop.values():
+        for hp, _, hm, _ in chans:
+            parts += [hp, hm]
+    new_inds = unique_rows(np.concatenate(parts + [vp, vm]))
     S = new_inds.shape[0]
     if S >= 2 ** 31:
         raise ValueError("The number of states is too large for signed 32-bit-integer indices.")
     diag = diag_values(model, new_inds)
     blook = searchsorted(new_inds, basis)
     g = float(model.g)
-    J = float(model.J)
-    triples = {
-        "hopping": [(hp, np.full(hp.shape[0], J), hpm), (hm, np.full(hm.shape[0], J), hmm)],
-        "vib_coupling": [
-            (vp, np.sqrt(occ[vpm] + 1, dtype=np.float64) * g, vpm),
-            (vm, np.sqrt(occ[vmm], dtype=np.float64) * g, vmm),
-        ],
-    }
+    Jt = {term: J for term, J, _, _ in hop_channels(model)}
+    triples = {}
+    for term, chans in hop.items():
+        lst = []
+        for hp, hpm, hm, hmm in chans:
+            lst += [(hp, np.full(hp.shape[0], Jt[term]), hpm), (hm, np.full(hm.shape[0], Jt[term]), hmm)]
+        triples[term] = lst
+    triples["vib_coupling"] = [
+        (vp, np.sqrt(occ[vpm] + 1, dtype=np.float64) * g, vpm),
+        (vm, np.sqrt(occ[vmm], dtype=np.float64) * g, vmm),
+    ]
     mats = {}
     for term, lst in triples.items():
         rows, cols, vals = [], [], []

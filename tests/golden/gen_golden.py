@@ -19,6 +19,7 @@ Fixtures written:
   obs_extra_n7c8.npz  hopping, mu_to_0, coupling and reduced density matrices
   scaled_n8c16.npz    a trajectory propagated with ExpmParams(use_scaling=True)
   tau_<weighting>_n8c16.npz  trajectories truncated by the look-ahead weights (tau=0.2)
+  lattice_<name>.npz  geo_dim > 1 lattices and the hopping2 term (open boundaries)
 """
 
 import argparse
@@ -359,6 +360,51 @@ def gen_traj_tau(paces, name, weighting, workdir):
                         config=np.array([nchain, dim, g, ms, 1, 30, 2, tau], dtype=np.float64))
 
 
+LATTICE_RUNS = {
+    # name: (nchain, geo_dim, max_ho_dim, g, J2 or None, delta_eps, maxstates, steps, initpos)
+    # delta_eps != 0 tilts the site energies, which breaks the lattice's mirror symmetries
+    # (mirror-image states would tie exactly at the truncation cut)
+    "geo2_n9c8": (9, 2, 8, 1.0, None, 0.13, 1500, 20, 1),
+    "hop2_n8c8": (8, 1, 8, 1.2, 0.4, 0.13, 1500, 20, 2),
+    "geo2hop2_n16c4": (16, 2, 4, 1.0, 0.3, 0.11, 2000, 15, 5),
+    "geo3_n27c4": (27, 3, 4, 1.0, None, 0.07, 2000, 12, 4),
+}
+
+
+def gen_lattice(paces, name, cfg, workdir):
+    """Lattices beyond the nearest-neighbour chain: geo_dim > 1 (hopping along every lattice
+    dimension, paces/models/holstein.py:210-232) and the next-nearest-neighbour "hopping2"
+    term (holstein.py:234-240), open boundaries.  Stores the observables of every step and
+    the last state."""
+    from paces.models import holstein
+    from paces.core.time_evolution import CoeffSaveParams, ExpmParams, TimeEvoParams
+    from paces.config import devices
+    nchain, geo, dim, g, J2, deps, ms, steps, initpos = cfg
+    use_terms = {"diag": dict(eps_sys=0.0, hbar_omega=1.0, delta_eps=deps), "hopping": dict(J=1.0)}
+    if J2 is not None:
+        use_terms["hopping2"] = dict(J2=J2)
+    use_terms["vib_coupling"] = dict(g=g)
+    with devices.vector_dev:
+        ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain, geo_dim=geo, use_terms=use_terms,
+                                   debug_verb=0)
+        te = holstein.TimeEvolution(ham, holstein.Observables, ["n_exc", "n_pho", "total_energy"], workdir,
+                                    TimeEvoParams(maxstates=ms, enlarge_steps=1, shuffle_seed=None),
+                                    ExpmParams(), os.path.join(workdir, "params.log"))
+        te.create_nonuniform_basis([1] * nchain, minpos=initpos, maxpos=initpos + 1)
+        te.create_initial_vector([1.0], [[initpos] + [0] * nchain])
+        te.generate_timeline(np.arange(steps + 1) * 0.05, CoeffSaveParams())
+        vec, who = np.asarray(te.vector), np.asarray(te.whoami)
+    od = os.path.join(workdir, "observables")
+    np.savez_compressed(os.path.join(HERE, f"lattice_{name}.npz"),
+                        n_exc=np.loadtxt(os.path.join(od, "n_exc.real")),
+                        n_pho=np.loadtxt(os.path.join(od, "n_pho.real")),
+                        energy=np.loadtxt(os.path.join(od, "total_energy.real")),
+                        diagnostics=np.loadtxt(os.path.join(od, "diagnostics.log")),
+                        vector=vec, whoami=who,
+                        config=np.array([nchain, geo, dim, g, np.nan if J2 is None else J2, deps, ms, steps,
+                                         initpos], dtype=np.float64))
+
+
 def gen_ed(paces, workdir):
     """N=4, max_ho_dims=4, J=g=omega=1: the full space (1024 states) fits, so paces == exact."""
     ham, te = make_objects(paces, 4, 4, 1.0, 100000, 1, 0, workdir)
@@ -397,6 +443,8 @@ def main():
     jobs.append(("scaled_n8c16", lambda: gen_traj_scaled(paces, fresh())))
     for name, weighting in TAU_RUNS.items():
         jobs.append((name, lambda name=name, w=weighting: gen_traj_tau(paces, name, w, fresh())))
+    for name, cfg in LATTICE_RUNS.items():
+        jobs.append((f"lattice_{name}", lambda name=name, cfg=cfg: gen_lattice(paces, name, cfg, fresh())))
     if args.long:
         for name, cfg in LONG_TRAJ_RUNS.items():
             jobs.append((f"traj_{name}", lambda name=name, cfg=cfg: gen_traj(paces, name, cfg, fresh())))

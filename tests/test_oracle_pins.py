@@ -214,3 +214,32 @@ def test_lookahead_weighting_matches_the_reference(weighting):
     np.testing.assert_allclose(tr.vector, f["vector"], rtol=0, atol=1e-14)
     plain = runs[0.0][0]
     assert plain.whoami.shape != f["whoami"].shape or not np.array_equal(plain.whoami, f["whoami"])
+
+
+@pytest.mark.parametrize("name", ["geo2_n9c8", "hop2_n8c8", "geo2hop2_n16c4", "geo3_n27c4"])
+def test_lattices_match_the_reference(name):
+    """The oracle's hopping channels (geo_dim > 1: hopping along every lattice dimension;
+    the next-nearest-neighbour hopping2 term) against the reference's own runs
+    (tests/golden/lattice_<name>.npz): observables at every step, basis sizes, the final
+    basis and amplitudes."""
+    f = np.load(os.path.join(GOLDEN, f"lattice_{name}.npz"))
+    nchain, geo, dim, g, J2, deps, ms, steps, initpos = f["config"]
+    nchain, geo, dim, ms, steps, initpos = (int(x) for x in (nchain, geo, dim, ms, steps, initpos))
+    m = po.Model(nchain, [dim] * nchain, g=float(g), geo_dim=geo, J2=None if np.isnan(J2) else float(J2),
+                 delta_eps=float(deps))
+    tr = po.Trajectory(m, po.initial_basis(m, initpos), np.array([1.0 + 0j]), ms, 1)
+    recs = tr.run(np.arange(steps + 1) * 0.05)
+    np.testing.assert_allclose(np.array([r.n_exc for r in recs]), f["n_exc"][:, 2:], rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(np.array([r.n_pho for r in recs]), f["n_pho"][:, 2:], rtol=1e-10, atol=1e-14)
+    assert [r.numstates for r in recs] == f["diagnostics"][:, 9].astype(int).tolist()
+    assert np.array_equal(tr.whoami, f["whoami"])
+    np.testing.assert_allclose(tr.vector, f["vector"], rtol=0, atol=1e-14)
+
+
+def test_lattice_model_validation():
+    with pytest.raises(ValueError):
+        po.Model(10, [4] * 10, geo_dim=2)              # 10 is not a square
+    with pytest.raises(ValueError):
+        po.Model(4, [4] * 4, geo_dim=2, J2=0.5)        # l = 2: no next-nearest neighbour
+    with pytest.raises(NotImplementedError):
+        po.Model(9, [4] * 9, geo_dim=2, periodic=True)
