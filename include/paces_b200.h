@@ -89,6 +89,13 @@ typedef struct paces_model_desc {
     double J;                  /* use_terms["hopping"]["J"] (real) */
     double g;                  /* use_terms["vib_coupling"]["g"] (real) */
     const double *site_eps;    /* host array of nchain per-site energies, or NULL */
+    /* lattices (paces/models/holstein.py:24-51, :150-240): geo_dim (0 or 1: chain) lattice
+     * dimensions of side l = nchain^(1/geo_dim), hopping along every dimension; hopping2 != 0
+     * adds the next-nearest-neighbour term use_terms["hopping2"]["J2"] (needs l >= 3).  Both
+     * need open boundaries. */
+    int32_t geo_dim;
+    int32_t hopping2;
+    double J2;
 } paces_model_desc;
 
 typedef struct paces_ctx paces_ctx;
@@ -109,6 +116,10 @@ typedef struct paces_hmat {
     int32_t *nbr;
     uint32_t *meta;
     int64_t cap;
+    /* lattices with more than one hopping channel (paces_hop_channels > 1): the other
+     * channels' neighbours, xnbr[2*(c-1)*cap + 2*r + {0,1}] = row of the state with the
+     * exciton moved by -/+ the distance of channel c (-1: absent); NULL otherwise */
+    int32_t *xnbr;
 } paces_hmat;
 
 typedef struct paces_step_params {
@@ -187,6 +198,9 @@ enum { PACES_WEIGHT_NONE = 0, PACES_WEIGHT_COHERENCE = 1, PACES_WEIGHT_NORM = 2,
 
 /* ---- context ----------------------------------------------------------------------- */
 int paces_create(const paces_model_desc *desc, paces_ctx **out);
+/* Hopping channels of the context's model: geo_dim for the hopping term, twice that with
+ * hopping2 (1 for the chain).  An H table of a model with more than one needs xnbr. */
+int paces_hop_channels(const paces_ctx *ctx);
 int paces_destroy(paces_ctx *ctx);
 const char *paces_last_error(const paces_ctx *ctx);
 int paces_key_words(const paces_ctx *ctx);         /* nw: uint64 words per key */

@@ -48,6 +48,9 @@ class ModelDesc(ctypes.Structure):
         ("J", ctypes.c_double),
         ("g", ctypes.c_double),
         ("site_eps", ctypes.POINTER(ctypes.c_double)),
+        ("geo_dim", ctypes.c_int32),
+        ("hopping2", ctypes.c_int32),
+        ("J2", ctypes.c_double),
     ]
 
 
@@ -56,7 +59,8 @@ class Basis(ctypes.Structure):
 
 
 class HMat(ctypes.Structure):
-    _fields_ = [("nbr", ctypes.c_void_p), ("meta", ctypes.c_void_p), ("cap", ctypes.c_int64)]
+    _fields_ = [("nbr", ctypes.c_void_p), ("meta", ctypes.c_void_p), ("cap", ctypes.c_int64),
+                ("xnbr", ctypes.c_void_p)]
 
 
 class StepParams(ctypes.Structure):
@@ -152,6 +156,7 @@ _SIGNATURES = {
     "paces_ref_words": [_P],
     "paces_key_layout": [_P, _P, _P, _P],
     "paces_version": [],
+    "paces_hop_channels": [_P],
     "paces_workspace_bytes": [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)],
     "paces_read_status": [_P, _P, ctypes.POINTER(ctypes.c_int32)],
     "paces_keys_from_ref": [_P, _P, ctypes.c_int64, ctypes.c_int32, _P, _P, _P],

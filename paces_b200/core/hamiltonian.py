@@ -187,17 +187,33 @@ def hmat_to_coo(eng, basis, h):
     if p.site_eps is not None:
         diag = diag + torch.as_tensor(p.site_eps, dtype=torch.float64, device=diag.device)[pos]
     rows = torch.arange(S, device=nbr.device)
+    # hopping channels: channel 0 in the int4 rows, the others in xnbr (channel c >= 1 at
+    # xnbr[c-1]); lattices with geo_dim d have d channels of "hopping", then d of "hopping2"
+    geo = int(getattr(p, "geo_dim", 1) or 1)
+    nhop = int(getattr(eng, "nhop", 1))
+    cols = {0: (nbr[:, 0], nbr[:, 1])}
+    for c in range(1, nhop):
+        x = h.xnbr[c - 1, :S].to(torch.int64)
+        cols[c] = (x[:, 0], x[:, 1])
+    terms = [("hopping", float(p.J), [c for c in range(nhop) if c < geo])]
+    if nhop > geo:
+        terms.append(("hopping2", float(p.J2), [c for c in range(nhop) if c >= geo]))
     coo = {}
-    for term, slots in (("hopping", (0, 1)), ("vib_coupling", (2, 3))):
+    for term, J, chans in terms:
         r_all, c_all, v_all = [], [], []
-        for s in slots:
-            ok = nbr[:, s] >= 0
-            r_all.append(rows[ok])
-            c_all.append(nbr[ok, s])
-            if term == "hopping":
-                v_all.append(torch.full((int(ok.sum()),), float(p.J), dtype=torch.float64, device=nbr.device))
-            else:
-                k = n[ok] if s == 2 else n[ok] + 1
-                v_all.append(torch.sqrt(k.to(torch.float64)) * float(p.g))
+        for c in chans:
+            for col in cols[c]:
+                ok = col >= 0
+                r_all.append(rows[ok])
+                c_all.append(col[ok])
+                v_all.append(torch.full((int(ok.sum()),), J, dtype=torch.float64, device=nbr.device))
         coo[term] = (torch.cat(v_all), (torch.cat(r_all), torch.cat(c_all)))
+    r_all, c_all, v_all = [], [], []
+    for s in (2, 3):
+        ok = nbr[:, s] >= 0
+        r_all.append(rows[ok])
+        c_all.append(nbr[ok, s])
+        k = n[ok] if s == 2 else n[ok] + 1
+        v_all.append(torch.sqrt(k.to(torch.float64)) * float(p.g))
+    coo["vib_coupling"] = (torch.cat(v_all), (torch.cat(r_all), torch.cat(c_all)))
     return coo, diag

@@ -87,6 +87,7 @@ struct Layout {
     size_t o_partials, o_out;
     size_t aw, keep;  // kept amplitudes of the truncation, proposal keep mask [kRuns][cap]
     size_t maps_e, keysN, blkN, n2b;  // split expansion: its maps, the new part, new part -> output
+    size_t maps_x;                    // lattices: maps of the assembly's passes 2 and 3
 };
 
 Layout make_layout(const paces_ctx* c, int64_t cap) {
@@ -138,6 +139,8 @@ Layout make_layout(const paces_ctx* c, int64_t cap) {
     l.aw = take((ucap + 1) * 4);
     l.keep = take(size_t(kRuns) * ucap);
     l.maps_e = take(size_t(kRuns) * ucap * 4);
+    const int passes = merge_passes(c->m);
+    l.maps_x = take(passes > 2 ? size_t(passes - 2) * kRuns * ucap * 4 : 0);
     l.keysN = take(ucap * nw * 8);
     l.blkN = take(size_t(L + 1) * 4);
     l.n2b = take(ucap * 4);
@@ -160,7 +163,15 @@ T* at(void* ws, size_t off) {
     return reinterpret_cast<T*>(static_cast<unsigned char*>(ws) + off);
 }
 
-MergeWs merge_ws(const Layout& l, void* ws) {
+// The model of a launch that reads the H table h: the extra channels' neighbours travel with it.
+ModelDev with_h(const paces_ctx* c, const paces_hmat* h) {
+    ModelDev m = c->m;
+    m.xnbr = h ? reinterpret_cast<const int2*>(h->xnbr) : nullptr;
+    m.xcap = h ? h->cap : 0;
+    return m;
+}
+
+MergeWs merge_ws(const paces_ctx* c, const Layout& l, void* ws) {
     MergeWs w;
     w.run_lo = at<int>(ws, l.m_run_lo);
     w.run_len = at<int>(ws, l.m_run_len);
@@ -175,6 +186,7 @@ MergeWs merge_ws(const Layout& l, void* ws) {
     w.tile_cap = int(l.tile_cap);
     w.keep = nullptr;
     w.keep_cap = 0;
+    merge_spec_standard(w, c->m);
     return w;
 }
 
@@ -220,12 +232,53 @@ __global__ void record_init_kernel(paces_step_record* rec, int diagnostics) {
     (void)diagnostics;
 }
 
-__global__ void record_counts_kernel(paces_step_record* rec, const int* sel_blk, const int* enl_blk,
-                                     const int* new_blk, int L) {
+// (n_select is written by the truncation: with several merge passes its buffer is reused)
+__global__ void record_counts_kernel(paces_step_record* rec, const int* enl_blk, const int* new_blk, int L) {
     if (threadIdx.x != 0) return;
-    rec->n_select = sel_blk[L];
     rec->n_enlarged = enl_blk[L];
     rec->n_states = new_blk[L];
+}
+
+// Expansion (assemble = false) or assembly of X over every hopping channel of a lattice:
+// merge_passes passes, pass 0 with the five standard runs, pass k >= 1 with the self run (the
+// previous pass's output) and the images of X under channels 2k-1 and 2k.  Passes before the
+// last write tmp[k & 1] (neither may alias X or fin's output); the last writes fin.  An
+// assembly's pass k writes its maps to the k-th map array of the layout, its last pass the
+// H rows of fin, and then the neighbour table (both parts) is filled from the maps.
+int merge_all_channels(paces_ctx* c, bool assemble, const Layout& l, void* ws, const paces_basis& X,
+                       const paces_basis* tmp, const MergeOut& fin, int* xnbr, int* ceiling, int* status,
+                       cudaStream_t st) {
+    const int P = merge_passes(c->m);
+    int* pass_maps[4] = {at<int>(ws, l.maps), at<int>(ws, l.maps_e), nullptr, nullptr};
+    if (P > 2) pass_maps[2] = at<int>(ws, l.maps_x);
+    if (P > 3) pass_maps[3] = at<int>(ws, l.maps_x) + size_t(kRuns) * l.cap;
+    const paces_basis* prev = nullptr;
+    for (int k = 0; k < P; ++k) {
+        const bool last = k == P - 1;
+        MergeWs mws = merge_ws(c, l, ws);
+        if (k > 0) merge_spec_hops(mws, c->m, 2 * k - 1, 2 * k < c->m.nhop ? 2 * k : -1);
+        MergeOut mo{};
+        if (last) {
+            mo = fin;
+        } else {
+            mo.keys = tmp[k & 1].keys;
+            mo.blk = tmp[k & 1].blk;
+            mo.cap = tmp[k & 1].cap;
+        }
+        if (assemble) {
+            mo.maps = pass_maps[k];
+            mo.map_cap = l.cap;
+        }
+        const int rc = launch_merge(c->nw, assemble ? MERGE_ASSEMBLE : MERGE_EXPAND, c->merge_stride, c->m,
+                                    k == 0 ? X.keys : prev->keys, k == 0 ? X.blk : prev->blk,
+                                    k == 0 ? nullptr : X.keys, k == 0 ? nullptr : X.blk, mws, mo,
+                                    k == 0 ? ceiling : nullptr, 0, status, c->num_sms, st);
+        if (rc != PACES_OK) return rc;
+        prev = last ? nullptr : &tmp[k & 1];
+    }
+    if (assemble && P > 1)
+        return launch_nbr_fill_multi(c->m, X.blk, pass_maps, P, l.cap, fin.nbr, xnbr, fin.nbr_cap, c->num_sms, st);
+    return PACES_OK;
 }
 
 // ---- the time step, in the pieces the single and the batched step share ---------------------
@@ -241,6 +294,7 @@ struct StepPlan {
     void* ws;
     paces_basis A, B;   // truncated basis, enlargement ping-pong
     paces_basis* cur;   // the enlarged basis (A or B after enlarge_steps merges)
+    const int* enl_blk; // block offsets of the enlarged basis (step_front)
     void* target;       // remapped amplitudes (the Taylor input when evolving)
 };
 
@@ -255,6 +309,12 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
         return fail(c, PACES_ERR_BADARG, "paces_step: bad parameters");
     if (prm->proposal && !prm->proposal_params)
         return fail(c, PACES_ERR_BADARG, "paces_step: proposal without MLP parameters");
+    if (c->m.nhop > 1) {
+        if (!h->xnbr) return fail(c, PACES_ERR_BADARG, "paces_step: the lattice's H table needs xnbr");
+        if (prm->proposal) return fail(c, PACES_ERR_BADARG, "paces_step: the learned proposal needs the chain model");
+        if (prm->weighting && (!prm->old_h || !prm->old_h->xnbr))
+            return fail(c, PACES_ERR_BADARG, "paces_step: the lattice's old H table needs xnbr");
+    }
     if (prm->weighting) {
         if (prm->weighting != PACES_WEIGHT_COHERENCE && prm->weighting != PACES_WEIGHT_NORM)
             return fail(c, PACES_ERR_BADARG, "paces_step: unknown weighting %d", int(prm->weighting));
@@ -288,10 +348,10 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
 // Kernels one step enqueues (merge: 5, +1 with the neighbour table; truncation: see
 // trunc_launches, +1 with look-ahead weights; remap 3; observables 2 or 3; Taylor 1;
 // renormalisation 3; record 2).
-unsigned long long step_launches(const paces_step_params& prm, bool c64, bool with_taylor) {
+unsigned long long step_launches(const paces_step_params& prm, bool c64, bool with_taylor, int passes) {
     const int wk = prm.weighting ? 2 : (c64 ? 1 : 0);
     return 2 + (prm.weighting ? 1 : 0) + trunc_launches(wk, prm.shuffle != 0) +
-           (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 5ull * prm.enlarge_steps + 6 +
+           (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 5ull * passes * (prm.enlarge_steps + 1) + 1 +
            3 + (prm.diagnostics ? 2 : 0) +
            (prm.evolve ? (with_taylor ? 1 : 0) + (prm.renormalize ? 3 : 0) : 0) + 3;
 }
@@ -314,14 +374,14 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     const double* weights = nullptr;
     if (prm->weighting) {
         double* w = at<double>(ws, l.v_TA);
-        PACES_CHECK_LAUNCH(c, launch_lookahead(c64, c->m, p.old_b->blk, prm->old_h->nbr, prm->old_h->meta, p.old_psi,
+        PACES_CHECK_LAUNCH(c, launch_lookahead(c64, with_h(c, prm->old_h), p.old_b->blk, prm->old_h->nbr, prm->old_h->meta, p.old_psi,
                                                prm->tau, prm->weighting, w, status, c->num_sms, st),
                            "step/weights");
         weights = w;
     }
     PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, weights, prm->maxstates,
                                           prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), p.A.keys,
-                                          p.A.blk, p.A.cap, at<float>(ws, l.aw), &rec->n_tied, status, c->num_sms, st),
+                                          p.A.blk, p.A.cap, at<float>(ws, l.aw), &rec->n_tied, &rec->n_select, status, c->num_sms, st),
                        "step/truncate");
     // 1b. learned proposal: score the truncated basis' images
     const bool propose = prm->proposal && prm->enlarge_steps > 0;
@@ -340,12 +400,45 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     //    the proposal the last enlargement B = P + images(P) is split: it also records where
     //    P's images landed and which states of B are new (N = B \ P), so the assembly merges
     //    B with the images of N only -- the images of P are in B already.
-    const bool split = prm->enlarge_steps > 0 && !propose;
+    const bool multi = c->m.nhop > 1;
+    const bool split = prm->enlarge_steps > 0 && !propose && !multi;
     paces_basis* cur = &p.A;
     paces_basis* other = &p.B;
     paces_basis nbasis{at<uint64_t>(ws, l.keysN), at<int32_t>(ws, l.blkN), l.cap};
-    for (int e = 0; e < prm->enlarge_steps; ++e) {
-        MergeWs mws = merge_ws(l, ws);
+    if (multi) {
+        // lattices: every expansion and the assembly in merge_passes passes, rotating three
+        // buffers (the truncated basis starts in A)
+        paces_basis bufs[3] = {p.A, p.B, nbasis};
+        int ci = 0;
+        const int P = merge_passes(c->m);
+        for (int e = 0; e < prm->enlarge_steps; ++e) {
+            const int o0 = (ci + 1) % 3, o1 = (ci + 2) % 3;
+            const paces_basis tmp[2] = {bufs[o0], bufs[o1]};
+            const int outi = ((P - 1) & 1) ? o1 : o0;
+            MergeOut fin{};
+            fin.keys = bufs[outi].keys;
+            fin.blk = bufs[outi].blk;
+            fin.cap = bufs[outi].cap;
+            PACES_CHECK_LAUNCH(c, merge_all_channels(c, false, l, ws, bufs[ci], tmp, fin, nullptr, nullptr, status, st),
+                               "step/expand");
+            ci = outi;
+        }
+        mark(2);
+        const paces_basis tmp[2] = {bufs[(ci + 1) % 3], bufs[(ci + 2) % 3]};
+        MergeOut fin{};
+        fin.keys = p.new_b->keys;
+        fin.blk = p.new_b->blk;
+        fin.cap = p.new_b->cap < p.h->cap ? p.new_b->cap : p.h->cap;
+        fin.meta = p.h->meta;
+        fin.nbr = p.h->nbr;
+        fin.nbr_cap = p.h->cap;
+        PACES_CHECK_LAUNCH(c, merge_all_channels(c, true, l, ws, bufs[ci], tmp, fin, p.h->xnbr, &rec->ceiling_hits,
+                                                 status, st),
+                           "step/assemble");
+        p.enl_blk = bufs[ci].blk;
+    }
+    for (int e = 0; e < prm->enlarge_steps && !multi; ++e) {
+        MergeWs mws = merge_ws(c, l, ws);
         if (propose && e == 0) {
             mws.keep = at<uint8_t>(ws, l.keep);
             mws.keep_cap = l.cap;
@@ -371,9 +464,10 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         cur = other;
         other = t;
     }
-    mark(2);
     // 3. new basis + H
-    {
+    if (!multi) {
+        mark(2);
+        p.enl_blk = cur->blk;
         MergeOut mo{};
         mo.keys = p.new_b->keys;
         mo.blk = p.new_b->blk;
@@ -384,7 +478,7 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.maps = at<int>(ws, l.maps);
         mo.map_cap = l.cap;
         PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, cur->keys, cur->blk,
-                                           split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(l, ws),
+                                           split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(c, l, ws),
                                            mo, &rec->ceiling_hits, split ? 1 : 0, status, c->num_sms, st),
                            "step/assemble");
         if (split)
@@ -402,8 +496,8 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     // 5. post-adaptation diagnostics
     if (prm->diagnostics) {
         ObsTarget t{&rec->post_adapt_norm, &rec->post_adapt_energy_re, &rec->post_adapt_energy_im, nullptr, nullptr};
-        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
-                                                 p.h->meta, p.target, PACES_OBS_NORM | PACES_OBS_ENERGY,
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, with_h(c, p.h), p.new_b->keys, p.new_b->blk, p.h->nbr,
+                                                 p.h->cap, p.h->meta, p.target, PACES_OBS_NORM | PACES_OBS_ENERGY,
                                                  at<double>(ws, l.o_partials), t, c->num_sms, st),
                            "step/diagnostics");
     }
@@ -422,7 +516,7 @@ int step_back(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     };
     if (prm->evolve && prm->renormalize) {
         ObsTarget t{&rec->norm, nullptr, nullptr, nullptr, nullptr};
-        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, with_h(c, p.h), p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
                                                  p.h->meta, p.new_psi, PACES_OBS_NORM, opart, t, c->num_sms, st),
                            "step/norm");
         PACES_CHECK_LAUNCH(c, launch_scale(c64, c->m, p.new_b->blk, p.new_psi, &rec->norm, c->num_sms, st),
@@ -432,13 +526,13 @@ int step_back(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     // 7. observables of the new state
     {
         ObsTarget t{&rec->norm, &rec->energy_re, &rec->energy_im, rec->n_exc, rec->n_pho};
-        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, c->m, p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
+        PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, with_h(c, p.h), p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
                                                  p.h->meta, p.new_psi,
                                                  PACES_OBS_NORM | PACES_OBS_ENERGY | PACES_OBS_SITES, opart, t,
                                                  c->num_sms, st),
                            "step/observables");
     }
-    record_counts_kernel<<<1, 32, 0, st>>>(rec, p.A.blk, p.cur->blk, p.new_b->blk, c->m.L);
+    record_counts_kernel<<<1, 32, 0, st>>>(rec, p.enl_blk, p.new_b->blk, c->m.L);
     mark(7);
     if (cudaGetLastError() != cudaSuccess) return cuda_fail(c, "step/record");
     return PACES_OK;
@@ -449,6 +543,8 @@ int step_back(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
 extern "C" {
 
 int paces_version(void) { return 10200; }
+
+int paces_hop_channels(const paces_ctx* c) { return c ? c->m.nhop : 0; }
 
 int paces_create(const paces_model_desc* d, paces_ctx** out) {
     if (!out) return PACES_ERR_BADARG;
@@ -469,6 +565,38 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
     m.J = d->J;
     m.g = d->g;
     m.has_site_eps = d->site_eps ? 1 : 0;
+    // hopping channels (paces/models/holstein.py:150-240): per term (hopping, then hopping2),
+    // one channel per lattice dimension d, moving the exciton by order * l^d
+    {
+        const int geo = d->geo_dim > 0 ? d->geo_dim : 1;
+        const int l = int(std::lround(std::pow(double(L), 1.0 / geo)));  // lattice_l, holstein.py:49
+        long long lp = 1;
+        for (int k = 0; k < geo; ++k) lp *= l;
+        if (geo > 3 || lp != L || (d->hopping2 && l - 1 < 2) || (d->periodic && (geo != 1 || d->hopping2))) {
+            delete c;
+            return PACES_ERR_BADARG;
+        }
+        m.J2 = d->hopping2 ? d->J2 : 0.0;
+        m.nhop = 0;
+        for (int t = 0; t < (d->hopping2 ? 2 : 1); ++t) {
+            long long ld = 1;
+            for (int k = 0; k < geo; ++k, ld *= l) {
+                m.hop_dist[m.nhop] = int((t + 1) * ld);
+                m.hop_mod[m.nhop] = int(ld * l);
+                m.hop_term[m.nhop] = t;
+                ++m.nhop;
+            }
+        }
+        // per term: neighbours below p (largest distance first), then above (smallest first)
+        for (int t = 0; t < 2; ++t) {
+            int n = 0;
+            for (int k = m.nhop - 1; k >= 0; --k)
+                if (m.hop_term[k] == t) m.hop_ord[t][n++] = int8_t(k << 1);
+            for (int k = 0; k < m.nhop; ++k)
+                if (m.hop_term[k] == t) m.hop_ord[t][n++] = int8_t((k << 1) | 1);
+            m.hop_n[t] = n;
+        }
+    }
     int word = 0, used = 0, total_bits = 0;
     for (int s = 0; s < L; ++s) {
         const int md = d->max_ho_dims[s];
@@ -677,8 +805,16 @@ int paces_expand(paces_ctx* c, const paces_basis* in, paces_basis* out, void* ws
     mo.keys = out->keys;
     mo.blk = out->blk;
     mo.cap = out->cap;
+    if (c->m.nhop > 1) {
+        const paces_basis tmp[2] = {{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap},
+                                    {at<uint64_t>(ws, l.keysB), at<int32_t>(ws, l.blkB), l.cap}};
+        PACES_CHECK_LAUNCH(c, merge_all_channels(c, false, l, ws, *in, tmp, mo, nullptr, nullptr, c->d_status,
+                                                 reinterpret_cast<cudaStream_t>(stream)),
+                           "expand");
+        return PACES_OK;
+    }
     PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_EXPAND, c->merge_stride, c->m, in->keys, in->blk, nullptr, nullptr,
-                                       merge_ws(l, ws), mo, nullptr, 0,
+                                       merge_ws(c, l, ws), mo, nullptr, 0,
                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "expand");
     return PACES_OK;
@@ -699,8 +835,17 @@ int paces_assemble(paces_ctx* c, const paces_basis* in, paces_basis* out, paces_
     mo.maps = at<int>(ws, l.maps);
     mo.map_cap = l.cap;
     if (h->cap < out->cap) mo.cap = h->cap;
+    if (c->m.nhop > 1) {
+        if (!h->xnbr) return fail(c, PACES_ERR_BADARG, "paces_assemble: the model's H needs xnbr");
+        const paces_basis tmp[2] = {{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap},
+                                    {at<uint64_t>(ws, l.keysB), at<int32_t>(ws, l.blkB), l.cap}};
+        PACES_CHECK_LAUNCH(c, merge_all_channels(c, true, l, ws, *in, tmp, mo, h->xnbr, dev_ceiling_hits, c->d_status,
+                                                 reinterpret_cast<cudaStream_t>(stream)),
+                           "assemble");
+        return PACES_OK;
+    }
     PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, in->keys, in->blk, nullptr, nullptr,
-                                       merge_ws(l, ws), mo, dev_ceiling_hits, 0,
+                                       merge_ws(c, l, ws), mo, dev_ceiling_hits, 0,
                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "assemble");
     return PACES_OK;
@@ -714,7 +859,7 @@ int paces_truncate(paces_ctx* c, const paces_basis* in, const void* psi, int64_t
     if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
     PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, psi, nullptr,
                                           maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
-                                          out->blk, out->cap, nullptr, nullptr, c->d_status, c->num_sms,
+                                          out->blk, out->cap, nullptr, nullptr, nullptr, c->d_status, c->num_sms,
                                           reinterpret_cast<cudaStream_t>(stream)),
                        "truncate");
     return PACES_OK;
@@ -728,7 +873,7 @@ int paces_truncate_weighted(paces_ctx* c, const paces_basis* in, const double* w
     if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
     PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, nullptr, weights,
                                           maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
-                                          out->blk, out->cap, nullptr, nullptr, c->d_status, c->num_sms,
+                                          out->blk, out->cap, nullptr, nullptr, nullptr, c->d_status, c->num_sms,
                                           reinterpret_cast<cudaStream_t>(stream)),
                        "truncate_weighted");
     return PACES_OK;
@@ -740,7 +885,7 @@ int paces_lookahead_weights(paces_ctx* c, const paces_basis* b, const paces_hmat
     if (weighting != PACES_WEIGHT_COHERENCE && weighting != PACES_WEIGHT_NORM && weighting != PACES_WEIGHT_HAM_ONES)
         return fail(c, PACES_ERR_BADARG, "paces_lookahead_weights: unknown weighting %d", int(weighting));
     if (!std::isfinite(tau)) return fail(c, PACES_ERR_BADARG, "paces_lookahead_weights: tau is not finite");
-    PACES_CHECK_LAUNCH(c, launch_lookahead(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->meta, psi, tau, weighting,
+    PACES_CHECK_LAUNCH(c, launch_lookahead(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->meta, psi, tau, weighting,
                                            w, c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "lookahead_weights");
     return PACES_OK;
@@ -795,7 +940,7 @@ int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
         o.c1_plus_c2 = &dev_info->c1_plus_c2;
         o.term_ratio = &dev_info->term_ratio;
     }
-    PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->cap, h->meta, psi_in,
+    PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->cap, h->meta, psi_in,
                                         psi_out, dt, m_star, tol, taylor_ws(l, ws), o, c->d_status, c->num_sms,
                                         c->taylor_bps, c->taylor_variant, reinterpret_cast<cudaStream_t>(stream)),
                        "taylor");
@@ -807,7 +952,7 @@ int paces_hnorms(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
     if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !dev_out || !ws) return PACES_ERR_BADARG;
     const Layout l = fit_layout(c, ws_bytes);
     const int nparts = c->num_sms * 2;  // the observables' partials hold far more than 2 * nparts doubles
-    PACES_CHECK_LAUNCH(c, launch_hnorms(c->m, b->blk, h->nbr, h->meta, dev_shift, at<double>(ws, l.o_partials), nparts,
+    PACES_CHECK_LAUNCH(c, launch_hnorms(with_h(c, h), b->blk, h->nbr, h->meta, dev_shift, at<double>(ws, l.o_partials), nparts,
                                         dev_out, reinterpret_cast<cudaStream_t>(stream)),
                        "hnorms");
     return PACES_OK;
@@ -828,7 +973,7 @@ int paces_expm_scaled(paces_ctx* c, const paces_basis* b, const paces_hmat* h, c
         o.c1_plus_c2 = &dev_info->c1_plus_c2;
         o.term_ratio = &dev_info->term_ratio;
     }
-    PACES_CHECK_LAUNCH(c, launch_expm_scaled(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->meta, psi_in, psi_out,
+    PACES_CHECK_LAUNCH(c, launch_expm_scaled(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->meta, psi_in, psi_out,
                                              t, shift, m_star, stages, tol, eta_re, eta_im, taylor_ws(l, ws), o,
                                              c->d_status, c->num_sms, c->taylor_grid,
                                              reinterpret_cast<cudaStream_t>(stream)),
@@ -842,7 +987,7 @@ int paces_observables(paces_ctx* c, const paces_basis* b, const paces_hmat* h, c
     const Layout l = fit_layout(c, ws_bytes);
     const int L = c->m.L;
     ObsTarget t{dev_out, dev_out + 1, dev_out + 2, dev_out + 3, dev_out + 3 + L};
-    PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c->precision == PACES_C64, c->m, b->keys, b->blk, h->nbr, h->cap,
+    PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c->precision == PACES_C64, with_h(c, h), b->keys, b->blk, h->nbr, h->cap,
                                              h->meta, psi, what, at<double>(ws, l.o_partials), t, c->num_sms,
                                              reinterpret_cast<cudaStream_t>(stream)),
                        "observables");
@@ -852,7 +997,7 @@ int paces_observables(paces_ctx* c, const paces_basis* b, const paces_hmat* h, c
 int paces_apply_h(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* x, void* y,
                   paces_stream_t stream) {
     if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !x || !y || x == y) return PACES_ERR_BADARG;
-    PACES_CHECK_LAUNCH(c, launch_apply_h(c->precision == PACES_C64, c->m, b->blk, h->nbr, h->meta, x, y, c->num_sms,
+    PACES_CHECK_LAUNCH(c, launch_apply_h(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->meta, x, y, c->num_sms,
                                          reinterpret_cast<cudaStream_t>(stream)),
                        "apply_h");
     return PACES_OK;
@@ -876,12 +1021,12 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
     const int rc = plan_step(c, old_b, old_psi, new_b, new_psi, h, prm, rec, ws, ws_bytes, &p);
     if (rc != PACES_OK) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    c->launches += step_launches(*prm, c->precision == PACES_C64, true);
+    c->launches += step_launches(*prm, c->precision == PACES_C64, true, merge_passes(c->m));
     int r = step_front(c, p, st, true);
     if (r != PACES_OK) return r;
     if (prm->evolve) {
         TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
-        PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, c->m, new_b->blk, h->nbr, h->cap, h->meta,
+        PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, with_h(c, h), new_b->blk, h->nbr, h->cap, h->meta,
                                             p.target, new_psi, prm->dt, prm->m_star, prm->tol, taylor_ws(p.l, ws), o,
                                             &rec->status, c->num_sms, c->taylor_bps, c->taylor_variant, st),
                            "step/taylor");
@@ -1059,10 +1204,11 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
         if (!it.ctx) return bfail(PACES_ERR_BADARG, "item %d: no context", i);
         if (it.ctx->precision != precision) return bfail(PACES_ERR_BADARG, "item %d: mixed precisions in one batch", i);
         if (it.ctx->device != b->device) return bfail(PACES_ERR_BADARG, "item %d: context on another device", i);
+        if (it.ctx->m.nhop > 1) return bfail(PACES_ERR_BADARG, "item %d: batched steps take chain models only", i);
         const int rc = plan_step(it.ctx, it.old_basis, it.old_psi, it.new_basis, it.new_psi, it.h, it.params,
                                  it.record, it.workspace, it.workspace_bytes, &plans[i]);
         if (rc != PACES_OK) return bfail(rc, "item %d: %s", i, it.ctx->err);
-        launches += step_launches(*it.params, it.ctx->precision == PACES_C64, false);
+        launches += step_launches(*it.params, it.ctx->precision == PACES_C64, false, merge_passes(it.ctx->m));
         n_evolve += it.params->evolve ? 1 : 0;
     }
     auto fork = [&]() -> bool {

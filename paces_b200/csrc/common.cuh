@@ -12,6 +12,7 @@ namespace paces {
 constexpr int kMaxSites = PACES_MAX_SITES;
 constexpr int kMaxKeyWords = 8;
 constexpr int kRuns = 5;  // candidate runs per exciton block: self, from-left, from-right, up, down
+constexpr int kMaxHop = 6;  // hopping channels: up to 3 lattice dimensions x 2 hopping terms
 enum Run : int { RUN_SELF = 0, RUN_FROM_LEFT = 1, RUN_FROM_RIGHT = 2, RUN_UP = 3, RUN_DOWN = 4 };
 // neighbour slots of the H table (paces_hmat.nbr)
 enum Slot : int { NB_LEFT = 0, NB_RIGHT = 1, NB_DOWN = 2, NB_UP = 3 };
@@ -32,7 +33,32 @@ struct ModelDev {
     // total phonon count of a key is sum_{q,b} popc(w[q] & plane[q][b]) << b
     int max_bits;
     uint64_t plane[kMaxKeyWords][8];
+    // Hopping channels.  Channel 0 is the nearest-neighbour hop along the first lattice
+    // dimension (the chain's only channel); channels 1.. are the further lattice dimensions
+    // of the "hopping" term and then the dimensions of the "hopping2" term.  A channel moves
+    // the exciton by +-hop_dist; with open boundaries the +dist hop from p exists when
+    // p % hop_mod < hop_mod - hop_dist (p stays in its row of the lattice).
+    int nhop;
+    int hop_dist[kMaxHop];
+    int hop_mod[kMaxHop];
+    int hop_term[kMaxHop];      // 0: hopping (J), 1: hopping2 (J2)
+    double J2;
+    // per term, the row's hopping elements in increasing column (= position) order:
+    // channel << 1 | side, side 0 = the neighbour at p - dist, 1 = at p + dist
+    int hop_n[2];
+    int8_t hop_ord[2][2 * kMaxHop];
+    // extra channels' neighbour table of the H a kernel reads ([nhop-1][xcap] int2: lower,
+    // upper neighbour), set per launch; null when nhop == 1
+    const int2* xnbr;
+    int64_t xcap;
 };
+
+// Whether the exciton at p has a neighbour through channel ch on side `up` (1: +dist, 0: -dist).
+__host__ __device__ __forceinline__ bool hop_exists(const ModelDev& m, int ch, int p, int up) {
+    if (m.periodic) return true;
+    const int d = m.hop_dist[ch], md = m.hop_mod[ch];
+    return up ? (p % md < md - d) : (p % md >= d);
+}
 
 template <int NW>
 struct Key {

@@ -59,7 +59,13 @@ hnorm_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nb
             const int4 nb = load_nbr(nbr, r);
             const int n = int((mm >> 8) & 0xffu);
             double a = fabs(d - d0);
-            a += (nb.x >= 0 ? fabs(m.J) : 0.0) + (nb.y >= 0 ? fabs(m.J) : 0.0);
+            if (m.nhop > 1) {
+                for (int t = 0; t < 2; ++t)
+                    for (int e = 0; e < m.hop_n[t]; ++e)
+                        if (hop_index(m, r, nb, m.hop_ord[t][e]) >= 0) a += fabs(t == 0 ? m.J : m.J2);
+            } else {
+                a += (nb.x >= 0 ? fabs(m.J) : 0.0) + (nb.y >= 0 ? fabs(m.J) : 0.0);
+            }
             a += (nb.z >= 0 ? fabs(m.g) * sqrt(double(n)) : 0.0) + (nb.w >= 0 ? fabs(m.g) * sqrt(double(n + 1)) : 0.0);
             mx = fmax(mx, a);
         }
@@ -144,11 +150,11 @@ expm_scaled_kernel(ModelDev m, const int* __restrict__ blk, const int* __restric
                 C y;
                 const C xr = __ldcg(src + r);
                 if constexpr (C64) {
-                    y = h_row_c64(m, s_sq, J, r, nbr, mm, src);
+                    y = h_row_c64_any(m, s_sq, J, r, load_nbr(nbr, r), mm, __ldcg(src + r), src);
                     y.x = fmaf(-sh, xr.x, y.x);
                     y.y = fmaf(-sh, xr.y, y.y);
                 } else {
-                    y = h_row_c128(m, s_sq, r, nbr, mm, src);
+                    y = h_row_c128_any(m, s_sq, r, load_nbr(nbr, r), mm, __ldcg(src + r), src);
                     y.x = __dsub_rn(y.x, __dmul_rn(sh, xr.x));
                     y.y = __dsub_rn(y.y, __dmul_rn(sh, xr.y));
                 }

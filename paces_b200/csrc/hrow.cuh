@@ -104,4 +104,111 @@ __device__ __forceinline__ float2 h_row_c64(const P& m, const float* sq, float J
     return h_row_c64_nb(m, sq, J, r, load_nbr(nbr, r), meta, __ldcg(x + r), x);
 }
 
+// ---- lattices with several hopping channels (ModelDev::nhop > 1) ---------------------------
+// The reference sums H x term by term -- diag * x, then the "hopping" CSR row, then the
+// "hopping2" row, then the vibronic row (paces/core/time_evolution.py:382-400, the terms in
+// the order of use_terms) -- and each CSR row in increasing column order, which for open
+// boundaries is increasing exciton position (hop_ord).  Channel 0 lives in the int4 row
+// (left = lower, right = upper), channels 1.. in m.xnbr.
+
+__device__ __forceinline__ int hop_index(const ModelDev& m, int64_t r, int4 nb, int code) {
+    const int ch = code >> 1, up = code & 1;
+    if (ch == 0) return up ? nb.y : nb.x;
+    const int2 e = __ldg(m.xnbr + int64_t(ch - 1) * m.xcap + r);
+    return up ? e.y : e.x;
+}
+
+__device__ __forceinline__ double2 h_row_c128_x(const ModelDev& m, const double* sq, int64_t r, int4 nb, uint32_t meta,
+                                                double2 xr, const double2* __restrict__ x) {
+    const int n = int((meta >> 8) & 0xffu);
+    const double d = diag_value(m, meta);
+    double2 y = make_double2(__dmul_rn(d, xr.x), __dmul_rn(d, xr.y));
+    for (int t = 0; t < 2; ++t) {
+        const double Jt = t == 0 ? m.J : m.J2;
+        double2 hs = make_double2(0.0, 0.0);
+        bool any = false;
+        for (int e = 0; e < m.hop_n[t]; ++e) {
+            const int idx = hop_index(m, r, nb, m.hop_ord[t][e]);
+            if (idx < 0) continue;
+            const double2 v = __ldcg(x + idx);
+            const double2 pv = make_double2(__dmul_rn(Jt, v.x), __dmul_rn(Jt, v.y));
+            hs = any ? make_double2(__dadd_rn(hs.x, pv.x), __dadd_rn(hs.y, pv.y)) : pv;
+            any = true;
+        }
+        if (any) y = make_double2(__dadd_rn(y.x, hs.x), __dadd_rn(y.y, hs.y));
+    }
+    const bool hd = nb.z >= 0, hu = nb.w >= 0;
+    const double2 xd = __ldcg(x + (hd ? nb.z : r));
+    const double2 xu = __ldcg(x + (hu ? nb.w : r));
+    const double cd = sq[n], cu = sq[n + 1];
+    const double2 pd = make_double2(__dmul_rn(cd, xd.x), __dmul_rn(cd, xd.y));
+    const double2 pu = make_double2(__dmul_rn(cu, xu.x), __dmul_rn(cu, xu.y));
+    const double2 vs = (hd && hu) ? make_double2(__dadd_rn(pd.x, pu.x), __dadd_rn(pd.y, pu.y)) : (hd ? pd : pu);
+    if (hd || hu) y = make_double2(__dadd_rn(y.x, vs.x), __dadd_rn(y.y, vs.y));
+    return y;
+}
+
+__device__ __forceinline__ float2 h_row_c64_x(const ModelDev& m, const float* sq, int64_t r, int4 nb, uint32_t meta,
+                                              float2 xr, const float2* __restrict__ x) {
+    const int n = int((meta >> 8) & 0xffu);
+    const float d = float(diag_value(m, meta));
+    float2 y = make_float2(d * xr.x, d * xr.y);
+    for (int t = 0; t < 2; ++t) {
+        const float Jt = float(t == 0 ? m.J : m.J2);
+        for (int e = 0; e < m.hop_n[t]; ++e) {
+            const int idx = hop_index(m, r, nb, m.hop_ord[t][e]);
+            if (idx < 0) continue;
+            const float2 v = __ldcg(x + idx);
+            y.x = fmaf(Jt, v.x, y.x);
+            y.y = fmaf(Jt, v.y, y.y);
+        }
+    }
+    const float2 xd = __ldcg(x + (nb.z >= 0 ? nb.z : r));
+    const float2 xu = __ldcg(x + (nb.w >= 0 ? nb.w : r));
+    const float cd = nb.z >= 0 ? sq[n] : 0.f, cu = nb.w >= 0 ? sq[n + 1] : 0.f;
+    y.x = fmaf(cd, xd.x, y.x);
+    y.y = fmaf(cd, xd.y, y.y);
+    y.x = fmaf(cu, xu.x, y.x);
+    y.y = fmaf(cu, xu.y, y.y);
+    return y;
+}
+
+// One row of H x for either model: the chain's fixed form, or the channel loop.
+__device__ __forceinline__ double2 h_row_c128_any(const ModelDev& m, const double* sq, int64_t r, int4 nb,
+                                                  uint32_t meta, double2 xr, const double2* __restrict__ x) {
+    return m.nhop > 1 ? h_row_c128_x(m, sq, r, nb, meta, xr, x) : h_row_c128_nb(m, sq, r, nb, meta, xr, x);
+}
+__device__ __forceinline__ float2 h_row_c64_any(const ModelDev& m, const float* sq, float J, int64_t r, int4 nb,
+                                                uint32_t meta, float2 xr, const float2* __restrict__ x) {
+    return m.nhop > 1 ? h_row_c64_x(m, sq, r, nb, meta, xr, x) : h_row_c64_nb(m, sq, J, r, nb, meta, xr, x);
+}
+
+// H 1 of one row: diag + the row sums term by term (total_ham_ones,
+// paces/core/time_evolution.py:403-420), in the order h_row_c128_x sums H x.
+__device__ __forceinline__ double h_ones_row_any(const ModelDev& m, const double* sq, int64_t r, int4 nb,
+                                                 uint32_t meta) {
+    const int n = int((meta >> 8) & 0xffu);
+    double h = diag_value(m, meta);
+    if (m.nhop > 1) {
+        for (int t = 0; t < 2; ++t) {
+            const double Jt = t == 0 ? m.J : m.J2;
+            double hs = 0.0;
+            bool any = false;
+            for (int e = 0; e < m.hop_n[t]; ++e) {
+                if (hop_index(m, r, nb, m.hop_ord[t][e]) < 0) continue;
+                hs = any ? __dadd_rn(hs, Jt) : Jt;
+                any = true;
+            }
+            if (any) h = __dadd_rn(h, hs);
+        }
+    } else {
+        const bool ha = nb.x >= 0, hb = nb.y >= 0;
+        if (ha || hb) h = __dadd_rn(h, (ha && hb) ? __dadd_rn(m.J, m.J) : m.J);
+    }
+    const bool hd = nb.z >= 0, hu = nb.w >= 0;
+    const double cd = sq[n], cu = sq[n + 1];
+    if (hd || hu) h = __dadd_rn(h, (hd && hu) ? __dadd_rn(cd, cu) : (hd ? cd : cu));
+    return h;
+}
+
 }  // namespace paces

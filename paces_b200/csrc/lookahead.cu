@@ -27,17 +27,6 @@ namespace paces {
 
 namespace {
 
-// (H 1)[r]: diag + (hopping row sum) + (vibronic row sum), total_ham_ones' grouping.
-__device__ __forceinline__ double h_ones_row(const ModelDev& m, const double* sq, int4 nb, uint32_t meta) {
-    const int n = int((meta >> 8) & 0xffu);
-    const bool ha = nb.x >= 0, hb = nb.y >= 0, hd = nb.z >= 0, hu = nb.w >= 0;
-    double h = diag_value(m, meta);
-    if (ha || hb) h = __dadd_rn(h, (ha && hb) ? __dadd_rn(m.J, m.J) : m.J);
-    const double cd = sq[n], cu = sq[n + 1];
-    if (hd || hu) h = __dadd_rn(h, (hd && hu) ? __dadd_rn(cd, cu) : (hd ? cd : cu));
-    return h;
-}
-
 template <bool C64>
 __global__ void __launch_bounds__(256) lookahead_kernel(ModelDev m, const int* __restrict__ blk,
                                                         const int* __restrict__ nbr,
@@ -62,17 +51,17 @@ __global__ void __launch_bounds__(256) lookahead_kernel(ModelDev m, const int* _
             if constexpr (C64) {
                 const float2* x = reinterpret_cast<const float2*>(psi);
                 const float2 xr = __ldcg(x + r);
-                const float2 hx = h_row_c64_nb(m, s_sqf, float(m.J), r, nb, mt, xr, x);
+                const float2 hx = h_row_c64_any(m, s_sqf, float(m.J), r, nb, mt, xr, x);
                 const float t = float(tau);
                 out = double(hypotf(xr.x + t * hx.y, xr.y - t * hx.x));
             } else {
                 const double2* x = reinterpret_cast<const double2*>(psi);
                 const double2 xr = __ldcg(x + r);
-                const double2 hx = h_row_c128_nb(m, s_sq, r, nb, mt, xr, x);
+                const double2 hx = h_row_c128_any(m, s_sq, r, nb, mt, xr, x);
                 out = hypot(__dadd_rn(xr.x, __dmul_rn(tau, hx.y)), __dsub_rn(xr.y, __dmul_rn(tau, hx.x)));
             }
         } else {
-            const double h1 = h_ones_row(m, s_sq, nb, mt);
+            const double h1 = h_ones_row_any(m, s_sq, r, nb, mt);
             if (kind == PACES_WEIGHT_HAM_ONES) {
                 out = h1;
             } else {

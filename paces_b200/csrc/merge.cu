@@ -10,10 +10,21 @@ constexpr unsigned long long kLbAgg = 1ull << 62;
 constexpr unsigned long long kLbInc = 2ull << 62;
 constexpr unsigned long long kLbMask = (1ull << 62) - 1;
 
-// Source block of run j of output block p, or -1.
-__device__ __forceinline__ int run_source(const ModelDev& m, int p, int j) {
-    if (j == RUN_FROM_LEFT) return p >= 1 ? p - 1 : (m.periodic ? m.L - 1 : -1);
-    if (j == RUN_FROM_RIGHT) return p + 1 < m.L ? p + 1 : (m.periodic ? 0 : -1);
+// Source block of run j of output block p, or -1.  A hop run reads the block its images come
+// from when that block's hop stays inside its lattice row (the ring wraps instead).
+__device__ __forceinline__ int run_source(const ModelDev& m, const MergeWs& ws, int p, int j) {
+    const int kind = ws.run_kind[j];
+    if (kind == RK_FROM_LOWER) {
+        const int s = p - ws.run_dist[j];
+        if (m.periodic) return s >= 0 ? s : s + m.L;
+        return (s >= 0 && s % ws.run_mod[j] < ws.run_mod[j] - ws.run_dist[j]) ? s : -1;
+    }
+    if (kind == RK_FROM_UPPER) {
+        const int s = p + ws.run_dist[j];
+        if (m.periodic) return s < m.L ? s : s - m.L;
+        return (s < m.L && s % ws.run_mod[j] >= ws.run_dist[j]) ? s : -1;
+    }
+    if (kind == RK_EMPTY) return -1;
     return p;
 }
 
@@ -26,12 +37,13 @@ __device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __re
     k = load_key<NW>(j == RUN_SELF ? X : Y, src);
     flag = 1;
     if (ws.keep && j != RUN_SELF && src < ws.keep_cap && !__ldg(ws.keep + j * ws.keep_cap + src)) flag = 2;
-    if (j == RUN_UP || j == RUN_DOWN) {
+    const int kind = ws.run_kind[j];
+    if (kind == RK_UP || kind == RK_DOWN) {
         const int w = m.word[p];
         const int sh = m.shift[p];
         const uint32_t n = get_field(m, k, p);
         const uint64_t low = sh == 0 ? 0ull : ((uint64_t(1) << sh) - 1);
-        if (j == RUN_UP) {
+        if (kind == RK_UP) {
             if (n + 1 >= m.maxd[p]) {
                 flag = 2;
 #pragma unroll
@@ -197,7 +209,7 @@ __global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, con
     const int L = m.L;
     for (int idx = threadIdx.x; idx < L * kRuns; idx += blockDim.x) {
         const int p = idx / kRuns, j = idx % kRuns;
-        const int src = run_source(m, p, j);
+        const int src = run_source(m, ws, p, j);
         const int* sb = j == RUN_SELF ? x_blk : y_blk;
         int lo = 0, len = 0;
         if (src >= 0) {
@@ -683,8 +695,8 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
         const int q = __ldcs(map + i);
         if (q < 0 || q >= nc) continue;
         auto ok = [&](int s) { return s >= 0 && s < nc; };
-        int sr = (p + 1 < L || m.periodic) ? __ldcs(map + int64_t(RUN_FROM_LEFT) * mc + i) : -1;
-        int sl = (p > 0 || m.periodic) ? __ldcs(map + int64_t(RUN_FROM_RIGHT) * mc + i) : -1;
+        int sr = hop_exists(m, 0, p, 1) ? __ldcs(map + int64_t(RUN_FROM_LEFT) * mc + i) : -1;
+        int sl = hop_exists(m, 0, p, 0) ? __ldcs(map + int64_t(RUN_FROM_RIGHT) * mc + i) : -1;
         int su = __ldcs(map + int64_t(RUN_UP) * mc + i);
         int sd = __ldcs(map + int64_t(RUN_DOWN) * mc + i);
         sr = ok(sr) ? sr : -1;
@@ -746,7 +758,7 @@ int launch_merge_t(int mode, int stride, const ModelDev& m, const uint64_t* X, c
     else launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, out, status, num_sms, st);
     merge_finalize_kernel<<<1, 32, 0, st>>>(m, ws, out, ceiling_out, ceiling_add, mode == MERGE_EXPAND_SPLIT ? 1 : 0,
                                             status);
-    if (mode == MERGE_ASSEMBLE && !split_input) nbr_fill_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, out);
+    if (mode == MERGE_ASSEMBLE && !split_input && out.nbr) nbr_fill_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, out);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
@@ -789,8 +801,8 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
             q = (b >= 0 && b < mc) ? __ldg(maps_s + b) : -1;
         }
         auto ok = [&](int s) { return s >= 0 && s < nc; };
-        int sr = (p + 1 < L || m.periodic) ? img(RUN_FROM_LEFT) : -1;
-        int sl = (p > 0 || m.periodic) ? img(RUN_FROM_RIGHT) : -1;
+        int sr = hop_exists(m, 0, p, 1) ? img(RUN_FROM_LEFT) : -1;
+        int sl = hop_exists(m, 0, p, 0) ? img(RUN_FROM_RIGHT) : -1;
         int su = img(RUN_UP);
         int sd = img(RUN_DOWN);
         if (q < 0 || q >= nc) return;
@@ -819,7 +831,71 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
     if (x < total) fill(x);
 }
 
+// Neighbour table of a lattice with several hopping channels, after the assembly's passes
+// (merge_passes): pass 0 mapped the enlarged basis X (five standard runs) into S_0; pass k >= 1
+// mapped S_{k-1} (its self run) and the images of X under channels 2k-1, 2k into S_k; S is
+// the last S_k.  An index of S_k becomes one of S through the self maps of the later passes.
+// Channel 0 and the phonon neighbours go to the int4 rows, channel c >= 1 to xnbr[c-1].
+struct PassMaps {
+    const int* maps[4];
+    int n;
+};
+
+__global__ void __launch_bounds__(256) nbr_fill_multi_kernel(ModelDev m, const int* __restrict__ x_blk, PassMaps pm,
+                                                             int64_t mc, int* __restrict__ nb, int2* __restrict__ xnb,
+                                                             int64_t nc) {
+    __shared__ int s_blk[kMaxSites + 1];
+    const int L = m.L;
+    for (int i = threadIdx.x; i <= L; i += blockDim.x) s_blk[i] = x_blk[i];
+    __syncthreads();
+    const int nx = s_blk[L];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const int p = block_of(s_blk, L, i);
+        // entry (run j) of pass k for source i, carried to an index of S
+        auto final_index = [&](int k, int j) -> int {
+            int v = __ldcs(pm.maps[k] + int64_t(j) * mc + i);
+            for (int kk = k + 1; kk < pm.n && v >= 0; ++kk) v = v < mc ? __ldg(pm.maps[kk] + v) : -1;
+            return (v >= 0 && v < nc) ? v : -1;
+        };
+        const int q = final_index(0, RUN_SELF);
+        if (q < 0) continue;
+        int4 row;
+        row.x = hop_exists(m, 0, p, 0) ? final_index(0, RUN_FROM_RIGHT) : -1;  // NB_LEFT
+        row.y = hop_exists(m, 0, p, 1) ? final_index(0, RUN_FROM_LEFT) : -1;   // NB_RIGHT
+        row.z = final_index(0, RUN_DOWN);                                      // NB_DOWN
+        row.w = final_index(0, RUN_UP);                                        // NB_UP
+        reinterpret_cast<int4*>(nb)[q] = row;
+        if (row.y >= 0) nb[4 * int64_t(row.y) + NB_LEFT] = q;
+        if (row.x >= 0) nb[4 * int64_t(row.x) + NB_RIGHT] = q;
+        if (row.w >= 0) nb[4 * int64_t(row.w) + NB_DOWN] = q;
+        if (row.z >= 0) nb[4 * int64_t(row.z) + NB_UP] = q;
+        for (int c = 1; c < m.nhop; ++c) {
+            const int k = 1 + (c - 1) / 2;
+            const int jl = (c - 1) % 2 == 0 ? 1 : 3;  // the pass's from-below run of channel c; from-above next
+            int2 e;
+            e.y = hop_exists(m, c, p, 1) ? final_index(k, jl) : -1;      // the +dist image: upper neighbour
+            e.x = hop_exists(m, c, p, 0) ? final_index(k, jl + 1) : -1;  // the -dist image: lower neighbour
+            int2* t = xnb + int64_t(c - 1) * nc;
+            t[q] = e;
+            if (e.y >= 0) reinterpret_cast<int*>(t + e.y)[0] = q;
+            if (e.x >= 0) reinterpret_cast<int*>(t + e.x)[1] = q;
+        }
+    }
+}
+
 }  // namespace
+
+int launch_nbr_fill_multi(const ModelDev& m, const int* x_blk, const int* const* pass_maps, int passes, int64_t map_cap,
+                          int* nbr, int* xnbr, int64_t nbr_cap, int num_sms, cudaStream_t st) {
+    if (passes < 1 || passes > 4 || !xnbr) return PACES_ERR_BADARG;
+    PassMaps pm{};
+    for (int k = 0; k < passes; ++k) pm.maps[k] = pass_maps[k];
+    pm.n = passes;
+    if (cudaMemsetAsync(xnbr, 0xff, size_t(m.nhop - 1) * size_t(nbr_cap) * 8, st) != cudaSuccess) return PACES_ERR_CUDA;
+    nbr_fill_multi_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, pm, map_cap, nbr, reinterpret_cast<int2*>(xnbr),
+                                                       nbr_cap);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
+}
 
 int launch_merge(int nw, int mode, int stride, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                  const uint64_t* y_keys, const int* y_blk, const MergeWs& ws, const MergeOut& out,

@@ -49,7 +49,44 @@ struct MergeWs {
     // ceiling holes (after real elements with the same key) and are never emitted
     const uint8_t* keep;
     int64_t keep_cap;
+    // what each run is (run 0 is always the self run): see RunKind; hop runs carry their
+    // channel's distance and boundary period
+    int run_kind[kRuns];
+    int run_dist[kRuns];
+    int run_mod[kRuns];
 };
+
+// FROM_LOWER: the images of block p - dist under the +dist hop; FROM_UPPER: of block p + dist
+// under the -dist hop; UP / DOWN: one phonon more / less at the exciton site; EMPTY: no run.
+enum RunKind : int { RK_SELF = 0, RK_FROM_LOWER = 1, RK_FROM_UPPER = 2, RK_UP = 3, RK_DOWN = 4, RK_EMPTY = 5 };
+
+// The standard runs: self, channel 0 from below and above, phonon up and down (the whole
+// Hamiltonian of the chain).
+inline void merge_spec_standard(MergeWs& w, const ModelDev& m) {
+    const int kinds[kRuns] = {RK_SELF, RK_FROM_LOWER, RK_FROM_UPPER, RK_UP, RK_DOWN};
+    for (int j = 0; j < kRuns; ++j) {
+        w.run_kind[j] = kinds[j];
+        w.run_dist[j] = m.hop_dist[0];
+        w.run_mod[j] = m.hop_mod[0];
+    }
+}
+
+// Self run plus the hop channels ca and cb (cb < 0: none) from below and above.
+inline void merge_spec_hops(MergeWs& w, const ModelDev& m, int ca, int cb) {
+    w.run_kind[0] = RK_SELF;
+    w.run_kind[1] = RK_FROM_LOWER;
+    w.run_kind[2] = RK_FROM_UPPER;
+    w.run_kind[3] = cb >= 0 ? RK_FROM_LOWER : RK_EMPTY;
+    w.run_kind[4] = cb >= 0 ? RK_FROM_UPPER : RK_EMPTY;
+    for (int j = 0; j < kRuns; ++j) {
+        const int ch = j <= 2 ? ca : (cb >= 0 ? cb : ca);
+        w.run_dist[j] = m.hop_dist[ch];
+        w.run_mod[j] = m.hop_mod[ch];
+    }
+}
+
+// Merge passes that cover every channel: the standard pass, then one per two further channels.
+inline int merge_passes(const ModelDev& m) { return 1 + (m.nhop - 1 + 1) / 2; }
 
 struct MergeOut {
     uint64_t* keys;
@@ -102,6 +139,11 @@ inline int64_t merge_tile_cap(int64_t split_cap, int L) { return split_cap / kMe
 int launch_merge(int nw, int mode, int stride, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                  const uint64_t* y_keys, const int* y_blk, const MergeWs& ws, const MergeOut& out,
                  int* ceiling_out, int ceiling_add, int* status, int num_sms, cudaStream_t st);
+
+// Neighbour table of a lattice with several hopping channels after the assembly's passes
+// (pass_maps[k]: the maps of pass k; see nbr_fill_multi_kernel).  xnbr: [nhop-1][nbr_cap] int2.
+int launch_nbr_fill_multi(const ModelDev& m, const int* x_blk, const int* const* pass_maps, int passes, int64_t map_cap,
+                          int* nbr, int* xnbr, int64_t nbr_cap, int num_sms, cudaStream_t st);
 
 // Neighbour table after a split expansion (maps_e, new part N with new_to_out) and the
 // assembly of its output with the images of N (maps_s): every state of the expansion's

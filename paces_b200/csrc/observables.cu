@@ -25,7 +25,7 @@ constexpr int kOThreads = 256;
 constexpr int kOWarps = kOThreads / 32;
 constexpr int kFpwMax = 16;  // register fast path: fields of >= 4 bits, at most 16 per word
 
-template <bool C64>
+template <bool C64, bool XHOP>
 __global__ void __launch_bounds__(kOThreads, 4)
 obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nbr, int64_t cap,
                   const uint32_t* __restrict__ meta, const void* __restrict__ psi, double* __restrict__ part) {
@@ -47,11 +47,11 @@ obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict
         const double zr = double(z.x), zi = double(z.y);
         double yr, yi;
         if constexpr (C64) {
-            const float2 y = h_row_c64_nb(m, s_sq, J, r, nb, mm, z, x);
+            const float2 y = XHOP ? h_row_c64_x(m, s_sq, r, nb, mm, z, x) : h_row_c64_nb(m, s_sq, J, r, nb, mm, z, x);
             yr = y.x;
             yi = y.y;
         } else {
-            const double2 y = h_row_c128_nb(m, s_sq, r, nb, mm, z, x);
+            const double2 y = XHOP ? h_row_c128_x(m, s_sq, r, nb, mm, z, x) : h_row_c128_nb(m, s_sq, r, nb, mm, z, x);
             yr = y.x;
             yi = y.y;
         }
@@ -284,8 +284,8 @@ __global__ void __launch_bounds__(kOThreads) apply_h_kernel(ModelDev m, const in
     C* y = reinterpret_cast<C*>(yout);
     for (int64_t r = int64_t(blockIdx.x) * kOThreads + threadIdx.x; r < S; r += int64_t(gridDim.x) * kOThreads) {
         const uint32_t mm = __ldg(meta + r);
-        if constexpr (C64) y[r] = h_row_c64(m, s_sq, float(m.J), r, nbr, mm, x);
-        else y[r] = h_row_c128(m, s_sq, r, nbr, mm, x);
+        if constexpr (C64) y[r] = h_row_c64_any(m, s_sq, float(m.J), r, load_nbr(nbr, r), mm, __ldcg(x + r), x);
+        else y[r] = h_row_c128_any(m, s_sq, r, load_nbr(nbr, r), mm, __ldcg(x + r), x);
     }
 }
 
@@ -320,9 +320,10 @@ template <int NW, bool C64>
 int launch_obs_t(const ModelDev& m, const uint64_t* keys, const int* blk, const int* nbr,
                  int64_t nbr_cap, const uint32_t* meta, const void* psi, int what, double* partials,
                  const ObsTarget& out, int num_sms, cudaStream_t st) {
-    static int grid_e = 0, grid_s = 0;
+    static int grid_e = 0, grid_ex = 0, grid_s = 0;
     if (grid_e == 0) {
-        grid_e = wave_blocks(obs_energy_kernel<C64>, num_sms);
+        grid_e = wave_blocks(obs_energy_kernel<C64, false>, num_sms);
+        grid_ex = wave_blocks(obs_energy_kernel<C64, true>, num_sms);
         grid_s = wave_blocks(obs_sites_kernel<NW, C64>, num_sms);
     }
     const bool energy = (what & PACES_OBS_ENERGY) != 0;
@@ -331,8 +332,13 @@ int launch_obs_t(const ModelDev& m, const uint64_t* keys, const int* blk, const 
     double* part_s = partials + size_t(obs_max_grid(num_sms)) * 3;
     int nb_e = 0, nb_s = 0;
     if (energy || !sites) {
-        obs_energy_kernel<C64><<<grid_e, kOThreads, 0, st>>>(m, blk, nbr, nbr_cap, meta, psi, part_e);
-        nb_e = grid_e;
+        if (m.nhop > 1) {
+            obs_energy_kernel<C64, true><<<grid_ex, kOThreads, 0, st>>>(m, blk, nbr, nbr_cap, meta, psi, part_e);
+            nb_e = grid_ex;
+        } else {
+            obs_energy_kernel<C64, false><<<grid_e, kOThreads, 0, st>>>(m, blk, nbr, nbr_cap, meta, psi, part_e);
+            nb_e = grid_e;
+        }
     }
     if (sites) {
         int ub = m.bits[0];

@@ -56,7 +56,8 @@ constexpr uint32_t chunk_bytes() {  // neighbour rows, metadata, result, own ter
     return uint32_t(kChunk) * (16 + 4 + 2 * (C64 ? 8 : 16));
 }
 
-template <bool C64, bool BULK>
+// XHOP: a lattice with several hopping channels (the channel loop of h_row_*_x).
+template <bool C64, bool BULK, bool XHOP>
 __global__ void __launch_bounds__(kTThreads, C64 ? 4 : 3)
 taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ nbr, int64_t cap,
               const uint32_t* __restrict__ meta, const void* v_in, void* res_out, TaylorWs ws,
@@ -101,8 +102,13 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
         double mx[4] = {0.0, 0.0, 0.0, 0.0};  // |term|, |res|, |v|, non-finite
         auto hrow = [&](int64_t r) -> C {
             const uint32_t mm = __ldg(meta + r);
-            if constexpr (C64) return h_row_c64(m, s_sq, J, r, nbr, mm, src);
-            else return h_row_c128(m, s_sq, r, nbr, mm, src);
+            if constexpr (XHOP) {
+                if constexpr (C64) return h_row_c64_x(m, s_sq, r, load_nbr(nbr, r), mm, __ldcg(src + r), src);
+                else return h_row_c128_x(m, s_sq, r, load_nbr(nbr, r), mm, __ldcg(src + r), src);
+            } else {
+                if constexpr (C64) return h_row_c64(m, s_sq, J, r, nbr, mm, src);
+                else return h_row_c128(m, s_sq, r, nbr, mm, src);
+            }
         };
         auto finish = [&](int64_t r, const C& y, const C& a) {
             C t, rr;
@@ -174,7 +180,15 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                     const C* srin = reinterpret_cast<const C*>(base + kOffRin);
                     const C* sself = reinterpret_cast<const C*>(base + kOffSelf);
                     C y0, y1;
-                    if constexpr (C64) {
+                    if constexpr (XHOP) {
+                        if constexpr (C64) {
+                            y0 = h_row_c64_x(m, s_sq, r0 + t0, snb[t0], smeta[t0], sself[t0], src);
+                            y1 = h_row_c64_x(m, s_sq, r0 + t1, snb[t1], smeta[t1], sself[t1], src);
+                        } else {
+                            y0 = h_row_c128_x(m, s_sq, r0 + t0, snb[t0], smeta[t0], sself[t0], src);
+                            y1 = h_row_c128_x(m, s_sq, r0 + t1, snb[t1], smeta[t1], sself[t1], src);
+                        }
+                    } else if constexpr (C64) {
                         y0 = h_row_c64_nb(m, s_sq, J, r0 + t0, snb[t0], smeta[t0], sself[t0], src);
                         y1 = h_row_c64_nb(m, s_sq, J, r0 + t1, snb[t1], smeta[t1], sself[t1], src);
                     } else {
@@ -249,11 +263,11 @@ size_t dyn_smem() {
     return BULK ? size_t(2) * chunk_bytes<C64>() : 0;
 }
 
-template <bool C64, bool BULK>
+template <bool C64, bool BULK, bool XHOP>
 int occupancy() {
     static int cached = 0;  // per process: the kernels' resources do not change
     if (cached) return cached;
-    auto kfn = taylor_kernel<C64, BULK>;
+    auto kfn = taylor_kernel<C64, BULK, XHOP>;
     if (BULK) cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn_smem<C64, BULK>()));
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTThreads, dyn_smem<C64, BULK>());
@@ -262,16 +276,35 @@ int occupancy() {
 }
 
 template <bool C64>
-int occupancy_any(int variant) {
-    return variant == 1 ? occupancy<C64, true>() : occupancy<C64, false>();
+int occupancy_any(int variant, bool xhop) {
+    if (xhop) return variant == 1 ? occupancy<C64, true, true>() : occupancy<C64, false, true>();
+    return variant == 1 ? occupancy<C64, true, false>() : occupancy<C64, false, false>();
+}
+
+template <bool C64, bool BULK, bool XHOP>
+cudaError_t launch_one(const cudaLaunchConfig_t& cfg, const ModelDev& m, const int* blk, const int* nbr, int64_t cap,
+                       const uint32_t* meta, const void* v_in, void* res, const TaylorWs& ws, double dt, int m_star,
+                       double tol, const TaylorOut& out, int* status) {
+    if (BULK) {  // the attribute belongs to the current device: set it on every launch
+        const cudaError_t a = cudaFuncSetAttribute(taylor_kernel<C64, BULK, XHOP>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   int(dyn_smem<C64, BULK>()));
+        if (a != cudaSuccess) return a;
+    }
+    return cudaLaunchKernelEx(&cfg, taylor_kernel<C64, BULK, XHOP>, m, blk, nbr, cap, meta, v_in, res, ws, dt, m_star,
+                              tol, out, status);
 }
 
 }  // namespace
 
 int taylor_max_grid(bool c64, int num_sms) {
-    const int a = c64 ? occupancy<true, false>() : occupancy<false, false>();
-    const int b = c64 ? occupancy<true, true>() : occupancy<false, true>();
-    return num_sms * (a > b ? a : b);
+    int best = 0;
+    for (int v = 0; v < 2; ++v)
+        for (int x = 0; x < 2; ++x) {
+            const int o = c64 ? occupancy_any<true>(v, x != 0) : occupancy_any<false>(v, x != 0);
+            best = o > best ? o : best;
+        }
+    return num_sms * best;
 }
 
 int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,
@@ -279,17 +312,11 @@ int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, i
                   double tol, const TaylorWs& ws, const TaylorOut& out, int* status, int num_sms,
                   int blocks_per_sm, int variant, cudaStream_t st) {
     if (m_star < 1 || variant < 0 || variant > 1) return PACES_ERR_BADARG;
+    if (m.nhop > 1 && !m.xnbr) return PACES_ERR_BADARG;
     if (cudaMemsetAsync(ws.barrier, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return PACES_ERR_CUDA;
-    const int occ = c64 ? occupancy_any<true>(variant) : occupancy_any<false>(variant);
+    const bool xhop = m.nhop > 1;
+    const int occ = c64 ? occupancy_any<true>(variant, xhop) : occupancy_any<false>(variant, xhop);
     const int grid = num_sms * (blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ);
-    if (variant == 1) {  // the attribute belongs to the current device: set it on every launch
-        const cudaError_t a =
-            c64 ? cudaFuncSetAttribute(taylor_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(dyn_smem<true, true>()))
-                : cudaFuncSetAttribute(taylor_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(dyn_smem<false, true>()));
-        if (a != cudaSuccess) return PACES_ERR_CUDA;
-    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kTThreads);
@@ -302,16 +329,15 @@ int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, i
     cfg.numAttrs = 1;
     const int64_t cap = nbr_cap;
     cudaError_t e;
-    if (c64)
-        e = variant == 1 ? cudaLaunchKernelEx(&cfg, taylor_kernel<true, true>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
-                                              m_star, tol, out, status)
-                         : cudaLaunchKernelEx(&cfg, taylor_kernel<true, false>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
-                                              m_star, tol, out, status);
-    else
-        e = variant == 1 ? cudaLaunchKernelEx(&cfg, taylor_kernel<false, true>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
-                                              m_star, tol, out, status)
-                         : cudaLaunchKernelEx(&cfg, taylor_kernel<false, false>, m, blk, nbr, cap, meta, v_in, res, ws, dt,
-                                              m_star, tol, out, status);
+#define PACES_TAYLOR_ONE(C, B, X) launch_one<C, B, X>(cfg, m, blk, nbr, cap, meta, v_in, res, ws, dt, m_star, tol, out, status)
+    if (c64) {
+        if (xhop) e = variant == 1 ? PACES_TAYLOR_ONE(true, true, true) : PACES_TAYLOR_ONE(true, false, true);
+        else e = variant == 1 ? PACES_TAYLOR_ONE(true, true, false) : PACES_TAYLOR_ONE(true, false, false);
+    } else {
+        if (xhop) e = variant == 1 ? PACES_TAYLOR_ONE(false, true, true) : PACES_TAYLOR_ONE(false, false, true);
+        else e = variant == 1 ? PACES_TAYLOR_ONE(false, true, false) : PACES_TAYLOR_ONE(false, false, false);
+    }
+#undef PACES_TAYLOR_ONE
     return e == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 

@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
 }
 
 __global__ void trunc_finalize_kernel(ModelDev m, const int* __restrict__ x_blk, int64_t maxstates,
-                                      TruncWs ws, int* out_blk, int64_t out_cap, int* n_tied_out,
+                                      TruncWs ws, int* out_blk, int64_t out_cap, int* n_tied_out, int* n_kept_out,
                                       float* cut_out, int* status) {
     if (threadIdx.x != 0) return;
     // the cut: |psi| of the smallest kept state when states were dropped, else 0
@@ -489,12 +489,13 @@ __global__ void trunc_finalize_kernel(ModelDev m, const int* __restrict__ x_blk,
     for (int p = L - 1; p >= 0; --p)
         if (x_blk[p] == x_blk[p + 1]) out_blk[p] = out_blk[p + 1];
     if (n_tied_out) *n_tied_out = int(ws.sel[SEL_ALL] ? 0 : ws.sel[SEL_TIES]);
+    if (n_kept_out) *n_kept_out = int(total);
 }
 
 template <int NW, int WK>
 int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_blk, const void* psi,
                       int64_t maxstates, int shuffle, uint64_t seed, uint64_t step, const TruncWs& ws,
-                      uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w, int* n_tied_out,
+                      uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w, int* n_tied_out, int* n_kept_out,
                       int* status, int num_sms, cudaStream_t st) {
     const int g = num_sms * 4;
     const int rounds = weight_rounds(WK);
@@ -515,7 +516,7 @@ int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_bl
     trunc_scan_kernel<<<1, 1024, 0, st>>>(ws);
     trunc_write_kernel<NW, WK><<<g, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
                                                    out_blk, out_cap, out_w, status);
-    trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out,
+    trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out, n_kept_out,
                                             out_w ? out_w + out_cap : nullptr, status);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
@@ -524,15 +525,15 @@ template <int NW>
 int dispatch_prec(bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                   const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed,
                   uint64_t step, const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
-                  float* out_w, int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
+                  float* out_w, int* n_tied_out, int* n_kept_out, int* status, int num_sms, cudaStream_t st) {
     if (weights)
         return launch_truncate_t<NW, 2>(m, x_keys, x_blk, weights, maxstates, shuffle, seed, step, ws,
-                                        out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
+                                        out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
     if (c64)
         return launch_truncate_t<NW, 1>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
-                                        out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
+                                        out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
     return launch_truncate_t<NW, 0>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
-                                    out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
+                                    out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
 }
 
 }  // namespace
@@ -540,11 +541,11 @@ int dispatch_prec(bool c64, const ModelDev& m, const uint64_t* x_keys, const int
 int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                     const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
                     const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
-                    int* n_tied_out, int* status, int num_sms, cudaStream_t st) {
+                    int* n_tied_out, int* n_kept_out, int* status, int num_sms, cudaStream_t st) {
 #define PACES_TRUNC_CASE(N)                                                                       \
     case N:                                                                                       \
         return dispatch_prec<N>(c64, m, x_keys, x_blk, psi, weights, maxstates, shuffle, seed, step, ws,   \
-                                out_keys, out_blk, out_cap, out_w, n_tied_out, status, num_sms, st);
+                                out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
     switch (nw) {
         PACES_TRUNC_CASE(1)
         PACES_TRUNC_CASE(2)

@@ -51,6 +51,6 @@ inline int trunc_launches(int wk, bool shuffle) { return 5 + 2 * weight_rounds(w
 int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
                     const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
                     const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
-                    int* n_tied_out, int* status, int num_sms, cudaStream_t st);
+                    int* n_tied_out, int* n_kept_out, int* status, int num_sms, cudaStream_t st);
 
 }  // namespace paces

@@ -32,6 +32,8 @@ class ModelParams:
     periodic: bool = False
     site_eps: list | None = None
     precision: str = "c128"   # "c128" (reference precision) or "c64"
+    geo_dim: int = 1          # lattice dimensions (holstein.py:24-51); nchain = l ** geo_dim
+    J2: float | None = None   # the next-nearest-neighbour "hopping2" term (holstein.py:234-240)
 
 
 def _ptr(t):
@@ -74,15 +76,21 @@ class DevBasis:
 
 
 class DevHMat:
-    """Neighbour table [cap, 4] (left, right, down, up; -1 = absent) and row metadata [cap]."""
+    """Neighbour table [cap, 4] (left, right, down, up; -1 = absent) and row metadata [cap];
+    for lattices with more hopping channels also xnbr [nhop-1, cap, 2] (the other channels'
+    lower and upper neighbours)."""
 
     def __init__(self, eng: "Engine", cap: int):
         self.cap = int(cap)
         self.nbr = torch.empty((max(self.cap, 1), 4), dtype=torch.int32, device=eng.device)
         self.meta = torch.empty(max(self.cap, 1), dtype=torch.int32, device=eng.device)
+        self.xnbr = None
+        if eng.nhop > 1:
+            self.xnbr = torch.empty((eng.nhop - 1, max(self.cap, 1), 2), dtype=torch.int32, device=eng.device)
 
     def c(self):
-        return nat.HMat(self.nbr.data_ptr(), self.meta.data_ptr(), self.cap)
+        return nat.HMat(self.nbr.data_ptr(), self.meta.data_ptr(), self.cap,
+                        self.xnbr.data_ptr() if self.xnbr is not None else None)
 
 
 class Engine:
@@ -105,13 +113,16 @@ class Engine:
         desc = nat.ModelDesc(self.L, 1 if params.periodic else 0, nat.C64 if self.c64 else nat.C128, 0,
                              dims, float(params.eps_sys), float(params.hbar_omega),
                              float(params.delta_eps), float(params.J), float(params.g),
-                             site if site is not None else ctypes.POINTER(ctypes.c_double)())
+                             site if site is not None else ctypes.POINTER(ctypes.c_double)(),
+                             int(params.geo_dim), 0 if params.J2 is None else 1,
+                             0.0 if params.J2 is None else float(params.J2))
         self._dims, self._site = dims, site
         ctx = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             nat.check(self.lib.paces_create(ctypes.byref(desc), ctypes.byref(ctx)), None, "paces_create")
         self.ctx = ctx
         self.nw = self.lib.paces_key_words(ctx)
+        self.nhop = int(self.lib.paces_hop_channels(ctx))  # hopping channels (1: the chain)
         self.ref_words = self.lib.paces_ref_words(ctx)
         self.cap = 0
         self.ws = None
@@ -465,7 +476,10 @@ class Trajectory:
         n = old_b.count()
         e._grow(int(e.cap * factor))
         keep_keys, keep_blk, keep_psi = old_b.keys[:n].clone(), old_b.blk.clone(), old_psi[:n].clone()
-        keep_h = (old_h.nbr[:n].clone(), old_h.meta[:n].clone()) if self._h_valid and self.weighting else None
+        keep_h = None
+        if self._h_valid and self.weighting:
+            keep_h = (old_h.nbr[:n].clone(), old_h.meta[:n].clone(),
+                      None if old_h.xnbr is None else old_h.xnbr[:, :n].clone())
         valid = self._h_valid
         self._alloc()
         b = self.bases[self.cur]
@@ -475,6 +489,8 @@ class Trajectory:
         if keep_h is not None:
             self.hs[self.cur].nbr[:n] = keep_h[0]
             self.hs[self.cur].meta[:n] = keep_h[1]
+            if keep_h[2] is not None:
+                self.hs[self.cur].xnbr[:, :n] = keep_h[2]
         self._h_valid = valid and keep_h is not None
 
     def set_state(self, basis: DevBasis, psi):

@@ -26,6 +26,7 @@ from ..core.observables import ObservablesFramework
 from ..core.time_evolution import TimeEvolutionFramework
 
 _DEVICE_TERMS = {"diag", "hopping", "vib_coupling"}
+_OPTIONAL_TERMS = {"hopping2"}
 
 
 class Hamiltonian(HamiltonianFramework):
@@ -40,22 +41,26 @@ class Hamiltonian(HamiltonianFramework):
         self.lattice_l = int(numpy.round(nchain ** (1 / geo_dim)))
         if self.lattice_l ** geo_dim != nchain:
             raise ValueError(f"Number of sites {nchain} is incompatible with dimension {geo_dim}.")
-        if geo_dim != 1:
-            raise NotImplementedError("the device path implements the 1D chain (geo_dim=1)")
+        if geo_dim > 3:
+            raise NotImplementedError("the device path implements lattices of up to 3 dimensions")
         super().__init__(max_dims=max_dims, **kwargs)
         self.input_args["nchain"] = nchain
         self.input_args["max_ho_dims"] = max_ho_dims
         self.input_args["geo_dim"] = geo_dim
         terms = set(self.use_terms)
-        if terms != _DEVICE_TERMS:
-            raise NotImplementedError(f"the device path implements exactly the terms {sorted(_DEVICE_TERMS)}; "
-                                      f"got {sorted(terms)}")
+        if not (_DEVICE_TERMS <= terms <= _DEVICE_TERMS | _OPTIONAL_TERMS):
+            raise NotImplementedError(f"the device path implements the terms {sorted(_DEVICE_TERMS)} (and optionally "
+                                      f"{sorted(_OPTIONAL_TERMS)}); got {sorted(terms)}")
+        if "hopping2" in terms and self.lattice_l - 1 < 2:
+            raise ValueError("Invalid value for base_order of hopping operator.")
         self.posbitwidth = int(self.bitwidths_v[0])
         self.qhobitwidth_v = self.bitwidths_v[1:]
         self.qhobitwidth_w = self.qhobitwidth_v
         self.periodic = bool(periodic)
         if self.periodic and nchain < 3:
             raise ValueError("a periodic chain needs at least 3 sites")
+        if self.periodic and (geo_dim != 1 or "hopping2" in terms):
+            raise NotImplementedError("Periodic hopping not yet implemented.")
 
     def native_model(self):
         from ..engine import ModelParams
@@ -66,7 +71,10 @@ class Hamiltonian(HamiltonianFramework):
                            eps_sys=float(d["eps_sys"]), hbar_omega=float(d["hbar_omega"]),
                            delta_eps=float(d.get("delta_eps", 0.0)), periodic=self.periodic,
                            site_eps=d.get("site_eps"),
-                           precision="c64" if self.complex_type == numpy.complex64 else "c128")
+                           precision="c64" if self.complex_type == numpy.complex64 else "c128",
+                           geo_dim=int(self.geo_dim),
+                           J2=float(numpy.real(self.use_terms["hopping2"]["J2"])) if "hopping2" in self.use_terms
+                           else None)
 
     # ---- fields (paces/models/holstein.py:68-147) ------------------------------------------
     def get_phonon_occ(self, arr, site):
@@ -126,24 +134,43 @@ class Hamiltonian(HamiltonianFramework):
         idx = self.searchsorted(cupy_unique(plus_inds), basis_states, allow_escapes=True)
         return idx < 0
 
-    def _generate_mel_hopping(self, basis_states, t_sys, raw_map_to=False):
+    def _generate_mel_hopping(self, basis_states, t_sys, base_order=1, cur_dim=0, raw_map_to=False):
+        """Hop images of one channel (paces/models/holstein.py:150-207): the exciton moves by
+        base_order * l**cur_dim and, with open boundaries, stays in its row of the lattice."""
+        if base_order < 1 or base_order > self.lattice_l - 1:
+            raise ValueError("Invalid value for base_order of hopping operator.")
         pos = layout.get_field_t(layout.rows_i64(basis_states), self._fields, 0)
-        L = self.nchain
-        plus_mask = torch.ones_like(pos, dtype=torch.bool) if self.periodic else pos < L - 1
-        minus_mask = torch.ones_like(pos, dtype=torch.bool) if self.periodic else pos > 0
-        plus_inds = self._shift_pos(basis_states[plus_mask], +1)
-        minus_all = self._shift_pos(basis_states[minus_mask], -1)
+        block = self.lattice_l ** (cur_dim + 1)
+        order = base_order * self.lattice_l ** cur_dim
+        if self.periodic:
+            plus_mask = torch.ones_like(pos, dtype=torch.bool)
+            minus_mask = torch.ones_like(pos, dtype=torch.bool)
+        else:
+            plus_mask = pos % block < block - order
+            minus_mask = pos % block > order - 1
+        plus_inds = self._shift_pos(basis_states[plus_mask], +order)
+        minus_all = self._shift_pos(basis_states[minus_mask], -order)
         if raw_map_to:
             return [plus_inds, minus_all]
         keep = self._o_star(basis_states, plus_inds)
         mm = minus_mask & keep
-        minus_inds = self._shift_pos(basis_states[mm], -1)
+        minus_inds = self._shift_pos(basis_states[mm], -order)
         return [MelTriple(plus_inds, t_sys, plus_mask), MelTriple(minus_inds, numpy.conjugate(t_sys), mm)]
+
+    def _hopping_dim_wrapper(self, basis_states, t_sys, order, raw_map_to):
+        """One channel per lattice dimension (paces/models/holstein.py:210-222)."""
+        res = self._generate_mel_hopping(basis_states, t_sys, order, raw_map_to=raw_map_to)
+        for d in range(1, self.geo_dim):
+            res += self._generate_mel_hopping(basis_states, t_sys, base_order=order, cur_dim=d, raw_map_to=raw_map_to)
+        return res if raw_map_to else (res, None)
 
     def generate_mel_hopping(self, basis_states, raw_map_to=False):
         """Nearest-neighbour hopping (paces/models/holstein.py:225-231)."""
-        res = self._generate_mel_hopping(basis_states, self.use_terms["hopping"]["J"], raw_map_to=raw_map_to)
-        return res if raw_map_to else (res, None)
+        return self._hopping_dim_wrapper(basis_states, self.use_terms["hopping"]["J"], 1, raw_map_to)
+
+    def generate_mel_hopping2(self, basis_states, raw_map_to=False):
+        """Next-nearest-neighbour hopping (paces/models/holstein.py:234-240)."""
+        return self._hopping_dim_wrapper(basis_states, self.use_terms["hopping2"]["J2"], 2, raw_map_to)
 
     @debug_lister(["ceiling_hits"])
     def generate_mel_vib_coupling(self, basis_states, raw_map_to=False):
