@@ -14,9 +14,9 @@
 // Taylor term; it runs once per step, before the truncation's radix select.
 //
 // Bit-exactness (complex128): every product and sum is rounded separately (no fused
-// multiply-add) in the reference's order.  The row sums need no order: each term matrix
-// has at most two elements in a row (hopping: left and right; vibronic: one phonon less
-// and one more), and a sum of two doubles does not depend on their order.  The product
+// multiply-add) in the reference's order.  The row sums need no order: the vibronic
+// matrix has at most two elements in a row, and every element of a hopping term's row is
+// the same J, so any order of their sum rounds alike.  The product
 // 1j * tau * Hpsi has the real part 0 * Re(Hpsi) - tau * Im(Hpsi) = -(tau * Im(Hpsi)) and
 // the imaginary part tau * Re(Hpsi), exactly, whatever the evaluation order.
 #include "kernels.cuh"

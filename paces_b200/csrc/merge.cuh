@@ -13,6 +13,8 @@
 //   FROM_RIGHT X_{p+1}                  (left hops)
 //   UP         X_p with n_p + 1         (b^dagger at the exciton site; ceiling n_p = maxd-1 is a hole)
 //   DOWN       X_p with n_p - 1         (b at the exciton site; floor n_p = 0 is a hole)
+// Lattices with more hopping channels (geo_dim > 1, hopping2) run further passes whose
+// runs are the previous output and two more channels' images (RunKind, merge_passes).
 // An expansion may also take a keep mask over the images (the learned proposal): a
 // dropped image keeps its key and sorts like a ceiling hole, so it is never emitted.
 // A hole keeps a placeholder key that preserves the run's order (DOWN: fields after p
