@@ -587,7 +587,7 @@ class Trajectory:
         psi = self.psis[self.cur]
         _, _, dbar = e.hnorms(b, h)
         _, a1, _ = e.hnorms(b, h, shift=dbar)
-        m, s = expm.choose(dt * a1)
+        m, s = expm.choose(dt * a1, d=lambda p: self._norm_power(dt, dbar, p))
         eta = np.exp(dt * 1j * dbar / s)
         out = self.psis[1 - self.cur]
         dbg = e.expm_scaled(b, h, psi, out, dt, dbar, m, s, eta, tol=expm.TOL if not e.c64 else e.tol)
@@ -608,6 +608,37 @@ class Trajectory:
             raise RuntimeError(f"Norm has exceeded preset explosion cutoff value ({self.explosion_cutoff})!")
         self.last = rec
         return rec
+
+    def _norm_power(self, dt, dbar, p):
+        """||(dt A)^p||_1^(1/p) for A = 1j (H - dbar I) on the current basis, by the block
+        1-norm estimator (expm.onenormest) with every product on the device H rows."""
+        from . import expm
+        e, b, h = self.eng, self.basis, self.h
+        n = b.count()
+        cap = max(b.cap, 1)
+        xin = torch.zeros(cap, dtype=e.cdtype, device=e.device)
+        yout = torch.empty(cap, dtype=e.cdtype, device=e.device)
+
+        def apply(X, sign):
+            out = torch.empty_like(X)
+            for j in range(X.shape[1]):
+                xin[:n] = X[:, j].to(e.cdtype)
+                e.apply_h(b, h, xin, yout)
+                hx = yout[:n].to(torch.complex128)
+                out[:, j] = (sign * 1j * dt) * (hx - dbar * X[:, j])
+            return out
+
+        def power(X, sign):
+            for _ in range(p):
+                X = apply(X, sign)
+            return X
+
+        if not hasattr(self, "_norm_gen"):
+            self._norm_gen = torch.Generator(device=e.device)
+            self._norm_gen.manual_seed(0x5EED)
+        est = expm.onenormest(lambda X: power(X, 1.0), lambda X: power(X, -1.0), n, t=expm.ELL, itmax=5,
+                              generator=self._norm_gen, device=e.device)
+        return est ** (1.0 / p)
 
     def step(self, evolve=True, dt=0.0, weighted=None):
         """One time step (first step: evolve=False).  Returns the step record.  `weighted`

@@ -20,6 +20,7 @@ Fixtures written:
   scaled_n8c16.npz    a trajectory propagated with ExpmParams(use_scaling=True)
   tau_<weighting>_n8c16.npz  trajectories truncated by the look-ahead weights (tau=0.2)
   lattice_<name>.npz  geo_dim > 1 lattices and the hopping2 term (open boundaries)
+  fragment31.npz      (m, s) of code fragment 3.1 for synthetic norms and norm estimates
 """
 
 import argparse
@@ -405,6 +406,24 @@ def gen_lattice(paces, name, cfg, workdir):
                                          initpos], dtype=np.float64))
 
 
+def gen_fragment(paces, workdir):
+    """Code fragment 3.1 of Al-Mohy and Higham (paces/aux/_scipy/_expm_multiply.py:395-450)
+    on synthetic norm data: t ||A||_1 and the 1-norm estimates d(p) = ||A^p||^(1/p) (the
+    estimator is bypassed, so the choice is deterministic).  Stores (m, s) per case."""
+    from paces.aux._scipy import _expm_multiply as em
+    rng = np.random.default_rng(7)
+    cases, out = [], []
+    for a1 in (5.0, 40.0, 63.0, 64.0, 80.0, 150.0, 400.0, 1000.0):
+        for decay in (1.0, 0.8, 0.5, 0.2):
+            d = {p: a1 * decay ** (p - 1) * (1 + 0.05 * rng.random()) for p in range(2, 11)}
+            info = em.LazyOperatorNormInfo(None, A_1_norm=a1)
+            info._d = dict(d)
+            m, s = em._fragment_3_1(info, 1, 2.0 ** -53)
+            cases.append([a1] + [d[p] for p in range(2, 11)])
+            out.append([m, s])
+    np.savez_compressed(os.path.join(HERE, "fragment31.npz"), cases=np.array(cases), choice=np.array(out))
+
+
 def gen_ed(paces, workdir):
     """N=4, max_ho_dims=4, J=g=omega=1: the full space (1024 states) fits, so paces == exact."""
     ham, te = make_objects(paces, 4, 4, 1.0, 100000, 1, 0, workdir)
@@ -443,6 +462,7 @@ def main():
     jobs.append(("scaled_n8c16", lambda: gen_traj_scaled(paces, fresh())))
     for name, weighting in TAU_RUNS.items():
         jobs.append((name, lambda name=name, w=weighting: gen_traj_tau(paces, name, w, fresh())))
+    jobs.append(("fragment31", lambda: gen_fragment(paces, fresh())))
     for name, cfg in LATTICE_RUNS.items():
         jobs.append((f"lattice_{name}", lambda name=name, cfg=cfg: gen_lattice(paces, name, cfg, fresh())))
     if args.long:

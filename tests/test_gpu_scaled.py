@@ -40,3 +40,37 @@ def test_scaled_propagation_matches_the_reference(tmp_path):
         who = te.whoami.view(torch.int32).cpu().numpy().view(np.uint32)
         assert np.array_equal(who, f["whoami"])
         np.testing.assert_allclose(te.vector.cpu().numpy(), f["vector"], rtol=0, atol=1e-13)
+
+
+def test_large_steps_use_norm_estimates():
+    """A time step so large that condition (3.13) fails: fragment 3.1 chooses (m, s) from
+    1-norm estimates of powers of A (equation 3.11, the block estimator over device H rows),
+    and the propagated state equals exp(+1j dt H) psi computed densely."""
+    import scipy.linalg as sla
+    import torch
+    from paces_b200 import expm
+    from tests import gpu_helpers
+    nchain, dim, g = 6, 8, 1.0
+    eng = gpu_helpers.engine_for(nchain, dim, g, cap=1 << 12)
+    tr, _ = gpu_helpers.grown_trajectory(eng, nchain, 300, initpos=1, dim=dim)
+    b, h = tr.basis, tr.h
+    S = b.count()
+    diag, mats, _ = gpu_helpers.csr_from_table(eng, b, h, 1.0, g)
+    H = np.diag(diag) + sum(mm.toarray() for mm in mats.values())
+    _, _, dbar = eng.hnorms(b, h)
+    _, a1, _ = eng.hnorms(b, h, shift=dbar)
+    dt = 80.0 / a1          # t ||A - mu I||_1 = 80: beyond condition (3.13)
+    assert not expm.condition_3_13(dt * a1)
+    A = 1j * (H - dbar * np.eye(S))
+    # the estimates are lower bounds of the exact norms, and close to them
+    for p in (2, 3):
+        est = tr._norm_power(dt, dbar, p) ** p
+        exact = np.abs(np.linalg.matrix_power(dt * A, p)).sum(axis=0).max()
+        assert est <= exact * (1 + 1e-10) and est >= exact / 3, (p, est, exact)
+    m, s = expm.choose(dt * a1, d=lambda p: tr._norm_power(dt, dbar, p))
+    psi0 = tr.vector.clone()
+    out = torch.zeros_like(tr.psis[tr.cur])
+    eta = np.exp(dt * 1j * dbar / s)
+    eng.expm_scaled(b, h, tr.psis[tr.cur], out, dt, dbar, m, s, eta)
+    want = sla.expm(1j * dt * H) @ psi0.cpu().numpy()
+    np.testing.assert_allclose(out[:S].cpu().numpy(), want, rtol=0, atol=1e-11)
