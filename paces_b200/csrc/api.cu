@@ -77,7 +77,7 @@ struct Layout {
     int64_t cap = 0;
     size_t keysA, blkA, keysB, blkB, maps;
     size_t m_run_lo, m_run_len, m_split_off, m_tile_off, m_counters, m_split_co, m_split_rank, m_ord_co,
-        m_tile_state;
+        m_tile_state, m_tile_desc;
     int64_t split_cap, tile_cap;
     size_t t_hist, t_cand, t_cand_idx, t_sel, t_tile_cnt, t_tile_pre;
     int t_tiles;
@@ -118,6 +118,7 @@ Layout make_layout(const paces_ctx* c, int64_t cap) {
     l.m_split_rank = take(size_t(l.split_cap) * 4);
     l.m_ord_co = take(size_t(l.split_cap) * kRuns * 4);
     l.m_tile_state = take(size_t(l.tile_cap) * 8);
+    l.m_tile_desc = take(size_t(l.tile_cap) * merge_desc_bytes());
     l.t_tiles = trunc_tiles_cap(cap);
     l.t_hist = take(4096 * 4);
     l.t_cand = take(ucap * 8);
@@ -182,6 +183,7 @@ MergeWs merge_ws(const paces_ctx* c, const Layout& l, void* ws) {
     w.split_rank = at<int>(ws, l.m_split_rank);
     w.ord_co = at<int>(ws, l.m_ord_co);
     w.tile_state = at<unsigned long long>(ws, l.m_tile_state);
+    w.tile_desc = at<unsigned char>(ws, l.m_tile_desc);
     w.split_cap = int(l.split_cap);
     w.tile_cap = int(l.tile_cap);
     w.keep = nullptr;
@@ -345,13 +347,13 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
     return PACES_OK;
 }
 
-// Kernels one step enqueues (merge: 5, +1 with the neighbour table; truncation: see
+// Kernels one step enqueues (merge: 6 per pass, +1 for the neighbour table; truncation: see
 // trunc_launches, +1 with look-ahead weights; remap 3; observables 2 or 3; Taylor 1;
 // renormalisation 3; record 2).
 unsigned long long step_launches(const paces_step_params& prm, bool c64, bool with_taylor, int passes) {
     const int wk = prm.weighting ? 2 : (c64 ? 1 : 0);
     return 2 + (prm.weighting ? 1 : 0) + trunc_launches(wk, prm.shuffle != 0) +
-           (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 5ull * passes * (prm.enlarge_steps + 1) + 1 +
+           (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 6ull * passes * (prm.enlarge_steps + 1) + 1 +
            3 + (prm.diagnostics ? 2 : 0) +
            (prm.evolve ? (with_taylor ? 1 : 0) + (prm.renormalize ? 3 : 0) : 0) + 3;
 }

@@ -345,6 +345,77 @@ __device__ long long lookback_warp(unsigned long long* state, int t, long long c
     return excl;
 }
 
+// Everything a tile needs before it loads its elements: its block, segments and merged
+// predecessor (the largest element before the start of any run).  Computed for all tiles at
+// once by merge_desc_kernel, read by the tile kernel with one coalesced load.
+template <int NW>
+struct TileDesc {
+    int p, tl, n, has_pred, pred_flag, pad;
+    int start[kRuns], off[kRuns + 1], lo[kRuns];
+    int pad2;
+    uint64_t pred[NW];
+};
+static_assert(sizeof(TileDesc<kMaxKeyWords>) <= merge_desc_bytes(), "tile descriptor size");
+
+template <int NW>
+__global__ void __launch_bounds__(256) merge_desc_kernel(ModelDev m, const uint64_t* __restrict__ X,
+                                                         const uint64_t* __restrict__ Y, MergeWs ws, int tmax,
+                                                         int* status) {
+    const int ntiles = ws.counters[1];
+    const int L = m.L;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+        TileDesc<NW> d;
+        const int p = find_segment(ws.tile_off, L, t);
+        const int tl = t - __ldg(ws.tile_off + p);
+        const int ob = __ldg(ws.split_off + p * kRuns);
+        const int nsb = __ldg(ws.split_off + (p + 1) * kRuns) - ob;
+        const int a = ob + tl * kMergeGroup;
+        const int bidx = tl * kMergeGroup + kMergeGroup;
+        d.p = p;
+        d.tl = tl;
+        d.pad = d.pad2 = 0;
+        int n = 0, has = 0, pf = 0;
+        Key<NW> pk;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) pk.w[q] = 0;
+        for (int j = 0; j < kRuns; ++j) {
+            const int st = __ldcg(ws.ord_co + int64_t(a) * kRuns + j);
+            const int en = bidx < nsb ? __ldcg(ws.ord_co + int64_t(ob + bidx) * kRuns + j)
+                                      : __ldg(ws.run_len + p * kRuns + j);
+            const int lo = __ldg(ws.run_lo + p * kRuns + j);
+            d.start[j] = st;
+            d.lo[j] = lo;
+            d.off[j] = n;
+            n += en - st;
+            if (st > 0) {
+                Key<NW> k;
+                int f;
+                run_elem<NW>(m, X, Y, ws, p, j, int64_t(lo) + st - 1, k, f);
+                // a later run wins ties: it sorts after the earlier one
+                if (!has || cmp_kf(k, f, pk, pf) >= 0) {
+                    pk = k;
+                    pf = f;
+                    has = 1;
+                }
+            }
+        }
+        d.off[kRuns] = n;
+        d.n = n;
+        if (n > tmax) {
+            // cannot happen for sorted runs (see merge_tmax); flag it and emit nothing
+            raise_status(status, PACES_ERR_CAPACITY);
+            for (int j = 0; j <= kRuns; ++j) d.off[j] = 0;
+            d.n = 0;
+            has = 0;
+        }
+        d.has_pred = has;
+        d.pred_flag = pf;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) d.pred[q] = pk.w[q];
+        *reinterpret_cast<TileDesc<NW>*>(ws.tile_desc + size_t(t) * merge_desc_bytes()) = d;
+    }
+}
+
 template <int NW, int MODE>
 __global__ void __launch_bounds__(kTileThreads)
 merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __restrict__ Y, MergeWs ws,
@@ -360,99 +431,39 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     uint16_t* s_cnt = s_lv1 + tmax;   // second merge level; then the inclusive count of first
                                       // occurrences per merged pos
     uint16_t* s_cntn = s_lv1;         // split: the same for first occurrences of the new part
-    __shared__ int s_t, s_p, s_tl, s_n;
+    __shared__ int s_t;
     __shared__ long long s_base, s_total;
     __shared__ int s_warpn[kTileThreads / 32];
-    __shared__ int s_start[kRuns], s_off[kRuns + 1], s_lo[kRuns];
-    __shared__ Key<NW> s_pred;
-    __shared__ int s_pred_flag, s_has_pred;
     __shared__ int s_warp[kTileThreads / 32];
     __shared__ int s_ceil;
+    __shared__ __align__(16) TileDesc<NW> s_d;
+    const int* s_start = s_d.start;
+    const int* s_off = s_d.off;
+    const int* s_lo = s_d.lo;
 
     const int tid = threadIdx.x;
-    __shared__ Key<NW> s_pk[kRuns];
-    __shared__ int s_pf[kRuns], s_pv[kRuns], s_len[kRuns];
-
-    const int L = m.L;
     const int ntiles = ws.counters[1];
+    constexpr int kDescWords = int(sizeof(TileDesc<NW>) / 4);
 
     for (;;) {
         if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
         __syncthreads();
         const int t = s_t;
         if (t >= ntiles) return;
-
-        // tile set-up: one thread per run (segment bounds and the element just before it)
-        if (tid < kRuns) {
-            const int j = tid;
-            const int p = find_segment(ws.tile_off, L, t);
-            const int tl = t - __ldg(ws.tile_off + p);
-            const int ob = __ldg(ws.split_off + p * kRuns);
-            const int nsb = __ldg(ws.split_off + (p + 1) * kRuns) - ob;
-            const int a = ob + tl * kMergeGroup;
-            const int bidx = tl * kMergeGroup + kMergeGroup;
-            const int st = __ldcg(ws.ord_co + int64_t(a) * kRuns + j);
-            const int en = bidx < nsb ? __ldcg(ws.ord_co + int64_t(ob + bidx) * kRuns + j)
-                                      : __ldg(ws.run_len + p * kRuns + j);
-            const int lo = __ldg(ws.run_lo + p * kRuns + j);
-            s_start[j] = st;
-            s_len[j] = en - st;
-            s_lo[j] = lo;
-            s_pv[j] = 0;
-            if (st > 0) {
-                Key<NW> k;
-                int f;
-                run_elem<NW>(m, X, Y, ws, p, j, int64_t(lo) + st - 1, k, f);
-                s_pk[j] = k;
-                s_pf[j] = f;
-                s_pv[j] = 1;
-            }
-            if (j == 0) {
-                s_p = p;
-                s_tl = tl;
-                s_ceil = 0;
-            }
-        }
+        // tile set-up: the precomputed descriptor
+        if (tid < kDescWords)
+            reinterpret_cast<int*>(&s_d)[tid] =
+                __ldcg(reinterpret_cast<const int*>(ws.tile_desc + size_t(t) * merge_desc_bytes()) + tid);
+        if (tid == 0) s_ceil = 0;
         __syncthreads();
-        if (tid == 0) {
-            int n = 0;
-            for (int j = 0; j < kRuns; ++j) {
-                s_off[j] = n;
-                n += s_len[j];
-            }
-            s_off[kRuns] = n;
-            s_n = n;
-            // merged predecessor of the tile: the largest element before the start of any run
-            int has = 0, pf = 0, pj = -1;
-            for (int j = 0; j < kRuns; ++j) {
-                if (!s_pv[j]) continue;
-                bool larger = !has;
-                if (has) {
-                    const int c = cmp_kf(s_pk[j], s_pf[j], s_pk[pj], pf);
-                    larger = c > 0 || (c == 0 && j > pj);
-                }
-                if (larger) {
-                    pf = s_pf[j];
-                    pj = j;
-                    has = 1;
-                }
-            }
-            s_has_pred = has;
-            if (has) {
-                s_pred = s_pk[pj];
-                s_pred_flag = pf;
-            }
-            if (n > tmax) {
-                // cannot happen for sorted runs (see merge_tmax); flag it and emit nothing
-                raise_status(status, PACES_ERR_CAPACITY);
-                for (int j = 0; j <= kRuns; ++j) s_off[j] = 0;
-                s_n = 0;
-                s_has_pred = 0;
-            }
-        }
-        __syncthreads();
-        const int n = min(s_n, tmax);
-        const int p = s_p;
+        const int n = min(s_d.n, tmax);
+        const int p = s_d.p;
+        const int s_tl = s_d.tl;
+        const int s_has_pred = s_d.has_pred;
+        const int s_pred_flag = s_d.pred_flag;
+        Key<NW> s_pred;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) s_pred.w[q] = s_d.pred[q];
 
         // 1. load the tile's segments (transforms applied on the fly)
         for (int e = tid; e < n; e += kTileThreads) {
@@ -753,6 +764,7 @@ int launch_merge_t(int mode, int stride, const ModelDev& m, const uint64_t* X, c
     const int g = num_sms * 8;
     merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, ws, stride);
     merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
+    merge_desc_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, ws, tmax, status);
     if (mode == MERGE_ASSEMBLE) launch_tile<NW, MERGE_ASSEMBLE>(tmax, m, X, Y, ws, out, status, num_sms, st);
     else if (mode == MERGE_EXPAND_SPLIT) launch_tile<NW, MERGE_EXPAND_SPLIT>(tmax, m, X, Y, ws, out, status, num_sms, st);
     else launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, out, status, num_sms, st);

@@ -44,6 +44,7 @@ struct MergeWs {
     int* split_rank; // [split_cap]
     int* ord_co;     // [split_cap * kRuns]
     unsigned long long* tile_state;  // [tile_cap] look-back words
+    unsigned char* tile_desc;        // [tile_cap] tile descriptors (merge_desc_bytes each)
     int split_cap;
     int tile_cap;
     // optional candidate filter (expansion only): keep[j * keep_cap + src] == 0 drops the
@@ -134,6 +135,8 @@ inline int64_t merge_split_cap(int64_t in_cap, int nw, int L) {
     return kRuns * (in_cap / kMinMergeStride + 1) + int64_t(kRuns) * L + 8;
 }
 inline int64_t merge_tile_cap(int64_t split_cap, int L) { return split_cap / kMergeGroup + L + 8; }
+// Bytes of one tile descriptor (any key width).
+constexpr size_t merge_desc_bytes() { return 128 + size_t(kMaxKeyWords) * 8; }
 
 // X feeds the self run, Y (null: X) the four image runs.  ceiling_out (optional) receives the
 // number of ceiling holes of the up run, or has it added (ceiling_add).  An assembly with
