@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--tau", type=float, default=0.2, help="plain: look-ahead time of --weighting")
     ap.add_argument("--no-graph", action="store_true", help="step without CUDA-graph replay")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--merge-stride", type=int, default=0, help="plain: this merge stride instead of tuning it")
     ap.add_argument("--batch", type=int, default=64, help="trajectories of the batched workload")
     ap.add_argument("--seed", type=int, default=0, help="seed of the batched workload's draws")
     ap.add_argument("--streams", type=int, default=8, help="streams of the batched step")
@@ -335,7 +336,13 @@ def run_ours(a):
     cs = 8 if a.precision == "c64" else 16
     tr, nprep = prepare(a, eng, a.maxstates)
     tuning = None
-    if not a.no_tune:
+    if a.merge_stride:
+        from paces_b200 import autotune
+        autotune.set_tuning(eng, merge_stride=a.merge_stride)
+        t = autotune.get_tuning(eng)
+        tuning = {"merge_stride": t.merge_stride, "taylor_blocks_per_sm": t.taylor_blocks_per_sm,
+                  "taylor_variant": t.taylor_variant}
+    elif not a.no_tune:
         from paces_b200 import autotune
         tuning = autotune.tune(tr, a.dt)
         log(a, f"tuning: {tuning}")
