@@ -229,7 +229,9 @@ def taylor_bytes_per_term(rec, cs):
 
 
 def step_bytes(rec, cs, nw, es):
-    """Algorithmic bytes of a whole step (measurement section)."""
+    """Algorithmic bytes of a whole step: truncation (S weights + M kept keys and weights),
+    expansion (M keys in, B keys out), assembly (B keys in, S keys and table rows out),
+    remap, the Taylor terms and the observables -- each stage's minimal HBM traffic."""
     kb = 8 * nw
     S, B, M = rec.n_states, rec.n_enlarged, rec.n_select
     truncate = S * cs + M * kb                      # read amplitudes, write kept keys
