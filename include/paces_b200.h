@@ -39,6 +39,8 @@
  *   paces_remap        vector remap in _generate_new_hilbert_space_cupy
  *                                                             paces/core/time_evolution.py:781-797
  *   paces_taylor       _simple_taylor + total_ham              paces/core/time_evolution.py:482-512, :382-400
+ *   paces_term_energies calculate_hopping / calculate_coupling / calculate_mu_to_0 sums
+ *                                                             paces/models/holstein.py:325-377
  *   paces_observables  calculate_n_exc / calculate_n_pho / calculate_total_energy / norm
  *                      paces/models/holstein.py:299-322, paces/core/observables.py:95-99,
  *                      paces/core/time_evolution.py:585-602
@@ -288,6 +290,13 @@ int paces_taylor(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, cons
 int paces_observables(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi,
                       int32_t what, double *dev_out, void *ws, size_t ws_bytes,
                       paces_stream_t stream);
+/* Per exciton position p (0..L-1) the energies of the hopping term and of the vibronic
+ * coupling, sum over the rows r of block p of conj(psi_r) (H_term psi)_r, and the sum of the
+ * amplitudes of the phonon-vacuum states: dev_out[4L + 2] = hop re[L], hop im[L], vib re[L],
+ * vib im[L], vacuum re, vacuum im.  The partitioned sums of calculate_hopping /
+ * calculate_coupling and the value of calculate_mu_to_0 (paces/models/holstein.py:325-377). */
+int paces_term_energies(paces_ctx *ctx, const paces_basis *b, const paces_hmat *h, const void *psi,
+                        double *dev_out, void *ws, size_t ws_bytes, paces_stream_t stream);
 /* Norms for the scaling-and-squaring propagation: dev_out[0] = trace of H, dev_out[1] =
  * the largest row 1-norm of H - (*dev_shift) I (0 when dev_shift is NULL), dev_out[2] =
  * trace / n (three doubles, device).  Reference: _trace and _exact_1_norm,

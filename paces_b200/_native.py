@@ -177,6 +177,7 @@ _SIGNATURES = {
     "paces_observables": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, ctypes.c_int32, _P, _P,
                           ctypes.c_size_t, _P],
     "paces_apply_h": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, _P],
+    "paces_term_energies": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, _P, ctypes.c_size_t, _P],
     "paces_hnorms": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, _P, ctypes.c_size_t, _P],
     "paces_expm_scaled": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, ctypes.c_double, ctypes.c_double,
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _P,

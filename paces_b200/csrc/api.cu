@@ -996,6 +996,18 @@ int paces_observables(paces_ctx* c, const paces_basis* b, const paces_hmat* h, c
     return PACES_OK;
 }
 
+int paces_term_energies(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi, double* dev_out,
+                        void* ws, size_t ws_bytes, paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !psi || !dev_out || !ws) return PACES_ERR_BADARG;
+    if (c->m.nhop > 1 && !h->xnbr) return fail(c, PACES_ERR_BADARG, "paces_term_energies: the lattice's H needs xnbr");
+    const Layout l = fit_layout(c, ws_bytes);
+    PACES_CHECK_LAUNCH(c, launch_term_energies(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->meta, psi,
+                                               at<double>(ws, l.o_partials), dev_out, c->num_sms,
+                                               reinterpret_cast<cudaStream_t>(stream)),
+                       "term_energies");
+    return PACES_OK;
+}
+
 int paces_apply_h(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* x, void* y,
                   paces_stream_t stream) {
     if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !x || !y || x == y) return PACES_ERR_BADARG;

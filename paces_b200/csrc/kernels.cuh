@@ -124,6 +124,10 @@ int launch_observables(int nw, bool c64, const ModelDev& m, const uint64_t* keys
                        cudaStream_t st);
 int launch_scale(bool c64, const ModelDev& m, const int* blk, void* psi, const double* norm,
                  int num_sms, cudaStream_t st);
+// Per exciton position the hopping and vibronic energies (re, im) and the phonon-vacuum
+// amplitude sum: out[4L + 2] = hop re[L], hop im[L], vib re[L], vib im[L], vacuum re, im.
+int launch_term_energies(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
+                         const void* psi, double* partials, double* out, int num_sms, cudaStream_t st);
 int launch_apply_h(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
                    const void* x, void* y, int num_sms, cudaStream_t st);
 

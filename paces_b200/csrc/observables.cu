@@ -289,6 +289,165 @@ __global__ void __launch_bounds__(kOThreads) apply_h_kernel(ModelDev m, const in
     }
 }
 
+// Per exciton position p: sum over the rows of block p of conj(psi_r) (H_hop psi)_r and of
+// conj(psi_r) (H_vib psi)_r -- the partitioned sums behind calculate_hopping and
+// calculate_coupling (paces/models/holstein.py:325-364, :380-396; H_hop is the "hopping"
+// term, every order-1 channel) -- and the sum of the amplitudes of phonon-vacuum rows
+// (calculate_mu_to_0, holstein.py:366-377).  Per-block partials [4L + 2] (hop re, im per
+// p, then vib re, im per p, then the vacuum sum), summed in a fixed order afterwards.
+template <bool C64>
+__global__ void __launch_bounds__(kOThreads) obs_terms_kernel(ModelDev m, const int* __restrict__ blk,
+                                                              const int* __restrict__ nbr,
+                                                              const uint32_t* __restrict__ meta,
+                                                              const void* __restrict__ psi,
+                                                              double* __restrict__ part) {
+    using C = typename std::conditional<C64, float2, double2>::type;
+    using R = typename std::conditional<C64, float, double>::type;
+    __shared__ R s_sq[260];
+    __shared__ double s_acc[kOWarps][4 * kMaxSites];
+    __shared__ double s_vac[kOWarps][2];
+    const int L = m.L;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < 260; k += kOThreads) s_sq[k] = R(__dmul_rn(sqrt(double(k)), m.g));
+    for (int k = threadIdx.x; k < kOWarps * 4 * kMaxSites; k += kOThreads) (&s_acc[0][0])[k] = 0.0;
+    __syncthreads();
+    const int64_t S = blk[L];
+    const C* x = reinterpret_cast<const C*>(psi);
+    double vac_r = 0.0, vac_i = 0.0;
+    for (int64_t base = (int64_t(blockIdx.x) * kOWarps + wid) * 32; base < S;
+         base += int64_t(gridDim.x) * kOWarps * 32) {
+        const int64_t r = base + lane;
+        const bool valid = r < S;
+        double eh_r = 0.0, eh_i = 0.0, ev_r = 0.0, ev_i = 0.0;
+        int pme = -1;
+        if (valid) {
+            const uint32_t mm = __ldg(meta + r);
+            pme = int(mm & 0xffu);
+            const int n = int((mm >> 8) & 0xffu);
+            const int4 nb = load_nbr(nbr, r);
+            const C z = __ldcg(x + r);
+            double hr = 0.0, hi = 0.0, vr = 0.0, vi = 0.0;
+            if constexpr (C64) {
+                float2 h = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
+                if (m.nhop > 1) {
+                    for (int e = 0; e < m.hop_n[0]; ++e) {
+                        const int idx = hop_index(m, r, nb, m.hop_ord[0][e]);
+                        if (idx < 0) continue;
+                        const float2 w = __ldcg(x + idx);
+                        h.x = fmaf(float(m.J), w.x, h.x);
+                        h.y = fmaf(float(m.J), w.y, h.y);
+                    }
+                } else {
+                    const float J = float(m.J);
+                    if (nb.x >= 0) { const float2 w = __ldcg(x + nb.x); h.x = fmaf(J, w.x, h.x); h.y = fmaf(J, w.y, h.y); }
+                    if (nb.y >= 0) { const float2 w = __ldcg(x + nb.y); h.x = fmaf(J, w.x, h.x); h.y = fmaf(J, w.y, h.y); }
+                }
+                if (nb.z >= 0) { const float2 w = __ldcg(x + nb.z); v.x = fmaf(s_sq[n], w.x, v.x); v.y = fmaf(s_sq[n], w.y, v.y); }
+                if (nb.w >= 0) { const float2 w = __ldcg(x + nb.w); v.x = fmaf(s_sq[n + 1], w.x, v.x); v.y = fmaf(s_sq[n + 1], w.y, v.y); }
+                hr = h.x; hi = h.y; vr = v.x; vi = v.y;
+            } else {
+                // the rows of the term matrices as the reference sums them (see hrow.cuh)
+                double2 h = make_double2(0.0, 0.0);
+                if (m.nhop > 1) {
+                    bool any = false;
+                    for (int e = 0; e < m.hop_n[0]; ++e) {
+                        const int idx = hop_index(m, r, nb, m.hop_ord[0][e]);
+                        if (idx < 0) continue;
+                        const double2 w = __ldcg(x + idx);
+                        const double2 pv = make_double2(__dmul_rn(m.J, w.x), __dmul_rn(m.J, w.y));
+                        h = any ? make_double2(__dadd_rn(h.x, pv.x), __dadd_rn(h.y, pv.y)) : pv;
+                        any = true;
+                    }
+                } else {
+                    const bool swap = nb.y >= 0 && (nb.x < 0 || nb.y < nb.x);
+                    const int a = swap ? nb.y : nb.x, b = swap ? nb.x : nb.y;
+                    const bool ha = a >= 0, hb = b >= 0;
+                    const double2 xa = ha ? __ldcg(x + a) : make_double2(0.0, 0.0);
+                    const double2 xb = hb ? __ldcg(x + b) : make_double2(0.0, 0.0);
+                    const double2 pa = make_double2(__dmul_rn(m.J, xa.x), __dmul_rn(m.J, xa.y));
+                    const double2 pb = make_double2(__dmul_rn(m.J, xb.x), __dmul_rn(m.J, xb.y));
+                    h = (ha && hb) ? make_double2(__dadd_rn(pa.x, pb.x), __dadd_rn(pa.y, pb.y))
+                                   : (ha ? pa : (hb ? pb : make_double2(0.0, 0.0)));
+                }
+                const bool hd = nb.z >= 0, hu = nb.w >= 0;
+                const double2 xd = hd ? __ldcg(x + nb.z) : make_double2(0.0, 0.0);
+                const double2 xu = hu ? __ldcg(x + nb.w) : make_double2(0.0, 0.0);
+                const double2 pd = make_double2(__dmul_rn(s_sq[n], xd.x), __dmul_rn(s_sq[n], xd.y));
+                const double2 pu = make_double2(__dmul_rn(s_sq[n + 1], xu.x), __dmul_rn(s_sq[n + 1], xu.y));
+                const double2 v = (hd && hu) ? make_double2(__dadd_rn(pd.x, pu.x), __dadd_rn(pd.y, pu.y))
+                                             : (hd ? pd : (hu ? pu : make_double2(0.0, 0.0)));
+                hr = h.x; hi = h.y; vr = v.x; vi = v.y;
+            }
+            const double zr = double(z.x), zi = double(z.y);
+            // conj(z) * y
+            eh_r = __dadd_rn(__dmul_rn(zr, hr), __dmul_rn(zi, hi));
+            eh_i = __dsub_rn(__dmul_rn(zr, hi), __dmul_rn(zi, hr));
+            ev_r = __dadd_rn(__dmul_rn(zr, vr), __dmul_rn(zi, vi));
+            ev_i = __dsub_rn(__dmul_rn(zr, vi), __dmul_rn(zi, vr));
+            if ((mm >> 16) == 0) {
+                vac_r += zr;
+                vac_i += zi;
+            }
+        }
+        // the warp's rows span consecutive exciton blocks: segmented sums per block
+        const int p0 = __shfl_sync(0xffffffffu, pme, 0);
+        const int vlast = __shfl_sync(0xffffffffu, pme, 31);
+        const int p1 = vlast < 0 ? L - 1 : vlast;
+        for (int pp = p0; pp <= p1 && pp >= 0; ++pp) {
+            double a0 = pme == pp ? eh_r : 0.0, a1 = pme == pp ? eh_i : 0.0;
+            double a2 = pme == pp ? ev_r : 0.0, a3 = pme == pp ? ev_i : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+                a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+            }
+            if (lane == 0) {
+                s_acc[wid][pp] += a0;
+                s_acc[wid][L + pp] += a1;
+                s_acc[wid][2 * L + pp] += a2;
+                s_acc[wid][3 * L + pp] += a3;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        vac_r += __shfl_xor_sync(0xffffffffu, vac_r, o);
+        vac_i += __shfl_xor_sync(0xffffffffu, vac_i, o);
+    }
+    if (lane == 0) {
+        s_vac[wid][0] = vac_r;
+        s_vac[wid][1] = vac_i;
+    }
+    __syncthreads();
+    const int nv = 4 * L + 2;
+    double* out = part + size_t(blockIdx.x) * nv;
+    for (int v = threadIdx.x; v < nv; v += kOThreads) {
+        double acc = 0.0;
+        for (int w = 0; w < kOWarps; ++w) acc += v < 4 * L ? s_acc[w][v] : s_vac[w][v - 4 * L];
+        out[v] = acc;
+    }
+}
+
+// out[v] = sum over blocks of part[b][v], one block per value, fixed order.
+__global__ void __launch_bounds__(256) terms_final_kernel(int nv, int nb, const double* __restrict__ part,
+                                                          double* __restrict__ out) {
+    __shared__ double s_w[8];
+    const int v = blockIdx.x;
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += part[size_t(b) * nv + v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += s_w[w];
+        out[v] = t;
+    }
+}
+
 template <bool C64>
 __global__ void scale_kernel(int L, const int* __restrict__ blk, void* psi, const double* norm) {
     using C = typename std::conditional<C64, float2, double2>::type;
@@ -378,6 +537,15 @@ int launch_observables(int nw, bool c64, const ModelDev& m, const uint64_t* keys
         default: return PACES_ERR_BADARG;
     }
 #undef PACES_OBS_CASE
+}
+
+int launch_term_energies(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
+                         const void* psi, double* partials, double* out, int num_sms, cudaStream_t st) {
+    const int grid = num_sms * 2;  // the partials hold obs_max_grid * (4 + 2L) doubles
+    if (c64) obs_terms_kernel<true><<<grid, kOThreads, 0, st>>>(m, blk, nbr, meta, psi, partials);
+    else obs_terms_kernel<false><<<grid, kOThreads, 0, st>>>(m, blk, nbr, meta, psi, partials);
+    terms_final_kernel<<<4 * m.L + 2, 256, 0, st>>>(4 * m.L + 2, grid, partials, out);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
 int launch_apply_h(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,

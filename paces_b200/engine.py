@@ -311,6 +311,18 @@ class Engine:
         e = nat.ExpmInfo.from_buffer_copy(info.cpu().numpy().tobytes())
         return [bool(e.converged), int(e.final_m), float(e.c1_plus_c2), float(e.term_ratio)]
 
+    def term_energies(self, b: DevBasis, h: DevHMat, psi):
+        """Per exciton position the hopping and vibronic energies <psi_p|H_term|psi> (complex
+        [L] each) and the sum of the phonon-vacuum amplitudes (paces_term_energies)."""
+        out = torch.empty(4 * self.L + 2, dtype=torch.float64, device=self.device)
+        ws, nb = self.workspace()
+        nat.check(self.lib.paces_term_energies(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(psi),
+                                               _ptr(out), ws, nb, _stream(self.device)), self.ctx, "term_energies")
+        L = self.L
+        hop = torch.complex(out[:L], out[L:2 * L])
+        vib = torch.complex(out[2 * L:3 * L], out[3 * L:4 * L])
+        return hop, vib, complex(out[4 * L].item(), out[4 * L + 1].item())
+
     def apply_h(self, b: DevBasis, h: DevHMat, x, y=None):
         """y = H x (total_ham)."""
         y = torch.empty_like(x) if y is None else y

@@ -237,17 +237,22 @@ class Observables(ObservablesFramework):
         """Phonon number per site (holstein.py:317-322), from the device."""
         return self._from_device(vector, "n_pho")
 
-    def _term_values(self, term, vector):
-        mats = self.teobj.sparse_mats_dict
-        m = mats[term].to(torch.complex128)
-        return vector.conj().to(torch.complex128) * torch.mv(m, vector.to(torch.complex128))
+    def _terms(self, vector):
+        """(hopping energy per position, vibronic energy per position, vacuum amplitude sum)
+        of `vector` on the current basis, from the device (paces_term_energies)."""
+        te = self.teobj
+        tr = te._traj
+        x = torch.zeros(max(tr.basis.cap, 1), dtype=te.engine.cdtype, device=te.engine.device)
+        n = vector.numel()
+        x[:n] = torch.as_tensor(vector).to(te.engine.device, te.engine.cdtype)
+        return te.engine.term_energies(tr.basis, tr.h, x)
 
     @obs_attrs(fname="V_hop", header=" ".join(f"V_{i}" for i in range(3)) + " etc.")
     def calculate_hopping(self, vector):
         """Hopping energy per bond (holstein.py:325-357)."""
         if self.hamobj.nchain % 2 == 0 and self.hamobj.periodic:
             raise NotImplementedError("This doesn't work for even chain lengths with periodic boundary conditions.")
-        hop_int_i = self._calculate_partitioned_sum(self._term_values("hopping", vector))
+        hop_int_i = self._terms(vector)[0]
         if self.hop_board is None:
             nc = self.hamobj.nchain
             cb = numpy.array([[1, 0] * ((nc + 1) // 2), [0, 1] * ((nc + 1) // 2)] * ((nc + 1) // 2))[:nc, :nc]
@@ -260,17 +265,13 @@ class Observables(ObservablesFramework):
 
     @obs_attrs(fname="V_vib_coupl", header=" ".join(f"V_{i}" for i in range(3)) + " etc.")
     def calculate_coupling(self, vector):
-        """Exciton-phonon coupling energy per site (holstein.py:360-364)."""
-        return self._calculate_partitioned_sum(self._term_values("vib_coupling", vector))
+        """Exciton-phonon coupling energy per site (holstein.py:360-364), from the device."""
+        return self._terms(vector)[1]
 
     @obs_attrs(fname="mu_to_0", header=r"<mu(t) mu(0)>")
     def calculate_mu_to_0(self, vector):
-        """Sum of the amplitudes on phonon-vacuum states (holstein.py:366-377)."""
-        r64 = layout.rows_i64(self.teobj.whoami)
-        mask = torch.ones(r64.shape[0], dtype=torch.bool, device=r64.device)
-        for s in range(self.hamobj.nchain):
-            mask &= layout.get_field_t(r64, self.hamobj._fields, s + 1) == 0
-        return vector[mask].sum()
+        """Sum of the amplitudes on phonon-vacuum states (holstein.py:366-377), from the device."""
+        return self._terms(vector)[2]
 
     def _calculate_partitioned_sum(self, sumvals):
         """Sum per exciton-position block (holstein.py:380-396)."""

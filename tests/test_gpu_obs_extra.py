@@ -57,3 +57,40 @@ def test_extra_observables_match_the_reference(tmp_path):
             rdm = obs.calculate_rdm(site, vec)
             assert isinstance(rdm, torch.Tensor)
             np.testing.assert_allclose(rdm.cpu().numpy(), f[key], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision,geo,J2", [("c128", 1, None), ("c64", 1, None), ("c128", 2, 0.3)])
+def test_term_energies_match_the_oracle(precision, geo, J2):
+    """paces_term_energies against the oracle's term matrices on the same basis and state:
+    per exciton position the hopping and vibronic energies, and the phonon-vacuum sum."""
+    import torch
+    from oracle import paces_oracle as po
+    from paces_b200.engine import Engine, ModelParams
+    from tests import gpu_helpers
+    nchain, dim, g = (9, 4, 1.3) if geo == 2 else (8, 8, 1.3)
+    eng = Engine(ModelParams(nchain=nchain, max_ho_dims=[dim] * nchain, g=g, geo_dim=geo, J2=J2,
+                             precision=precision), cap=1 << 15)
+    m = po.Model(nchain, [dim] * nchain, g=g, geo_dim=geo, J2=J2)
+    b = eng.basis_from_ref(gpu_helpers.initial_rows(nchain, dim, 1))
+    for _ in range(3):
+        b = eng.expand(b)
+    new, h, _ = eng.assemble(b)
+    S = new.count()
+    asm = po.generate_mel(m, gpu_helpers.ref_rows(eng, b), 0)
+    rng = np.random.default_rng(5)
+    v = (rng.standard_normal(S) + 1j * rng.standard_normal(S)) / np.sqrt(S)
+    psi = torch.zeros(max(new.cap, 1), dtype=eng.cdtype, device=eng.device)
+    psi[:S] = torch.as_tensor(v, device=eng.device).to(eng.cdtype)
+    vv = psi[:S].cpu().numpy().astype(np.complex128)
+    hop, vib, vac = eng.term_energies(new, h, psi)
+    pos = po.get_pos(m, asm.new_inds)
+    want_hop = np.bincount(pos, weights=(vv.conj() * asm.mats["hopping"].dot(vv)).real, minlength=nchain) + \
+        1j * np.bincount(pos, weights=(vv.conj() * asm.mats["hopping"].dot(vv)).imag, minlength=nchain)
+    ev = vv.conj() * asm.mats["vib_coupling"].dot(vv)
+    want_vib = np.bincount(pos, weights=ev.real, minlength=nchain) + 1j * np.bincount(pos, weights=ev.imag,
+                                                                                       minlength=nchain)
+    vacuum = po.sum_all_phonons(m, asm.new_inds) == 0
+    tol = dict(rtol=1e-11, atol=1e-13) if precision == "c128" else dict(rtol=2e-5, atol=2e-6)
+    np.testing.assert_allclose(hop.cpu().numpy(), want_hop, **tol)
+    np.testing.assert_allclose(vib.cpu().numpy(), want_vib, **tol)
+    np.testing.assert_allclose(vac, vv[vacuum].sum(), **tol)
