@@ -53,6 +53,14 @@ struct ModelDev {
     int64_t xcap;
 };
 
+// Blocks for a grid-stride pass over at most `items` elements handled `per_block` at a time:
+// a full wave (`max_blocks`) for large problems, fewer for small ones (the trajectories of a
+// batch), so that a small launch does not pay for a wave of idle blocks.
+inline int grid_for(int64_t items, int per_block, int max_blocks) {
+    const int64_t b = (items + per_block - 1) / per_block;
+    return int(b < 1 ? 1 : (b > max_blocks ? max_blocks : b));
+}
+
 // Whether the exciton at p has a neighbour through channel ch on side `up` (1: +dist, 0: -dist).
 __host__ __device__ __forceinline__ bool hop_exists(const ModelDev& m, int ch, int p, int up) {
     if (m.periodic) return true;

@@ -743,7 +743,8 @@ void launch_tile(int tmax, const ModelDev& m, const uint64_t* X, const uint64_t*
     cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTileThreads, smem);
-    kfn<<<num_sms * max(per_sm, 1), kTileThreads, smem, st>>>(m, X, Y, ws, tmax, out, status);
+    const int grid = num_sms * max(per_sm, 1);
+    kfn<<<grid < ws.tile_cap ? grid : max(ws.tile_cap, 1), kTileThreads, smem, st>>>(m, X, Y, ws, tmax, out, status);
 }
 
 template <int NW>
@@ -761,16 +762,17 @@ int launch_merge_t(int mode, int stride, const ModelDev& m, const uint64_t* X, c
     }
     const int tmax = merge_tmax(stride);
     merge_plan_kernel<<<1, 1024, 0, st>>>(m, x_blk, y_blk, ws, stride, status);
-    const int g = num_sms * 8;
+    const int g = grid_for(ws.split_cap, 256, num_sms * 8);
     merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, ws, stride);
     merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
-    merge_desc_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, ws, tmax, status);
+    merge_desc_kernel<NW><<<grid_for(ws.tile_cap, 256, num_sms * 8), 256, 0, st>>>(m, X, Y, ws, tmax, status);
     if (mode == MERGE_ASSEMBLE) launch_tile<NW, MERGE_ASSEMBLE>(tmax, m, X, Y, ws, out, status, num_sms, st);
     else if (mode == MERGE_EXPAND_SPLIT) launch_tile<NW, MERGE_EXPAND_SPLIT>(tmax, m, X, Y, ws, out, status, num_sms, st);
     else launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, out, status, num_sms, st);
     merge_finalize_kernel<<<1, 32, 0, st>>>(m, ws, out, ceiling_out, ceiling_add, mode == MERGE_EXPAND_SPLIT ? 1 : 0,
                                             status);
-    if (mode == MERGE_ASSEMBLE && !split_input && out.nbr) nbr_fill_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, out);
+    if (mode == MERGE_ASSEMBLE && !split_input && out.nbr)
+        nbr_fill_kernel<<<grid_for(out.map_cap, 256, num_sms * 8), 256, 0, st>>>(m, x_blk, out);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
@@ -904,7 +906,8 @@ int launch_nbr_fill_multi(const ModelDev& m, const int* x_blk, const int* const*
     for (int k = 0; k < passes; ++k) pm.maps[k] = pass_maps[k];
     pm.n = passes;
     if (cudaMemsetAsync(xnbr, 0xff, size_t(m.nhop - 1) * size_t(nbr_cap) * 8, st) != cudaSuccess) return PACES_ERR_CUDA;
-    nbr_fill_multi_kernel<<<num_sms * 8, 256, 0, st>>>(m, x_blk, pm, map_cap, nbr, reinterpret_cast<int2*>(xnbr),
+    nbr_fill_multi_kernel<<<grid_for(map_cap, 256, num_sms * 8), 256, 0, st>>>(m, x_blk, pm, map_cap, nbr,
+                                                                              reinterpret_cast<int2*>(xnbr),
                                                        nbr_cap);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
@@ -933,7 +936,8 @@ int launch_merge(int nw, int mode, int stride, const ModelDev& m, const uint64_t
 int launch_nbr_fill_split(const ModelDev& m, const int* p_blk, const int* n_blk, const int* maps_e,
                           const int* maps_s, const int* new_to_out, int64_t map_cap, int* nbr, int64_t nbr_cap,
                           int num_sms, cudaStream_t st) {
-    nbr_fill_split_kernel<<<num_sms * 8, 256, 0, st>>>(m, p_blk, n_blk, maps_e, maps_s, new_to_out, map_cap, nbr,
+    nbr_fill_split_kernel<<<grid_for(map_cap, 512, num_sms * 8), 256, 0, st>>>(m, p_blk, n_blk, maps_e, maps_s,
+                                                                              new_to_out, map_cap, nbr,
                                                        nbr_cap);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }

@@ -475,6 +475,9 @@ int wave_blocks(K kernel, int num_sms) {
     return num_sms * per_sm;
 }
 
+// The observables' grids stay a full wave whatever the problem size: the partial sums are
+// summed per block, so the grid sets the order of the additions, and results must not
+// change when a trajectory's buffers grow.
 template <int NW, bool C64>
 int launch_obs_t(const ModelDev& m, const uint64_t* keys, const int* blk, const int* nbr,
                  int64_t nbr_cap, const uint32_t* meta, const void* psi, int what, double* partials,

@@ -157,8 +157,10 @@ int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const v
                    const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws, int* status,
                    int num_sms, cudaStream_t st) {
     remap_plan_kernel<<<1, 32, 0, st>>>(m, ob, nb, ws, remap_tile(NW), status);
-    remap_split_kernel<NW><<<num_sms * 2, 256, 0, st>>>(m, ok, ob, nk, nb, ws, remap_tile(NW));
-    remap_tile_kernel<NW, C64><<<num_sms * 4, kRThreads, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi, ws);
+    remap_split_kernel<NW><<<grid_for(int64_t(ws.tile_cap) * 2, 256, num_sms * 2), 256, 0, st>>>(m, ok, ob, nk, nb, ws,
+                                                                                                remap_tile(NW));
+    remap_tile_kernel<NW, C64><<<grid_for(ws.tile_cap, 1, num_sms * 4), kRThreads, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi,
+                                                                                            ws);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 

@@ -316,7 +316,9 @@ int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, i
     if (cudaMemsetAsync(ws.barrier, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return PACES_ERR_CUDA;
     const bool xhop = m.nhop > 1;
     const int occ = c64 ? occupancy_any<true>(variant, xhop) : occupancy_any<false>(variant, xhop);
-    const int grid = num_sms * (blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ);
+    // a wave of blocks, or one block per 2048 rows of a small problem (fewer blocks at the grid
+    // barriers; the results do not depend on the grid)
+    const int grid = grid_for(nbr_cap, 2048, num_sms * (blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kTThreads);

@@ -497,7 +497,8 @@ int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_bl
                       int64_t maxstates, int shuffle, uint64_t seed, uint64_t step, const TruncWs& ws,
                       uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w, int* n_tied_out, int* n_kept_out,
                       int* status, int num_sms, cudaStream_t st) {
-    const int g = num_sms * 4;
+    const int g = grid_for(ws.cap, 1024, num_sms * 4);          // streaming passes
+    const int gt = grid_for(ws.cap, kTruncTile, num_sms * 4);   // passes over 4096-state tiles
     const int rounds = weight_rounds(WK);
     trunc_init_kernel<<<1, 1024, 0, st>>>(m, x_blk, maxstates, ws);
     for (int r = 0; r < rounds; ++r) {
@@ -512,9 +513,9 @@ int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_bl
             trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_H, r, 0);
         }
     }
-    trunc_count_kernel<WK><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
+    trunc_count_kernel<WK><<<gt, 256, 0, st>>>(psi, ws, seed, step, status);
     trunc_scan_kernel<<<1, 1024, 0, st>>>(ws);
-    trunc_write_kernel<NW, WK><<<g, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
+    trunc_write_kernel<NW, WK><<<gt, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
                                                    out_blk, out_cap, out_w, status);
     trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out, n_kept_out,
                                             out_w ? out_w + out_cap : nullptr, status);
