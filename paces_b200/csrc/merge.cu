@@ -75,23 +75,6 @@ __device__ __forceinline__ int cmp_kf(const Key<NW>& a, int fa, const Key<NW>& b
     return c != 0 ? c : (fa - fb);
 }
 
-// Elements of run (p, j) that precede (key, flag): strictly smaller, or not larger when
-// `upper` (the element's own run index is larger than j).
-template <int NW>
-__device__ int run_bound(const ModelDev& m, const uint64_t* __restrict__ X, const uint64_t* __restrict__ Y,
-                         const MergeWs& ws, int p, int j, int lo, int len, const Key<NW>& key, int flag, bool upper) {
-    int a = 0, b = len;
-    while (a < b) {
-        const int mid = (a + b) >> 1;
-        Key<NW> k2;
-        int f2;
-        run_elem<NW>(m, X, Y, ws, p, j, lo + mid, k2, f2);
-        const int c = cmp_kf(k2, f2, key, flag);
-        if (upper ? (c <= 0) : (c < 0)) a = mid + 1; else b = mid;
-    }
-    return a;
-}
-
 // Tile keys in shared memory, word-major (w[q*stride + e]): a probe reads 8 bytes of word 0
 // and touches the next word only on a tie, which keeps bank conflicts low.
 template <int NW>
@@ -259,13 +242,34 @@ __global__ void __launch_bounds__(256) merge_split_kernel(ModelDev m, const uint
         Key<NW> k;
         int f;
         run_elem<NW>(m, X, Y, ws, p, j, ws.run_lo[r] + i, k, f);
-        int rank = 0;
-#pragma unroll 1
+        // the bounds in the other runs: all searches advance one step per round, so their
+        // dependent loads are in flight together
+        int lo_[kRuns], a_[kRuns], b_[kRuns];
+#pragma unroll
         for (int jj = 0; jj < kRuns; ++jj) {
-            int co;
-            if (jj == j) co = i;
-            else co = run_bound<NW>(m, X, Y, ws, p, jj, ws.run_lo[p * kRuns + jj], ws.run_len[p * kRuns + jj],
-                                    k, f, jj < j);
+            lo_[jj] = ws.run_lo[p * kRuns + jj];
+            a_[jj] = 0;
+            b_[jj] = jj == j ? 0 : ws.run_len[p * kRuns + jj];
+        }
+        for (;;) {
+            bool any = false;
+#pragma unroll
+            for (int jj = 0; jj < kRuns; ++jj) {
+                if (a_[jj] >= b_[jj]) continue;
+                any = true;
+                const int mid = (a_[jj] + b_[jj]) >> 1;
+                Key<NW> k2;
+                int f2;
+                run_elem<NW>(m, X, Y, ws, p, jj, lo_[jj] + mid, k2, f2);
+                const int c = cmp_kf(k2, f2, k, f);
+                if ((jj < j) ? (c <= 0) : (c < 0)) a_[jj] = mid + 1; else b_[jj] = mid;
+            }
+            if (!any) break;
+        }
+        int rank = 0;
+#pragma unroll
+        for (int jj = 0; jj < kRuns; ++jj) {
+            const int co = jj == j ? i : a_[jj];
             ws.split_co[int64_t(s) * kRuns + jj] = co;
             rank += co;
         }
@@ -282,16 +286,25 @@ __global__ void __launch_bounds__(256) merge_order_kernel(ModelDev m, MergeWs ws
         const int own = s - ws.split_off[r];
         const int rank = ws.split_rank[s];
         int o = own;
+        int a_[kRuns], b_[kRuns], base_[kRuns];
+#pragma unroll
         for (int jj = 0; jj < kRuns; ++jj) {
-            if (jj == j) continue;
-            int a = ws.split_off[p * kRuns + jj], b = ws.split_off[p * kRuns + jj + 1];
-            const int base = a;
-            while (a < b) {
-                const int mid = (a + b) >> 1;
-                if (ws.split_rank[mid] < rank) a = mid + 1; else b = mid;
-            }
-            o += a - base;
+            a_[jj] = base_[jj] = ws.split_off[p * kRuns + jj];
+            b_[jj] = jj == j ? a_[jj] : ws.split_off[p * kRuns + jj + 1];
         }
+        for (;;) {  // lockstep searches, as in the split kernel
+            bool any = false;
+#pragma unroll
+            for (int jj = 0; jj < kRuns; ++jj) {
+                if (a_[jj] >= b_[jj]) continue;
+                any = true;
+                const int mid = (a_[jj] + b_[jj]) >> 1;
+                if (ws.split_rank[mid] < rank) a_[jj] = mid + 1; else b_[jj] = mid;
+            }
+            if (!any) break;
+        }
+#pragma unroll
+        for (int jj = 0; jj < kRuns; ++jj) o += a_[jj] - base_[jj];
         const int64_t dst = int64_t(ws.split_off[p * kRuns]) + o;
         if (dst >= ws.split_off[(p + 1) * kRuns]) continue;  // inconsistent ranks: cannot happen for sorted runs
 #pragma unroll
