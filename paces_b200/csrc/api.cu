@@ -347,14 +347,14 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
     return PACES_OK;
 }
 
-// Kernels one step enqueues (merge: 6 per pass, +1 for the neighbour table; truncation: see
-// trunc_launches, +1 with look-ahead weights; remap 3; observables 2 or 3; Taylor 1;
+// Kernels one step enqueues (merge: 4 per pass, +1 for the neighbour table; truncation: see
+// trunc_launches, +1 with look-ahead weights; remap 2; observables 2 or 3; Taylor 1;
 // renormalisation 3; record 2).
 unsigned long long step_launches(const paces_step_params& prm, bool c64, bool with_taylor, int passes) {
     const int wk = prm.weighting ? 2 : (c64 ? 1 : 0);
     return 2 + (prm.weighting ? 1 : 0) + trunc_launches(wk, prm.shuffle != 0) +
-           (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 6ull * passes * (prm.enlarge_steps + 1) + 1 +
-           3 + (prm.diagnostics ? 2 : 0) +
+           (prm.proposal && prm.enlarge_steps > 0 ? 1 : 0) + 4ull * passes * (prm.enlarge_steps + 1) + 1 +
+           2 + (prm.diagnostics ? 2 : 0) +
            (prm.evolve ? (with_taylor ? 1 : 0) + (prm.renormalize ? 3 : 0) : 0) + 3;
 }
 

@@ -185,12 +185,26 @@ __device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t
     }
 }
 
-__global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, const int* __restrict__ y_blk,
-                                  MergeWs ws, int stride, int* status) {
+// Splitters every `stride` elements of each run, with their co-ranks in the block's other
+// runs.  The plan comes first and every block derives it from the block offsets: the runs'
+// extents, the splitter prefix over (block, run) and the tile prefix over blocks (a tile is
+// kMergeGroup splitter intervals of one block).  Block 0 publishes it, sets the counters and
+// every block clears its share of the look-back words for the tile kernel.
+template <int NW>
+__global__ void __launch_bounds__(256) merge_split_kernel(ModelDev m, const uint64_t* __restrict__ X,
+                                                          const uint64_t* __restrict__ Y,
+                                                          const int* __restrict__ x_blk,
+                                                          const int* __restrict__ y_blk, MergeWs ws, int stride,
+                                                          int* status) {
+    __shared__ int s_lo[kMaxSites * kRuns];
     __shared__ int s_len[kMaxSites * kRuns];
-    __shared__ int s_tiles;
+    __shared__ int s_off[kMaxSites * kRuns + 1];
+    __shared__ int s_pos[kMaxSites + 1];  // splitters per block, then their prefix
+    __shared__ int s_toff[kMaxSites + 1];
+    __shared__ int s_total, s_tiles;
     const int L = m.L;
-    for (int idx = threadIdx.x; idx < L * kRuns; idx += blockDim.x) {
+    const int nr = L * kRuns;
+    for (int idx = threadIdx.x; idx < nr; idx += blockDim.x) {
         const int p = idx / kRuns, j = idx % kRuns;
         const int src = run_source(m, ws, p, j);
         const int* sb = j == RUN_SELF ? x_blk : y_blk;
@@ -199,57 +213,80 @@ __global__ void merge_plan_kernel(ModelDev m, const int* __restrict__ x_blk, con
             lo = sb[src];
             len = sb[src + 1] - lo;
         }
-        ws.run_lo[idx] = lo;
-        ws.run_len[idx] = len;
+        s_lo[idx] = lo;
         s_len[idx] = len;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < L; p += blockDim.x) {
+        int c = 0;
+#pragma unroll
+        for (int j = 0; j < kRuns; ++j) c += (s_len[p * kRuns + j] + stride - 1) / stride;
+        s_pos[p] = c;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         int acc = 0, tacc = 0;
         for (int p = 0; p < L; ++p) {
-            const int first = acc;
-            for (int j = 0; j < kRuns; ++j) {
-                ws.split_off[p * kRuns + j] = acc;
-                acc += (s_len[p * kRuns + j] + stride - 1) / stride;
-            }
-            ws.tile_off[p] = tacc;
-            tacc += (acc - first + kMergeGroup - 1) / kMergeGroup;
+            const int c = s_pos[p];
+            s_pos[p] = acc;
+            s_toff[p] = tacc;
+            acc += c;
+            tacc += (c + kMergeGroup - 1) / kMergeGroup;
         }
-        ws.split_off[L * kRuns] = acc;
-        ws.tile_off[L] = tacc;
+        s_pos[L] = acc;
+        s_toff[L] = tacc;
         const bool ok = acc <= ws.split_cap && tacc <= ws.tile_cap;
-        if (!ok) raise_status(status, PACES_ERR_CAPACITY);
-        ws.counters[0] = ok ? acc : 0;
-        ws.counters[1] = ok ? tacc : 0;
-        ws.counters[2] = 0;
-        ws.counters[3] = 0;
-        ws.counters[4] = 0;
+        s_total = ok ? acc : 0;
         s_tiles = ok ? tacc : 0;
+        if (blockIdx.x == 0) {
+            if (!ok) raise_status(status, PACES_ERR_CAPACITY);
+            ws.counters[0] = s_total;
+            ws.counters[1] = s_tiles;
+            ws.counters[2] = 0;
+            ws.counters[3] = 0;
+            ws.counters[4] = 0;
+            ws.counters[5] = 0;
+        }
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < s_tiles; t += blockDim.x) ws.tile_state[t] = 0ull;
-}
+    for (int p = threadIdx.x; p < L; p += blockDim.x) {
+        int acc = s_pos[p];
+#pragma unroll
+        for (int j = 0; j < kRuns; ++j) {
+            s_off[p * kRuns + j] = acc;
+            acc += (s_len[p * kRuns + j] + stride - 1) / stride;
+        }
+    }
+    if (threadIdx.x == 0) s_off[nr] = s_pos[L];
+    __syncthreads();
+    if (blockIdx.x == 0) {
+        for (int idx = threadIdx.x; idx < nr; idx += blockDim.x) {
+            ws.run_lo[idx] = s_lo[idx];
+            ws.run_len[idx] = s_len[idx];
+            ws.split_off[idx] = s_off[idx];
+        }
+        for (int p = threadIdx.x; p <= L; p += blockDim.x) ws.tile_off[p] = s_toff[p];
+        if (threadIdx.x == 0) ws.split_off[nr] = s_off[nr];
+    }
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < s_tiles; t += gridDim.x * blockDim.x)
+        ws.tile_state[t] = 0ull;
 
-template <int NW>
-__global__ void __launch_bounds__(256) merge_split_kernel(ModelDev m, const uint64_t* __restrict__ X,
-                                                          const uint64_t* __restrict__ Y, MergeWs ws, int stride) {
-    const int total = ws.counters[0];
-    const int nr = m.L * kRuns;
+    const int total = s_total;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
-        const int r = find_segment(ws.split_off, nr, s);
+        const int r = find_segment(s_off, nr, s);
         const int p = r / kRuns, j = r % kRuns;
-        const int i = (s - ws.split_off[r]) * stride;
+        const int i = (s - s_off[r]) * stride;
         Key<NW> k;
         int f;
-        run_elem<NW>(m, X, Y, ws, p, j, ws.run_lo[r] + i, k, f);
+        run_elem<NW>(m, X, Y, ws, p, j, s_lo[r] + i, k, f);
         // the bounds in the other runs: all searches advance one step per round, so their
         // dependent loads are in flight together
         int lo_[kRuns], a_[kRuns], b_[kRuns];
 #pragma unroll
         for (int jj = 0; jj < kRuns; ++jj) {
-            lo_[jj] = ws.run_lo[p * kRuns + jj];
+            lo_[jj] = s_lo[p * kRuns + jj];
             a_[jj] = 0;
-            b_[jj] = jj == j ? 0 : ws.run_len[p * kRuns + jj];
+            b_[jj] = jj == j ? 0 : s_len[p * kRuns + jj];
         }
         for (;;) {
             bool any = false;
@@ -429,10 +466,44 @@ __global__ void __launch_bounds__(256) merge_desc_kernel(ModelDev m, const uint6
     }
 }
 
+// Output block offsets for blocks without tiles, the output count, capacity check (split:
+// the same for the new part).
+// Run by one thread of the tile block that finishes last.
+__device__ void merge_finalize(const ModelDev& m, const MergeWs& ws, const MergeOut& out, int* ceiling_out,
+                               int ceiling_add, int split, int* status) {
+    const int L = m.L;
+    const int ntiles = __ldcg(ws.counters + 1);
+    long long packed = 0;
+    if (ntiles > 0) packed = (long long)(__ldcg(ws.tile_state + ntiles - 1) & kLbMask);
+    long long total = packed & kPackLow, total_n = packed >> kPackShift;
+    if (total > out.cap) {
+        raise_status(status, PACES_ERR_CAPACITY);
+        total = out.cap;
+    }
+    out.blk[L] = int(total);
+    for (int p = L - 1; p >= 0; --p) {
+        if (ntiles == 0 || __ldcg(ws.tile_off + p) == __ldcg(ws.tile_off + p + 1)) out.blk[p] = out.blk[p + 1];
+        if (out.blk[p] > total) out.blk[p] = int(total);
+    }
+    if (split) {
+        if (total_n > out.new_cap) {
+            raise_status(status, PACES_ERR_CAPACITY);
+            total_n = out.new_cap;
+        }
+        out.new_blk[L] = int(total_n);
+        for (int p = L - 1; p >= 0; --p) {
+            if (ntiles == 0 || __ldcg(ws.tile_off + p) == __ldcg(ws.tile_off + p + 1)) out.new_blk[p] = out.new_blk[p + 1];
+            if (out.new_blk[p] > total_n) out.new_blk[p] = int(total_n);
+        }
+    }
+    ws.counters[4] = int(total);
+    if (ceiling_out) *ceiling_out = (ceiling_add ? *ceiling_out : 0) + __ldcg(ws.counters + 3);
+}
+
 template <int NW, int MODE>
 __global__ void __launch_bounds__(kTileThreads)
 merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __restrict__ Y, MergeWs ws,
-                  int tmax, MergeOut out, int* status) {
+                  int tmax, MergeOut out, int* ceiling_out, int ceiling_add, int* status) {
     constexpr bool ASM = MODE == MERGE_ASSEMBLE;
     constexpr bool SPLIT = MODE == MERGE_EXPAND_SPLIT;
     constexpr bool MAPS = ASM || SPLIT;
@@ -462,7 +533,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
         if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
         __syncthreads();
         const int t = s_t;
-        if (t >= ntiles) return;
+        if (t >= ntiles) break;
         // tile set-up: the precomputed descriptor
         if (tid < kDescWords)
             reinterpret_cast<int*>(&s_d)[tid] =
@@ -663,40 +734,15 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
         }
         __syncthreads();
     }
-}
-
-// Output block offsets for blocks without tiles, the output count, capacity check (split:
-// the same for the new part).
-__global__ void merge_finalize_kernel(ModelDev m, MergeWs ws, MergeOut out, int* ceiling_out, int ceiling_add,
-                                      int split, int* status) {
-    if (threadIdx.x != 0) return;
-    const int L = m.L;
-    const int ntiles = ws.counters[1];
-    long long packed = 0;
-    if (ntiles > 0) packed = (long long)(ws.tile_state[ntiles - 1] & kLbMask);
-    long long total = packed & kPackLow, total_n = packed >> kPackShift;
-    if (total > out.cap) {
-        raise_status(status, PACES_ERR_CAPACITY);
-        total = out.cap;
-    }
-    out.blk[L] = int(total);
-    for (int p = L - 1; p >= 0; --p) {
-        if (ntiles == 0 || ws.tile_off[p] == ws.tile_off[p + 1]) out.blk[p] = out.blk[p + 1];
-        if (out.blk[p] > total) out.blk[p] = int(total);
-    }
-    if (split) {
-        if (total_n > out.new_cap) {
-            raise_status(status, PACES_ERR_CAPACITY);
-            total_n = out.new_cap;
-        }
-        out.new_blk[L] = int(total_n);
-        for (int p = L - 1; p >= 0; --p) {
-            if (ntiles == 0 || ws.tile_off[p] == ws.tile_off[p + 1]) out.new_blk[p] = out.new_blk[p + 1];
-            if (out.new_blk[p] > total_n) out.new_blk[p] = int(total_n);
+    // the block that finishes last writes the block offsets and the totals: every block makes
+    // its tiles' words and counts visible before it takes its exit ticket
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&ws.counters[5], 1) == int(gridDim.x) - 1) {
+            __threadfence();
+            merge_finalize(m, ws, out, ceiling_out, ceiling_add, SPLIT ? 1 : 0, status);
         }
     }
-    ws.counters[4] = int(total);
-    if (ceiling_out) *ceiling_out = (ceiling_add ? *ceiling_out : 0) + ws.counters[3];
 }
 
 // H neighbour table from the per-source index maps (assemble only).  Source i of the
@@ -750,14 +796,15 @@ size_t tile_smem_bytes(int tmax, int mode) {
 
 template <int NW, int MODE>
 void launch_tile(int tmax, const ModelDev& m, const uint64_t* X, const uint64_t* Y, const MergeWs& ws,
-                 const MergeOut& out, int* status, int num_sms, cudaStream_t st) {
+                 const MergeOut& out, int* ceiling_out, int ceiling_add, int* status, int num_sms, cudaStream_t st) {
     const size_t smem = tile_smem_bytes<NW>(tmax, MODE);
     auto kfn = merge_tile_kernel<NW, MODE>;
     cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTileThreads, smem);
     const int grid = num_sms * max(per_sm, 1);
-    kfn<<<grid < ws.tile_cap ? grid : max(ws.tile_cap, 1), kTileThreads, smem, st>>>(m, X, Y, ws, tmax, out, status);
+    kfn<<<grid < ws.tile_cap ? grid : max(ws.tile_cap, 1), kTileThreads, smem, st>>>(m, X, Y, ws, tmax, out, ceiling_out,
+                                                                                  ceiling_add, status);
 }
 
 template <int NW>
@@ -774,16 +821,16 @@ int launch_merge_t(int mode, int stride, const ModelDev& m, const uint64_t* X, c
         y_blk = x_blk;
     }
     const int tmax = merge_tmax(stride);
-    merge_plan_kernel<<<1, 1024, 0, st>>>(m, x_blk, y_blk, ws, stride, status);
     const int g = grid_for(ws.split_cap, 256, num_sms * 8);
-    merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, ws, stride);
+    merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, x_blk, y_blk, ws, stride, status);
     merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
     merge_desc_kernel<NW><<<grid_for(ws.tile_cap, 256, num_sms * 8), 256, 0, st>>>(m, X, Y, ws, tmax, status);
-    if (mode == MERGE_ASSEMBLE) launch_tile<NW, MERGE_ASSEMBLE>(tmax, m, X, Y, ws, out, status, num_sms, st);
-    else if (mode == MERGE_EXPAND_SPLIT) launch_tile<NW, MERGE_EXPAND_SPLIT>(tmax, m, X, Y, ws, out, status, num_sms, st);
-    else launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, out, status, num_sms, st);
-    merge_finalize_kernel<<<1, 32, 0, st>>>(m, ws, out, ceiling_out, ceiling_add, mode == MERGE_EXPAND_SPLIT ? 1 : 0,
-                                            status);
+    if (mode == MERGE_ASSEMBLE)
+        launch_tile<NW, MERGE_ASSEMBLE>(tmax, m, X, Y, ws, out, ceiling_out, ceiling_add, status, num_sms, st);
+    else if (mode == MERGE_EXPAND_SPLIT)
+        launch_tile<NW, MERGE_EXPAND_SPLIT>(tmax, m, X, Y, ws, out, ceiling_out, ceiling_add, status, num_sms, st);
+    else
+        launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, out, ceiling_out, ceiling_add, status, num_sms, st);
     if (mode == MERGE_ASSEMBLE && !split_input && out.nbr)
         nbr_fill_kernel<<<grid_for(out.map_cap, 256, num_sms * 8), 256, 0, st>>>(m, x_blk, out);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;

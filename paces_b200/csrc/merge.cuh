@@ -40,6 +40,7 @@ struct MergeWs {
     int* split_off;  // [L*kRuns + 1] prefix of splitter counts
     int* tile_off;   // [L + 1] prefix of tile counts
     int* counters;   // [0] splitters [1] tiles [2] tile ticket [3] ceiling holes [4] output count
+                     // [5] tile blocks done
     int* split_co;   // [split_cap * kRuns]
     int* split_rank; // [split_cap]
     int* ord_co;     // [split_cap * kRuns]

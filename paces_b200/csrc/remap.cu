@@ -32,34 +32,46 @@ __device__ int merge_path(const uint64_t* __restrict__ A, int na, const uint64_t
     return begin;
 }
 
-__global__ void remap_plan_kernel(ModelDev m, const int* __restrict__ ob, const int* __restrict__ nb,
-                                  RemapWs ws, int tile, int* status) {
-    if (threadIdx.x != 0) return;
-    int acc = 0;
-    for (int p = 0; p < m.L; ++p) {
-        ws.tile_off[p] = acc;
-        const int tot = (ob[p + 1] - ob[p]) + (nb[p + 1] - nb[p]);
-        acc += (tot + tile - 1) / tile;
-    }
-    ws.tile_off[m.L] = acc;
-    if (acc > ws.tile_cap) {
-        raise_status(status, PACES_ERR_CAPACITY);
-        acc = 0;
-    }
-    ws.counters[0] = acc;
-}
-
 // split[2t] / split[2t+1]: old elements before the tile's first / past its last diagonal.
+// Every block first derives the tile offsets per exciton block (tiles of `tile` diagonals of
+// the merged old + new block) from the block offsets; block 0 publishes them and the tile
+// count for the tile kernel.
 template <int NW>
 __global__ void __launch_bounds__(256) remap_split_kernel(ModelDev m, const uint64_t* __restrict__ old_keys,
                                                           const int* __restrict__ ob,
                                                           const uint64_t* __restrict__ new_keys,
-                                                          const int* __restrict__ nb, RemapWs ws, int tile) {
-    const int ntiles = ws.counters[0];
+                                                          const int* __restrict__ nb, RemapWs ws, int tile,
+                                                          int* status) {
+    __shared__ int s_toff[kMaxSites + 1];
+    __shared__ int s_ntiles;
+    for (int p = threadIdx.x; p < m.L; p += blockDim.x) {
+        const int tot = (ob[p + 1] - ob[p]) + (nb[p + 1] - nb[p]);
+        s_toff[p] = (tot + tile - 1) / tile;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int p = 0; p < m.L; ++p) {
+            const int c = s_toff[p];
+            s_toff[p] = acc;
+            acc += c;
+        }
+        s_toff[m.L] = acc;
+        const bool ok = acc <= ws.tile_cap;
+        s_ntiles = ok ? acc : 0;
+        if (blockIdx.x == 0) {
+            if (!ok) raise_status(status, PACES_ERR_CAPACITY);
+            ws.counters[0] = s_ntiles;
+        }
+    }
+    __syncthreads();
+    if (blockIdx.x == 0)
+        for (int p = threadIdx.x; p <= m.L; p += blockDim.x) ws.tile_off[p] = s_toff[p];
+    const int ntiles = s_ntiles;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * ntiles; i += gridDim.x * blockDim.x) {
         const int t = i >> 1;
-        const int p = find_segment(ws.tile_off, m.L, t);
-        const int tl = t - ws.tile_off[p];
+        const int p = find_segment(s_toff, m.L, t);
+        const int tl = t - s_toff[p];
         const int o0 = ob[p], no = ob[p + 1] - o0;
         const int n0 = nb[p], nn = nb[p + 1] - n0;
         const int d = (i & 1) ? min((tl + 1) * tile, no + nn) : tl * tile;
@@ -156,9 +168,8 @@ template <int NW, bool C64>
 int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const void* opsi,
                    const uint64_t* nk, const int* nb, void* npsi, const RemapWs& ws, int* status,
                    int num_sms, cudaStream_t st) {
-    remap_plan_kernel<<<1, 32, 0, st>>>(m, ob, nb, ws, remap_tile(NW), status);
     remap_split_kernel<NW><<<grid_for(int64_t(ws.tile_cap) * 2, 256, num_sms * 2), 256, 0, st>>>(m, ok, ob, nk, nb, ws,
-                                                                                                remap_tile(NW));
+                                                                                                remap_tile(NW), status);
     remap_tile_kernel<NW, C64><<<grid_for(ws.tile_cap, 1, num_sms * 4), kRThreads, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi,
                                                                                             ws);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
@@ -166,8 +177,8 @@ int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const v
 
 // Scratch of the workspace-free remap (paces_remap_noalloc): block tile offsets, the tile
 // counter and two splits per tile, 256 KiB in total.  Every GPU that loads the library
-// holds one copy until the process exits.  Nothing in it has to start at zero: the plan
-// kernel rewrites the offsets and the counter, the split kernel every split it uses.
+// holds one copy until the process exits.  Nothing in it has to start at zero: the split
+// kernel rewrites the offsets, the counter and every split it uses.
 constexpr size_t kStaticRemapBytes = size_t(256) << 10;
 constexpr size_t kStaticHeaderBytes = 1024;  // tile_off[kMaxSites+1] and counters
 
