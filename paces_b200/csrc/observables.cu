@@ -88,8 +88,12 @@ obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict
 }
 
 // `uniform`: every field is `ub` bits wide and word q holds sites q*fpw .. q*fpw+fpw-1
-// MSB-first (NW <= 4), so thread-private register accumulators cover all sites.
-template <int NW, bool C64>
+// MSB-first (NW <= 4), so thread-private register accumulators cover all sites.  UB = 4
+// (the width for occupation cut-offs up to 15) takes the fields at constant shifts; UB = 0
+// reads the width from `ub`.  A field value becomes a double exactly by the 2^52 offset (its
+// bits under the exponent of 2^52, minus 2^52): two FP64-pipe operations instead of an
+// integer conversion, whose pipe is a quarter as wide.
+template <int NW, bool C64, int UB>
 __global__ void __launch_bounds__(kOThreads, NW <= 2 ? 2 : 1)
 obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict__ blk,
                  const uint32_t* __restrict__ meta, const void* __restrict__ psi, double* __restrict__ part,
@@ -167,11 +171,15 @@ obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __res
 #pragma unroll
                 for (int q = 0; q < NW; ++q) {
                     const uint64_t word = k.w[q];
+                    const uint32_t whi = uint32_t(word >> 32), wlo = uint32_t(word);
 #pragma unroll
                     for (int f = 0; f < kFpwMax; ++f) {
-                        if (f < fpw) {
-                            const uint32_t nf = uint32_t((word >> (64 - ub * (f + 1))) & umask);
-                            racc[q * kFpwMax + f] += w * double(nf);
+                        if (UB == 4 || f < fpw) {
+                            uint32_t nf;
+                            if constexpr (UB == 4) nf = ((f < 8 ? whi : wlo) >> (28 - 4 * (f & 7))) & 15u;
+                            else nf = uint32_t((word >> (64 - ub * (f + 1))) & umask);
+                            const double dn = __hiloint2double(0x43300000, int(nf)) - 4503599627370496.0;
+                            racc[q * kFpwMax + f] = fma(w, dn, racc[q * kFpwMax + f]);
                         }
                     }
                 }
@@ -482,11 +490,12 @@ template <int NW, bool C64>
 int launch_obs_t(const ModelDev& m, const uint64_t* keys, const int* blk, const int* nbr,
                  int64_t nbr_cap, const uint32_t* meta, const void* psi, int what, double* partials,
                  const ObsTarget& out, int num_sms, cudaStream_t st) {
-    static int grid_e = 0, grid_ex = 0, grid_s = 0;
+    static int grid_e = 0, grid_ex = 0, grid_s = 0, grid_s4 = 0;
     if (grid_e == 0) {
         grid_e = wave_blocks(obs_energy_kernel<C64, false>, num_sms);
         grid_ex = wave_blocks(obs_energy_kernel<C64, true>, num_sms);
-        grid_s = wave_blocks(obs_sites_kernel<NW, C64>, num_sms);
+        grid_s = wave_blocks(obs_sites_kernel<NW, C64, 0>, num_sms);
+        if constexpr (NW <= 4) grid_s4 = wave_blocks(obs_sites_kernel<NW, C64, 4>, num_sms);
     }
     const bool energy = (what & PACES_OBS_ENERGY) != 0;
     const bool sites = (what & PACES_OBS_SITES) != 0;
@@ -508,9 +517,19 @@ int launch_obs_t(const ModelDev& m, const uint64_t* keys, const int* blk, const 
         bool uniform = ub >= 4 && NW <= 4;
         for (int s = 0; s < m.L && uniform; ++s)
             uniform = m.bits[s] == ub && m.word[s] == s / fpw && m.shift[s] == 64 - ub * (s % fpw + 1);
-        obs_sites_kernel<NW, C64><<<grid_s, kOThreads, 0, st>>>(m, keys, blk, meta, psi, part_s, uniform ? 1 : 0,
-                                                               ub, fpw);
-        nb_s = grid_s;
+        bool done = false;
+        if constexpr (NW <= 4) {
+            if (uniform && ub == 4) {
+                obs_sites_kernel<NW, C64, 4><<<grid_s4, kOThreads, 0, st>>>(m, keys, blk, meta, psi, part_s, 1, ub, fpw);
+                nb_s = grid_s4;
+                done = true;
+            }
+        }
+        if (!done) {
+            obs_sites_kernel<NW, C64, 0><<<grid_s, kOThreads, 0, st>>>(m, keys, blk, meta, psi, part_s,
+                                                                      uniform ? 1 : 0, ub, fpw);
+            nb_s = grid_s;
+        }
     }
     obs_final_kernel<<<sites ? 3 + 2 * m.L : 3, 256, 0, st>>>(m.L, nb_e, part_e, nb_s, part_s, out);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
