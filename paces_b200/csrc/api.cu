@@ -381,7 +381,10 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
                            "step/weights");
         weights = w;
     }
-    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, weights, prm->maxstates,
+    // without look-ahead weights the same buffer holds |psi| after the first radix round
+    void* wscratch = weights ? nullptr : at<void>(ws, l.v_TA);
+    PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, weights, wscratch,
+                                          prm->maxstates,
                                           prm->shuffle, prm->shuffle_seed, prm->step_index, trunc_ws(l, ws), p.A.keys,
                                           p.A.blk, p.A.cap, at<float>(ws, l.aw), &rec->n_tied, &rec->n_select, status, c->num_sms, st),
                        "step/truncate");
@@ -860,7 +863,7 @@ int paces_truncate(paces_ctx* c, const paces_basis* in, const void* psi, int64_t
     const Layout l = fit_layout(c, ws_bytes);
     if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
     PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, psi, nullptr,
-                                          maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
+                                          at<void>(ws, l.v_TA), maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
                                           out->blk, out->cap, nullptr, nullptr, nullptr, c->d_status, c->num_sms,
                                           reinterpret_cast<cudaStream_t>(stream)),
                        "truncate");
@@ -874,7 +877,7 @@ int paces_truncate_weighted(paces_ctx* c, const paces_basis* in, const double* w
     const Layout l = fit_layout(c, ws_bytes);
     if (in->cap > l.cap) return fail(c, PACES_ERR_CAPACITY, "workspace holds %lld states, input basis %lld", (long long)l.cap, (long long)in->cap);
     PACES_CHECK_LAUNCH(c, launch_truncate(c->nw, c->precision == PACES_C64, c->m, in->keys, in->blk, nullptr, weights,
-                                          maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
+                                          nullptr, maxstates, shuffle, shuffle_seed, step_index, trunc_ws(l, ws), out->keys,
                                           out->blk, out->cap, nullptr, nullptr, nullptr, c->d_status, c->num_sms,
                                           reinterpret_cast<cudaStream_t>(stream)),
                        "truncate_weighted");

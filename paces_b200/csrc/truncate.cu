@@ -25,10 +25,18 @@ __host__ __device__ constexpr int round_bits(int r) { return r < 5 ? 12 : 4; }
 
 // The ranked weight of state i: WK 0 = |psi| of complex128 amplitudes, 1 = |psi| of
 // complex64 amplitudes, 2 = precomputed non-negative fp64 weights (the look-ahead
-// weighting).  Non-negative doubles order like their bit patterns.  The load and the
-// conversion are separate so that loops can issue several loads before the first use.
+// weighting, or |psi| of complex128 amplitudes stored by the first radix round), 3 = |psi|
+// of complex64 amplitudes stored as fp32 by the first round (exact: hypotf's result,
+// widened like WK 1 widens it).  Non-negative doubles order like their bit patterns.  The
+// load and the conversion are separate so that loops can issue several loads before the
+// first use.
 template <int WK>
-using RawW = typename std::conditional<WK == 0, double2, typename std::conditional<WK == 1, float2, double>::type>::type;
+using RawW = typename std::conditional<
+    WK == 0, double2,
+    typename std::conditional<WK == 1, float2, typename std::conditional<WK == 2, double, float>::type>::type>::type;
+
+// the kind the first round stores for later passes (WK 0 -> 2, WK 1 -> 3)
+__host__ __device__ constexpr int stored_kind(int wk) { return wk == 1 ? 3 : 2; }
 
 template <int WK>
 __device__ __forceinline__ RawW<WK> load_raw(const void* psi, int64_t i) {
@@ -40,7 +48,7 @@ __device__ __forceinline__ unsigned long long raw_bits(const RawW<WK>& z, int* s
     double w;
     if constexpr (WK == 1) w = double(hypotf(z.x, z.y));
     else if constexpr (WK == 0) w = hypot(z.x, z.y);
-    else w = z;
+    else w = double(z);
     if (!(w <= 1.7976931348623157e308)) raise_status(status, PACES_ERR_NONFINITE);
     return (unsigned long long)__double_as_longlong(w);
 }
@@ -136,9 +144,11 @@ __global__ void __launch_bounds__(1024) trunc_select_kernel(TruncWs ws, int base
 // pass per round -- no candidate list, so no global counter and no scattered writes.  Lanes
 // with the same digit add to the shared histogram once (warp-aggregated: in round 0 most
 // states share a few binades).
-template <int WK>
+// STORE (round 0 of |psi| kinds): also write every state's weight to `wout` in the stored
+// kind, which the later passes read instead of recomputing |psi|.
+template <int WK, bool STORE>
 __global__ void __launch_bounds__(256) trunc_hist_pass_kernel(const void* __restrict__ psi, TruncWs ws, int round,
-                                                              int* status) {
+                                                              void* __restrict__ wout, int* status) {
     __shared__ unsigned h[4096];
     if (!ws.sel[SEL_W + 3]) return;
     const int bits = round_bits(round), shift = round_shift(round);
@@ -166,6 +176,11 @@ __global__ void __launch_bounds__(256) trunc_hist_pass_kernel(const void* __rest
             unsigned bin = 0xffffffffu;
             if (i < S) {
                 const unsigned long long k = raw_bits<WK>(z[u], status);
+                if constexpr (STORE) {
+                    const double wv = __longlong_as_double((long long)k);
+                    if constexpr (stored_kind(WK) == 3) reinterpret_cast<float*>(wout)[i] = float(wv);
+                    else reinterpret_cast<double*>(wout)[i] = wv;
+                }
                 match = (k & msk) == pre;
                 if (match) bin = unsigned((k >> shift) & dm);
             }
@@ -335,9 +350,12 @@ __global__ void __launch_bounds__(1024) trunc_scan_kernel(TruncWs ws) {
 // hash keeps (ballots); pass 2 walks the same states 32 at a time and places every kept
 // state at its rank among the kept ones (ballot prefixes).  Lanes read consecutive keys
 // and the kept ones write consecutive outputs, so both sides coalesce.
-template <int NW, int WK>
+// The weights come from `wsrc` (kind WK); when every state is kept the selection rounds
+// did not run, so the out_w weights come from `psi` (kind WKA).
+template <int NW, int WK, int WKA>
 __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint64_t* __restrict__ x_keys,
                                                           const int* __restrict__ x_blk,
+                                                          const void* __restrict__ wsrc,
                                                           const void* __restrict__ psi, TruncWs ws,
                                                           uint64_t seed, uint64_t step,
                                                           uint64_t* __restrict__ out_keys,
@@ -370,17 +388,22 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
         int ca = 0, ct = 0, ch = 0;
         if (!all || out_w) {
             constexpr int kU = 4;  // loads in flight per lane
-            for (int q0 = q_lo; q0 < q_hi; q0 += 32 * kU) {
-                RawW<WK> z[kU];
+            if (WK != WKA && all) {
+                // every state kept (early steps only): out_w from the amplitudes
+                for (int q = q_lo + lane; q < q_hi; q += 32) s_k[q] = raw_bits<WKA>(load_raw<WKA>(psi, i0 + q), status);
+            } else {
+                for (int q0 = q_lo; q0 < q_hi; q0 += 32 * kU) {
+                    RawW<WK> z[kU];
 #pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    const int q = q0 + 32 * u + lane;
-                    if (q < q_hi) z[u] = load_raw<WK>(psi, i0 + q);
-                }
+                    for (int u = 0; u < kU; ++u) {
+                        const int q = q0 + 32 * u + lane;
+                        if (q < q_hi) z[u] = load_raw<WK>(wsrc, i0 + q);
+                    }
 #pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    const int q = q0 + 32 * u + lane;
-                    if (q < q_hi) s_k[q] = raw_bits<WK>(z[u], status);
+                    for (int u = 0; u < kU; ++u) {
+                        const int q = q0 + 32 * u + lane;
+                        if (q < q_hi) s_k[q] = raw_bits<WK>(z[u], status);
+                    }
                 }
             }
             __syncwarp();
@@ -492,31 +515,36 @@ __global__ void trunc_finalize_kernel(ModelDev m, const int* __restrict__ x_blk,
     if (n_kept_out) *n_kept_out = int(total);
 }
 
-template <int NW, int WK>
-int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_blk, const void* psi,
+// WK: the kind of `psi`.  WKS: the kind the passes after round 0 read from `src` -- WK
+// itself reading `psi`, or the stored kind reading the weights round 0 wrote to scratch.
+template <int NW, int WK, int WKS>
+int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_blk, const void* psi, void* scratch,
                       int64_t maxstates, int shuffle, uint64_t seed, uint64_t step, const TruncWs& ws,
                       uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w, int* n_tied_out, int* n_kept_out,
                       int* status, int num_sms, cudaStream_t st) {
+    constexpr bool kStore = WKS != WK;
+    const void* src = kStore ? scratch : psi;
     const int g = grid_for(ws.cap, 1024, num_sms * 4);          // streaming passes
     const int gt = grid_for(ws.cap, kTruncTile, num_sms * 4);   // passes over 4096-state tiles
     const int rounds = weight_rounds(WK);
     trunc_init_kernel<<<1, 1024, 0, st>>>(m, x_blk, maxstates, ws);
     for (int r = 0; r < rounds; ++r) {
-        trunc_hist_pass_kernel<WK><<<g, 256, 0, st>>>(psi, ws, r, status);
+        if (r == 0) trunc_hist_pass_kernel<WK, kStore><<<g, 256, 0, st>>>(psi, ws, r, scratch, status);
+        else trunc_hist_pass_kernel<WKS, false><<<g, 256, 0, st>>>(src, ws, r, nullptr, status);
         trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_W, r, r == rounds - 1);
     }
     if (shuffle) {
         trunc_shuffle_prep_kernel<<<1, 32, 0, st>>>(ws, status);
-        trunc_collect_ties_kernel<WK><<<g, 256, 0, st>>>(psi, ws, seed, step, status);
+        trunc_collect_ties_kernel<WKS><<<g, 256, 0, st>>>(src, ws, seed, step, status);
         for (int r = 0; r < kRounds; ++r) {
             trunc_hist_cand_kernel<<<g, 256, 0, st>>>(ws, SEL_H, r);
             trunc_select_kernel<<<1, 1024, 0, st>>>(ws, SEL_H, r, 0);
         }
     }
-    trunc_count_kernel<WK><<<gt, 256, 0, st>>>(psi, ws, seed, step, status);
+    trunc_count_kernel<WKS><<<gt, 256, 0, st>>>(src, ws, seed, step, status);
     trunc_scan_kernel<<<1, 1024, 0, st>>>(ws);
-    trunc_write_kernel<NW, WK><<<gt, 256, 0, st>>>(m, x_keys, x_blk, psi, ws, seed, step, out_keys,
-                                                   out_blk, out_cap, out_w, status);
+    trunc_write_kernel<NW, WKS, WK><<<gt, 256, 0, st>>>(m, x_keys, x_blk, src, psi, ws, seed, step, out_keys,
+                                                        out_blk, out_cap, out_w, status);
     trunc_finalize_kernel<<<1, 32, 0, st>>>(m, x_blk, maxstates, ws, out_blk, out_cap, n_tied_out, n_kept_out,
                                             out_w ? out_w + out_cap : nullptr, status);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
@@ -524,28 +552,32 @@ int launch_truncate_t(const ModelDev& m, const uint64_t* x_keys, const int* x_bl
 
 template <int NW>
 int dispatch_prec(bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                  const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed,
+                  const void* psi, const double* weights, void* scratch, int64_t maxstates, int shuffle, uint64_t seed,
                   uint64_t step, const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap,
                   float* out_w, int* n_tied_out, int* n_kept_out, int* status, int num_sms, cudaStream_t st) {
-    if (weights)
-        return launch_truncate_t<NW, 2>(m, x_keys, x_blk, weights, maxstates, shuffle, seed, step, ws,
-                                        out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
-    if (c64)
-        return launch_truncate_t<NW, 1>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
-                                        out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
-    return launch_truncate_t<NW, 0>(m, x_keys, x_blk, psi, maxstates, shuffle, seed, step, ws,
-                                    out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
+#define PACES_TRUNC_LAUNCH(WK, WKS, SRC)                                                                     \
+    return launch_truncate_t<NW, WK, WKS>(m, x_keys, x_blk, SRC, scratch, maxstates, shuffle, seed, step, ws, \
+                                          out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status,  \
+                                          num_sms, st)
+    if (weights) PACES_TRUNC_LAUNCH(2, 2, weights);
+    if (c64) {
+        if (scratch) PACES_TRUNC_LAUNCH(1, stored_kind(1), psi);
+        PACES_TRUNC_LAUNCH(1, 1, psi);
+    }
+    if (scratch) PACES_TRUNC_LAUNCH(0, stored_kind(0), psi);
+    PACES_TRUNC_LAUNCH(0, 0, psi);
+#undef PACES_TRUNC_LAUNCH
 }
 
 }  // namespace
 
 int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                    const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
-                    const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
+                    const void* psi, const double* weights, void* scratch, int64_t maxstates, int shuffle, uint64_t seed,
+                    uint64_t step, const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
                     int* n_tied_out, int* n_kept_out, int* status, int num_sms, cudaStream_t st) {
 #define PACES_TRUNC_CASE(N)                                                                       \
     case N:                                                                                       \
-        return dispatch_prec<N>(c64, m, x_keys, x_blk, psi, weights, maxstates, shuffle, seed, step, ws,   \
+        return dispatch_prec<N>(c64, m, x_keys, x_blk, psi, weights, scratch, maxstates, shuffle, seed, step, ws, \
                                 out_keys, out_blk, out_cap, out_w, n_tied_out, n_kept_out, status, num_sms, st);
     switch (nw) {
         PACES_TRUNC_CASE(1)

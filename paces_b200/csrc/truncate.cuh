@@ -45,12 +45,15 @@ inline int trunc_launches(int wk, bool shuffle) { return 5 + 2 * weight_rounds(w
 
 // weights (optional, one non-negative double per state): rank by these instead of |psi|
 // (the look-ahead weighting, lookahead.cu).
+// scratch (optional, without weights: 4 bytes per state for complex64, 8 for complex128):
+// the first radix round stores |psi| there and the later passes read it instead of the
+// amplitudes, so |psi| is computed once per state.
 // out_w (optional, out_cap + 1 floats): the ranked weight (|psi|) of every kept state in the
 // new basis' order, and at out_w[out_cap] the cut -- the weight of the smallest kept state, 0
 // when nothing was dropped.
 int launch_truncate(int nw, bool c64, const ModelDev& m, const uint64_t* x_keys, const int* x_blk,
-                    const void* psi, const double* weights, int64_t maxstates, int shuffle, uint64_t seed, uint64_t step,
-                    const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
+                    const void* psi, const double* weights, void* scratch, int64_t maxstates, int shuffle, uint64_t seed,
+                    uint64_t step, const TruncWs& ws, uint64_t* out_keys, int* out_blk, int64_t out_cap, float* out_w,
                     int* n_tied_out, int* n_kept_out, int* status, int num_sms, cudaStream_t st);
 
 }  // namespace paces
