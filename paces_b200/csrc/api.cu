@@ -482,6 +482,7 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.nbr_cap = p.h->cap;
         mo.maps = at<int>(ws, l.maps);
         mo.map_cap = l.cap;
+        mo.self_rows_filled = split ? 1 : 0;  // nbr_fill_split writes the rows of the enlarged basis
         PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, cur->keys, cur->blk,
                                            split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(c, l, ws),
                                            mo, &rec->ceiling_hits, split ? 1 : 0, status, c->num_sms, st),

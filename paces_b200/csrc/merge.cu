@@ -691,7 +691,9 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
                     const uint32_t ntot = total_phonons(m, k);
                     if (u < out.nbr_cap) {
                         out.meta[u] = uint32_t(p) | (nex << 8) | (ntot << 16);
-                        reinterpret_cast<int4*>(out.nbr)[u] = make_int4(-1, -1, -1, -1);
+                        // a group's first element is its self-run element when it has one
+                        if (!out.self_rows_filled || e >= s_off[1])
+                            reinterpret_cast<int4*>(out.nbr)[u] = make_int4(-1, -1, -1, -1);
                     }
                 }
                 if constexpr (SPLIT) {
@@ -821,25 +823,28 @@ int launch_merge_t(int mode, int stride, const ModelDev& m, const uint64_t* X, c
         y_blk = x_blk;
     }
     const int tmax = merge_tmax(stride);
+    MergeOut o = out;
+    if (mode == MERGE_ASSEMBLE && !split_input && out.nbr) o.self_rows_filled = 1;  // nbr_fill_kernel below
     const int g = grid_for(ws.split_cap, 256, num_sms * 8);
     merge_split_kernel<NW><<<g, 256, 0, st>>>(m, X, Y, x_blk, y_blk, ws, stride, status);
     merge_order_kernel<<<g, 256, 0, st>>>(m, ws);
     merge_desc_kernel<NW><<<grid_for(ws.tile_cap, 256, num_sms * 8), 256, 0, st>>>(m, X, Y, ws, tmax, status);
     if (mode == MERGE_ASSEMBLE)
-        launch_tile<NW, MERGE_ASSEMBLE>(tmax, m, X, Y, ws, out, ceiling_out, ceiling_add, status, num_sms, st);
+        launch_tile<NW, MERGE_ASSEMBLE>(tmax, m, X, Y, ws, o, ceiling_out, ceiling_add, status, num_sms, st);
     else if (mode == MERGE_EXPAND_SPLIT)
-        launch_tile<NW, MERGE_EXPAND_SPLIT>(tmax, m, X, Y, ws, out, ceiling_out, ceiling_add, status, num_sms, st);
+        launch_tile<NW, MERGE_EXPAND_SPLIT>(tmax, m, X, Y, ws, o, ceiling_out, ceiling_add, status, num_sms, st);
     else
-        launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, out, ceiling_out, ceiling_add, status, num_sms, st);
+        launch_tile<NW, MERGE_EXPAND>(tmax, m, X, Y, ws, o, ceiling_out, ceiling_add, status, num_sms, st);
     if (mode == MERGE_ASSEMBLE && !split_input && out.nbr)
-        nbr_fill_kernel<<<grid_for(out.map_cap, 256, num_sms * 8), 256, 0, st>>>(m, x_blk, out);
+        nbr_fill_kernel<<<grid_for(out.map_cap, 256, num_sms * 8), 256, 0, st>>>(m, x_blk, o);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
 // Neighbour table after a split expansion: sources are the expansion's input P (images
 // through the expansion's maps into its output B, then through the assembly's self map into
-// S) and the new part N (images through the assembly's maps).  Same row and reverse stores
-// as nbr_fill_kernel.
+// S) and the new part N (images through the assembly's maps).  Every row of B gets its
+// 16-byte store as in nbr_fill_kernel; reverse entries go only from N's rows, since those of
+// P's rows land in rows of B, which carry them already.
 __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const int* __restrict__ p_blk,
                                                              const int* __restrict__ n_blk,
                                                              const int* __restrict__ maps_e,
@@ -890,6 +895,9 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
         row.z = sd;  // NB_DOWN
         row.w = su;  // NB_UP
         reinterpret_cast<int4*>(nb)[q] = row;
+        // the images of P are states of the enlarged basis, sources themselves, whose own row
+        // holds the reverse entry: only the images of N can lie outside it
+        if (from_p) return;
         if (sr >= 0) nb[4 * int64_t(sr) + NB_LEFT] = q;
         if (sl >= 0) nb[4 * int64_t(sl) + NB_RIGHT] = q;
         if (su >= 0) nb[4 * int64_t(su) + NB_DOWN] = q;

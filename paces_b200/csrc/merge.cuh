@@ -111,6 +111,9 @@ struct MergeOut {
     int* new_blk;
     int* new_to_out;
     int64_t new_cap;
+    // assemble: the neighbour fill that follows writes every row of a self-run state whole,
+    // so the assembly initialises only the other rows (their entries arrive one by one)
+    int self_rows_filled;
 };
 
 // Merge modes.  EXPAND: keys only.  ASSEMBLE: keys, the H rows' metadata and neighbour
