@@ -175,8 +175,10 @@ obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __res
 #pragma unroll
                     for (int f = 0; f < kFpwMax; ++f) {
                         if (UB == 4 || f < fpw) {
+                            // UB = 4: the field left in place, n * 2^(28 - 4 (f mod 8)) of its
+                            // 32-bit half (one AND); the sum is scaled back at the end
                             uint32_t nf;
-                            if constexpr (UB == 4) nf = ((f < 8 ? whi : wlo) >> (28 - 4 * (f & 7))) & 15u;
+                            if constexpr (UB == 4) nf = (f < 8 ? whi : wlo) & (15u << (28 - 4 * (f & 7)));
                             else nf = uint32_t((word >> (64 - ub * (f + 1))) & umask);
                             const double dn = __hiloint2double(0x43300000, int(nf)) - 4503599627370496.0;
                             racc[q * kFpwMax + f] = fma(w, dn, racc[q * kFpwMax + f]);
@@ -212,7 +214,10 @@ obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __res
     if (uniform) {
 #pragma unroll
         for (int i = 0; i < kAcc; ++i) {
-            double v = racc[i];
+            // UB = 4 sums carry the field's position 2^(28 - 4 (f mod 8)): every product and
+            // partial sum is exactly that power of two times the unscaled one (no overflow or
+            // underflow at these magnitudes), so the scaled-back sum has the same bits
+            double v = UB == 4 ? racc[i] * (1.0 / double(1u << (28 - 4 * ((i % kFpwMax) & 7)))) : racc[i];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             const int q = i / kFpwMax, f = i % kFpwMax;
