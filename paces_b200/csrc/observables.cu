@@ -89,10 +89,10 @@ obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict
 
 // `uniform`: every field is `ub` bits wide and word q holds sites q*fpw .. q*fpw+fpw-1
 // MSB-first (NW <= 4), so thread-private register accumulators cover all sites.  UB = 4
-// (the width for occupation cut-offs up to 15) takes the fields at constant shifts; UB = 0
-// reads the width from `ub`.  A field value becomes a double exactly by the 2^52 offset (its
-// bits under the exponent of 2^52, minus 2^52): two FP64-pipe operations instead of an
-// integer conversion, whose pipe is a quarter as wide.
+// (the width for occupation cut-offs up to 15) masks each field in place at a constant
+// position; UB = 0 reads the width from `ub`.  A field value becomes a double exactly by
+// the 2^52 offset (its bits under the exponent of 2^52, minus 2^52): two FP64-pipe
+// operations instead of an integer conversion, whose pipe is a quarter as wide.
 template <int NW, bool C64, int UB>
 __global__ void __launch_bounds__(kOThreads, NW <= 2 ? 2 : 1)
 obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __restrict__ blk,
