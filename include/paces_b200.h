@@ -251,6 +251,7 @@ int paces_keys_to_ref(paces_ctx *ctx, const paces_basis *b, int32_t ref_words, u
                       paces_stream_t stream);
 
 /* ---- stages -------------------------------------------------------------------------- */
+/* Every stage uses its workspace `ws` as scratch: no input or output may lie inside it. */
 int paces_expand(paces_ctx *ctx, const paces_basis *in, paces_basis *out, void *ws,
                  size_t ws_bytes, paces_stream_t stream);
 int paces_assemble(paces_ctx *ctx, const paces_basis *in, paces_basis *out, paces_hmat *h,
