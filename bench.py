@@ -412,7 +412,7 @@ def run_ours(a):
     step_alg = statistics.mean(step_bytes(r, cs, eng.nw, a.enlarge_steps) for r in recs)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        v, desc, _, _ = oracle_sample(a, 1 << 16, 5, 0)
+        v, desc, _, _ = oracle_sample(a, 1 << 16, 15, 1)  # about 10 s of timed CPU work
         cpu = {"value": v, "unit": "time-steps/s", "cores": 1, "kind": "port", "sample": desc}
     if rank == 0:
         cfg = {"workload": workload_name(a), "nchain": a.nchain, "cutoff": 15, "g": a.g, "omega0": 1.0, "J": 1.0,
