@@ -117,6 +117,16 @@ obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __res
     const int64_t S = blk[L];
     const C* x = reinterpret_cast<const C*>(psi);
     double norm2 = 0.0;
+    int pcur = -1;      // uniform layouts: the warp's current exciton block (warp-uniform)
+    double eacc = 0.0;  // and this lane's running sum of |psi|^2 in it
+    auto flush_exc = [&]() {  // all lanes of the warp together
+        if (pcur < 0) return;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, o);
+        if (lane == 0) s_site[wid][pcur] += eacc;
+        eacc = 0.0;
+        pcur = -1;
+    };
     // the loads of the next 32 rows are issued before the current rows are summed (the
     // accumulators hold the occupancy at two blocks per SM, so the memory parallelism has
     // to come from within each thread)
@@ -156,16 +166,27 @@ obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __res
         }
         norm2 += w;
         if (uniform) {
-            // n_exc: a warp spans one or two exciton blocks
+            // n_exc: the warp's rows lie in one exciton block or straddle a few; while they stay
+            // in the block of the previous rows, each lane keeps adding to its own sum
             const int pme = int(mm & 0xffu);
             const int p0 = __shfl_sync(0xffffffffu, pme, 0);
             const int vlast = __shfl_sync(0xffffffffu, valid ? pme : -1, 31);
             const int p1 = vlast < 0 ? L - 1 : vlast;
-            for (int pp = p0; pp <= p1; ++pp) {
-                double v = (valid && pme == pp) ? w : 0.0;
+            if (p0 == p1 && p0 == pcur) {
+                eacc += w;
+            } else {
+                flush_exc();
+                if (p0 == p1) {
+                    pcur = p0;
+                    eacc = w;
+                } else {
+                    for (int pp = p0; pp <= p1; ++pp) {
+                        double v = (valid && pme == pp) ? w : 0.0;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) s_site[wid][pp] += v;
+                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                        if (lane == 0) s_site[wid][pp] += v;
+                    }
+                }
             }
             if (valid && w != 0.0) {
 #pragma unroll
@@ -208,6 +229,7 @@ obs_sites_kernel(ModelDev m, const uint64_t* __restrict__ keys, const int* __res
             }
         }
     }
+    flush_exc();
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) norm2 += __shfl_xor_sync(0xffffffffu, norm2, o);
     if (lane == 0) s_red[wid] = norm2;
