@@ -483,14 +483,17 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.maps = at<int>(ws, l.maps);
         mo.map_cap = l.cap;
         mo.self_rows_filled = split ? 1 : 0;  // nbr_fill_split writes the rows of the enlarged basis
+        // which rows those are, for nbr_fill_split (the Taylor term buffer is free until the
+        // propagation; S bytes)
+        mo.self_flag = split ? at<uint8_t>(ws, l.v_TA) : nullptr;
         PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, cur->keys, cur->blk,
                                            split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(c, l, ws),
                                            mo, &rec->ceiling_hits, split ? 1 : 0, status, c->num_sms, st),
                            "step/assemble");
         if (split)
             PACES_CHECK_LAUNCH(c, launch_nbr_fill_split(c->m, other->blk, nbasis.blk, at<int>(ws, l.maps_e),
-                                                        at<int>(ws, l.maps), at<int>(ws, l.n2b), l.cap, p.h->nbr,
-                                                        p.h->cap, c->num_sms, st),
+                                                        at<int>(ws, l.maps), at<int>(ws, l.n2b), mo.self_flag, l.cap,
+                                                        p.h->nbr, p.h->cap, c->num_sms, st),
                                "step/neighbours");
     }
     mark(3);

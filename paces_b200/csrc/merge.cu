@@ -694,6 +694,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
                         // a group's first element is its self-run element when it has one
                         if (!out.self_rows_filled || e >= s_off[1])
                             reinterpret_cast<int4*>(out.nbr)[u] = make_int4(-1, -1, -1, -1);
+                        if (out.self_flag) out.self_flag[u] = uint8_t(e < s_off[1]);
                     }
                 }
                 if constexpr (SPLIT) {
@@ -849,7 +850,8 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
                                                              const int* __restrict__ n_blk,
                                                              const int* __restrict__ maps_e,
                                                              const int* __restrict__ maps_s,
-                                                             const int* __restrict__ new_to_out, int64_t mc,
+                                                             const int* __restrict__ new_to_out,
+                                                             const uint8_t* __restrict__ self_flag, int64_t mc,
                                                              int* __restrict__ nb, int64_t nc) {
     __shared__ int s_pb[kMaxSites + 1], s_nb[kMaxSites + 1];
     const int L = m.L;
@@ -896,12 +898,13 @@ __global__ void __launch_bounds__(256) nbr_fill_split_kernel(ModelDev m, const i
         row.w = su;  // NB_UP
         reinterpret_cast<int4*>(nb)[q] = row;
         // the images of P are states of the enlarged basis, sources themselves, whose own row
-        // holds the reverse entry: only the images of N can lie outside it
+        // holds the reverse entry: only the images of N can lie outside it, and only those
+        // outside it (no self-run element) need the entry from here
         if (from_p) return;
-        if (sr >= 0) nb[4 * int64_t(sr) + NB_LEFT] = q;
-        if (sl >= 0) nb[4 * int64_t(sl) + NB_RIGHT] = q;
-        if (su >= 0) nb[4 * int64_t(su) + NB_DOWN] = q;
-        if (sd >= 0) nb[4 * int64_t(sd) + NB_UP] = q;
+        if (sr >= 0 && !__ldg(self_flag + sr)) nb[4 * int64_t(sr) + NB_LEFT] = q;
+        if (sl >= 0 && !__ldg(self_flag + sl)) nb[4 * int64_t(sl) + NB_RIGHT] = q;
+        if (su >= 0 && !__ldg(self_flag + su)) nb[4 * int64_t(su) + NB_DOWN] = q;
+        if (sd >= 0 && !__ldg(self_flag + sd)) nb[4 * int64_t(sd) + NB_UP] = q;
     };
     // two sources a grid stride apart per iteration: their map reads are in flight together
     const int64_t gs = int64_t(gridDim.x) * blockDim.x;
@@ -1002,11 +1005,12 @@ int launch_merge(int nw, int mode, int stride, const ModelDev& m, const uint64_t
 }
 
 int launch_nbr_fill_split(const ModelDev& m, const int* p_blk, const int* n_blk, const int* maps_e,
-                          const int* maps_s, const int* new_to_out, int64_t map_cap, int* nbr, int64_t nbr_cap,
-                          int num_sms, cudaStream_t st) {
+                          const int* maps_s, const int* new_to_out, const uint8_t* self_flag, int64_t map_cap,
+                          int* nbr, int64_t nbr_cap, int num_sms, cudaStream_t st) {
+    if (!self_flag) return PACES_ERR_BADARG;
     nbr_fill_split_kernel<<<grid_for(map_cap, 512, num_sms * 8), 256, 0, st>>>(m, p_blk, n_blk, maps_e, maps_s,
-                                                                              new_to_out, map_cap, nbr,
-                                                       nbr_cap);
+                                                                              new_to_out, self_flag, map_cap, nbr,
+                                                                              nbr_cap);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 

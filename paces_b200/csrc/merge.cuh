@@ -114,6 +114,8 @@ struct MergeOut {
     // assemble: the neighbour fill that follows writes every row of a self-run state whole,
     // so the assembly initialises only the other rows (their entries arrive one by one)
     int self_rows_filled;
+    // assemble (optional, nbr_cap bytes): 1 where the output state has a self-run element
+    uint8_t* self_flag;
 };
 
 // Merge modes.  EXPAND: keys only.  ASSEMBLE: keys, the H rows' metadata and neighbour
@@ -156,9 +158,11 @@ int launch_nbr_fill_multi(const ModelDev& m, const int* x_blk, const int* const*
 
 // Neighbour table after a split expansion (maps_e, new part N with new_to_out) and the
 // assembly of its output with the images of N (maps_s): every state of the expansion's
-// input P and of N is a source.  p_blk / n_blk: block offsets of P and N.
+// input P and of N is a source.  p_blk / n_blk: block offsets of P and N.  self_flag: the
+// assembly's MergeOut::self_flag (rows of the expansion's output, which carry their reverse
+// entries themselves).
 int launch_nbr_fill_split(const ModelDev& m, const int* p_blk, const int* n_blk, const int* maps_e,
-                          const int* maps_s, const int* new_to_out, int64_t map_cap, int* nbr, int64_t nbr_cap,
-                          int num_sms, cudaStream_t st);
+                          const int* maps_s, const int* new_to_out, const uint8_t* self_flag, int64_t map_cap,
+                          int* nbr, int64_t nbr_cap, int num_sms, cudaStream_t st);
 
 }  // namespace paces
