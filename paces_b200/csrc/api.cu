@@ -483,9 +483,9 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         mo.maps = at<int>(ws, l.maps);
         mo.map_cap = l.cap;
         mo.self_rows_filled = split ? 1 : 0;  // nbr_fill_split writes the rows of the enlarged basis
-        // which rows those are, for nbr_fill_split (the Taylor term buffer is free until the
-        // propagation; S bytes)
-        mo.self_flag = split ? at<uint8_t>(ws, l.v_TA) : nullptr;
+        // which rows those are, for the neighbour fill (the Taylor term buffer is free until
+        // the propagation; S bytes)
+        mo.self_flag = at<uint8_t>(ws, l.v_TA);
         PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, cur->keys, cur->blk,
                                            split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(c, l, ws),
                                            mo, &rec->ceiling_hits, split ? 1 : 0, status, c->num_sms, st),
@@ -843,6 +843,7 @@ int paces_assemble(paces_ctx* c, const paces_basis* in, paces_basis* out, paces_
     mo.nbr_cap = h->cap;
     mo.maps = at<int>(ws, l.maps);
     mo.map_cap = l.cap;
+    mo.self_flag = at<uint8_t>(ws, l.v_TA);  // S bytes of the workspace's Taylor term buffer
     if (h->cap < out->cap) mo.cap = h->cap;
     if (c->m.nhop > 1) {
         if (!h->xnbr) return fail(c, PACES_ERR_BADARG, "paces_assemble: the model's H needs xnbr");

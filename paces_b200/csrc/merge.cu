@@ -782,10 +782,13 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
         row.z = sd;  // NB_DOWN
         row.w = su;  // NB_UP
         reinterpret_cast<int4*>(nb)[q] = row;
-        if (sr >= 0) nb[4 * int64_t(sr) + NB_LEFT] = q;
-        if (sl >= 0) nb[4 * int64_t(sl) + NB_RIGHT] = q;
-        if (su >= 0) nb[4 * int64_t(su) + NB_DOWN] = q;
-        if (sd >= 0) nb[4 * int64_t(sd) + NB_UP] = q;
+        // a row of an X state gets its own store above: reverse entries only into the others
+        // when the assembly flagged them
+        const uint8_t* sf = out.self_flag;
+        if (sr >= 0 && !(sf && __ldg(sf + sr))) nb[4 * int64_t(sr) + NB_LEFT] = q;
+        if (sl >= 0 && !(sf && __ldg(sf + sl))) nb[4 * int64_t(sl) + NB_RIGHT] = q;
+        if (su >= 0 && !(sf && __ldg(sf + su))) nb[4 * int64_t(su) + NB_DOWN] = q;
+        if (sd >= 0 && !(sf && __ldg(sf + sd))) nb[4 * int64_t(sd) + NB_UP] = q;
     }
 }
 
