@@ -59,15 +59,17 @@ obs_energy_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict
         er += zr * yr + zi * yi;
         ei += zr * yi - zi * yr;
     };
-    // two rows a grid stride apart per iteration: their loads are independent and in flight
+    // four rows a grid stride apart per iteration: their loads are independent and in flight
     // together
     const int64_t gs = int64_t(gridDim.x) * kOThreads;
     int64_t r = int64_t(blockIdx.x) * kOThreads + threadIdx.x;
-    for (; r + gs < S; r += 2 * gs) {
+    for (; r + 3 * gs < S; r += 4 * gs) {
         row(r);
         row(r + gs);
+        row(r + 2 * gs);
+        row(r + 3 * gs);
     }
-    if (r < S) row(r);
+    for (; r < S; r += gs) row(r);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         norm2 += __shfl_xor_sync(0xffffffffu, norm2, o);
