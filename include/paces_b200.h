@@ -213,6 +213,13 @@ int paces_version(void);                            /* 10000*major + 100*minor +
 /* Copy the context's device status word (errors raised by kernels of the stage entry points)
  * to the host, synchronising `stream`, and clear it. */
 int paces_read_status(paces_ctx *ctx, paces_stream_t stream, int32_t *host_status);
+/* Test hook for the bounded device waits that replace the reference's device assert
+ * (paces/aux/cupy_search.py:205-228 traps; this library raises PACES_ERR_TIMEOUT and returns).
+ * wait_limit_ns (0 = the default 2 s, at most 2 s) bounds each grid-barrier wait of this
+ * context's Taylor and scaling-and-squaring kernels; skip_barrier_block >= 0 makes that block
+ * give up at its first grid barrier without arriving, so every other block's wait runs out
+ * (-1 = off).  Results are unaffected while the hooks are off. */
+int paces_set_test_hooks(paces_ctx *ctx, uint64_t wait_limit_ns, int32_t skip_barrier_block);
 /* Stage timing (no counterpart in the reference, which only prints wall-clock times):
  * with profiling on, paces_step records CUDA events between its stages, and
  * paces_stage_times waits for the last step and returns 7 durations in ms: truncate,
@@ -280,8 +287,10 @@ int paces_remap(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi,
  * GPU that loads the library until the process exits; it bounds the two bases together
  * to about 64M states (2048 per remap tile for keys of 1-2 words, 1024 for 3-4, 512
  * beyond).  Capacities beyond that return PACES_ERR_CAPACITY before anything is
- * launched.  The first call on a device looks up the array's device address with that
- * device current: make it before any stream capture.  All calls share the one array, so
+ * launched.  The first call in each CUDA context (a device's primary context, or one the
+ * host made current) looks up the array's device address in that context: make it before
+ * any stream capture.  A context destroyed and replaced by a new one at the same handle
+ * keeps the cached address, so do not call this after destroying a context.  All calls share the one array, so
  * calls that overlap on the GPU (other streams, other threads) race: serialise them. */
 int paces_remap_noalloc(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi,
                         const paces_basis *new_b, void *new_psi, paces_stream_t stream);
@@ -411,6 +420,8 @@ unsigned long long paces_batch_kernel_launches(const paces_batch *batch);
  * its three phases; paces_batch_stage_times waits for the last step and returns their
  * durations in ms: per-trajectory front stages, the batched Taylor launch, back stages. */
 int paces_batch_set_profiling(paces_batch *batch, int32_t on);
+/* The same test hook for the batch's persistent Taylor launch (paces_set_test_hooks). */
+int paces_batch_set_test_hooks(paces_batch *batch, uint64_t wait_limit_ns, int32_t skip_barrier_block);
 int paces_batch_stage_times(paces_batch *batch, float *ms);
 
 #ifdef __cplusplus

@@ -187,6 +187,7 @@ _SIGNATURES = {
     "paces_step": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, ctypes.POINTER(HMat),
                    ctypes.POINTER(StepParams), _P, _P, ctypes.c_size_t, _P],
     "paces_set_profiling": [_P, ctypes.c_int32],
+    "paces_set_test_hooks": [_P, ctypes.c_uint64, ctypes.c_int32],
     "paces_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
     "paces_kernel_launches": [_P],
     "paces_get_tuning": [_P, ctypes.POINTER(Tuning)],
@@ -209,6 +210,7 @@ _SIGNATURES = {
     "paces_batch_last_error": [_P],
     "paces_batch_kernel_launches": [_P],
     "paces_batch_set_profiling": [_P, ctypes.c_int32],
+    "paces_batch_set_test_hooks": [_P, ctypes.c_uint64, ctypes.c_int32],
     "paces_batch_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
 }
 _RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_kernel_launches": ctypes.c_ulonglong,

@@ -27,6 +27,8 @@ struct paces_ctx {
     int profiling;  // record stage events in paces_step
     cudaEvent_t ev[8];
     unsigned long long launches;  // kernels launched by paces_step since creation
+    uint64_t test_wait_ns;   // test hook: grid-barrier wait limit of the Taylor kernels (0: kWaitLimitNs)
+    int test_skip_block;     // test hook: block that skips its grid-barrier arrival (-1: none)
     char err[512];
 };
 
@@ -44,6 +46,8 @@ struct paces_batch {
     int profiling;                // record events around the three phases of a batch step
     cudaEvent_t ev[4];
     unsigned long long launches;  // kernels enqueued by paces_batch_step
+    uint64_t test_wait_ns;        // test hook: grid-barrier wait limit (0: kWaitLimitNs)
+    int test_skip_block;          // test hook: block that skips its grid-barrier arrival (-1: none)
     char err[512];
 };
 
@@ -214,13 +218,20 @@ RemapWs remap_ws(const Layout& l, void* ws) {
     return w;
 }
 
-TaylorWs taylor_ws(const Layout& l, void* ws) {
+TaylorWs taylor_ws(const paces_ctx* c, const Layout& l, void* ws) {
     TaylorWs w;
     w.ta = at<void>(ws, l.v_TA);
     w.tb = at<void>(ws, l.v_TB);
     w.partials = at<double>(ws, l.v_partials);
     w.barrier = at<unsigned>(ws, l.v_bar);
+    w.wait_ns = c->test_wait_ns ? c->test_wait_ns : kWaitLimitNs;
+    w.skip_block = c->test_skip_block;
     return w;
+}
+
+// Output rows the assembly can flag in the Taylor term buffer (one byte each).
+int64_t self_flag_cap(const paces_ctx* c, const Layout& l) {
+    return l.cap * int64_t(c->precision == PACES_C64 ? 8 : 16);
 }
 
 bool valid_basis(const paces_basis* b) { return b && b->keys && b->blk && b->cap >= 0; }
@@ -486,6 +497,7 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         // which rows those are, for the neighbour fill (the Taylor term buffer is free until
         // the propagation; S bytes)
         mo.self_flag = at<uint8_t>(ws, l.v_TA);
+        if (mo.cap > self_flag_cap(c, l)) mo.cap = self_flag_cap(c, l);
         PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, cur->keys, cur->blk,
                                            split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(c, l, ws),
                                            mo, &rec->ceiling_hits, split ? 1 : 0, status, c->num_sms, st),
@@ -663,6 +675,8 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
     c->merge_stride = merge_stride(c->nw);
     c->taylor_bps = 0;
     c->taylor_variant = 1;
+    c->test_wait_ns = 0;
+    c->test_skip_block = -1;
     // constants block: status words, per-site energies and the sqrt(k) * g tables
     {
         const size_t o_eps = 64, o_sq = o_eps + kMaxSites * 8, o_sqf = o_sq + kSqrtTable * 8;
@@ -691,6 +705,14 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
         c->d_sqf = reinterpret_cast<float*>(base + o_sqf);
     }
     *out = c;
+    return PACES_OK;
+}
+
+int paces_set_test_hooks(paces_ctx* c, uint64_t wait_limit_ns, int32_t skip_barrier_block) {
+    if (!c || skip_barrier_block < -1) return PACES_ERR_BADARG;
+    if (wait_limit_ns > kWaitLimitNs) return fail(c, PACES_ERR_BADARG, "wait limit above %llu ns", (unsigned long long)kWaitLimitNs);
+    c->test_wait_ns = wait_limit_ns;
+    c->test_skip_block = skip_barrier_block;
     return PACES_OK;
 }
 
@@ -845,6 +867,9 @@ int paces_assemble(paces_ctx* c, const paces_basis* in, paces_basis* out, paces_
     mo.map_cap = l.cap;
     mo.self_flag = at<uint8_t>(ws, l.v_TA);  // S bytes of the workspace's Taylor term buffer
     if (h->cap < out->cap) mo.cap = h->cap;
+    // the tile kernel flags every output row in that buffer: an output larger than it raises
+    // PACES_ERR_CAPACITY instead of writing past it
+    if (mo.cap > self_flag_cap(c, l)) mo.cap = self_flag_cap(c, l);
     if (c->m.nhop > 1) {
         if (!h->xnbr) return fail(c, PACES_ERR_BADARG, "paces_assemble: the model's H needs xnbr");
         const paces_basis tmp[2] = {{at<uint64_t>(ws, l.keysA), at<int32_t>(ws, l.blkA), l.cap},
@@ -951,7 +976,7 @@ int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
         o.term_ratio = &dev_info->term_ratio;
     }
     PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->cap, h->meta, psi_in,
-                                        psi_out, dt, m_star, tol, taylor_ws(l, ws), o, c->d_status, c->num_sms,
+                                        psi_out, dt, m_star, tol, taylor_ws(c, l, ws), o, c->d_status, c->num_sms,
                                         c->taylor_bps, c->taylor_variant, reinterpret_cast<cudaStream_t>(stream)),
                        "taylor");
     return PACES_OK;
@@ -984,7 +1009,7 @@ int paces_expm_scaled(paces_ctx* c, const paces_basis* b, const paces_hmat* h, c
         o.term_ratio = &dev_info->term_ratio;
     }
     PACES_CHECK_LAUNCH(c, launch_expm_scaled(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->meta, psi_in, psi_out,
-                                             t, shift, m_star, stages, tol, eta_re, eta_im, taylor_ws(l, ws), o,
+                                             t, shift, m_star, stages, tol, eta_re, eta_im, taylor_ws(c, l, ws), o,
                                              c->d_status, c->num_sms, c->taylor_grid,
                                              reinterpret_cast<cudaStream_t>(stream)),
                        "expm_scaled");
@@ -1049,7 +1074,7 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
     if (prm->evolve) {
         TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
         PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, with_h(c, h), new_b->blk, h->nbr, h->cap, h->meta,
-                                            p.target, new_psi, prm->dt, prm->m_star, prm->tol, taylor_ws(p.l, ws), o,
+                                            p.target, new_psi, prm->dt, prm->m_star, prm->tol, taylor_ws(c, p.l, ws), o,
                                             &rec->status, c->num_sms, c->taylor_bps, c->taylor_variant, st),
                            "step/taylor");
     }
@@ -1148,6 +1173,8 @@ int paces_batch_create(int32_t max_items, int32_t n_streams, paces_batch** out) 
     b->streams = new cudaStream_t[n_streams]();
     b->join = new cudaEvent_t[n_streams]();
     b->desc = new TaylorBatch();
+    b->test_wait_ns = 0;
+    b->test_skip_block = -1;
     bool ok = cudaGetDevice(&b->device) == cudaSuccess &&
               cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
@@ -1180,6 +1207,13 @@ int paces_batch_destroy(paces_batch* b) {
 }
 
 const char* paces_batch_last_error(const paces_batch* b) { return b ? b->err : "no batch"; }
+
+int paces_batch_set_test_hooks(paces_batch* b, uint64_t wait_limit_ns, int32_t skip_barrier_block) {
+    if (!b || skip_barrier_block < -1 || wait_limit_ns > kWaitLimitNs) return PACES_ERR_BADARG;
+    b->test_wait_ns = wait_limit_ns;
+    b->test_skip_block = skip_barrier_block;
+    return PACES_OK;
+}
 
 int paces_batch_set_profiling(paces_batch* b, int32_t on) {
     if (!b) return PACES_ERR_BADARG;
@@ -1272,7 +1306,7 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
             if (!prm->evolve) continue;
             paces_ctx* c = items[i].ctx;
             const StepPlan& p = plans[i];
-            const TaylorWs tw = taylor_ws(p.l, p.ws);
+            const TaylorWs tw = taylor_ws(c, p.l, p.ws);
             TaylorItem& ti = bt.items[bt.n++];
             ti.blk = p.new_b->blk;
             ti.nbr = p.h->nbr;
@@ -1301,6 +1335,8 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
         TaylorBatchWs tws;
         tws.barrier = static_cast<unsigned*>(b->d_ws);
         tws.maxima = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(b->d_ws) + 256);
+        tws.wait_ns = b->test_wait_ns ? b->test_wait_ns : kWaitLimitNs;
+        tws.skip_block = b->test_skip_block;
         if (launch_taylor_batch(precision == PACES_C64, bt, tws, b->num_sms, items[0].ctx->taylor_bps, st) != PACES_OK)
             return bfail(PACES_ERR_CUDA, "batched Taylor: %s", cudaGetErrorString(cudaGetLastError()));
         launches += 1;

@@ -183,7 +183,7 @@ expm_scaled_kernel(ModelDev m, const int* __restrict__ blk, const int* __restric
                 double* pp = ws.partials + (size_t((final_m & 1) * nblocks) + blockIdx.x) * 4;
                 for (int k = 0; k < 4; ++k) pp[k] = s_fin[k];
             }
-            if (!grid_barrier(ws.barrier, nblocks, gen, status)) {
+            if (!grid_barrier(ws.barrier, nblocks, gen, status, ws.wait_ns, int(blockIdx.x) == ws.skip_block)) {
                 stop = true;
                 break;
             }
@@ -227,7 +227,9 @@ expm_scaled_kernel(ModelDev m, const int* __restrict__ blk, const int* __restric
             res[r] = f;
             tb[r] = f;
         }
-        if (st + 1 < stages && !grid_barrier(ws.barrier, nblocks, gen, status)) break;
+        if (st + 1 < stages && !grid_barrier(ws.barrier, nblocks, gen, status, ws.wait_ns,
+                                             int(blockIdx.x) == ws.skip_block))
+            break;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (out.converged) *out.converged = conv;

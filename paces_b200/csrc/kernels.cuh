@@ -47,6 +47,8 @@ struct TaylorWs {
     void* tb;            // [cap] complex
     double* partials;    // [2][max_grid][4]
     unsigned* barrier;   // [2]
+    uint64_t wait_ns;    // grid-barrier wait limit (kWaitLimitNs unless a test shortens it)
+    int skip_block;      // test hook: this block skips its first grid-barrier arrival (-1: none)
 };
 int taylor_max_grid(bool c64, int num_sms);
 // blocks_per_sm: 0 = as many as fit (the grid never exceeds taylor_max_grid);
@@ -102,6 +104,8 @@ struct TaylorBatch {
 struct TaylorBatchWs {
     unsigned* barrier;             // [2]
     unsigned long long* maxima;    // [3][kMaxBatch][4] per-term maxima (fp64 bit patterns)
+    uint64_t wait_ns;              // grid-barrier wait limit (kWaitLimitNs unless a test shortens it)
+    int skip_block;                // test hook: this block skips its first grid-barrier arrival (-1: none)
 };
 constexpr size_t kTaylorBatchWsBytes = 256 + size_t(3) * kMaxBatch * 4 * 8;
 int taylor_batch_max_grid(bool c64, int num_sms);

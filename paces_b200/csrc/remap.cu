@@ -188,26 +188,71 @@ static __device__ __align__(256) unsigned char g_remap_scratch[kStaticRemapBytes
 
 int remap_static_tile_cap() { return int((kStaticRemapBytes - kStaticHeaderBytes) / (2 * sizeof(int))); }
 
+// The array's device address belongs to a CUDA context: the cache below is keyed on the
+// context current at the call (the device's primary context, or one the host created), read
+// through the driver's cuCtxGetCurrent.
+using CtxGetCurrentFn = int (*)(void**);
+
+void* current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
 int remap_static_ws(RemapWs* ws, const char** err) {
+    constexpr int kSlots = 64;
     static std::mutex mu;
-    static void* addr[64] = {};
+    static void* ctx_of[kSlots] = {};
+    static void* addr_of[kSlots] = {};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         *err = "no current CUDA device";
         return PACES_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        // host code cannot use the array's name as a device address: ask the runtime, once per
-        // device, with that device current
-        void* p = nullptr;
+    // host code cannot use the array's name as a device address: ask the runtime, once per
+    // context, with that context current
+    void* p = nullptr;
+    auto lookup = [&]() {
         if (cudaGetSymbolAddress(&p, g_remap_scratch) != cudaSuccess || !p) {
             *err = "cudaGetSymbolAddress of the static remap scratch failed";
+            return false;
+        }
+        return true;
+    };
+    void* ctx = current_context();
+    if (!ctx) {
+        // no context yet: the lookup makes the device's primary context current
+        if (!lookup()) return PACES_ERR_CUDA;
+        ctx = current_context();
+        if (!ctx) {
+            *err = "cuCtxGetCurrent is unavailable or reports no current context";
             return PACES_ERR_CUDA;
         }
-        addr[dev] = p;
     }
-    unsigned char* base = static_cast<unsigned char*>(addr[dev]);
+    std::lock_guard<std::mutex> lock(mu);
+    int slot = -1;
+    for (int s = 0; s < kSlots && slot < 0; ++s)
+        if (ctx_of[s] == ctx) slot = s;
+    if (slot < 0) {
+        if (!p && !lookup()) return PACES_ERR_CUDA;
+        for (int s = 0; s < kSlots && slot < 0; ++s)
+            if (!ctx_of[s]) slot = s;
+        if (slot < 0) {
+            *err = "more than 64 CUDA contexts have called paces_remap_noalloc";
+            return PACES_ERR_CUDA;
+        }
+        ctx_of[slot] = ctx;
+        addr_of[slot] = p;
+    }
+    unsigned char* base = static_cast<unsigned char*>(addr_of[slot]);
     ws->tile_off = reinterpret_cast<int*>(base);
     ws->counters = reinterpret_cast<int*>(base + sizeof(int) * (kMaxSites + 8));
     ws->split = reinterpret_cast<int*>(base + kStaticHeaderBytes);

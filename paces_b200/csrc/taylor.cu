@@ -223,7 +223,7 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
             pp[2] = s_fin[2];
             pp[3] = s_fin[3];
         }
-        if (!grid_barrier(ws.barrier, nblocks, gen, status)) {
+        if (!grid_barrier(ws.barrier, nblocks, gen, status, ws.wait_ns, int(blockIdx.x) == ws.skip_block)) {
             fin_j = j;
             break;
         }

@@ -185,7 +185,7 @@ taylor_batch_kernel(const __grid_constant__ TaylorBatch bt, TaylorBatchWs ws) {
             if (v) atomicMax(&gmax[e], v);
             s_max[e >> 2][e & 3] = 0ull;
         }
-        if (!grid_barrier(ws.barrier, nblocks, gen, nullptr)) {
+        if (!grid_barrier(ws.barrier, nblocks, gen, nullptr, ws.wait_ns, int(blockIdx.x) == ws.skip_block)) {
             for (int i = tid; i < n; i += kBThreads) {
                 if (!s_active[i]) continue;
                 raise_status(bt.items[i].status, PACES_ERR_TIMEOUT);

@@ -350,6 +350,12 @@ class Engine:
             return None
         return self.read_record()
 
+    def set_test_hooks(self, wait_limit_ns=0, skip_barrier_block=-1):
+        """Test hook of the bounded grid-barrier waits (paces_set_test_hooks): a shorter wait
+        limit and a block that skips its arrival, so a test can make a wait run out."""
+        nat.check(self.lib.paces_set_test_hooks(self.ctx, int(wait_limit_ns), int(skip_barrier_block)), self.ctx,
+                  "set_test_hooks")
+
     def set_profiling(self, on=True):
         nat.check(self.lib.paces_set_profiling(self.ctx, 1 if on else 0), self.ctx, "set_profiling")
 
@@ -752,6 +758,11 @@ class TrajectoryBatch:
 
     def kernel_launches(self):
         return int(self.lib.paces_batch_kernel_launches(self.handle))
+
+    def set_test_hooks(self, wait_limit_ns=0, skip_barrier_block=-1):
+        """The batch's Taylor launch test hook (paces_batch_set_test_hooks)."""
+        nat.check(self.lib.paces_batch_set_test_hooks(self.handle, int(wait_limit_ns), int(skip_barrier_block)),
+                  None, "batch_set_test_hooks")
 
     def set_profiling(self, on=True):
         nat.check(self.lib.paces_batch_set_profiling(self.handle, 1 if on else 0), None, "batch_set_profiling")

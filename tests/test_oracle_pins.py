@@ -11,6 +11,7 @@ import os
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 from oracle import paces_oracle as po
 
@@ -164,6 +165,89 @@ def test_periodic_extension_reduces_and_is_exact():
     np.testing.assert_allclose(np.array([r.n_exc for r in recs]), exact, atol=1e-12)
     # ring symmetry: starting on the middle site of 3, sites 0 and 2 stay equal
     np.testing.assert_allclose(exact[:, 0], exact[:, 2], atol=1e-12)
+
+
+def _kron_hamiltonian(L, d, J, g, w0, site, delta_eps, periodic):
+    """The Holstein Hamiltonian on the full product space |pos> (x) |n_0 ... n_{L-1}>, each
+    oscillator truncated to d levels, written from its definition with Kronecker products
+    and independent of the oracle's key packing, images and o-star rule:
+    H = J sum_p (|p+1><p| + h.c.) + sum_p e_p |p><p| + w0 sum_s n_s
+        + g sum_p |p><p| (b_p + b_p^dagger),  e_p = site[p] + delta_eps * p,
+    with the hop L-1 -> 0 present when periodic.  Basis index: pos * d^L + sum_s n_s d^(L-1-s)."""
+    I_d = sp.identity(d, format="csr")
+    b = sp.diags(np.sqrt(np.arange(1, d, dtype=np.float64)), 1, shape=(d, d), format="csr")  # lowers n
+    n_op = sp.diags(np.arange(d, dtype=np.float64), 0, format="csr")
+
+    def on_site(op, s):
+        out = sp.identity(1, format="csr")
+        for k in range(L):
+            out = sp.kron(out, op if k == s else I_d, format="csr")
+        return out
+
+    hop = sp.lil_matrix((L, L))
+    for p in range(L - 1 if not periodic else L):
+        q = (p + 1) % L
+        hop[q, p] += J
+        hop[p, q] += J
+    ph_dim = d ** L
+    H = sp.kron(hop.tocsr(), sp.identity(ph_dim, format="csr"), format="csr")
+    e = np.asarray(site, dtype=np.float64) + delta_eps * np.arange(L)
+    H = H + sp.kron(sp.diags(e), sp.identity(ph_dim, format="csr"), format="csr")
+    nsum = sum(on_site(n_op, s) for s in range(L))
+    H = H + w0 * sp.kron(sp.identity(L, format="csr"), nsum, format="csr")
+    for p in range(L):
+        proj = sp.csr_matrix(([1.0], ([p], [p])), shape=(L, L))
+        H = H + g * sp.kron(proj, on_site(b + b.T, p), format="csr")
+    return H.tocsr()
+
+
+@pytest.mark.parametrize("L,d,g,w0,periodic,seed,delta_eps,init", [
+    (5, 3, 0.8, 1.0, True, None, 0.0, 0),       # a ring of 5: a wrong wrap is visible
+    (6, 3, 1.1, 0.7, True, 4, 0.0, 2),          # ring, site disorder, hbar_omega != 1
+    (5, 3, 0.9, 1.3, False, 9, 0.25, 1),        # open chain, disorder and a linear potential
+], ids=["ring5", "ring6_disorder_w0.7", "open5_disorder_linear"])
+def test_extensions_against_an_independent_hamiltonian(L, d, g, w0, periodic, seed, delta_eps, init):
+    """Periodic wrap, per-site energies, hbar_omega != 1 and delta_eps against exact dynamics
+    of the Hamiltonian built from its definition (_kron_hamiltonian), not from the oracle's
+    images: the adaptive-basis oracle run (no truncation) and the oracle's own full-space
+    assembly must both equal it, n_exc and n_pho at every step."""
+    import scipy.sparse.linalg as spla
+    site = np.zeros(L) if seed is None else np.random.default_rng(seed).normal(0.0, 0.5, L)
+    m = po.Model(L, [d] * L, g=g, hbar_omega=w0, periodic=periodic, delta_eps=delta_eps,
+                 site_eps=None if seed is None else site)
+    H = _kron_hamiltonian(L, d, 1.0, g, w0, site, delta_eps, periodic)
+    v = np.zeros(H.shape[0], dtype=np.complex128)
+    v[init * d ** L] = 1.0
+    occ = np.array(list(np.ndindex(*([d] * L))), dtype=np.float64)        # [d^L, L] in index order
+    t = np.arange(16) * 0.05
+    exact_ne, exact_np = [], []
+    for i in range(len(t)):
+        if i:
+            v = spla.expm_multiply(-1j * 0.05 * H, v)
+        p = (np.abs(v) ** 2).reshape(L, d ** L)
+        exact_ne.append(p.sum(axis=1))
+        exact_np.append(p.sum(axis=0) @ occ)
+    exact_ne, exact_np = np.array(exact_ne), np.array(exact_np)
+    # the oracle run starts on the full space (a localised start grows its basis over the
+    # first steps, and the states it has not reached yet carry ~1e-10 of phonon weight)
+    import itertools
+    raw = np.array(list(itertools.product(range(L), *([range(d)] * L))), dtype=np.uint32)
+    full = po.unique_rows(po.compress(m, raw))
+    v0 = np.zeros(full.shape[0], dtype=np.complex128)
+    v0[po.searchsorted(full, po.initial_basis(m, init))[0]] = 1.0
+    tr = po.Trajectory(m, full, v0, 10 ** 6, 1)
+    recs = tr.run(t)
+    assert recs[-1].numstates == L * d ** L
+    np.testing.assert_allclose(np.array([r.n_exc for r in recs]), exact_ne, atol=1e-12)
+    np.testing.assert_allclose(np.array([r.n_pho for r in recs]), exact_np, atol=1e-12)
+    np.testing.assert_allclose(po.exact_dynamics(m, 10 ** 5, t, init_pos=init), exact_ne, atol=1e-12)
+    if periodic:
+        # the same model without the wrap is a different dynamics: the pin discriminates
+        open_H = _kron_hamiltonian(L, d, 1.0, g, w0, site, delta_eps, False)
+        u = np.zeros(H.shape[0], dtype=np.complex128)
+        u[init * d ** L] = 1.0
+        u = spla.expm_multiply(-1j * 0.75 * open_H, u)
+        assert np.abs((np.abs(u) ** 2).reshape(L, -1).sum(axis=1) - exact_ne[-1]).max() > 1e-3
 
 
 def test_site_disorder_extension_is_exact():
