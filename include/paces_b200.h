@@ -78,6 +78,8 @@ enum paces_precision {
 };
 
 #define PACES_MAX_SITES 128
+/* largest ExpmParams.lanczos_order (Krylov vectors: order + 1) */
+#define PACES_MAX_LANCZOS_ORDER 63
 
 typedef struct paces_model_desc {
     int32_t nchain;            /* number of sites L (1D chain), 1 <= L <= 128 */
@@ -154,6 +156,14 @@ typedef struct paces_step_params {
     int32_t reserved0;
     double tau;
     const paces_hmat *old_h;
+    /* ExpmParams.lanczos_order: with lanczos_order > 0 the propagation is the Lanczos step
+     * (paces_lanczos) in the caller's Krylov workspace krylov (paces_lanczos_bytes for the
+     * new basis' capacity and this order); the record's Taylor fields are 0, as the
+     * reference's placeholder diagnostics. */
+    int32_t lanczos_order;
+    int32_t reserved1;
+    void *krylov;
+    size_t krylov_bytes;
 } paces_step_params;
 
 /* Written on the device by paces_step; the caller copies it back (one transfer per step). */
@@ -213,12 +223,25 @@ int paces_version(void);                            /* 10000*major + 100*minor +
 /* Copy the context's device status word (errors raised by kernels of the stage entry points)
  * to the host, synchronising `stream`, and clear it. */
 int paces_read_status(paces_ctx *ctx, paces_stream_t stream, int32_t *host_status);
+/* Lanczos propagation: replaces _lanczos (paces/core/time_evolution.py:515-549), selected
+ * by ExpmParams.lanczos_order = order (1 .. PACES_MAX_LANCZOS_ORDER, :577-578).  psi_out =
+ * |psi| V exp(-i dt T) e_0 from order + 1 Lanczos vectors of H on the basis (fewer when
+ * the Krylov space closes, beta < 1e-15), all in one cooperative launch: the Krylov
+ * vectors in the precision of the context, alpha, beta and the small exponential in fp64.
+ * dev_info (device, may be NULL) receives the reference's placeholder diagnostics
+ * [0, 0, 0, 0].  krylov is a caller-owned device buffer of paces_lanczos_bytes(cap,
+ * order) bytes with cap >= basis->cap; no other workspace is needed. */
+int paces_lanczos_bytes(const paces_ctx *ctx, int64_t cap, int32_t order, size_t *bytes);
+int paces_lanczos(paces_ctx *ctx, const paces_basis *basis, const paces_hmat *h, const void *psi_in,
+                  void *psi_out, double dt, int32_t order, paces_expm_info *dev_info, void *krylov,
+                  size_t krylov_bytes, paces_stream_t stream);
 /* Test hook for the bounded device waits that replace the reference's device assert
  * (paces/aux/cupy_search.py:205-228 traps; this library raises PACES_ERR_TIMEOUT and returns).
  * wait_limit_ns (0 = the default 2 s, at most 2 s) bounds each grid-barrier wait of this
  * context's Taylor and scaling-and-squaring kernels; skip_barrier_block >= 0 makes that block
  * give up at its first grid barrier without arriving, so every other block's wait runs out
- * (-1 = off).  Results are unaffected while the hooks are off. */
+ * (-1 = off); the Lanczos kernel's grid barriers obey the same hooks.  Results are
+ * unaffected while the hooks are off. */
 int paces_set_test_hooks(paces_ctx *ctx, uint64_t wait_limit_ns, int32_t skip_barrier_block);
 /* Stage timing (no counterpart in the reference, which only prints wall-clock times):
  * with profiling on, paces_step records CUDA events between its stages, and

@@ -508,6 +508,41 @@ def taylor(asm: Assembly, v, dt, m_star=100, tol=TAYLOR_TOL_F64):
     return res, [converged, j_ind, c1_plus_c2, term_ratio]
 
 
+def lanczos(asm: Assembly, v, dt, order):
+    """exp(-i dt H) v in an (order+1)-dimensional Krylov space.  paces/core/time_evolution.py:
+    515-549 (_lanczos): plain Lanczos recurrence without re-orthogonalisation from v/|v|,
+    alpha_i = vdot(H q_i - beta_i q_{i-1}, q_i) (complex), beta_{i+1} = |w|, a stop when
+    beta < 1e-15; the (order+1)^2 tridiagonal matrix exponentiated densely and its first
+    column combined with the Krylov vectors.  Returns (F, [False, 0, 0, 0]) -- the
+    reference's placeholder diagnostics."""
+    import scipy.linalg
+    m = int(order)
+    small = np.zeros((m + 1, m + 1), dtype=complex)
+    vmat = np.zeros((v.shape[0], m + 1), dtype=complex)
+    orig_norm = np.linalg.norm(v)
+    normed = v / orig_norm
+    w = apply_h(asm, normed)
+    a = np.vdot(w, normed)
+    w -= a * normed
+    small[0, 0] = a
+    vmat[:, 0] = normed
+    for i in range(1, m + 1):
+        b = np.linalg.norm(w)
+        if b < 1e-15:
+            break
+        new = w / b
+        w = apply_h(asm, new) - b * normed
+        a = np.vdot(w, new)
+        w -= a * new
+        normed = new
+        small[i, i] = a
+        small[i - 1, i] = b
+        small[i, i - 1] = b
+        vmat[:, i] = normed
+    leftcol = scipy.linalg.expm(-1j * dt * small)[:, 0]
+    return orig_norm * (vmat @ leftcol), [False, 0, 0.0, 0.0]
+
+
 # theta_m of Al-Mohy and Higham (2011), table 3.1 (m <= 30: Higham, Functions of
 # Matrices, table A.3) -- the bounds paces/aux/_scipy/_expm_multiply.py:205-245 tabulates.
 _THETA = {
@@ -643,7 +678,7 @@ class Trajectory:
 
     def __init__(self, model, whoami, vector, maxstates, enlarge_steps, m_star=100,
                  tol=TAYLOR_TOL_F64, diagnostics=True, shuffle_rng=None, renormalize=False,
-                 explosion_cutoff=2.0, use_scaling=False, tau=0.0, weighting="coherence"):
+                 explosion_cutoff=2.0, use_scaling=False, tau=0.0, weighting="coherence", lanczos_order=0):
         self.model = model
         self.whoami = whoami
         self.vector = np.asarray(vector, dtype=np.complex128)
@@ -658,6 +693,7 @@ class Trajectory:
         self.use_scaling = use_scaling
         self.tau = tau
         self.weighting = weighting
+        self.lanczos_order = int(lanczos_order)
         self.asm = None
         self.records = []
 
@@ -698,7 +734,9 @@ class Trajectory:
     def step(self, t, dt):
         """paces/core/time_evolution.py:552-613."""
         pan, pae = self._new_space(weighted=True)
-        if self.use_scaling:
+        if self.lanczos_order > 0:              # time_evolution.py:577-578
+            self.vector, dbg = lanczos(self.asm, self.vector, dt, self.lanczos_order)
+        elif self.use_scaling:
             self.vector, dbg = expm_scaled(self.asm, self.vector, dt)
         else:
             self.vector, dbg = taylor(self.asm, self.vector, dt, self.m_star, self.tol)

@@ -31,6 +31,7 @@ ERR_SHUFFLE = 8
 C128 = 0
 C64 = 1
 MAX_SITES = 128
+MAX_LANCZOS_ORDER = 63
 OBS_NORM, OBS_ENERGY, OBS_SITES = 1, 2, 4
 WEIGHT_NONE, WEIGHT_COHERENCE, WEIGHT_NORM, WEIGHT_HAM_ONES = 0, 1, 2, 3
 
@@ -84,6 +85,10 @@ class StepParams(ctypes.Structure):
         ("reserved0", ctypes.c_int32),
         ("tau", ctypes.c_double),
         ("old_h", ctypes.c_void_p),
+        ("lanczos_order", ctypes.c_int32),
+        ("reserved1", ctypes.c_int32),
+        ("krylov", ctypes.c_void_p),
+        ("krylov_bytes", ctypes.c_size_t),
     ]
 
 
@@ -172,6 +177,9 @@ _SIGNATURES = {
                                 _P, _P],
     "paces_remap": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P, ctypes.c_size_t, _P],
     "paces_remap_noalloc": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P],
+    "paces_lanczos_bytes": [_P, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t)],
+    "paces_lanczos": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, ctypes.c_double, ctypes.c_int32, _P, _P,
+                      ctypes.c_size_t, _P],
     "paces_taylor": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, ctypes.c_double, ctypes.c_int32,
                      ctypes.c_double, _P, _P, ctypes.c_size_t, _P],
     "paces_observables": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, ctypes.c_int32, _P, _P,

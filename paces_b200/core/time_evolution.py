@@ -46,9 +46,9 @@ class CoeffSaveParams:
 class ExpmParams:
     """Matrix-exponential parameters (paces/core/time_evolution.py:57-82).
 
-    The device runs the truncated Taylor series, or with use_scaling=True the scaling-and-
-    squaring series of paces_b200.expm; lanczos_order > 0 is not implemented and raises
-    when a timeline starts.
+    The device runs the truncated Taylor series; with lanczos_order > 0 the Lanczos step
+    (paces_lanczos, which takes precedence as in the reference, time_evolution.py:577-580),
+    else with use_scaling=True the scaling-and-squaring series of paces_b200.expm.
     """
     m_star: int = 100
     explosion_cutoff: float = 2.0
@@ -167,7 +167,7 @@ class TimeEvolutionFramework:
             self._traj = Trajectory(self.engine, tp.maxstates, tp.enlarge_steps, m_star=ep.m_star,
                                     diagnostics=tp.diagnostics, shuffle_seed=tp.shuffle_seed,
                                     renormalize=ep.renormalize, explosion_cutoff=ep.explosion_cutoff,
-                                    weighting=weighting, tau=tp.tau)
+                                    weighting=weighting, tau=tp.tau, lanczos_order=ep.lanczos_order)
         return self._traj
 
     def _commit_state(self):
@@ -378,8 +378,6 @@ class TimeEvolutionFramework:
             print("Setting up generate_timeline function...")
         self.write_current_params_to_file(inspect.currentframe(), time.time())
         ep, tp = self.expm_params, self.te_params
-        if ep.lanczos_order > 0:
-            raise NotImplementedError("Lanczos propagation (lanczos_order > 0) is not implemented")
         if tp.garbage_tol >= 0:
             raise NotImplementedError("garbage_tol is not implemented")
         if tp.use_two_streams:
@@ -402,7 +400,7 @@ class TimeEvolutionFramework:
                 rec = self._traj.step(evolve=False)
                 expm_dbg = [0, 0, 0, 0]
             else:
-                if ep.use_scaling:
+                if ep.use_scaling and ep.lanczos_order == 0:
                     rec = self._traj.step_scaled(float(t_curr - t_array[i - 1]))
                 else:
                     rec = self._traj.step(evolve=True, dt=float(t_curr - t_array[i - 1]))

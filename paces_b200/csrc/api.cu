@@ -234,6 +234,57 @@ int64_t self_flag_cap(const paces_ctx* c, const Layout& l) {
     return l.cap * int64_t(c->precision == PACES_C64 ? 8 : 16);
 }
 
+// The caller's Krylov workspace of the Lanczos step: order+1 vectors, two w buffers, the
+// per-block partial sums and the barrier words.
+struct KrylovLayout {
+    size_t u, w0, w1, partials, barrier, total;
+    int max_grid;
+};
+
+KrylovLayout krylov_layout(const paces_ctx* c, int64_t cap, int order) {
+    KrylovLayout k;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) & ~size_t(255);
+        return o;
+    };
+    const size_t cs = c->precision == PACES_C64 ? 8 : 16;
+    k.max_grid = lanczos_max_grid(c->num_sms);
+    k.u = take(size_t(order + 1) * size_t(cap) * cs);
+    k.w0 = take(size_t(cap) * cs);
+    k.w1 = take(size_t(cap) * cs);
+    k.partials = take(size_t(2) * k.max_grid * 4 * 8);
+    k.barrier = take(16);
+    k.total = off;
+    return k;
+}
+
+// Largest capacity whose Krylov layout fits `bytes` (0 when none does).
+int64_t krylov_cap(const paces_ctx* c, size_t bytes, int order) {
+    int64_t lo = 0, hi = int64_t(bytes / 8) + 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) / 2;
+        if (krylov_layout(c, mid, order).total <= bytes) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+LanczosWs lanczos_ws(const paces_ctx* c, void* krylov, int64_t cap, int order) {
+    const KrylovLayout k = krylov_layout(c, cap, order);
+    LanczosWs w;
+    w.u = at<void>(krylov, k.u);
+    w.w0 = at<void>(krylov, k.w0);
+    w.w1 = at<void>(krylov, k.w1);
+    w.partials = at<double>(krylov, k.partials);
+    w.barrier = at<unsigned>(krylov, k.barrier);
+    w.cap = cap;
+    w.max_grid = k.max_grid;
+    w.skip_block = c->test_skip_block;
+    w.wait_ns = c->test_wait_ns ? c->test_wait_ns : kWaitLimitNs;
+    return w;
+}
+
 bool valid_basis(const paces_basis* b) { return b && b->keys && b->blk && b->cap >= 0; }
 
 __global__ void record_init_kernel(paces_step_record* rec, int diagnostics) {
@@ -322,6 +373,15 @@ int plan_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, paces
         return fail(c, PACES_ERR_BADARG, "paces_step: bad parameters");
     if (prm->proposal && !prm->proposal_params)
         return fail(c, PACES_ERR_BADARG, "paces_step: proposal without MLP parameters");
+    if (prm->lanczos_order < 0 || prm->lanczos_order > kMaxLanczosOrder)
+        return fail(c, PACES_ERR_BADARG, "paces_step: lanczos_order %d outside 0..%d", int(prm->lanczos_order),
+                    kMaxLanczosOrder);
+    if (prm->evolve && prm->lanczos_order > 0) {
+        if (!prm->krylov) return fail(c, PACES_ERR_BADARG, "paces_step: the Lanczos step needs a Krylov workspace");
+        if (krylov_cap(c, prm->krylov_bytes, prm->lanczos_order) < new_b->cap)
+            return fail(c, PACES_ERR_CAPACITY, "paces_step: the Krylov workspace holds fewer than %lld states",
+                        (long long)new_b->cap);
+    }
     if (c->m.nhop > 1) {
         if (!h->xnbr) return fail(c, PACES_ERR_BADARG, "paces_step: the lattice's H table needs xnbr");
         if (prm->proposal) return fail(c, PACES_ERR_BADARG, "paces_step: the learned proposal needs the chain model");
@@ -982,6 +1042,36 @@ int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
     return PACES_OK;
 }
 
+int paces_lanczos_bytes(const paces_ctx* c, int64_t cap, int32_t order, size_t* bytes) {
+    if (!c || !bytes || cap < 0 || order < 1 || order > kMaxLanczosOrder) return PACES_ERR_BADARG;
+    *bytes = krylov_layout(c, cap, order).total;
+    return PACES_OK;
+}
+
+int paces_lanczos(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const void* psi_in, void* psi_out,
+                  double dt, int32_t order, paces_expm_info* dev_info, void* krylov, size_t krylov_bytes,
+                  paces_stream_t stream) {
+    if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !psi_in || !psi_out || psi_in == psi_out || !krylov)
+        return PACES_ERR_BADARG;
+    if (order < 1 || order > kMaxLanczosOrder)
+        return fail(c, PACES_ERR_BADARG, "paces_lanczos: order %d outside 1..%d", int(order), kMaxLanczosOrder);
+    if (c->m.nhop > 1 && !h->xnbr) return fail(c, PACES_ERR_BADARG, "paces_lanczos: the lattice's H needs xnbr");
+    const int64_t kcap = krylov_cap(c, krylov_bytes, order);
+    if (kcap < b->cap) return fail(c, PACES_ERR_CAPACITY, "Krylov workspace holds %lld states, basis %lld", (long long)kcap, (long long)b->cap);
+    TaylorOut o{};
+    if (dev_info) {
+        o.converged = &dev_info->converged;
+        o.final_m = &dev_info->final_m;
+        o.c1_plus_c2 = &dev_info->c1_plus_c2;
+        o.term_ratio = &dev_info->term_ratio;
+    }
+    PACES_CHECK_LAUNCH(c, launch_lanczos(c->precision == PACES_C64, with_h(c, h), b->blk, h->nbr, h->meta, psi_in, psi_out,
+                                         dt, order, lanczos_ws(c, krylov, kcap, order), o, c->d_status, c->num_sms,
+                                         reinterpret_cast<cudaStream_t>(stream)),
+                       "lanczos");
+    return PACES_OK;
+}
+
 int paces_hnorms(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const double* dev_shift, double* dev_out,
                  void* ws, size_t ws_bytes, paces_stream_t stream) {
     if (!c || !valid_basis(b) || !h || !h->nbr || !h->meta || !dev_out || !ws) return PACES_ERR_BADARG;
@@ -1073,10 +1163,20 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
     if (r != PACES_OK) return r;
     if (prm->evolve) {
         TaylorOut o{&rec->converged, &rec->final_m, &rec->c1_plus_c2, &rec->term_ratio};
-        PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, with_h(c, h), new_b->blk, h->nbr, h->cap, h->meta,
-                                            p.target, new_psi, prm->dt, prm->m_star, prm->tol, taylor_ws(c, p.l, ws), o,
-                                            &rec->status, c->num_sms, c->taylor_bps, c->taylor_variant, st),
-                           "step/taylor");
+        if (prm->lanczos_order > 0) {
+            const int64_t kcap = krylov_cap(c, prm->krylov_bytes, prm->lanczos_order);
+            PACES_CHECK_LAUNCH(c, launch_lanczos(c->precision == PACES_C64, with_h(c, h), new_b->blk, h->nbr, h->meta,
+                                                 p.target, new_psi, prm->dt, prm->lanczos_order,
+                                                 lanczos_ws(c, prm->krylov, kcap, prm->lanczos_order), o, &rec->status,
+                                                 c->num_sms, st),
+                               "step/lanczos");
+        } else {
+            PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, with_h(c, h), new_b->blk, h->nbr, h->cap,
+                                                h->meta, p.target, new_psi, prm->dt, prm->m_star, prm->tol,
+                                                taylor_ws(c, p.l, ws), o, &rec->status, c->num_sms, c->taylor_bps,
+                                                c->taylor_variant, st),
+                               "step/taylor");
+        }
     }
     return step_back(c, p, st, true);
 }
@@ -1261,6 +1361,8 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
         if (it.ctx->precision != precision) return bfail(PACES_ERR_BADARG, "item %d: mixed precisions in one batch", i);
         if (it.ctx->device != b->device) return bfail(PACES_ERR_BADARG, "item %d: context on another device", i);
         if (it.ctx->m.nhop > 1) return bfail(PACES_ERR_BADARG, "item %d: batched steps take chain models only", i);
+        if (it.params && it.params->lanczos_order > 0)
+            return bfail(PACES_ERR_BADARG, "item %d: batched steps propagate by the Taylor series only", i);
         const int rc = plan_step(it.ctx, it.old_basis, it.old_psi, it.new_basis, it.new_psi, it.h, it.params,
                                  it.record, it.workspace, it.workspace_bytes, &plans[i]);
         if (rc != PACES_OK) return bfail(rc, "item %d: %s", i, it.ctx->err);

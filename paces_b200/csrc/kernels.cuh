@@ -51,6 +51,24 @@ struct TaylorWs {
     int skip_block;      // test hook: this block skips its first grid-barrier arrival (-1: none)
 };
 int taylor_max_grid(bool c64, int num_sms);
+
+// ---- Lanczos ----------------------------------------------------------------------------
+constexpr int kMaxLanczosOrder = PACES_MAX_LANCZOS_ORDER;
+struct LanczosWs {
+    void* u;             // [order+1][cap] complex: the Krylov vectors q_i (columns of V)
+    void* w0;            // [cap] complex: the recurrence's w, double-buffered
+    void* w1;
+    double* partials;    // [2][max_grid][4]
+    unsigned* barrier;   // [2]
+    int64_t cap;         // rows of each vector
+    int max_grid;
+    int skip_block;      // test hook (see TaylorWs)
+    uint64_t wait_ns;
+};
+int lanczos_max_grid(int num_sms);
+int launch_lanczos(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
+                   const void* v_in, void* res, double dt, int order, const LanczosWs& ws, const TaylorOut& out,
+                   int* status, int num_sms, cudaStream_t st);
 // blocks_per_sm: 0 = as many as fit (the grid never exceeds taylor_max_grid);
 // variant: 0 = direct grid-stride rows, 1 = chunks prefetched by bulk TMA copies
 int launch_taylor(bool c64, const ModelDev& m, const int* blk, const int* nbr, int64_t nbr_cap,

@@ -278,6 +278,28 @@ class Engine:
         e = nat.ExpmInfo.from_buffer_copy(raw)
         return psi_out, [bool(e.converged), int(e.final_m), float(e.c1_plus_c2), float(e.term_ratio)]
 
+    def krylov_bytes(self, cap, order):
+        nbytes = ctypes.c_size_t()
+        nat.check(self.lib.paces_lanczos_bytes(self.ctx, int(cap), int(order), ctypes.byref(nbytes)), self.ctx,
+                  "lanczos_bytes")
+        return int(nbytes.value)
+
+    def new_krylov(self, cap, order):
+        """Device workspace of the Lanczos step for bases of up to `cap` states."""
+        return torch.empty(self.krylov_bytes(cap, order), dtype=torch.uint8, device=self.device)
+
+    def lanczos(self, b: DevBasis, h: DevHMat, psi_in, dt, order, psi_out=None, krylov=None):
+        """psi_out = exp(-i dt H) psi_in from order + 1 Lanczos vectors (paces_lanczos)."""
+        psi_out = self.new_vector(b.cap) if psi_out is None else psi_out
+        krylov = self.new_krylov(b.cap, order) if krylov is None else krylov
+        info = torch.zeros(ctypes.sizeof(nat.ExpmInfo), dtype=torch.uint8, device=self.device)
+        nat.check(self.lib.paces_lanczos(self.ctx, ctypes.byref(b.c()), ctypes.byref(h.c()), _ptr(psi_in),
+                                         _ptr(psi_out), float(dt), int(order), _ptr(info), _ptr(krylov),
+                                         int(krylov.numel()), _stream(self.device)), self.ctx, "lanczos")
+        self.raise_status("lanczos")
+        e = nat.ExpmInfo.from_buffer_copy(info.cpu().numpy().tobytes())
+        return psi_out, [bool(e.converged), int(e.final_m), float(e.c1_plus_c2), float(e.term_ratio)]
+
     def observables(self, b: DevBasis, h: DevHMat, psi, what=nat.OBS_NORM | nat.OBS_ENERGY | nat.OBS_SITES):
         out = torch.zeros(3 + 2 * self.L, dtype=torch.float64, device=self.device)
         ws, nb = self.workspace()
@@ -446,13 +468,16 @@ class Trajectory:
 
     def __init__(self, eng: Engine, maxstates, enlarge_steps, m_star=100, diagnostics=True,
                  shuffle_seed=None, renormalize=False, explosion_cutoff=2.0, cap=None, graph=False,
-                 weighting=nat.WEIGHT_NONE, tau=0.0):
+                 weighting=nat.WEIGHT_NONE, tau=0.0, lanczos_order=0):
         if weighting not in (nat.WEIGHT_NONE, nat.WEIGHT_COHERENCE, nat.WEIGHT_NORM):
             raise ValueError(f"unknown weighting {weighting}")
         if weighting != nat.WEIGHT_NONE and tau == 0:
             raise ValueError("Specify a non-zero tau for this function to use U-weighting.")
         self.weighting = int(weighting)
         self.tau = float(tau)
+        if not 0 <= int(lanczos_order) <= nat.MAX_LANCZOS_ORDER:
+            raise ValueError(f"lanczos_order must lie in 0..{nat.MAX_LANCZOS_ORDER}")
+        self.lanczos_order = int(lanczos_order)
         self.eng = eng
         self.maxstates = int(maxstates)
         self.enlarge_steps = int(enlarge_steps)
@@ -480,6 +505,8 @@ class Trajectory:
         h = e.new_hmat()
         self.hs = [h, e.new_hmat() if self.weighting else h]
         self._h_valid = False   # hs[cur] holds the table of bases[cur]
+        # the Lanczos step's Krylov vectors (ExpmParams.lanczos_order > 0)
+        self.krylov = e.new_krylov(e.cap, self.lanczos_order) if self.lanczos_order else None
 
     @property
     def h(self) -> DevHMat:
@@ -547,6 +574,10 @@ class Trajectory:
         p.shuffle_seed = 0 if self.shuffle_seed is None else int(self.shuffle_seed) & 0xFFFFFFFFFFFFFFFF
         p.step_index = self.step_index
         p.explosion_cutoff = self.explosion_cutoff
+        if self.lanczos_order:
+            p.lanczos_order = self.lanczos_order
+            p.krylov = self.krylov.data_ptr()
+            p.krylov_bytes = int(self.krylov.numel())
         if self.proposal is not None:
             p.proposal = 1
             p.proposal_threshold = float(self.proposal[1])

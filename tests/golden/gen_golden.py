@@ -18,6 +18,7 @@ Fixtures written:
   ed_n4.npz           exact-diagonalisation known answer (full Hilbert space)
   obs_extra_n7c8.npz  hopping, mu_to_0, coupling and reduced density matrices
   scaled_n8c16.npz    a trajectory propagated with ExpmParams(use_scaling=True)
+  lanczos_<name>.npz  trajectories propagated with ExpmParams(lanczos_order=m)
   tau_<weighting>_n8c16.npz  trajectories truncated by the look-ahead weights (tau=0.2)
   lattice_<name>.npz  geo_dim > 1 lattices and the hopping2 term (open boundaries)
   fragment31.npz      (m, s) of code fragment 3.1 for synthetic norms and norm estimates
@@ -324,6 +325,44 @@ def gen_traj_scaled(paces, workdir):
                         config=np.array([nchain, dim, g, 2000, 1, 30, 2], dtype=np.float64))
 
 
+LANCZOS_RUNS = {
+    # name: (nchain, max_ho_dim, g, maxstates, steps, initpos, lanczos_order, dt)
+    # open chains off their mirror axis; a short Krylov space over long steps, whose error
+    # tells it from the Taylor series; and one whose Krylov space closes exactly (g = 0: the
+    # exciton on the end site of a 4-site chain spans 4 vectors, then beta = 0)
+    "n8c16_m12": (8, 16, 1.2, 2000, 30, 2, 12, 0.05),
+    "n6c8_m25": (6, 8, 1.0, 800, 20, 1, 25, 0.05),
+    "n8c16_m3_dt0.15": (8, 16, 1.2, 2000, 20, 2, 3, 0.15),
+    "g0_n4c4_m10": (4, 4, 0.0, 500, 10, 0, 10, 0.05),
+}
+
+
+def gen_traj_lanczos(paces, name, cfg, workdir):
+    """The Lanczos propagation (ExpmParams(lanczos_order=m): the reference's _lanczos,
+    paces/core/time_evolution.py:515-549, selected at :577-578)."""
+    from paces.models import holstein
+    from paces.core.time_evolution import CoeffSaveParams, ExpmParams, TimeEvoParams
+    from paces.config import devices
+    nchain, dim, g, maxstates, steps, initpos, order, dt = cfg
+    with devices.vector_dev:
+        ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain, use_terms=terms(g), debug_verb=0)
+        te = holstein.TimeEvolution(ham, holstein.Observables, ["n_exc", "n_pho", "total_energy"], workdir,
+                                    TimeEvoParams(maxstates=maxstates, enlarge_steps=1, shuffle_seed=None),
+                                    ExpmParams(lanczos_order=order), os.path.join(workdir, "params.log"))
+        te.create_nonuniform_basis([1] * nchain, minpos=initpos, maxpos=initpos + 1)
+        te.create_initial_vector([1.0], [[initpos] + [0] * nchain])
+        te.generate_timeline(np.arange(steps + 1) * dt, CoeffSaveParams())
+        vec, who = np.asarray(te.vector), np.asarray(te.whoami)
+    od = os.path.join(workdir, "observables")
+    np.savez_compressed(os.path.join(HERE, f"lanczos_{name}.npz"),
+                        n_exc=np.loadtxt(os.path.join(od, "n_exc.real")),
+                        n_pho=np.loadtxt(os.path.join(od, "n_pho.real")),
+                        energy=np.loadtxt(os.path.join(od, "total_energy.real")),
+                        diagnostics=np.loadtxt(os.path.join(od, "diagnostics.log")),
+                        vector=vec, whoami=who,
+                        config=np.array([nchain, dim, g, maxstates, 1, steps, initpos, order, dt], dtype=np.float64))
+
+
 TAU_RUNS = {
     # name: weighting_name -- N=8, dim 16, g=1, maxstates 1500, 30 steps of dt 0.05, tau 0.2
     "tau_coherence_n8c16": "coherence",
@@ -460,6 +499,8 @@ def main():
     jobs.append(("ed_n4", lambda: gen_ed(paces, fresh())))
     jobs.append(("obs_extra_n7c8", lambda: gen_obs_extra(paces, fresh())))
     jobs.append(("scaled_n8c16", lambda: gen_traj_scaled(paces, fresh())))
+    for name, cfg in LANCZOS_RUNS.items():
+        jobs.append((f"lanczos_{name}", lambda name=name, cfg=cfg: gen_traj_lanczos(paces, name, cfg, fresh())))
     for name, weighting in TAU_RUNS.items():
         jobs.append((name, lambda name=name, w=weighting: gen_traj_tau(paces, name, w, fresh())))
     jobs.append(("fragment31", lambda: gen_fragment(paces, fresh())))

@@ -327,3 +327,36 @@ def test_lattice_model_validation():
         po.Model(4, [4] * 4, geo_dim=2, J2=0.5)        # l = 2: no next-nearest neighbour
     with pytest.raises(NotImplementedError):
         po.Model(9, [4] * 9, geo_dim=2, periodic=True)
+
+
+LANCZOS = sorted(glob.glob(os.path.join(GOLDEN, "lanczos_*.npz")))
+
+
+@pytest.mark.parametrize("path", LANCZOS, ids=os.path.basename)
+def test_lanczos_matches_the_reference(path):
+    """The oracle's Lanczos propagation inside a trajectory against the reference's runs with
+    ExpmParams(lanczos_order=m) (tests/golden/lanczos_*.npz): observables at every step,
+    basis sizes, the placeholder diagnostics, the final basis and amplitudes."""
+    f = np.load(path)
+    nchain, dim, g, ms, es, steps, initpos, order, dt = f["config"]
+    nchain, dim, ms, es, steps, initpos, order = (int(x) for x in (nchain, dim, ms, es, steps, initpos, order))
+    m = po.Model(nchain, [dim] * nchain, g=float(g))
+    t = np.arange(steps + 1) * float(dt)
+    tr = po.Trajectory(m, po.initial_basis(m, initpos), np.array([1.0 + 0j]), ms, es, lanczos_order=order)
+    recs = tr.run(t)
+    np.testing.assert_allclose(np.array([r.n_exc for r in recs]), f["n_exc"][:, 2:], rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(np.array([r.n_pho for r in recs]), f["n_pho"][:, 2:], rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(np.array([r.norm for r in recs]), f["n_exc"][:, 1], rtol=1e-12)
+    diag = f["diagnostics"]
+    assert [r.numstates for r in recs] == diag[:, 9].astype(int).tolist()
+    assert np.all(diag[1:, 5:9] == 0)      # [False, 0, 0, 0]: the reference's placeholder
+    assert np.array_equal(tr.whoami, f["whoami"])
+    np.testing.assert_allclose(tr.vector, f["vector"], rtol=0, atol=1e-13)
+    # the fixture tells the Krylov path from the Taylor series: the latter records its term
+    # counts and stop flags where the Lanczos step writes the placeholder
+    taylor = po.Trajectory(m, po.initial_basis(m, initpos), np.array([1.0 + 0j]), ms, es)
+    t_recs = taylor.run(t[:3])
+    assert int(t_recs[1].expm_dbg[1]) > 0 and bool(t_recs[1].expm_dbg[0])
+    if order < 5:  # and a short Krylov space over long steps moves the observables
+        dev = np.abs(np.array([r.n_exc for r in t_recs]) - f["n_exc"][:3, 2:]).max()
+        assert dev > 1e-6, dev
