@@ -39,7 +39,7 @@ if HERE not in sys.path:
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="c64", choices=["c128", "c64"],
@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--open-chain", action="store_true", help="open boundaries (the reference's only mode)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="plain: skip the learned form over the metric's window (training takes ~a minute)")
+    ap.add_argument("--ref-steps", type=int, default=3,
+                    help="reference arm: oracle steps timed at the configuration (each about a minute)")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "learned", "longchain"],
                     help="plain: one N=32 chain at maxstates 2^22; batched: 64 trajectories drawn from --seed; "
@@ -206,6 +210,16 @@ def prepare(a, eng, maxstates):
     return tr, nprep
 
 
+# The metric is quoted over t = 10/J at dt = 0.05: steps 51..200, the first 50 steps (basis growth
+# and saturation) are the untimed lead-in.
+WINDOW_FROM, WINDOW_TO = 50, 200
+
+
+def evolving_steps(tr):
+    """Evolving steps the trajectory has taken (its first step does not evolve)."""
+    return tr.step_index - 1
+
+
 def autotune_shapes():
     from paces_b200 import autotune
     return autotune.SHAPES
@@ -265,55 +279,82 @@ def read_profile_traffic(precision):
 # --------------------------------------------------------------------------------------------
 # CPU restatement (reference arm and cpu_baseline)
 # --------------------------------------------------------------------------------------------
-def oracle_sample(a, m_s, steps, warmup):
-    """Time the CPU oracle on a bounded sample of the workload: the same chain at a reduced
-    maxstates m_s, grown to saturation untimed, then `warmup` + `steps` timed oracle steps.
-    Returns steps/s scaled linearly to a.maxstates (the oracle's cost grows at least
-    linearly with the basis, so the scaled figure favours the CPU), and a description."""
+def oracle_at_config(a, dev, steps, warmup):
+    """Time the CPU oracle (the NumPy restatement of the reference's step) at the workload's own
+    configuration: the same chain and maxstates, from the saturated state at t = WINDOW_FROM * dt.
+    That input state comes from a complex128 device run of the same trajectory (the oracle itself
+    would need tens of minutes to grow it); the timed steps are the oracle's alone, each a full
+    time step of the reference algorithm (truncation, expansion, lexsort/unique, searchsorted
+    lookups, COO/CSR assembly, Taylor series with SciPy CSR SpMV, observables, diagnostics).
+    Returns (steps/s, description)."""
+    import torch
     from oracle import paces_oracle as po
+    from paces_b200.engine import Engine
+    eng = Engine(model_params(a, "c128"), device=dev)
+    tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps)
+    while evolving_steps(tr) < WINDOW_FROM:
+        tr.step(evolve=True, dt=a.dt)
+    rows = eng.basis_to_ref(tr.basis).cpu().numpy().view(np.uint32).copy()
+    vec = tr.vector.cpu().numpy().astype(np.complex128)
+    S0 = int(rows.shape[0])
+    eng.close()
+    del tr, eng
+    torch.cuda.empty_cache()
     model = po.Model(a.nchain, [16] * a.nchain, g=a.g, periodic=not a.open_chain)
-    tr = po.Trajectory(model, po.initial_basis(model, 0), np.array([1.0 + 0j]), m_s, a.enlarge_steps)
-    t = 0.0
-    tr.first_step(t)
-    n = 0
-    while True:
-        t += a.dt
-        rec = tr.step(t, a.dt)
-        n += 1
-        if len(tr.records) > 3 and rec.numstates > 3 * m_s and n > 3:
-            break
-        if n > 200:
-            break
+    otr = po.Trajectory(model, rows, vec, a.maxstates, a.enlarge_steps)
+    t = WINDOW_FROM * a.dt
     for _ in range(warmup):
         t += a.dt
-        tr.step(t, a.dt)
+        otr.step(t, a.dt)
     t0 = time.perf_counter()
     for _ in range(steps):
         t += a.dt
-        tr.step(t, a.dt)
-    dt_wall = time.perf_counter() - t0
-    sps = steps / dt_wall
-    scaled = sps * m_s / a.maxstates
-    desc = (f"{steps} oracle steps of the same chain at maxstates={m_s} (saturated, S~{tr.records[-1].numstates}),"
-            f" {dt_wall:.1f} s, scaled by {m_s}/{a.maxstates} (cost linear in maxstates)")
-    return scaled, desc, sps, m_s
+        otr.step(t, a.dt)
+    wall = time.perf_counter() - t0
+    threads = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "MKL_NUM_THREADS", "OPENBLAS_NUM_THREADS")}
+    desc = (f"{steps} oracle steps (after {warmup} untimed) of the configuration itself, maxstates={a.maxstates}, "
+            f"from the saturated state at step {WINDOW_FROM} (S={S0} -> {otr.records[-1].numstates}), "
+            f"{wall:.1f} s; host nproc={os.cpu_count()}, threads {threads}: NumPy lexsort/searchsorted and "
+            f"SciPy CSR SpMV run on one core")
+    return steps / wall, desc
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    steps = max(1, a.steps)
-    value, desc, _, _ = oracle_sample(a, 1 << 16, steps, max(0, a.warmup))
-    cfg = {"workload": workload_name(a), "nchain": a.nchain, "maxstates": a.maxstates, "g": a.g,
-           "enlarge_steps": a.enlarge_steps, "precision": "c128", "bench_sample": "bounded, see cpu_baseline"}
-    line = {"impl": "reference", "metric": "time-steps/s at 4M states: learned+FP32 vs plain FP64, observable err <=1e-5",
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    # each oracle step at the configuration takes about a minute: a bounded sample of the
+    # requested steps, at the configuration itself (not scaled from a smaller one)
+    steps = max(1, min(a.steps, a.ref_steps))
+    warmup = min(max(a.warmup, 0), 1)
+    value, desc = oracle_at_config(a, f"cuda:{local}", steps, warmup)
+    line = {"impl": "reference", "metric": metric_name(a),
             "value": value, "unit": "time-steps/s",
-            "n_gpus": a.gpus, "steps": steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": cfg,
+            "n_gpus": a.gpus, "steps": steps, "warmup": warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": workload_config(a, "c128"),
+            "sample": f"{steps} of the {a.steps} requested steps (each about a minute of CPU work)",
             "cpu_baseline": {"value": value, "unit": "time-steps/s", "cores": 1, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": "time-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def metric_name(a):
+    """The line's metric: BASELINE's time-steps/s at 4M states, with the form the value measures."""
+    if a.precision == "c64":
+        return ("time-steps/s at 4M states: FP32 (complex64, fp64 scalars) vs plain FP64, observable err <=1e-5; "
+                "the learned+FP32 form is reported beside it (window.learned_c64)")
+    return "time-steps/s at 4M states (plain FP64)"
+
+
+def workload_config(a, precision):
+    return {"workload": workload_name(a), "nchain": a.nchain, "cutoff": 15, "g": a.g, "omega0": 1.0, "J": 1.0,
+            "dt": a.dt, "maxstates": a.maxstates, "enlarge_steps": a.enlarge_steps,
+            "boundary": "open" if a.open_chain else "periodic", "precision": precision,
+            "timed_steps_from": WINDOW_FROM + 1}
 
 
 # --------------------------------------------------------------------------------------------
@@ -348,8 +389,12 @@ def run_ours(a):
         from paces_b200 import autotune
         tuning = autotune.tune(tr, a.dt)
         log(a, f"tuning: {tuning}")
-    for _ in range(max(a.warmup, 0)):
+    # warm-up: at least W steps, and up to step WINDOW_FROM, so the timed steps are the
+    # metric's window (steps 51.. of t = 10/J)
+    nwarm = max(a.warmup, WINDOW_FROM - evolving_steps(tr))
+    for _ in range(nwarm):
         tr.step(evolve=True, dt=a.dt)
+    first_timed = evolving_steps(tr) + 1
 
     def barrier():
         torch.cuda.synchronize()
@@ -397,7 +442,7 @@ def run_ours(a):
 
     compare = None
     if a.precision == "c64" and not a.no_compare and a.weighting == "none":
-        compare = compare_precisions(a, f"cuda:{local}", dist)
+        compare = compare_precisions(a, f"cuda:{local}", dist, learned=not a.no_learned)
 
     total_steps = a.steps * world
     value = total_steps / (ms / 1e3)
@@ -412,22 +457,21 @@ def run_ours(a):
     step_alg = statistics.mean(step_bytes(r, cs, eng.nw, a.enlarge_steps) for r in recs)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        v, desc, _, _ = oracle_sample(a, 1 << 16, 15, 1)  # about 10 s of timed CPU work
+        v, desc = oracle_at_config(a, f"cuda:{local}", 1, 0)  # one full oracle step at the configuration
         cpu = {"value": v, "unit": "time-steps/s", "cores": 1, "kind": "port", "sample": desc}
     if rank == 0:
-        cfg = {"workload": workload_name(a), "nchain": a.nchain, "cutoff": 15, "g": a.g, "omega0": 1.0, "J": 1.0,
-               "dt": a.dt, "maxstates": a.maxstates, "enlarge_steps": a.enlarge_steps,
-               "boundary": "open" if a.open_chain else "periodic", "precision": a.precision,
-               "states_per_step": int(S_mean), "taylor_terms_per_step": terms, "prep_steps": nprep,
-               "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}",
-               "cuda_graph": not a.no_graph,
-               "weighting": None if a.weighting == "none" else {"name": a.weighting, "tau": a.tau},
-               "tuning": None if tuning is None else {k: tuning[k] for k in autotune_shapes()},
-               "form": ("complex64 amplitudes and SpMV, fp64 norms / stop test / sums; learned proposal off "
-                        "(--workload learned measures it)") if a.precision == "c64" else "complex128 plain"}
+        cfg = workload_config(a, a.precision)
+        cfg.update({"timed_steps": f"{first_timed}..{first_timed + a.steps - 1}",
+                    "states_per_step": int(S_mean), "taylor_terms_per_step": terms, "prep_steps": nprep,
+                    "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}",
+                    "cuda_graph": not a.no_graph,
+                    "weighting": None if a.weighting == "none" else {"name": a.weighting, "tau": a.tau},
+                    "tuning": None if tuning is None else {k: tuning[k] for k in autotune_shapes()},
+                    "form": ("plain method in complex64: amplitudes and SpMV in fp32, norms, stop test and sums in "
+                             "fp64; the learned proposal is off in the timed steps (window.learned_c64 measures "
+                             "the learned form)") if a.precision == "c64" else "complex128 plain"})
         line = {
-            "metric": "time-steps/s at 4M states: learned+FP32 vs plain FP64, observable err <=1e-5"
-                      if a.precision == "c64" else "time-steps/s at 4M states (plain FP64)",
+            "metric": metric_name(a),
             "value": value, "unit": "time-steps/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic", "config": cfg,
@@ -447,37 +491,111 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
-def compare_precisions(a, dev, dist, total=200, window_from=50):
-    """The same trajectory (t = 0 .. total * dt) in complex128 -- the FP64 plain oracle --
-    and in complex64: time-steps/s of both over steps window_from..total and the largest
-    difference of every observable over the whole run."""
+def window_observables(recs, L):
+    return {"n_exc": np.array([list(r.n_exc)[:L] for r in recs]), "n_pho": np.array([list(r.n_pho)[:L] for r in recs]),
+            "energy": np.array([r.energy_re for r in recs]), "norm": np.array([r.norm for r in recs])}
+
+
+def timed_steps(fn, n):
+    """Run fn() n times on the current stream between two CUDA events; (results, ms)."""
+    import torch
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = [fn() for _ in range(n)]
+    e1.record(stream)
+    e1.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def train_proposal(a, dev, lf=WINDOW_FROM):
+    """The learned proposal's training on the GPU: keep/drop labels from the first lf steps of
+    plain complex64 runs at shuffle seeds 0..train_seeds-1, then the MLP fitted by the library's
+    forward/backward/Adam kernels and the keep threshold set for the target recall on held-out
+    steps.  Returns (mlp, threshold, info)."""
     import torch
     from paces_b200.engine import Engine
-    stream = torch.cuda.current_stream()
+    from paces_b200.proposal import ProposalMLP, collect, threshold_for_recall
+    xs, ys, sws, hold = [], [], [], None
+    t0 = time.perf_counter()
+    for seed in range(a.train_seeds):
+        eng = Engine(model_params(a, "c64"), device=dev)
+        tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps)
+        tr.shuffle_seed = seed
+        ds, h = collect(tr, lf, a.dt, neg_per_pos=4, max_pos=25_000, seed=seed, held_out=lf - 5)
+        xs.append(ds.x)
+        ys.append(ds.y)
+        sws.append(ds.sw)
+        hold = hold or h
+        eng.close()
+    collect_s = time.perf_counter() - t0
+    x, y, sw = torch.cat(xs), torch.cat(ys), torch.cat(sws)
+    mlp = ProposalMLP(dev, seed=0)
+    t0 = time.perf_counter()
+    losses = mlp.fit(x, y, sw, epochs=2, batch=8192, lr=2e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    thr0 = threshold_for_recall(mlp.forward(hold[0]), hold[1], a.recall)
+    info = {"runs": a.train_seeds, "steps_per_run": lf, "samples": int(x.shape[0]), "positives": int(y.sum().item()),
+            "epochs": 2, "loss": losses, "collect_s": collect_s, "train_s": train_s}
+    return mlp, thr0, info
+
+
+def learned_run(a, dev, mlp, thr0, lf=WINDOW_FROM, total=WINDOW_TO):
+    """Plain complex64 for lf steps, then the proposal (full-expansion judge every 10th step)
+    until step `total`: (records of steps 0..total, ms of steps lf+1..total, the learned
+    trajectory, its engine)."""
+    from paces_b200.engine import Engine
+    from paces_b200.proposal import LearnedTrajectory
+    eng = Engine(model_params(a, "c64"), device=dev)
+    tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
+    recs = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(lf)]
+    lt = LearnedTrajectory(tr, mlp, thr0, judge_every=10, target_recall=a.recall)
+    window, ms = timed_steps(lambda: lt.step(a.dt), total - lf)
+    return recs + window, ms, lt, eng
+
+
+def compare_precisions(a, dev, dist, total=WINDOW_TO, window_from=WINDOW_FROM, learned=True):
+    """The metric's comparison over t = 0 .. total * dt, on fresh runs of the same trajectory:
+    complex128 (the FP64 plain oracle), complex64, and with `learned` the learned proposal in
+    complex64 (trained first on the GPU).  Time-steps/s of each over steps window_from+1..total
+    and the largest difference of every observable from the complex128 run."""
+    from paces_b200.engine import Engine
     obs, rate = {}, {}
     for prec in ("c128", "c64"):
         eng = Engine(model_params(a, prec), device=dev)
         tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
         recs = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(window_from)]
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        recs += [tr.step(evolve=True, dt=a.dt) for _ in range(total - window_from)]
-        e1.record(stream)
-        e1.synchronize()
-        ms = max_over_ranks(e0.elapsed_time(e1), dist)
-        rate[prec] = (total - window_from) / (ms / 1e3)
-        L = a.nchain
-        obs[prec] = {"n_exc": np.array([list(r.n_exc)[:L] for r in recs]),
-                     "n_pho": np.array([list(r.n_pho)[:L] for r in recs]),
-                     "energy": np.array([r.energy_re for r in recs]), "norm": np.array([r.norm for r in recs])}
+        window, ms = timed_steps(lambda: tr.step(evolve=True, dt=a.dt), total - window_from)
+        rate[prec] = (total - window_from) / (max_over_ranks(ms, dist) / 1e3)
+        obs[prec] = window_observables(recs + window, a.nchain)
         eng.close()
-    err = {k: float(np.max(np.abs(obs["c128"][k] - obs["c64"][k]))) for k in obs["c128"]}
-    return {"plain_c128": {"value": rate["c128"], "unit": "time-steps/s",
-                           "window": f"steps {window_from + 1}..{total} of a fresh run"},
-            "c64_same_window": {"value": rate["c64"], "unit": "time-steps/s"},
-            "speedup_c64_vs_c128": rate["c64"] / rate["c128"],
-            "observable_error": {"c64_vs_c128": err, "t_end": total * a.dt, "bound": 1e-5,
-                                 "within_bound": all(v <= 1e-5 for v in err.values())}}
+    training = None
+    lt = None
+    if learned:
+        mlp, thr0, training = train_proposal(a, dev, window_from)
+        recs, ms, lt, eng = learned_run(a, dev, mlp, thr0, window_from, total)
+        rate["learned_c64"] = (total - window_from) / (max_over_ranks(ms, dist) / 1e3)
+        obs["learned_c64"] = window_observables(recs, a.nchain)
+        win = recs[window_from + 1:]
+        training.update({"target_recall": a.recall, "threshold_start": thr0, "threshold_end": lt.threshold,
+                         "states_per_step": statistics.mean(r.n_states for r in win),
+                         "enlarged_per_step": statistics.mean(r.n_enlarged for r in win),
+                         "judge_steps": len(lt.judges)})
+        eng.close()
+    err = {form: {k: float(np.max(np.abs(obs["c128"][k] - obs[form][k]))) for k in obs["c128"]}
+           for form in obs if form != "c128"}
+    out = {"steps": f"{window_from + 1}..{total} of fresh runs (t = {total * a.dt:g}/J)",
+           "plain_c128": {"value": rate["c128"], "unit": "time-steps/s"},
+           "plain_c64": {"value": rate["c64"], "unit": "time-steps/s"},
+           "ratio_c64_vs_c128": rate["c64"] / rate["c128"],
+           "observable_error_vs_c128": err, "bound": 1e-5,
+           "within_bound": {form: all(v <= 1e-5 for v in e.values()) for form, e in err.items()}}
+    if learned:
+        out["learned_c64"] = {"value": rate["learned_c64"], "unit": "time-steps/s", "training": training}
+        out["ratio_learned_vs_c128"] = rate["learned_c64"] / rate["c128"]
+        out["ratio_learned_vs_plain_c64"] = rate["learned_c64"] / rate["c64"]
+    return {"window": out}
 
 
 def run_e2e(a, eng, tr, barrier, dist):
@@ -692,7 +810,6 @@ def run_learned(a):
     import torch
     from paces_b200 import _native as nat
     from paces_b200.engine import Engine
-    from paces_b200.proposal import LearnedTrajectory, ProposalMLP, collect, threshold_for_recall
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -732,36 +849,13 @@ def run_learned(a):
     # 1. the plain complex128 run (the oracle of the comparison) and the plain complex64 run
     ref, ms128 = plain("c128")
     r64, ms64 = plain("c64")
-    # 2. training data: the first learn_from steps of plain complex64 runs at shuffle seeds 0..n-1
-    xs, ys, sws, hold = [], [], [], None
-    t0 = time.perf_counter()
-    for seed in range(a.train_seeds):
-        eng = Engine(model_params(a, "c64"), device=dev)
-        tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps)
-        tr.shuffle_seed = seed
-        ds, h = collect(tr, lf, a.dt, neg_per_pos=4, max_pos=25_000, seed=seed, held_out=lf - 5)
-        xs.append(ds.x)
-        ys.append(ds.y)
-        sws.append(ds.sw)
-        hold = hold or h
-        eng.close()
-    collect_s = time.perf_counter() - t0
-    x, y, sw = torch.cat(xs), torch.cat(ys), torch.cat(sws)
-    mlp = ProposalMLP(dev, seed=0)
-    t0 = time.perf_counter()
-    losses = mlp.fit(x, y, sw, epochs=2, batch=8192, lr=2e-3)
-    torch.cuda.synchronize()
-    train_s = time.perf_counter() - t0
-    thr0 = threshold_for_recall(mlp.forward(hold[0]), hold[1], a.recall)
-    # 3. the learned run: plain complex64 for learn_from steps, then the proposal
-    eng = Engine(model_params(a, "c64"), device=dev)
-    tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
-    recs = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(lf)]
-    lt = LearnedTrajectory(tr, mlp, thr0, judge_every=10, target_recall=a.recall)
+    # 2. training on the GPU, then 3. the learned run: plain complex64 for learn_from steps, then
+    #    the proposal
+    mlp, thr0, training = train_proposal(a, dev, lf)
     with ClockSampler(local) as clk:
-        window, ms = timed(lambda: [lt.step(a.dt) for _ in range(steps - lf)])
+        recs, ms, lt, eng = learned_run(a, dev, mlp, thr0, lf, steps)
     clocks = clk.summary()
-    recs += window
+    tr = lt.tr
     # stage split of proposal (non-judge) steps
     eng.set_profiling(True)
     use_graph, tr.use_graph = tr.use_graph, False
@@ -798,9 +892,7 @@ def run_learned(a):
                "nchain": a.nchain, "g": a.g, "omega0": 1.0, "J": 1.0, "dt": a.dt, "maxstates": a.maxstates,
                "enlarge_steps": a.enlarge_steps, "precision": "c64 (fp64 norms, stop test and sums)",
                "timed_steps": f"{lf + 1}..{steps} (proposal steps and every 10th a full-expansion judge step)",
-               "training": {"runs": a.train_seeds, "steps_per_run": lf, "samples": int(x.shape[0]),
-                            "positives": int(y.sum().item()), "epochs": 2, "loss": losses, "collect_s": collect_s,
-                            "train_s": train_s},
+               "training": training,
                "target_recall": a.recall, "threshold_start": thr0, "threshold_end": lt.threshold,
                "states_per_step_learned": statistics.mean(r.n_states for r in win),
                "states_per_step_plain": statistics.mean(r.n_states for r in ref[lf + 1:]),

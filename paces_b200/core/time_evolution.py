@@ -311,12 +311,19 @@ class TimeEvolutionFramework:
         raise NotImplementedError("the Hamiltonian is assembled on the device by every time step")
 
     def create_ham_mat(self):
-        raise NotImplementedError("the explicit total Hamiltonian (use_scaling=True) is not implemented")
+        """The total Hamiltonian of the current basis as self.ham_mat (paces/core/time_evolution.py:
+        375-379): here a device operator over the step's neighbour table (HamiltonianOperator),
+        not an assembled sparse matrix; `ham_mat @ v`, `1j * ham_mat` and
+        paces.aux.expm_multiply_simple(1j * ham_mat, v, t) run on the GPU."""
+        self.ham_mat = HamiltonianOperator(self)
+        return self.ham_mat
 
     def total_ham(self, vector, use_ham_mat=False):
         """H applied to a vector of the current basis (paces/core/time_evolution.py:382-400)."""
         if use_ham_mat:
-            raise NotImplementedError("use_ham_mat=True (explicit total Hamiltonian) is not implemented")
+            if self.ham_mat is None:
+                raise ValueError("use_ham_mat=True needs create_ham_mat() first")
+            return self.ham_mat @ vector
         x = torch.as_tensor(vector).to(self.engine.device, self.engine.cdtype).contiguous()
         return self.engine.apply_h(self._traj.basis, self._traj.h, x)
 
@@ -331,10 +338,9 @@ class TimeEvolutionFramework:
     def total_ham_ones(self, use_ham_mat=False):
         """H applied to a vector of ones: diag + the row sums of every term matrix
         (paces/core/time_evolution.py:403-420), float64 on the GPU.  (The reference adds the
-        row sums into its diag_vals array in place; here the diagonal is left unchanged.)"""
+        row sums into its diag_vals array in place; here the diagonal is left unchanged.)
+        use_ham_mat gives the same numbers: the operator is the same device H."""
         from .. import _native as nat
-        if use_ham_mat:
-            raise NotImplementedError("use_ham_mat=True (explicit total Hamiltonian) is not implemented")
         return self._weights(None, 0.0, nat.WEIGHT_HAM_ONES)
 
     def coherence_weighting_func(self, vector, tau):
@@ -408,6 +414,8 @@ class TimeEvolutionFramework:
                 if not ep.renormalize and rec.norm > ep.explosion_cutoff:
                     raise RuntimeError(f"Norm has exceeded preset explosion cutoff value ({ep.explosion_cutoff})!")
             self._whoami_cache = None
+            if ep.use_scaling and ep.lanczos_order == 0:
+                self.create_ham_mat()   # as the reference does for this path (time_evolution.py:801-803)
             # the reference's threshold is for complex128; complex64 amplitudes carry ~1e-7
             # relative rounding into <psi|H|psi>
             imag_tol = 1e-6 if self.engine.c64 else 1e-12
@@ -462,3 +470,51 @@ class TimeEvolutionFramework:
             with open(self.obsobj.fname_dict["diagnostics"], "a", encoding="utf-8") as diag_f:
                 numpy.savetxt(diag_f, line, newline=" ")
                 diag_f.write("\n")
+
+
+class HamiltonianOperator:
+    """The total Hamiltonian of a TimeEvolution's current basis as a device linear operator,
+    times a scalar: what create_ham_mat builds in the reference (diags(diag_vals) plus the
+    term matrices, paces/core/time_evolution.py:375-379), kept as the step's neighbour table.
+    `op @ v` is the device H row kernel (paces_apply_h) times the scalar; `c * op` scales it,
+    as the reference passes 1j * ham_mat to expm_multiply_simple.  The operator belongs to the
+    basis it was created on: after the next time step it raises instead of acting on a
+    different basis."""
+
+    def __init__(self, te, scale=1.0, _step=None):
+        if te._traj is None or te._traj.last is None:
+            raise ValueError("no Hamiltonian yet: take a time step (generate_timeline) first")
+        self.te = te
+        self.scale = complex(scale)
+        self._step = te._traj.step_index if _step is None else _step
+        n = te.numstates
+        self.shape = (n, n)
+        self.dtype = te.engine.cdtype
+
+    def _live(self):
+        if self.te._traj.step_index != self._step:
+            raise RuntimeError("this Hamiltonian operator belongs to an earlier basis; call create_ham_mat() again")
+        return self.te._traj
+
+    def __matmul__(self, vector):
+        tr = self._live()
+        eng = self.te.engine
+        n = self.shape[0]
+        x = torch.zeros(max(tr.basis.cap, 1), dtype=eng.cdtype, device=eng.device)
+        x[:n] = torch.as_tensor(vector).to(eng.device, eng.cdtype)[:n]
+        y = eng.apply_h(tr.basis, tr.h, x)[:n]
+        return y if self.scale == 1 else y * self.scale
+
+    def dot(self, vector):
+        return self @ vector
+
+    def __mul__(self, c):
+        return HamiltonianOperator(self.te, self.scale * complex(c), self._step)
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return self * -1.0
+
+    def __repr__(self):
+        return f"<HamiltonianOperator {self.shape[0]}x{self.shape[1]} x {self.scale}>"

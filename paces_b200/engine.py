@@ -630,16 +630,11 @@ class Trajectory:
         built by a non-evolving paces_step; the norms, stage count and order come from
         paces_b200.expm; the observables of the propagated state are measured again.
         Returns the step record."""
-        from . import expm
         rec = self.step(evolve=False, weighted=True)
         e, b, h = self.eng, self.basis, self.h
         psi = self.psis[self.cur]
-        _, _, dbar = e.hnorms(b, h)
-        _, a1, _ = e.hnorms(b, h, shift=dbar)
-        m, s = expm.choose(dt * a1, d=lambda p: self._norm_power(dt, dbar, p))
-        eta = np.exp(dt * 1j * dbar / s)
         out = self.psis[1 - self.cur]
-        dbg = e.expm_scaled(b, h, psi, out, dt, dbar, m, s, eta, tol=expm.TOL if not e.c64 else e.tol)
+        dbg = self.expm_apply(psi, out, dt)
         psi.copy_(out)
         n = b.count()
         if self.renormalize:
@@ -657,6 +652,21 @@ class Trajectory:
             raise RuntimeError(f"Norm has exceeded preset explosion cutoff value ({self.explosion_cutoff})!")
         self.last = rec
         return rec
+
+    def expm_apply(self, psi_in, psi_out, t):
+        """psi_out = exp(t * 1j H) psi_in on the current basis by scaling and squaring
+        (expm_multiply_simple(1j * H, psi, t), paces/aux/_scipy/_expm_multiply.py:106-202):
+        the trace shift and 1-norm from the device H rows, stages and order from
+        paces_b200.expm, every term on the device.  psi_in and psi_out hold the basis'
+        capacity.  Returns [converged, final_m, c1_plus_c2, term_ratio]."""
+        from . import expm
+        e, b, h = self.eng, self.basis, self.h
+        _, _, dbar = e.hnorms(b, h)
+        _, a1, _ = e.hnorms(b, h, shift=dbar)
+        ta = abs(t)  # the choice depends on |t| ||A||; a negative t propagates backwards
+        m, s = expm.choose(ta * a1, d=lambda p: self._norm_power(ta, dbar, p))
+        eta = np.exp(t * 1j * dbar / s)
+        return e.expm_scaled(b, h, psi_in, psi_out, t, dbar, m, s, eta, tol=expm.TOL if not e.c64 else e.tol)
 
     def _norm_power(self, dt, dbar, p):
         """||(dt A)^p||_1^(1/p) for A = 1j (H - dbar I) on the current basis, by the block

@@ -74,3 +74,49 @@ def test_large_steps_use_norm_estimates():
     eng.expm_scaled(b, h, tr.psis[tr.cur], out, dt, dbar, m, s, eta)
     want = sla.expm(1j * dt * H) @ psi0.cpu().numpy()
     np.testing.assert_allclose(out[:S].cpu().numpy(), want, rtol=0, atol=1e-11)
+
+
+def test_expm_multiply_simple_through_the_drop_in(tmp_path):
+    """paces.aux.expm_multiply_simple(1j * te.ham_mat, v, t) -- the reference's own call of its
+    scaling-and-squaring routine (paces/core/time_evolution.py:579-581) -- on the device H of
+    a drop-in time evolution: equal to dense exp(+-1j t H) v, the operator's products equal to
+    the explicit matrix, and a stale operator (after another step) refuses to act."""
+    import scipy.linalg as sla
+    import torch
+    from paces.aux import expm_multiply_simple
+    from paces.config import devices
+    from paces.core.time_evolution import CoeffSaveParams, ExpmParams, TimeEvoParams
+    from paces.models import holstein
+    from tests import gpu_helpers
+    if not devices.configure_called:
+        devices.configure()
+    nchain, dim, g = 6, 8, 1.3
+    terms = {"diag": dict(eps_sys=0.0, hbar_omega=1.0, delta_eps=0.0), "hopping": dict(J=1.0),
+             "vib_coupling": dict(g=g)}
+    ham = holstein.Hamiltonian(nchain=nchain, max_ho_dims=[dim] * nchain, use_terms=terms, debug_verb=0)
+    te = holstein.TimeEvolution(ham, holstein.Observables, ["n_exc"], str(tmp_path),
+                                TimeEvoParams(maxstates=400, enlarge_steps=1, shuffle_seed=None), ExpmParams(),
+                                str(tmp_path / "params.log"))
+    te.create_nonuniform_basis([1] * nchain, minpos=1, maxpos=2)
+    te.create_initial_vector([1.0], [[1] + [0] * nchain])
+    te.generate_timeline(np.arange(6) * 0.05, CoeffSaveParams())
+    op = te.create_ham_mat()
+    tr = te._traj
+    diag, mats, _ = gpu_helpers.csr_from_table(te.engine, tr.basis, tr.h, 1.0, g)
+    H = np.diag(diag) + sum(mm.toarray() for mm in mats.values())
+    v = te.vector.cpu().numpy()
+    np.testing.assert_allclose((op @ te.vector).cpu().numpy(), H @ v, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(te.total_ham(te.vector, use_ham_mat=True).cpu().numpy(), H @ v, rtol=0, atol=1e-13)
+    for t, A in ((0.05, 1j * op), (0.3, 1j * op), (0.05, -1j * op)):
+        F, dbg = expm_multiply_simple(A, te.vector, t=t, return_dbg=True)
+        sign = 1.0 if A.scale == 1j else -1.0
+        want = sla.expm(sign * 1j * t * H) @ v
+        np.testing.assert_allclose(F.cpu().numpy(), want, rtol=0, atol=1e-12)
+        assert bool(dbg[0]) and dbg[1] > 0
+    with pytest.raises(TypeError):
+        expm_multiply_simple(torch.eye(3), torch.ones(3))
+    with pytest.raises(NotImplementedError):
+        expm_multiply_simple(2.0 * op, te.vector)
+    te.generate_timeline(np.arange(2) * 0.05 + 1.0, CoeffSaveParams())
+    with pytest.raises(RuntimeError):
+        op @ te.vector
