@@ -223,6 +223,21 @@ int paces_version(void);                            /* 10000*major + 100*minor +
 /* Copy the context's device status word (errors raised by kernels of the stage entry points)
  * to the host, synchronising `stream`, and clear it. */
 int paces_read_status(paces_ctx *ctx, paces_stream_t stream, int32_t *host_status);
+/* Rows of `words` uint32 (1..16) in the reference's whoami layout, compared lexicographically
+ * (word 0 most significant); no context needed.  For the host API (the time step itself
+ * never searches or sorts rows).
+ * paces_rows_lower_bound replaces searchsorted_full_binary (paces/aux/cupy_search.py:78-93):
+ * out[i] = lower bound of query row i in the sorted rows of pb (n when beyond the end); with
+ * allow_escapes == 0 a query that is not present sets *dev_missing (device int) to 1 instead
+ * of the reference's device assert (:205-228).
+ * paces_rows_sort_unique replaces cupy_unique (paces/aux/helpers.py:63-75): the sorted unique
+ * rows of `rows` into out (room for n rows) and their number into *dev_count (device),
+ * using a caller-owned workspace of paces_rows_sort_bytes(n) bytes; n < 2^31. */
+int paces_rows_lower_bound(const uint32_t *pb, int64_t n, const uint32_t *q, int64_t nq, int32_t words,
+                           int32_t allow_escapes, int64_t *out, int32_t *dev_missing, paces_stream_t stream);
+size_t paces_rows_sort_bytes(int64_t n);
+int paces_rows_sort_unique(const uint32_t *rows, int64_t n, int32_t words, uint32_t *out, int64_t *dev_count,
+                           void *ws, size_t ws_bytes, paces_stream_t stream);
 /* Lanczos propagation: replaces _lanczos (paces/core/time_evolution.py:515-549), selected
  * by ExpmParams.lanczos_order = order (1 .. PACES_MAX_LANCZOS_ORDER, :577-578).  psi_out =
  * |psi| V exp(-i dt T) e_0 from order + 1 Lanczos vectors of H on the basis (fewer when

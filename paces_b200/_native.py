@@ -177,6 +177,9 @@ _SIGNATURES = {
                                 _P, _P],
     "paces_remap": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P, ctypes.c_size_t, _P],
     "paces_remap_noalloc": [_P, ctypes.POINTER(Basis), _P, ctypes.POINTER(Basis), _P, _P],
+    "paces_rows_lower_bound": [_P, ctypes.c_int64, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
+    "paces_rows_sort_bytes": [ctypes.c_int64],
+    "paces_rows_sort_unique": [_P, ctypes.c_int64, ctypes.c_int32, _P, _P, _P, ctypes.c_size_t, _P],
     "paces_lanczos_bytes": [_P, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t)],
     "paces_lanczos": [_P, ctypes.POINTER(Basis), ctypes.POINTER(HMat), _P, _P, ctypes.c_double, ctypes.c_int32, _P, _P,
                       ctypes.c_size_t, _P],
@@ -221,7 +224,7 @@ _SIGNATURES = {
     "paces_batch_set_test_hooks": [_P, ctypes.c_uint64, ctypes.c_int32],
     "paces_batch_stage_times": [_P, ctypes.POINTER(ctypes.c_float)],
 }
-_RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_kernel_launches": ctypes.c_ulonglong,
+_RESTYPES = {"paces_last_error": ctypes.c_char_p, "paces_rows_sort_bytes": ctypes.c_size_t, "paces_kernel_launches": ctypes.c_ulonglong,
              "paces_mlp_param_bytes": ctypes.c_size_t, "paces_mlp_master_floats": ctypes.c_int32,
              "paces_batch_last_error": ctypes.c_char_p, "paces_batch_kernel_launches": ctypes.c_ulonglong}
 STAGES = ("truncate", "expand", "assemble", "remap", "diagnostics", "taylor", "observables")

@@ -2,52 +2,38 @@
 
 The time step never calls these: its lookups are index maps produced by the device merge
 and the merge-path remap.  They serve the host API (e.g. custom observables), operate on
-the reference's uint32 row layout and run on the device with PyTorch.
+the reference's uint32 row layout; the search runs in libpaces_b200 (paces_rows_lower_bound).
 """
 
 import torch
 
-from .. import layout
-
-
-def _lex_less(a, b):
-    """Row-wise lexicographic a < b for int64 tensors of uint32 words."""
-    res = torch.zeros(a.shape[0], dtype=torch.bool, device=a.device)
-    decided = torch.zeros_like(res)
-    for w in range(a.shape[1]):
-        lt = a[:, w] < b[:, w]
-        gt = a[:, w] > b[:, w]
-        res |= ~decided & lt
-        decided |= lt | gt
-    return res
-
 
 def searchsorted_full_binary(phonebook, findme, allow_escapes=False):
     """Lower bound of every row of `findme` in the sorted rows of `phonebook`
-    (paces/aux/cupy_search.py:78-93).  Escapes return len(phonebook); with
-    allow_escapes=False a missing row raises LookupError (the reference's kernel asserts)."""
-    pb = layout.rows_i64(phonebook)
-    q = layout.rows_i64(findme).to(pb.device)
-    if pb.shape[1] != q.shape[1]:
+    (paces/aux/cupy_search.py:78-93), on the GPU by paces_rows_lower_bound.  Escapes return
+    len(phonebook); with allow_escapes=False a missing row raises LookupError (the
+    reference's kernel asserts)."""
+    import ctypes
+    from .. import _native as nat
+    from .helpers import _device_rows
+    pb, _ = _device_rows(phonebook)
+    q, _ = _device_rows(findme)
+    q = q.to(pb.device)
+    if pb.dim() != 2 or q.dim() != 2 or pb.shape[1] != q.shape[1]:
         raise ValueError("Incompatible array shapes.")
-    n, nq = pb.shape[0], q.shape[0]
-    lo = torch.zeros(nq, dtype=torch.int64, device=pb.device)
-    if nq == 0 or n == 0:
-        return lo
-    hi = torch.full((nq,), n, dtype=torch.int64, device=pb.device)
-    while bool((lo < hi).any()):
-        active = lo < hi
-        mid = (lo + hi) // 2
-        below = _lex_less(pb[mid.clamp(max=n - 1)], q)
-        lo = torch.where(active & below, mid + 1, lo)
-        hi = torch.where(active & ~below, mid, hi)
-    if not allow_escapes:
-        ok = lo < n
-        hit = torch.zeros_like(ok)
-        hit[ok] = (pb[lo[ok]] == q[ok]).all(dim=1)
-        if not bool(hit.all()):
-            raise LookupError("Target values not found in phonebook.")
-    return lo
+    n, nq, w = int(pb.shape[0]), int(q.shape[0]), int(pb.shape[1])
+    out = torch.zeros(max(nq, 1), dtype=torch.int64, device=pb.device)
+    if nq == 0:
+        return out[:0]
+    missing = torch.zeros(1, dtype=torch.int32, device=pb.device)
+    lib = nat.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream(pb.device).cuda_stream)
+    nat.check(lib.paces_rows_lower_bound(ctypes.c_void_p(pb.data_ptr()), n, ctypes.c_void_p(q.data_ptr()), nq, w,
+                                         1 if allow_escapes else 0, ctypes.c_void_p(out.data_ptr()),
+                                         ctypes.c_void_p(missing.data_ptr()), stream), None, "rows_lower_bound")
+    if not allow_escapes and int(missing.item()):
+        raise LookupError("Target values not found in phonebook.")
+    return out[:nq]
 
 
 def calc_partition_lens(partition_by, uniquevals):

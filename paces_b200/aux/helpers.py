@@ -4,7 +4,6 @@ import numpy
 import torch
 
 from ..config import SEARCHSORTED_TIMING_LEVEL
-from .. import layout
 
 
 def cartesian_product(*arrays):
@@ -41,16 +40,45 @@ def flatten_dbg_dict(d):
     return [x for lst in [d[k] for k in d] for x in lst]
 
 
-def cupy_unique(array):
-    """Sorted unique rows of a 2D uint32 array (paces/aux/helpers.py:63-75).
+def _device_rows(array):
+    """The rows as a contiguous int32 CUDA tensor, and a function that returns a result in the
+    input's type (torch tensor on its device, or a NumPy uint32 array)."""
+    if isinstance(array, torch.Tensor):
+        dev = array.device if array.is_cuda else torch.device("cuda", torch.cuda.current_device())
+        if array.dtype in (torch.int32, torch.uint32):
+            t = array.to(dev).contiguous().view(torch.int32)
+        else:
+            t = array.to(dev, torch.int64).to(torch.int32).contiguous()
+        if array.dtype == torch.uint32:
+            back = lambda x: x.view(torch.uint32)  # noqa: E731
+        elif array.dtype == torch.int32:
+            back = lambda x: x  # noqa: E731
+        else:
+            back = lambda x: x.to(torch.int64) & 0xFFFFFFFF  # noqa: E731
+        if not array.is_cuda:
+            return t, (lambda x: back(x).cpu())
+        return t, back
+    a = numpy.ascontiguousarray(numpy.asarray(array).astype(numpy.uint32, copy=False))
+    t = torch.from_numpy(a.view(numpy.int32)).to("cuda")
+    return t, (lambda x: x.cpu().numpy().view(numpy.uint32))
 
-    Returns the same type as the input (torch device tensor or NumPy array).  Used by the
-    host API only; the time step deduplicates inside the device merge.
-    """
+
+def cupy_unique(array):
+    """Sorted unique rows of a 2D uint32 array (paces/aux/helpers.py:63-75: a lexsort and an
+    adjacent-row dedup), computed on the GPU by paces_rows_sort_unique.  Returns the same type
+    as the input (torch tensor on its device, or a NumPy array)."""
+    import ctypes
+    from .. import _native as nat
     if len(array.shape) != 2:
         raise ValueError("Input array must be 2D.")
-    if isinstance(array, torch.Tensor):
-        host = layout.rows_i64(array.cpu()).numpy().astype(numpy.uint32)
-        out = layout.sort_unique_rows(host)
-        return torch.from_numpy(out.view(numpy.int32)).to(array.device).view(torch.uint32)
-    return layout.sort_unique_rows(numpy.asarray(array))
+    rows, back = _device_rows(array)
+    n, w = int(rows.shape[0]), int(rows.shape[1])
+    lib = nat.load()
+    out = torch.empty((max(n, 1), w), dtype=torch.int32, device=rows.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=rows.device)
+    ws = torch.empty(max(int(lib.paces_rows_sort_bytes(n)), 1), dtype=torch.uint8, device=rows.device)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(rows.device).cuda_stream)
+    nat.check(lib.paces_rows_sort_unique(ctypes.c_void_p(rows.data_ptr()), n, w, ctypes.c_void_p(out.data_ptr()),
+                                         ctypes.c_void_p(cnt.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                         stream), None, "rows_sort_unique")
+    return back(out[: int(cnt.item())])

@@ -1042,6 +1042,37 @@ int paces_taylor(paces_ctx* c, const paces_basis* b, const paces_hmat* h, const 
     return PACES_OK;
 }
 
+namespace {
+int current_sms() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        return 0;
+    return sms;
+}
+}  // namespace
+
+int paces_rows_lower_bound(const uint32_t* pb, int64_t n, const uint32_t* q, int64_t nq, int32_t words,
+                           int32_t allow_escapes, int64_t* out, int32_t* dev_missing, paces_stream_t stream) {
+    if (n < 0 || nq < 0 || (nq > 0 && (!q || !out)) || (n > 0 && !pb) || (!allow_escapes && !dev_missing))
+        return PACES_ERR_BADARG;
+    const int sms = current_sms();
+    if (!sms) return PACES_ERR_CUDA;
+    return launch_rows_lower_bound(pb, n, q, nq, words, allow_escapes ? 0 : 1, out, dev_missing, sms,
+                                   reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t paces_rows_sort_bytes(int64_t n) { return n < 0 ? 0 : rows_sort_ws_bytes(n); }
+
+int paces_rows_sort_unique(const uint32_t* rows, int64_t n, int32_t words, uint32_t* out, int64_t* dev_count,
+                           void* ws, size_t ws_bytes, paces_stream_t stream) {
+    if (n < 0 || !dev_count || (n > 0 && (!rows || !out || !ws))) return PACES_ERR_BADARG;
+    if (n > 0 && ws_bytes < rows_sort_ws_bytes(n)) return PACES_ERR_CAPACITY;
+    const int sms = current_sms();
+    if (!sms) return PACES_ERR_CUDA;
+    return launch_rows_sort_unique(rows, n, words, out, dev_count, ws, sms, reinterpret_cast<cudaStream_t>(stream));
+}
+
 int paces_lanczos_bytes(const paces_ctx* c, int64_t cap, int32_t order, size_t* bytes) {
     if (!c || !bytes || cap < 0 || order < 1 || order > kMaxLanczosOrder) return PACES_ERR_BADARG;
     *bytes = krylov_layout(c, cap, order).total;

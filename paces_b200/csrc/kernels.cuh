@@ -66,6 +66,13 @@ struct LanczosWs {
     uint64_t wait_ns;
 };
 int lanczos_max_grid(int num_sms);
+
+// ---- rows of uint32 words (host API helpers) ---------------------------------------------
+size_t rows_sort_ws_bytes(int64_t n);
+int launch_rows_lower_bound(const uint32_t* pb, int64_t n, const uint32_t* q, int64_t nq, int words, int must,
+                            int64_t* out, int* missing, int num_sms, cudaStream_t st);
+int launch_rows_sort_unique(const uint32_t* rows, int64_t n, int words, uint32_t* out, int64_t* count, void* ws,
+                            int num_sms, cudaStream_t st);
 int launch_lanczos(bool c64, const ModelDev& m, const int* blk, const int* nbr, const uint32_t* meta,
                    const void* v_in, void* res, double dt, int order, const LanczosWs& ws, const TaylorOut& out,
                    int* status, int num_sms, cudaStream_t st);

@@ -58,16 +58,6 @@ def test_layout_helpers_match_reference_packing(name):
     assert np.array_equal(got, f["keys_up"])
 
 
-def test_search_helpers_match_reference():
-    from paces_b200.aux import cupy_search
-    f = np.load(os.path.join(GOLDEN, "layout_n32c16.npz"))
-    uniq = torch.from_numpy(f["unique_out"].view(np.int32))
-    idx = cupy_search.searchsorted_full_binary(uniq, torch.from_numpy(f["search_hit_q"].view(np.int32)))
-    assert np.array_equal(idx.numpy(), f["search_hit_idx"].astype(np.int64))
-    with pytest.raises(LookupError):
-        cupy_search.searchsorted_full_binary(uniq, torch.from_numpy(f["search_any_q"].view(np.int32)))
-
-
 def test_drop_in_module_paths():
     import paces
     from paces.config import devices, INIT_VERBOSITY_LEVEL, SEARCHSORTED_TIMING_LEVEL
