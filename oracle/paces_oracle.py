@@ -96,6 +96,16 @@ def _window(keys, wi):
 
 def get_field(model: Model, keys, index):
     """n at field `index` (0 = exciton position) -- paces/core/hamiltonian.py:291-318."""
+    if np.ndim(index) == 0:
+        # one field for every row: plain column arithmetic on the (one or two) words holding it
+        i = int(index)
+        b0, w = int(model.bit_offset[i]), int(model.bitwidths[i])
+        wi = b0 // 32
+        n2 = b0 + w - 32 * wi
+        val = keys[:, wi].astype(np.uint64) << np.uint64(32)
+        if wi + 1 < keys.shape[1]:
+            val |= keys[:, wi + 1].astype(np.uint64)
+        return ((val >> np.uint64(64 - n2)) & np.uint64((1 << w) - 1)).astype(np.uint32)
     index = np.asarray(index, dtype=np.int64)
     b0 = model.bit_offset[index]
     w = model.bitwidths[index]
