@@ -64,6 +64,7 @@ def parse():
                     help="plain: one N=32 chain at maxstates 2^22; batched: 64 trajectories drawn from --seed; "
                          "learned: the learned proposal + complex64 against the plain complex128 run")
     ap.add_argument("--recall", type=float, default=0.999, help="learned: target recall of the keep threshold")
+    ap.add_argument("--judge-every", type=int, default=10, help="learned: a full-expansion judge step every n steps")
     ap.add_argument("--train-seeds", type=int, default=8, help="learned: plain training runs (shuffle seeds 0..n-1)")
     ap.add_argument("--learn-from", type=int, default=50, help="learned: plain steps before the proposal is used")
     ap.add_argument("--total-steps", type=int, default=200, help="learned: steps of the compared trajectories")
@@ -74,6 +75,8 @@ def parse():
     ap.add_argument("--weighting", default="none", choices=["none", "coherence", "norm"],
                     help="plain: rank the truncation by the look-ahead weights (TimeEvoParams.weighting_name)")
     ap.add_argument("--tau", type=float, default=0.2, help="plain: look-ahead time of --weighting")
+    ap.add_argument("--lanczos-order", type=int, default=0,
+                    help="plain: propagate by the Lanczos step of this order (ExpmParams.lanczos_order)")
     ap.add_argument("--no-graph", action="store_true", help="step without CUDA-graph replay")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--merge-stride", type=int, default=0, help="plain: this merge stride instead of tuning it")
@@ -168,14 +171,15 @@ def initial_rows(nchain, initpos=0):
     return layout.pack_rows(raw, layout.bitwidths_for([nchain] + [16] * nchain))
 
 
-def start_trajectory(eng, nchain, maxstates, es, initpos=0, graph=False, weighting="none", tau=0.0):
+def start_trajectory(eng, nchain, maxstates, es, initpos=0, graph=False, weighting="none", tau=0.0, lanczos_order=0):
     """grow_optimal_basis(fillfac=1) around the exciton on `initpos` in the phonon vacuum,
     amplitude 1 on that state, then the first (non-evolving) step."""
     import torch
     from paces_b200 import _native as nat
     from paces_b200.engine import Trajectory
     kind = {"none": nat.WEIGHT_NONE, "coherence": nat.WEIGHT_COHERENCE, "norm": nat.WEIGHT_NORM}[weighting]
-    tr = Trajectory(eng, maxstates, es, graph=graph, weighting=kind, tau=tau if kind else 0.0)
+    tr = Trajectory(eng, maxstates, es, graph=graph, weighting=kind, tau=tau if kind else 0.0,
+                    lanczos_order=lanczos_order)
     rows = initial_rows(nchain, initpos)
     b = eng.basis_from_ref(rows)
     while True:
@@ -196,7 +200,8 @@ def prepare(a, eng, maxstates):
     """Grow the basis (grow_optimal_basis, fillfac=1), first step, then propagate until the
     truncation keeps exactly maxstates states; returns the saturated trajectory."""
     tr = start_trajectory(eng, a.nchain, maxstates, a.enlarge_steps, graph=not a.no_graph,
-                          weighting=getattr(a, "weighting", "none"), tau=getattr(a, "tau", 0.0))
+                          weighting=getattr(a, "weighting", "none"), tau=getattr(a, "tau", 0.0),
+                          lanczos_order=getattr(a, "lanczos_order", 0))
     nprep = 1
     while True:
         rec = tr.step(evolve=True, dt=a.dt)
@@ -240,6 +245,15 @@ def taylor_bytes_per_term(rec, cs):
     """Algorithmic bytes of one Taylor term on S rows: neighbour table (16 B), row metadata
     (4 B), previous term read once, result read and written, new term written (4*cs)."""
     return rec.n_states * (16 + 4 + 4 * cs)
+
+
+def lanczos_bytes(rec, cs, order):
+    """Algorithmic bytes of one Lanczos propagation on S rows with order + 1 vectors: the norm
+    pass (S*cs); per vector sweep A (table 16 B, metadata 4 B, the gathered source, q_{i-1}
+    read, q_i and w written: 4*cs) and, but for the last vector, sweep B (w read and written,
+    q_i read: 3*cs); the final combination (order + 1 vectors read, the result written)."""
+    k = order + 1
+    return rec.n_states * (cs + k * (20 + 4 * cs) + (k - 1) * 3 * cs + (k + 1) * cs)
 
 
 def step_bytes(rec, cs, nw, es):
@@ -441,7 +455,7 @@ def run_ours(a):
         e2e = run_e2e(a, eng, tr, barrier, dist)
 
     compare = None
-    if a.precision == "c64" and not a.no_compare and a.weighting == "none":
+    if a.precision == "c64" and not a.no_compare and a.weighting == "none" and not a.lanczos_order:
         compare = compare_precisions(a, f"cuda:{local}", dist, learned=not a.no_learned)
 
     total_steps = a.steps * world
@@ -449,7 +463,10 @@ def run_ours(a):
     taylor_ms = stage_sum["taylor"] / n_prof
     terms = statistics.mean(r.final_m + 1 for r in recs)
     S_mean = statistics.mean(r.n_states for r in recs)
-    taylor_alg = statistics.mean(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in prof_recs)
+    if a.lanczos_order:
+        taylor_alg = statistics.mean(lanczos_bytes(r, cs, a.lanczos_order) for r in prof_recs)
+    else:
+        taylor_alg = statistics.mean(taylor_bytes_per_term(r, cs) * (r.final_m + 1) for r in prof_recs)
     achieved = taylor_alg / (taylor_ms / 1e3) / 1e9
     peak, peak_kind = read_peaks()
     per_row_term = read_profile_traffic(a.precision)
@@ -466,6 +483,7 @@ def run_ours(a):
                     "l2": "inputs larger than L2 (state and H table > 126 MB)", "parallelism": f"replicas x{world}",
                     "cuda_graph": not a.no_graph,
                     "weighting": None if a.weighting == "none" else {"name": a.weighting, "tau": a.tau},
+                    "propagator": f"lanczos order {a.lanczos_order}" if a.lanczos_order else "taylor",
                     "tuning": None if tuning is None else {k: tuning[k] for k in autotune_shapes()},
                     "form": ("plain method in complex64: amplitudes and SpMV in fp32, norms, stop test and sums in "
                              "fp64; the learned proposal is off in the timed steps (window.learned_c64 measures "
@@ -475,8 +493,10 @@ def run_ours(a):
             "value": value, "unit": "time-steps/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "kernel": "taylor_kernel", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "roofline": {"bound": "hbm", "kernel": "lanczos_kernel" if a.lanczos_order else "taylor_kernel",
+                         "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None if a.lanczos_order else traffic,
                          "algorithmic_bytes": taylor_alg, "launch_ms": taylor_ms},
             "step_roofline": {"achieved": step_alg / (ms / a.steps / 1e3) / 1e9, "unit": "GB/s",
                               "frac": step_alg / (ms / a.steps / 1e3) / 1e9 / peak},
@@ -550,7 +570,7 @@ def learned_run(a, dev, mlp, thr0, lf=WINDOW_FROM, total=WINDOW_TO):
     eng = Engine(model_params(a, "c64"), device=dev)
     tr = start_trajectory(eng, a.nchain, a.maxstates, a.enlarge_steps, graph=not a.no_graph)
     recs = [tr.last] + [tr.step(evolve=True, dt=a.dt) for _ in range(lf)]
-    lt = LearnedTrajectory(tr, mlp, thr0, judge_every=10, target_recall=a.recall)
+    lt = LearnedTrajectory(tr, mlp, thr0, judge_every=a.judge_every, target_recall=a.recall)
     window, ms = timed_steps(lambda: lt.step(a.dt), total - lf)
     return recs + window, ms, lt, eng
 

@@ -96,11 +96,15 @@ def _lookup(key, use_cache):
 
 def _search(apply, measure, strides, bpss, variants):
     """Coordinate search: the stride by its stages' time, then the Taylor schedule and grid
-    by the Taylor time."""
+    by the Taylor time.  The strides are timed in two passes, the second in reverse order,
+    and each keeps its faster pass: a basis that still grows during the search then favours
+    no end of the candidate list."""
     timings = {"merge_stride": {}, "taylor": {}}
-    for s in strides:
-        apply(s, 0, variants[0])
-        timings["merge_stride"][s] = measure()["merge"]
+    for order in (list(strides), list(reversed(strides))):
+        for s in order:
+            apply(s, 0, variants[0])
+            ms = measure()["merge"]
+            timings["merge_stride"][s] = min(ms, timings["merge_stride"].get(s, ms))
     best_s = min(timings["merge_stride"], key=timings["merge_stride"].get)
     for v in variants:
         for b in bpss:

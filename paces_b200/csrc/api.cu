@@ -732,7 +732,7 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
         return PACES_ERR_CUDA;
     }
     c->taylor_grid = taylor_max_grid(c->precision == PACES_C64, c->num_sms);
-    c->merge_stride = merge_stride(c->nw);
+    c->merge_stride = merge_default_stride(c->nw);
     c->taylor_bps = 0;
     c->taylor_variant = 1;
     c->test_wait_ns = 0;

@@ -75,50 +75,61 @@ __device__ __forceinline__ int cmp_kf(const Key<NW>& a, int fa, const Key<NW>& b
     return c != 0 ? c : (fa - fb);
 }
 
-// Tile keys in shared memory, word-major (w[q*stride + e]): a probe reads 8 bytes of word 0
-// and touches the next word only on a tie, which keeps bank conflicts low.
+// Tile keys in shared memory, element-major (w[e*NW + q]): a probe of an element reads its
+// whole key with 16-byte loads (NW even) instead of one load per word.
 template <int NW>
 struct SKeys {
     uint64_t* w;
-    int stride;
     __device__ __forceinline__ Key<NW> get(int e) const {
         Key<NW> k;
+        if constexpr (NW % 2 == 0) {
+            const ulonglong2* p = reinterpret_cast<const ulonglong2*>(w + size_t(e) * NW);
 #pragma unroll
-        for (int q = 0; q < NW; ++q) k.w[q] = w[q * stride + e];
+            for (int q = 0; q < NW / 2; ++q) {
+                const ulonglong2 v = p[q];
+                k.w[2 * q] = v.x;
+                k.w[2 * q + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < NW; ++q) k.w[q] = w[size_t(e) * NW + q];
+        }
         return k;
     }
     __device__ __forceinline__ void set(int e, const Key<NW>& k) const {
+        if constexpr (NW % 2 == 0) {
+            ulonglong2* p = reinterpret_cast<ulonglong2*>(w + size_t(e) * NW);
 #pragma unroll
-        for (int q = 0; q < NW; ++q) w[q * stride + e] = k.w[q];
-    }
-    __device__ __forceinline__ int cmp(int e, const Key<NW>& key) const {
+            for (int q = 0; q < NW / 2; ++q) p[q] = make_ulonglong2(k.w[2 * q], k.w[2 * q + 1]);
+        } else {
 #pragma unroll
-        for (int q = 0; q < NW; ++q) {
-            const uint64_t a = w[q * stride + e];
-            if (a != key.w[q]) return a < key.w[q] ? -1 : 1;
+            for (int q = 0; q < NW; ++q) w[size_t(e) * NW + q] = k.w[q];
         }
-        return 0;
-    }
-    __device__ __forceinline__ bool eq(int e1, int e2) const {
-#pragma unroll
-        for (int q = 0; q < NW; ++q)
-            if (w[q * stride + e1] != w[q * stride + e2]) return false;
-        return true;
     }
 };
 
-// (key, flag) of tile element x strictly below that of element y.  Branch-free: every word
-// is read and the comparison folds from the least significant end, so a warp's lanes never
-// diverge on where their keys first differ.
+// (key, flag) pairs held in registers: a strictly below b.  Branch-free fold from the least
+// significant word, so a warp's lanes never diverge on where their keys first differ.
+template <int NW>
+__device__ __forceinline__ bool reg_less(const Key<NW>& a, int fa, const Key<NW>& b, int fb) {
+    bool lt = fa < fb;
+#pragma unroll
+    for (int q = NW - 1; q >= 0; --q) lt = (a.w[q] < b.w[q]) | ((a.w[q] == b.w[q]) & lt);
+    return lt;
+}
+
+template <int NW>
+__device__ __forceinline__ bool reg_eq(const Key<NW>& a, const Key<NW>& b) {
+    bool eq = true;
+#pragma unroll
+    for (int q = 0; q < NW; ++q) eq &= a.w[q] == b.w[q];
+    return eq;
+}
+
+// (key, flag) of tile element x strictly below that of element y.
 template <int NW>
 __device__ __forceinline__ bool tile_less(const SKeys<NW>& keys, const uint8_t* flags, int x, int y) {
-    bool lt = flags[x] < flags[y];
-#pragma unroll
-    for (int q = NW - 1; q >= 0; --q) {
-        const uint64_t a = keys.w[q * keys.stride + x], b = keys.w[q * keys.stride + y];
-        lt = (a < b) | ((a == b) & lt);
-    }
-    return lt;
+    return reg_less<NW>(keys.get(x), flags[x], keys.get(y), flags[y]);
 }
 
 // A sorted sequence of tile elements: element k is ptr[k] (a merged level) or base + k
@@ -130,14 +141,32 @@ struct Seq {
     __device__ __forceinline__ int at(int k) const { return ptr ? int(ptr[k]) : base + k; }
 };
 
-// (key, flag) pairs held in registers: a strictly below b.  Branch-free fold from the least
-// significant word.
-template <int NW>
-__device__ __forceinline__ bool reg_less(const Key<NW>& a, int fa, const Key<NW>& b, int fb) {
-    bool lt = fa < fb;
-#pragma unroll
-    for (int q = NW - 1; q >= 0; --q) lt = (a.w[q] < b.w[q]) | ((a.w[q] == b.w[q]) & lt);
-    return lt;
+// Bounds [lo, hi] on the number of A elements before merged position d0 of a sub-merge of the
+// tile: A = the runs [ja, jb), B = the runs [jb, jc) (each already merged), An and Bn their
+// lengths.  The tile's splitter frontiers sc[k] (k = 0 .. nsp, the last the tile's end) are
+// points of every sub-merge's path, so the search is confined to the frontier interval that
+// holds d0.
+__device__ __forceinline__ void frontier_bounds(const uint16_t (*sc)[kRuns], int nsp, int ja, int jb, int jc, int d0,
+                                                int An, int Bn, int& lo, int& hi) {
+    lo = max(0, d0 - Bn);
+    hi = min(d0, An);
+    int a0 = 0, b0 = 0, a1 = An, b1 = Bn;
+    for (int k = 0; k <= nsp; ++k) {
+        int a = 0, b = 0;
+        for (int j = ja; j < jb; ++j) a += sc[k][j];
+        for (int j = jb; j < jc; ++j) b += sc[k][j];
+        if (a + b <= d0) {
+            a0 = a;
+            b0 = b;
+        } else {
+            a1 = a;
+            b1 = b;
+            break;
+        }
+    }
+    lo = max(lo, max(a0, d0 - b1));
+    hi = min(hi, min(a1, d0 - b0));
+    if (lo > hi) lo = hi;  // cannot happen for consistent frontiers
 }
 
 // Output positions [d0, d1) of the merge of two sorted sequences of tile elements, A and B;
@@ -146,8 +175,8 @@ __device__ __forceinline__ bool reg_less(const Key<NW>& a, int fa, const Key<NW>
 // per step reads only the next element of the side it took, without branches.
 template <int NW>
 __device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t* flags, Seq A, Seq B, int d0,
-                                            int d1, uint16_t* out) {
-    int lo = max(0, d0 - B.n), hi = min(d0, A.n);
+                                            int d1, uint16_t* out, int lo, int hi) {
+    // [lo, hi] brackets the number of A elements before d0 (see frontier_bounds)
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (!tile_less<NW>(keys, flags, B.at(d0 - 1 - mid), A.at(mid))) lo = mid + 1; else hi = mid;
@@ -183,6 +212,89 @@ __device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t
             fb = fn;
         }
     }
+}
+
+// The last merge level, fused with the dedup: output positions [d0, d1) of the merge of A and
+// B (as merge_range), and for each position whether it holds the first real element of its key
+// -- a real element whose predecessor in merged order (held in registers; at d0 the later of
+// the two heads' predecessors, at 0 the tile's merged predecessor) is not a real element with
+// the same key.  cnt[d] = running count of firsts in [d0, d] | first << 15; with SPLIT the same
+// for the firsts of the new part (element index >= o1: the group has no self-run element)
+// into cntn.  Returns the counts (firsts | new-part firsts << 16).
+template <int NW, bool SPLIT>
+__device__ __forceinline__ int merge_range_first(const SKeys<NW>& keys, const uint8_t* flags, Seq A, Seq B, int d0,
+                                                 int d1, uint16_t* out, uint16_t* cnt, uint16_t* cntn, int o1,
+                                                 bool tile_has_pred, const Key<NW>& tile_pred, int tile_pred_flag,
+                                                 int lo, int hi) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (!tile_less<NW>(keys, flags, B.at(d0 - 1 - mid), A.at(mid))) lo = mid + 1; else hi = mid;
+    }
+    int i = lo, j = d0 - lo;
+    // the predecessor of position d0
+    bool have = false;
+    Key<NW> pk = tile_pred;
+    int pf = tile_pred_flag;
+    if (d0 == 0) {
+        have = tile_has_pred;
+    } else {
+        int pe;
+        if (i == 0) {
+            pe = B.at(j - 1);
+        } else if (j == 0) {
+            pe = A.at(i - 1);
+        } else {
+            const int xa = A.at(i - 1), xb = B.at(j - 1);
+            pe = tile_less<NW>(keys, flags, xb, xa) ? xa : xb;  // equal keys: B's element comes later
+        }
+        pk = keys.get(pe);
+        pf = flags[pe];
+        have = true;
+    }
+    int ea = i < A.n ? A.at(i) : -1;
+    int eb = j < B.n ? B.at(j) : -1;
+    Key<NW> ka = keys.get(ea >= 0 ? ea : 0), kb = keys.get(eb >= 0 ? eb : 0);
+    int fa = flags[ea >= 0 ? ea : 0], fb = flags[eb >= 0 ? eb : 0];
+    int c = 0, cn = 0;
+    for (int d = d0; d < d1; ++d) {
+        const bool take_a = (ea >= 0) & ((eb < 0) | !reg_less<NW>(kb, fb, ka, fa));
+        const int e = take_a ? ea : eb;
+        const int f = take_a ? fa : fb;
+        Key<NW> k;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) k.w[q] = take_a ? ka.w[q] : kb.w[q];
+        out[d] = uint16_t(e);
+        const int first = (f == 1) & !(have & (pf == 1) & reg_eq<NW>(k, pk));
+        c += first;
+        cnt[d] = uint16_t(c | (first << 15));
+        if constexpr (SPLIT) {
+            const int fn = first & (e >= o1);
+            cn += fn;
+            cntn[d] = uint16_t(cn | (fn << 15));
+        }
+        pk = k;
+        pf = f;
+        have = true;
+        // the next head of the side taken
+        const int kk = take_a ? ++i : ++j;
+        const uint16_t* sp = take_a ? A.ptr : B.ptr;
+        const int sb = take_a ? A.base : B.base, sn = take_a ? A.n : B.n;
+        int en = -1;
+        if (kk < sn) en = sp ? int(sp[kk]) : sb + kk;
+        const int el = en >= 0 ? en : 0;
+        const Key<NW> kn = keys.get(el);
+        const int fnx = flags[el];
+        if (take_a) {
+            ea = en;
+            ka = kn;
+            fa = fnx;
+        } else {
+            eb = en;
+            kb = kn;
+            fb = fnx;
+        }
+    }
+    return c | (cn << 16);
 }
 
 // Splitters every `stride` elements of each run, with their co-ranks in the block's other
@@ -400,10 +512,14 @@ __device__ long long lookback_warp(unsigned long long* state, int t, long long c
 // once by merge_desc_kernel, read by the tile kernel with one coalesced load.
 template <int NW>
 struct TileDesc {
-    int p, tl, n, has_pred, pred_flag, pad;
+    int p, tl, n, has_pred, pred_flag, nsp;
     int start[kRuns], off[kRuns + 1], lo[kRuns];
     int pad2;
     uint64_t pred[NW];
+    // the merge frontier at the tile's splitters k = 0 .. nsp-1 and at its end (k = nsp): how
+    // many elements of each run's segment precede it (every sub-merge of the tile passes
+    // through these points)
+    uint16_t sc[kMergeGroup + 1][kRuns];
 };
 static_assert(sizeof(TileDesc<kMaxKeyWords>) <= merge_desc_bytes(), "tile descriptor size");
 
@@ -423,7 +539,9 @@ __global__ void __launch_bounds__(256) merge_desc_kernel(ModelDev m, const uint6
         const int bidx = tl * kMergeGroup + kMergeGroup;
         d.p = p;
         d.tl = tl;
-        d.pad = d.pad2 = 0;
+        d.pad2 = 0;
+        const int nsp = min(kMergeGroup, nsb - tl * kMergeGroup);
+        d.nsp = nsp;
         int n = 0, has = 0, pf = 0;
         Key<NW> pk;
 #pragma unroll
@@ -437,6 +555,11 @@ __global__ void __launch_bounds__(256) merge_desc_kernel(ModelDev m, const uint6
             d.lo[j] = lo;
             d.off[j] = n;
             n += en - st;
+            for (int k = 0; k <= kMergeGroup; ++k) {
+                int c = en - st;  // the end (and unused points)
+                if (k < nsp) c = __ldcg(ws.ord_co + int64_t(a + k) * kRuns + j) - st;
+                d.sc[k][j] = uint16_t(min(max(c, 0), en - st));
+            }
             if (st > 0) {
                 Key<NW> k;
                 int f;
@@ -508,17 +631,17 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     constexpr bool SPLIT = MODE == MERGE_EXPAND_SPLIT;
     constexpr bool MAPS = ASM || SPLIT;
     extern __shared__ __align__(16) unsigned char smem[];
-    const SKeys<NW> s_key{reinterpret_cast<uint64_t*>(smem), tmax};
+    const SKeys<NW> s_key{reinterpret_cast<uint64_t*>(smem)};
     uint8_t* s_flag = smem + size_t(tmax) * NW * 8;
     uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_flag + ((tmax + 15) & ~15));  // merged pos -> element
-    uint16_t* s_lv1 = s_perm + tmax;  // first merge level; then (split) s_cntn
-    uint16_t* s_cnt = s_lv1 + tmax;   // second merge level; then the inclusive count of first
-                                      // occurrences per merged pos
-    uint16_t* s_cntn = s_lv1;         // split: the same for first occurrences of the new part
+    uint16_t* s_lv1 = s_perm + tmax;   // first merge level; then the per-thread counts of firsts
+    uint16_t* s_lv2 = s_lv1 + tmax;    // second merge level
+    uint16_t* s_cnt = s_lv1;           // after level 2: running count of firsts | first << 15
+    uint16_t* s_cntn = s_lv2 + tmax;   // split only: the same for the new part
     __shared__ int s_t;
-    __shared__ long long s_base, s_total;
-    __shared__ int s_warpn[kTileThreads / 32];
-    __shared__ int s_warp[kTileThreads / 32];
+    __shared__ long long s_base;
+    __shared__ int s_thr[kTileThreads], s_thrn[kTileThreads];  // exclusive count before each thread
+    __shared__ int s_warp[kTileThreads / 32], s_warpn[kTileThreads / 32];
     __shared__ int s_ceil;
     __shared__ __align__(16) TileDesc<NW> s_d;
     const int* s_start = s_d.start;
@@ -526,25 +649,28 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     const int* s_lo = s_d.lo;
 
     const int tid = threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
     const int ntiles = ws.counters[1];
     constexpr int kDescWords = int(sizeof(TileDesc<NW>) / 4);
 
+    // tiles are taken by ticket when a block starts them (the order the decoupled look-back
+    // waits in): the next ticket is drawn at the end of each tile, before its last barrier
+    if (tid == 0) {
+        s_t = atomicAdd(&ws.counters[2], 1);
+        s_ceil = 0;
+    }
+    __syncthreads();
     for (;;) {
-        if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
-        __syncthreads();
         const int t = s_t;
         if (t >= ntiles) break;
         // tile set-up: the precomputed descriptor
         if (tid < kDescWords)
             reinterpret_cast<int*>(&s_d)[tid] =
                 __ldcg(reinterpret_cast<const int*>(ws.tile_desc + size_t(t) * merge_desc_bytes()) + tid);
-        if (tid == 0) s_ceil = 0;
         __syncthreads();
         const int n = min(s_d.n, tmax);
         const int p = s_d.p;
         const int s_tl = s_d.tl;
-        const int s_has_pred = s_d.has_pred;
-        const int s_pred_flag = s_d.pred_flag;
         Key<NW> s_pred;
 #pragma unroll
         for (int q = 0; q < NW; ++q) s_pred.w[q] = s_d.pred[q];
@@ -559,70 +685,52 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
             run_elem<NW>(m, X, Y, ws, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
             s_key.set(e, k);
             s_flag[e] = uint8_t(f);
-            s_perm[e] = 0xffff;  // every rank must be claimed below
         }
         __syncthreads();
 
         // 2. merged order: pairwise merge tree (runs 0+1, 2+3) -> (0123) -> (01234) in shared
-        //    memory; every thread merges a contiguous output range after a merge-path split.
-        //    The level buffers alias s_cntn / s_cnt, which are filled only afterwards.
+        //    memory; every thread merges a contiguous output range after a merge-path split.  The
+        //    last level also flags and counts the first occurrences (the dedup).
+        const int o1 = s_off[1], o2 = s_off[2], o3 = s_off[3], o4 = s_off[4];
+        const int per = max((n + kTileThreads - 1) / kTileThreads, 1);
+        int cnt = 0, cntn = 0;
         {
-            uint16_t* lv1 = s_lv1;
-            uint16_t* lv2 = s_cnt;
-            const int o1 = s_off[1], o2 = s_off[2], o3 = s_off[3], o4 = s_off[4];
             const int n01 = o2, n0123 = o4;
-            auto ident = [](int base, int n) { return Seq{nullptr, base, n}; };
-            auto arr = [](const uint16_t* a, int n) { return Seq{a, 0, n}; };
-            int per = (n0123 + kTileThreads - 1) / kTileThreads;
-            int d0 = min(tid * per, n0123), d1 = min(d0 + per, n0123);
-            if (d0 < n01)
-                merge_range<NW>(s_key, s_flag, ident(0, o1), ident(o1, o2 - o1), d0, min(d1, n01), lv1);
-            if (d1 > n01)
-                merge_range<NW>(s_key, s_flag, ident(o2, o3 - o2), ident(o3, o4 - o3), max(d0, n01) - n01,
-                                d1 - n01, lv1 + n01);
+            auto ident = [](int base, int len) { return Seq{nullptr, base, len}; };
+            auto arr = [](const uint16_t* x, int len) { return Seq{x, 0, len}; };
+            const int per4 = (n0123 + kTileThreads - 1) / kTileThreads;
+            const int nsp = s_d.nsp;
+            int lo, hi;
+            int d0 = min(tid * per4, n0123), d1 = min(d0 + per4, n0123);
+            if (d0 < n01) {
+                frontier_bounds(s_d.sc, nsp, 0, 1, 2, d0, o1, o2 - o1, lo, hi);
+                merge_range<NW>(s_key, s_flag, ident(0, o1), ident(o1, o2 - o1), d0, min(d1, n01), s_lv1, lo, hi);
+            }
+            if (d1 > n01) {
+                const int e0 = max(d0, n01) - n01;
+                frontier_bounds(s_d.sc, nsp, 2, 3, 4, e0, o3 - o2, o4 - o3, lo, hi);
+                merge_range<NW>(s_key, s_flag, ident(o2, o3 - o2), ident(o3, o4 - o3), e0, d1 - n01, s_lv1 + n01, lo,
+                                hi);
+            }
             __syncthreads();
-            d0 = min(tid * per, n0123);
-            d1 = min(d0 + per, n0123);
-            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv1, n01), arr(lv1 + n01, n0123 - n01), d0, d1, lv2);
+            if (d0 < d1) {
+                frontier_bounds(s_d.sc, nsp, 0, 2, 4, d0, n01, n0123 - n01, lo, hi);
+                merge_range<NW>(s_key, s_flag, arr(s_lv1, n01), arr(s_lv1 + n01, n0123 - n01), d0, d1, s_lv2, lo, hi);
+            }
             __syncthreads();
-            per = (n + kTileThreads - 1) / kTileThreads;
             d0 = min(tid * per, n);
             d1 = min(d0 + per, n);
-            if (d0 < d1) merge_range<NW>(s_key, s_flag, arr(lv2, n0123), ident(o4, n - o4), d0, d1, s_perm);
+            if (d0 < d1) {
+                frontier_bounds(s_d.sc, nsp, 0, 4, 5, d0, n0123, n - o4, lo, hi);
+                const int c = merge_range_first<NW, SPLIT>(s_key, s_flag, arr(s_lv2, n0123), ident(o4, n - o4), d0,
+                                                           d1, s_perm, s_cnt, s_cntn, o1, s_d.has_pred != 0, s_pred,
+                                                           s_d.pred_flag, lo, hi);
+                cnt = c & 0xffff;
+                cntn = c >> 16;
+            }
         }
-        __syncthreads();
 
-        // 3. first-occurrence flags over a contiguous chunk per thread, then a block scan (split:
-        //    also of the first occurrences that start a group without a self-run element --
-        //    the self run sorts first among equal keys, so that is a group's first element)
-        const int per = (n + kTileThreads - 1) / kTileThreads;
-        const int q0 = min(tid * per, n);
-        const int q1 = min(q0 + per, n);
-        const int o1 = s_off[1];
-        int cnt = 0, cntn = 0;
-        for (int q = q0; q < q1; ++q) {
-            const int e = s_perm[q];
-            int first = 0;
-            if (e >= n) {
-                raise_status(status, PACES_ERR_BADARG);
-            } else if (s_flag[e] == 1) {
-                if (q == 0) {
-                    first = !s_has_pred || s_pred_flag != 1 || s_key.cmp(e, s_pred) != 0;
-                } else {
-                    const int pe = s_perm[q - 1];
-                    first = pe >= n || s_flag[pe] != 1 || !s_key.eq(pe, e);
-                }
-            }
-            s_cnt[q] = uint16_t(first);  // turned into an inclusive count below
-            cnt += first;
-            if constexpr (SPLIT) {
-                const int fn = first && e >= o1;
-                s_cntn[q] = uint16_t(fn);
-                cntn += fn;
-            }
-        }
-        // block exclusive scan of cnt (and cntn)
-        const int lane = tid & 31, wid = tid >> 5;
+        // 3. block exclusive scan of the per-thread counts (and of the new part's)
         int incl = cnt, incln = cntn;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -637,21 +745,30 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
             s_warp[wid] = incl;
             s_warpn[wid] = incln;
         }
-        __syncthreads();
-        if (tid == 0) {
-            int acc = 0, accn = 0;
-            for (int w = 0; w < kTileThreads / 32; ++w) {
-                const int v = s_warp[w], vn = s_warpn[w];
-                s_warp[w] = acc;
-                s_warpn[w] = accn;
-                acc += v;
-                accn += vn;
-            }
-            s_total = (long long)acc | ((long long)accn << kPackShift);
-        }
+        s_thr[tid] = incl - cnt;  // exclusive inside the warp; the warp's offset is added below
+        s_thrn[tid] = incln - cntn;
         __syncthreads();
         if (wid == 0) {
-            const long long b = lookback_warp(ws.tile_state, t, s_total, status);
+            int v = lane < kTileThreads / 32 ? s_warp[lane] : 0;
+            int vn = lane < kTileThreads / 32 ? s_warpn[lane] : 0;
+            int tot = v, totn = vn;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int a = __shfl_up_sync(0xffffffffu, tot, o);
+                const int an = __shfl_up_sync(0xffffffffu, totn, o);
+                if (lane >= o) {
+                    tot += a;
+                    totn += an;
+                }
+            }
+            if (lane < kTileThreads / 32) {
+                s_warp[lane] = tot - v;    // exclusive over warps
+                s_warpn[lane] = totn - vn;
+            }
+            const int all = __shfl_sync(0xffffffffu, tot, 31);
+            const int alln = __shfl_sync(0xffffffffu, totn, 31);
+            const long long b = lookback_warp(ws.tile_state, t, (long long)all | ((long long)alln << kPackShift),
+                                              status);
             if (lane == 0) {
                 s_base = b;
                 if (s_tl == 0) {
@@ -663,78 +780,75 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
         __syncthreads();
         const int base = int(s_base & kPackLow);
         const int basen = int(s_base >> kPackShift);
-        {
-            // inclusive count of firsts at every merged position (for strided writes)
-            int run = s_warp[wid] + incl - cnt;
-            int runn = s_warpn[wid] + incln - cntn;
-            for (int q = q0; q < q1; ++q) {
-                run += s_cnt[q];
-                s_cnt[q] = uint16_t(run);
-                if constexpr (SPLIT) {
-                    runn += s_cntn[q];
-                    s_cntn[q] = uint16_t(runn);
-                }
-            }
-        }
-        __syncthreads();
 
-        // 4a. new keys (and H rows, or the new part), consecutive threads -> consecutive outputs
+        // 4. one pass over the merged positions, consecutive threads -> consecutive outputs: the
+        //    new keys (and H rows, or the new part) at first occurrences, and every element's
+        //    index map (its group's output: the running count at its merged position)
+        int ceil_local = 0;
         for (int q = tid; q < n; q += kTileThreads) {
-            if (s_cnt[q] == (q > 0 ? s_cnt[q - 1] : 0)) continue;  // not a first occurrence
+            const int owner = q / per;
+            const unsigned raw = s_cnt[q];
+            const int c = int(raw & 0x7fffu) + s_thr[owner] + s_warp[owner >> 5];  // firsts in the tile up to q
             const int e = s_perm[q];
-            const int64_t u = int64_t(base) + s_cnt[q] - 1;
-            if (u < out.cap) {
-                const Key<NW> k = s_key.get(e);
-                store_key<NW>(out.keys, u, k);
-                if constexpr (ASM) {
-                    const uint32_t nex = get_field(m, k, p);
-                    const uint32_t ntot = total_phonons(m, k);
-                    if (u < out.nbr_cap) {
-                        out.meta[u] = uint32_t(p) | (nex << 8) | (ntot << 16);
-                        // a group's first element is its self-run element when it has one
-                        if (!out.self_rows_filled || e >= s_off[1])
-                            reinterpret_cast<int4*>(out.nbr)[u] = make_int4(-1, -1, -1, -1);
-                        if (out.self_flag) out.self_flag[u] = uint8_t(e < s_off[1]);
-                    }
-                }
-                if constexpr (SPLIT) {
-                    if (s_cntn[q] != (q > 0 ? s_cntn[q - 1] : 0)) {
-                        const int64_t v = int64_t(basen) + s_cntn[q] - 1;
-                        if (v < out.new_cap) {
-                            store_key<NW>(out.new_keys, v, k);
-                            out.new_to_out[v] = int(u);
-                        } else {
-                            raise_status(status, PACES_ERR_CAPACITY);
+            if (e >= n) {  // every position is written by level 3: cannot happen
+                raise_status(status, PACES_ERR_BADARG);
+                continue;
+            }
+            const int64_t u = int64_t(base) + c - 1;
+            if (raw >> 15) {
+                if (u < out.cap) {
+                    const Key<NW> k = s_key.get(e);
+                    store_key<NW>(out.keys, u, k);
+                    if constexpr (ASM) {
+                        const uint32_t nex = get_field(m, k, p);
+                        const uint32_t ntot = total_phonons(m, k);
+                        if (u < out.nbr_cap) {
+                            out.meta[u] = uint32_t(p) | (nex << 8) | (ntot << 16);
+                            // a group's first element is its self-run element when it has one
+                            if (!out.self_rows_filled || e >= o1)
+                                reinterpret_cast<int4*>(out.nbr)[u] = make_int4(-1, -1, -1, -1);
+                            if (out.self_flag) out.self_flag[u] = uint8_t(e < o1);
                         }
                     }
+                    if constexpr (SPLIT) {
+                        const unsigned rawn = s_cntn[q];
+                        if (rawn >> 15) {
+                            const int64_t v =
+                                int64_t(basen) + int(rawn & 0x7fffu) + s_thrn[owner] + s_warpn[owner >> 5] - 1;
+                            if (v < out.new_cap) {
+                                store_key<NW>(out.new_keys, v, k);
+                                out.new_to_out[v] = int(u);
+                            } else {
+                                raise_status(status, PACES_ERR_CAPACITY);
+                            }
+                        }
+                    }
+                } else {
+                    raise_status(status, PACES_ERR_CAPACITY);
                 }
-            } else {
-                raise_status(status, PACES_ERR_CAPACITY);
             }
-        }
-        // 4b. index maps in merged order: an element's output is its group's, the running
-        //    count at its merged position (five interleaved streams of ascending sources)
-        int ceil_local = 0;
-        if constexpr (MAPS) {
-            for (int q = tid; q < n; q += kTileThreads) {
-                const int e = s_perm[q];
-                if (e >= n) continue;  // flagged in 3
+            if constexpr (MAPS) {
                 int j = 0;
 #pragma unroll
                 for (int qq = 1; qq < kRuns; ++qq) j += (e >= s_off[qq]);
                 const int64_t src = int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]);
                 const int f = s_flag[e];
-                int u = -1;
-                if (f == 1) u = base + s_cnt[q] - 1;
                 ceil_local += (f == 2);
-                if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = u;
+                if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = f == 1 ? int(u) : -1;
             }
+        }
+        if constexpr (MAPS) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) ceil_local += __shfl_xor_sync(0xffffffffu, ceil_local, o);
             if (lane == 0 && ceil_local) atomicAdd(&s_ceil, ceil_local);
             __syncthreads();
-            if (tid == 0 && s_ceil) atomicAdd(&ws.counters[3], s_ceil);
+            if (tid == 0) {
+                if (s_ceil) atomicAdd(&ws.counters[3], s_ceil);
+                s_ceil = 0;
+            }
         }
+        // every thread has read this tile's ticket and descriptor: draw the next one
+        if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
         __syncthreads();
     }
     // the block that finishes last writes the block offsets and the totals: every block makes
@@ -794,10 +908,10 @@ __global__ void __launch_bounds__(256) nbr_fill_kernel(ModelDev m, const int* __
 
 template <int NW>
 size_t tile_smem_bytes(int tmax, int mode) {
-    // keys, order flags, then three uint16 arrays (merged order and two merge levels, which
-    // become the running counts)
-    (void)mode;
-    return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) + size_t(tmax) * 6;
+    // keys, order flags, then uint16 arrays: merged order, two merge levels (the first becomes
+    // the running counts) and, for the split expansion, the new part's running counts
+    return size_t(tmax) * sizeof(Key<NW>) + size_t((tmax + 15) & ~15) +
+           size_t(tmax) * (mode == MERGE_EXPAND_SPLIT ? 8 : 6);
 }
 
 template <int NW, int MODE>

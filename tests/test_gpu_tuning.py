@@ -39,7 +39,7 @@ def test_out_of_range_shapes_are_rejected():
     from paces_b200 import autotune
     eng = gpu_helpers.engine_for(8, 16, 1.0, cap=1 << 10)
     t = autotune.get_tuning(eng)
-    assert t.merge_stride == t.merge_stride_max == 240 and t.merge_stride_min == 64
+    assert t.merge_stride == 160 and t.merge_stride_max == 240 and t.merge_stride_min == 64
     for bad in (48, 250, 72):
         with pytest.raises(nat.PacesError):
             autotune.set_tuning(eng, merge_stride=bad)
