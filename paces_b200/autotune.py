@@ -94,11 +94,12 @@ def _lookup(key, use_cache):
     return _load_file().get(key)
 
 
-def _search(apply, measure, strides, bpss, variants):
+def _search(apply, measure, strides, bpss, variants, measure_taylor=None):
     """Coordinate search: the stride by its stages' time, then the Taylor schedule and grid
     by the Taylor time.  The strides are timed in two passes, the second in reverse order,
     and each keeps its faster pass: a basis that still grows during the search then favours
-    no end of the candidate list."""
+    no end of the candidate list.  measure_taylor (when given) times the Taylor candidates
+    on one fixed input, so that no candidate is judged on a step with fewer terms."""
     timings = {"merge_stride": {}, "taylor": {}}
     for order in (list(strides), list(reversed(strides))):
         for s in order:
@@ -109,7 +110,7 @@ def _search(apply, measure, strides, bpss, variants):
     for v in variants:
         for b in bpss:
             apply(best_s, b, v)
-            timings["taylor"][(v, b)] = measure()["taylor"]
+            timings["taylor"][(v, b)] = measure_taylor() if measure_taylor else measure()["taylor"]
     best_v, best_b = min(timings["taylor"], key=timings["taylor"].get)
     apply(best_s, best_b, best_v)
     timings["taylor"] = {f"variant{v}_bps{b}": ms for (v, b), ms in timings["taylor"].items()}
@@ -140,9 +141,25 @@ def tune(tr, dt, steps=2, use_cache=True):
             acc["taylor"] += st["taylor"]
         return {k: v / steps for k, v in acc.items()}
 
+    def measure_taylor(reps=3):
+        # the whole series on the trajectory's current state, the same input for every candidate
+        b, h, psi = tr.basis, tr.h, tr.psis[tr.cur]
+        out = torch.empty_like(psi)
+        stream = torch.cuda.current_stream(eng.device)
+        best = None
+        for _ in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.taylor(b, h, psi, dt, psi_out=out)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        return best
+
     try:
         choice = _search(lambda s, b, v: set_tuning(eng, s, b, v), measure, stride_candidates(t0), bps_candidates(t0),
-                         VARIANTS)
+                         VARIANTS, measure_taylor=measure_taylor)
     finally:
         eng.set_profiling(False)
         tr.use_graph = use_graph

@@ -200,11 +200,11 @@ lanczos_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ 
         const C* qp = i > 0 ? U + int64_t(i - 1) * cap : nullptr;
         const double bi = i > 0 ? s_beta[i] : 0.0;
         double pa[2] = {0.0, 0.0};
-        for (int64_t r = r0; r < S; r += stride) {
+        // (H s)_r and s_r of one row (all its loads issued here)
+        auto load_row = [&](int64_t r, C& y, C& xr) {
             const uint32_t mm = __ldg(meta + r);
             const int4 nb = load_nbr(nbr, r);
-            const C xr = __ldcg(src + r);
-            C y;
+            xr = __ldcg(src + r);
             if constexpr (XHOP) {
                 if constexpr (C64) y = h_row_c64_x(m, s_sq, r, nb, mm, xr, src);
                 else y = h_row_c128_x(m, s_sq, r, nb, mm, xr, src);
@@ -212,29 +212,47 @@ lanczos_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ 
                 if constexpr (C64) y = h_row_c64_nb(m, s_sq, J, r, nb, mm, xr, src);
                 else y = h_row_c128_nb(m, s_sq, r, nb, mm, xr, src);
             }
+        };
+        // q_r = s_r / beta, w_r = (H s)_r / beta - beta_i q_{i-1,r}; the vdot partial
+        const double rb = 1.0 / beta;
+        auto finish_row = [&](int64_t r, const C& y, const C& xr, const C& p) {
             C q, wr;
             if constexpr (C64) {
-                const float b = float(beta), bp = float(bi);
-                q = make_float2(xr.x / b, xr.y / b);
-                wr = make_float2(y.x / b, y.y / b);
-                if (i > 0) {
-                    const C p = qp[r];
-                    wr.x = fmaf(-bp, p.x, wr.x);
-                    wr.y = fmaf(-bp, p.y, wr.y);
-                }
+                const float b = float(rb), bp = float(bi);
+                q = make_float2(xr.x * b, xr.y * b);
+                wr = make_float2(y.x * b, y.y * b);
+                wr.x = fmaf(-bp, p.x, wr.x);
+                wr.y = fmaf(-bp, p.y, wr.y);
             } else {
-                q = make_double2(__ddiv_rn(xr.x, beta), __ddiv_rn(xr.y, beta));
-                wr = make_double2(__ddiv_rn(y.x, beta), __ddiv_rn(y.y, beta));
-                if (i > 0) {
-                    const C p = qp[r];
-                    wr = make_double2(__dsub_rn(wr.x, __dmul_rn(bi, p.x)), __dsub_rn(wr.y, __dmul_rn(bi, p.y)));
-                }
+                q = make_double2(__dmul_rn(xr.x, rb), __dmul_rn(xr.y, rb));
+                wr = make_double2(__dmul_rn(y.x, rb), __dmul_rn(y.y, rb));
+                wr = make_double2(__dsub_rn(wr.x, __dmul_rn(bi, p.x)), __dsub_rn(wr.y, __dmul_rn(bi, p.y)));
             }
             qi[r] = q;
             w[r] = wr;
             // vdot(w, q) = sum conj(w) q
             pa[0] += double(wr.x) * double(q.x) + double(wr.y) * double(q.y);
             pa[1] += double(wr.x) * double(q.y) - double(wr.y) * double(q.x);
+        };
+        C zero;
+        zero.x = 0;
+        zero.y = 0;
+        {
+            // two rows a grid stride apart per iteration: their loads are in flight together
+            int64_t r = r0;
+            for (; r + stride < S; r += 2 * stride) {
+                C y0, x0, y1, x1;
+                load_row(r, y0, x0);
+                load_row(r + stride, y1, x1);
+                const C p0 = qp ? qp[r] : zero, p1 = qp ? qp[r + stride] : zero;
+                finish_row(r, y0, x0, p0);
+                finish_row(r + stride, y1, x1, p1);
+            }
+            if (r < S) {
+                C y0, x0;
+                load_row(r, y0, x0);
+                finish_row(r, y0, x0, qp ? qp[r] : zero);
+            }
         }
         if (!grid_sum<2>(pa, ws, parity, gen, status, s_red, s_fin)) {
             ok = false;
@@ -255,9 +273,7 @@ lanczos_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ 
         if (i == order) break;
         // B_i
         double pb[1] = {0.0};
-        for (int64_t r = r0; r < S; r += stride) {
-            const C q = qi[r];
-            C wr = w[r];
+        auto axpy_row = [&](int64_t r, const C& q, C wr) {
             if constexpr (C64) {
                 const float ar = float(are), ai = float(aim);
                 wr.x -= ar * q.x - ai * q.y;
@@ -269,6 +285,15 @@ lanczos_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ 
             }
             w[r] = wr;
             pb[0] += double(wr.x) * double(wr.x) + double(wr.y) * double(wr.y);
+        };
+        {
+            int64_t r = r0;
+            for (; r + stride < S; r += 2 * stride) {
+                const C q0 = qi[r], w0 = w[r], q1 = qi[r + stride], w1 = w[r + stride];
+                axpy_row(r, q0, w0);
+                axpy_row(r + stride, q1, w1);
+            }
+            if (r < S) axpy_row(r, qi[r], w[r]);
         }
         if (!grid_sum<1>(pb, ws, parity, gen, status, s_red, s_fin)) {
             ok = false;

@@ -7,7 +7,12 @@ tolerance is 2^-24 instead of 2^-53.  The bounds asserted here are the measured 
 absolute differences over 200 steps of dt = 0.05 with about a 3x margin (measured:
 N=32, maxstates 2^18: n_exc 7.2e-7, n_pho 2.3e-6, energy 3.3e-6, norm 8.7e-7;
 N=32, maxstates 2^22: 1.7e-7, 5.6e-7, 1.3e-6, 5.6e-7; N=16, g=1, maxstates 2^16:
-4.0e-6, 7.0e-6, 1.4e-5, 2.3e-6)."""
+4.0e-6, 7.0e-6, 1.4e-5, 2.3e-6).
+
+The 1e-5 bound holds at the metric's size (N=32, 2^22) and at 2^18; it does NOT hold for
+small bases: at N=16, 2^16 the energy moves by 1.4e-5, because rounding moves states across
+the truncation threshold and a different kept set dominates the difference, so that case
+is asserted at 5e-5."""
 
 import numpy as np
 import pytest
