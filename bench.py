@@ -357,7 +357,7 @@ def run_reference(a):
 
 
 def metric_name(a):
-    """The line's metric: BASELINE's time-steps/s at 4M states, with the form the value measures."""
+    """The line's metric: time-steps/s at 4M states, named with the form the value measures."""
     if a.precision == "c64":
         return ("time-steps/s at 4M states: FP32 (complex64, fp64 scalars) vs plain FP64, observable err <=1e-5; "
                 "the learned+FP32 form is reported beside it (window.learned_c64)")
