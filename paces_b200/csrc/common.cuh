@@ -125,10 +125,12 @@ __device__ __forceinline__ bool key_eq(const Key<NW>& a, const Key<NW>& b) {
 template <int NW>
 __device__ __forceinline__ uint32_t get_field(const ModelDev& m, const Key<NW>& k, int s) {
     const uint64_t mask = (uint64_t(1) << m.bits[s]) - 1;
+    // a mask per word instead of a select: the compiler would turn a select on the word index
+    // into an indexed access of a local copy of the key
+    const int ws = m.word[s];
     uint64_t word = 0;
 #pragma unroll
-    for (int w = 0; w < NW; ++w)
-        if (w == m.word[s]) word = k.w[w];
+    for (int w = 0; w < NW; ++w) word |= k.w[w] & (uint64_t(0) - uint64_t(w == ws));
     return uint32_t((word >> m.shift[s]) & mask);
 }
 
@@ -136,9 +138,10 @@ __device__ __forceinline__ uint32_t get_field(const ModelDev& m, const Key<NW>& 
 template <int NW>
 __device__ __forceinline__ void add_field(const ModelDev& m, Key<NW>& k, int s, int delta) {
     const uint64_t one = uint64_t(1) << m.shift[s];
+    const uint64_t d = delta > 0 ? one : (uint64_t(0) - one);
+    const int ws = m.word[s];
 #pragma unroll
-    for (int w = 0; w < NW; ++w)
-        if (w == m.word[s]) k.w[w] = delta > 0 ? k.w[w] + one : k.w[w] - one;
+    for (int w = 0; w < NW; ++w) k.w[w] += d & (uint64_t(0) - uint64_t(w == ws));
 }
 
 // Sum of all occupation fields: one popcount per word and bit plane.

@@ -47,10 +47,8 @@ __device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __re
             if (n + 1 >= m.maxd[p]) {
                 flag = 2;
 #pragma unroll
-                for (int q = 0; q < NW; ++q) {
-                    if (q == w) k.w[q] |= low;
-                    else if (q > w) k.w[q] = ~0ull;
-                }
+                for (int q = 0; q < NW; ++q)
+                    k.w[q] = (k.w[q] | (low & (0ull - uint64_t(q == w)))) | (0ull - uint64_t(q > w));
             } else {
                 add_field(m, k, p, +1);
             }
@@ -58,10 +56,8 @@ __device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __re
             if (n == 0) {
                 flag = 0;
 #pragma unroll
-                for (int q = 0; q < NW; ++q) {
-                    if (q == w) k.w[q] &= ~low;
-                    else if (q > w) k.w[q] = 0ull;
-                }
+                for (int q = 0; q < NW; ++q)
+                    k.w[q] = (k.w[q] & ~(low & (0ull - uint64_t(q == w)))) & ~(0ull - uint64_t(q > w));
             } else {
                 add_field(m, k, p, -1);
             }
@@ -126,109 +122,156 @@ __device__ __forceinline__ bool reg_eq(const Key<NW>& a, const Key<NW>& b) {
     return eq;
 }
 
-// (key, flag) of tile element x strictly below that of element y.
-template <int NW>
-__device__ __forceinline__ bool tile_less(const SKeys<NW>& keys, const uint8_t* flags, int x, int y) {
-    return reg_less<NW>(keys.get(x), flags[x], keys.get(y), flags[y]);
-}
+// Entries of a merged level (and of the tile's merged order): the element's index in the tile
+// in the low kEntBits bits, its order flag above them, so that reading an entry gives both.
+constexpr int kEntBits = 12;
+constexpr int kEntMask = (1 << kEntBits) - 1;
+static_assert(merge_tmax(merge_stride(1)) <= (1 << kEntBits), "tile element index must fit an entry");
 
-// A sorted sequence of tile elements: element k is ptr[k] (a merged level) or base + k
-// (a run segment, ptr == nullptr).
+__device__ __forceinline__ uint16_t make_ent(int e, int f) { return uint16_t(e | (f << kEntBits)); }
+
+// A sorted sequence of tile elements: a run segment (element k is base + k, its flag in the
+// tile's flag array) or a merged level (entry k of ptr).  Which of the two a sequence is, is a
+// template argument of every function that reads one (ARR: a merged level).
 struct Seq {
     const uint16_t* ptr;
     int base;
     int n;
-    __device__ __forceinline__ int at(int k) const { return ptr ? int(ptr[k]) : base + k; }
 };
 
-// Bounds [lo, hi] on the number of A elements before merged position d0 of a sub-merge of the
-// tile: A = the runs [ja, jb), B = the runs [jb, jc) (each already merged), An and Bn their
-// lengths.  The tile's splitter frontiers sc[k] (k = 0 .. nsp, the last the tile's end) are
-// points of every sub-merge's path, so the search is confined to the frontier interval that
-// holds d0.
-__device__ __forceinline__ void frontier_bounds(const uint16_t (*sc)[kRuns], int nsp, int ja, int jb, int jc, int d0,
-                                                int An, int Bn, int& lo, int& hi) {
-    lo = max(0, d0 - Bn);
-    hi = min(d0, An);
-    int a0 = 0, b0 = 0, a1 = An, b1 = Bn;
-    for (int k = 0; k <= nsp; ++k) {
-        int a = 0, b = 0;
-        for (int j = ja; j < jb; ++j) a += sc[k][j];
-        for (int j = jb; j < jc; ++j) b += sc[k][j];
-        if (a + b <= d0) {
-            a0 = a;
-            b0 = b;
-        } else {
-            a1 = a;
-            b1 = b;
-            break;
-        }
+template <bool ARR>
+__device__ __forceinline__ void seq_at(const Seq& s, const uint8_t* flags, int k, int& e, int& f) {
+    if constexpr (ARR) {
+        const int v = s.ptr[k];
+        e = v & kEntMask;
+        f = v >> kEntBits;
+    } else {
+        e = s.base + k;
+        f = flags[e];
     }
-    lo = max(lo, max(a0, d0 - b1));
-    hi = min(hi, min(a1, d0 - b0));
+}
+
+// Merge-path frontier tables of a tile: for each sub-merge of the tree (A = runs [ja, jb),
+// B = runs [jb, jc)) and each splitter frontier k = 0 .. nsp (the last the tile's end), the
+// number of A elements | B elements << 16 before the frontier.  Every sub-merge's path passes
+// through these points.
+enum SubMerge : int { SM_01 = 0, SM_23 = 1, SM_0123 = 2, SM_ALL = 3, kSubMerges = 4 };
+constexpr int kFrontiers = kMergeGroup + 1;
+
+__device__ __forceinline__ void frontier_table(const uint16_t (*sc)[kRuns], int nsp, uint32_t (*ft)[kFrontiers],
+                                               int idx) {
+    if (idx >= kSubMerges * kFrontiers) return;
+    const int c = idx / kFrontiers, k = idx % kFrontiers;
+    const int ja = c == SM_23 ? 2 : 0;
+    const int jb = c == SM_01 ? 1 : (c == SM_23 ? 3 : (c == SM_0123 ? 2 : 4));
+    const int jc = c == SM_01 ? 2 : (c == SM_ALL ? 5 : 4);
+    const int kk = k <= nsp ? k : nsp;  // unused points repeat the end
+    int a = 0, b = 0;
+    for (int j = ja; j < jb; ++j) a += sc[kk][j];
+    for (int j = jb; j < jc; ++j) b += sc[kk][j];
+    ft[c][k] = uint32_t(a) | (uint32_t(b) << 16);
+}
+
+// Bounds [lo, hi] on the number of A elements before merged position d0 of a sub-merge (A and B
+// of lengths An, Bn): the frontier interval that holds d0 (a binary search over the frontier
+// points, whose positions a + b do not decrease).
+__device__ __forceinline__ void frontier_bounds(const uint32_t* ft, int d0, int An, int Bn, int& lo, int& hi) {
+    int k0 = -1, k1 = kFrontiers;  // last point at or before d0, first point after it
+    while (k1 - k0 > 1) {
+        const int mid = (k0 + k1) >> 1;
+        const uint32_t v = ft[mid];
+        if (int(v & 0xffffu) + int(v >> 16) <= d0) k0 = mid; else k1 = mid;
+    }
+    int a0 = 0, b0 = 0, a1 = An, b1 = Bn;
+    if (k0 >= 0) {
+        a0 = int(ft[k0] & 0xffffu);
+        b0 = int(ft[k0] >> 16);
+    }
+    if (k1 < kFrontiers) {
+        a1 = int(ft[k1] & 0xffffu);
+        b1 = int(ft[k1] >> 16);
+    }
+    lo = max(max(0, d0 - Bn), max(a0, d0 - b1));
+    hi = min(min(d0, An), min(a1, d0 - b0));
     if (lo > hi) lo = hi;  // cannot happen for consistent frontiers
 }
 
 // Output positions [d0, d1) of the merge of two sorted sequences of tile elements, A and B;
 // an element of A precedes an equal element of B (A always holds the lower run indices).
-// Merge-path split, then a sequential merge that keeps both heads' keys in registers and
-// per step reads only the next element of the side it took, without branches.
-template <int NW>
-__device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t* flags, Seq A, Seq B, int d0,
-                                            int d1, uint16_t* out, int lo, int hi) {
+// Merge-path split, then a sequential merge that keeps both heads (key, flag, element) in
+// registers and per step reads only the next element of the side it took, without branches.
+// Writes entries (element | flag) to out.
+template <int NW, bool AARR, bool BARR>
+__device__ __forceinline__ void merge_range(const SKeys<NW>& keys, const uint8_t* flags, const Seq& A, const Seq& B,
+                                            int d0, int d1, uint16_t* out, int lo, int hi) {
     // [lo, hi] brackets the number of A elements before d0 (see frontier_bounds)
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (!tile_less<NW>(keys, flags, B.at(d0 - 1 - mid), A.at(mid))) lo = mid + 1; else hi = mid;
+        int ea, fa, eb, fb;
+        seq_at<BARR>(B, flags, d0 - 1 - mid, eb, fb);
+        seq_at<AARR>(A, flags, mid, ea, fa);
+        if (!reg_less<NW>(keys.get(eb), fb, keys.get(ea), fa)) lo = mid + 1; else hi = mid;
     }
     int i = lo, j = d0 - lo;
-    int ea = i < A.n ? A.at(i) : -1;
-    int eb = j < B.n ? B.at(j) : -1;
-    Key<NW> ka, kb;
-    int fa = 0, fb = 0;
-    ka = keys.get(ea >= 0 ? ea : 0);
-    fa = flags[ea >= 0 ? ea : 0];
-    kb = keys.get(eb >= 0 ? eb : 0);
-    fb = flags[eb >= 0 ? eb : 0];
+    bool va = i < A.n, vb = j < B.n;
+    // an exhausted side's head is element 0, never taken
+    int ea = 0, fa = 0, eb = 0, fb = 0;
+    if (va) seq_at<AARR>(A, flags, i, ea, fa);
+    if (vb) seq_at<BARR>(B, flags, j, eb, fb);
+    Key<NW> ka = keys.get(ea), kb = keys.get(eb);
     for (int d = d0; d < d1; ++d) {
-        const bool take_a = (ea >= 0) & ((eb < 0) | !reg_less<NW>(kb, fb, ka, fa));
-        out[d] = uint16_t(take_a ? ea : eb);
-        // the next head of the side taken
+        const bool take_a = va & (!vb | !reg_less<NW>(kb, fb, ka, fa));
+        out[d] = take_a ? make_ent(ea, fa) : make_ent(eb, fb);
         const int k = take_a ? ++i : ++j;
-        const uint16_t* sp = take_a ? A.ptr : B.ptr;
-        const int sb = take_a ? A.base : B.base, sn = take_a ? A.n : B.n;
-        int en = -1;
-        if (k < sn) en = sp ? int(sp[k]) : sb + k;
-        const int el = en >= 0 ? en : 0;
-        const Key<NW> kn = keys.get(el);
-        const int fn = flags[el];
+        const bool valid = k < (take_a ? A.n : B.n);
+        const int kk = valid ? k : 0;  // entry 0 of the side taken exists (it was not empty)
+        int en, fn;
+        if constexpr (AARR == BARR) {
+            Seq s;
+            s.ptr = take_a ? A.ptr : B.ptr;
+            s.base = take_a ? A.base : B.base;
+            seq_at<AARR>(s, flags, kk, en, fn);
+        } else {
+            int e1, f1, e2, f2;
+            seq_at<AARR>(A, flags, take_a ? kk : 0, e1, f1);
+            seq_at<BARR>(B, flags, take_a ? 0 : kk, e2, f2);
+            en = take_a ? e1 : e2;
+            fn = take_a ? f1 : f2;
+        }
+        const Key<NW> kn = keys.get(en);
         if (take_a) {
             ea = en;
-            ka = kn;
             fa = fn;
+            ka = kn;
+            va = valid;
         } else {
             eb = en;
-            kb = kn;
             fb = fn;
+            kb = kn;
+            vb = valid;
         }
     }
 }
 
-// The last merge level, fused with the dedup: output positions [d0, d1) of the merge of A and
-// B (as merge_range), and for each position whether it holds the first real element of its key
-// -- a real element whose predecessor in merged order (held in registers; at d0 the later of
-// the two heads' predecessors, at 0 the tile's merged predecessor) is not a real element with
-// the same key.  cnt[d] = running count of firsts in [d0, d] | first << 15; with SPLIT the same
-// for the firsts of the new part (element index >= o1: the group has no self-run element)
-// into cntn.  Returns the counts (firsts | new-part firsts << 16).
+// The last merge level, fused with the dedup: output positions [d0, d1) of the merge of A (a
+// merged level) and B (a run segment), as merge_range, and for each position whether it holds
+// the first real element of its key -- a real element whose predecessor in merged order (held
+// in registers; at d0 the later of the two heads' predecessors, at 0 the tile's merged
+// predecessor) is not a real element with the same key.  cnt[d] = running count of firsts in
+// [d0, d] | first << 15; with SPLIT the same for the firsts of the new part (element index >=
+// o1: the group has no self-run element) into cntn.  Returns the counts (firsts | new-part
+// firsts << 16).
 template <int NW, bool SPLIT>
-__device__ __forceinline__ int merge_range_first(const SKeys<NW>& keys, const uint8_t* flags, Seq A, Seq B, int d0,
-                                                 int d1, uint16_t* out, uint16_t* cnt, uint16_t* cntn, int o1,
-                                                 bool tile_has_pred, const Key<NW>& tile_pred, int tile_pred_flag,
-                                                 int lo, int hi) {
+__device__ __forceinline__ int merge_range_first(const SKeys<NW>& keys, const uint8_t* flags, const Seq& A,
+                                                 const Seq& B, int d0, int d1, uint16_t* out, uint16_t* cnt,
+                                                 uint16_t* cntn, int o1, bool tile_has_pred,
+                                                 const Key<NW>& tile_pred, int tile_pred_flag, int lo, int hi) {
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (!tile_less<NW>(keys, flags, B.at(d0 - 1 - mid), A.at(mid))) lo = mid + 1; else hi = mid;
+        int ea, fa, eb, fb;
+        seq_at<false>(B, flags, d0 - 1 - mid, eb, fb);
+        seq_at<true>(A, flags, mid, ea, fa);
+        if (!reg_less<NW>(keys.get(eb), fb, keys.get(ea), fa)) lo = mid + 1; else hi = mid;
     }
     int i = lo, j = d0 - lo;
     // the predecessor of position d0
@@ -238,60 +281,63 @@ __device__ __forceinline__ int merge_range_first(const SKeys<NW>& keys, const ui
     if (d0 == 0) {
         have = tile_has_pred;
     } else {
-        int pe;
-        if (i == 0) {
-            pe = B.at(j - 1);
-        } else if (j == 0) {
-            pe = A.at(i - 1);
-        } else {
-            const int xa = A.at(i - 1), xb = B.at(j - 1);
-            pe = tile_less<NW>(keys, flags, xb, xa) ? xa : xb;  // equal keys: B's element comes later
+        int xa = 0, fa = 0, xb = 0, fb = 0;
+        if (i > 0) seq_at<true>(A, flags, i - 1, xa, fa);
+        if (j > 0) seq_at<false>(B, flags, j - 1, xb, fb);
+        int pe = xb;
+        pf = fb;
+        if (i > 0 && (j == 0 || reg_less<NW>(keys.get(xb), fb, keys.get(xa), fa))) {  // equal: B's comes later
+            pe = xa;
+            pf = fa;
         }
         pk = keys.get(pe);
-        pf = flags[pe];
         have = true;
     }
-    int ea = i < A.n ? A.at(i) : -1;
-    int eb = j < B.n ? B.at(j) : -1;
-    Key<NW> ka = keys.get(ea >= 0 ? ea : 0), kb = keys.get(eb >= 0 ? eb : 0);
-    int fa = flags[ea >= 0 ? ea : 0], fb = flags[eb >= 0 ? eb : 0];
+    bool va = i < A.n, vb = j < B.n;
+    int ea = 0, fa = 0, eb = 0, fb = 0;
+    if (va) seq_at<true>(A, flags, i, ea, fa);
+    if (vb) seq_at<false>(B, flags, j, eb, fb);
+    Key<NW> ka = keys.get(ea), kb = keys.get(eb);
     int c = 0, cn = 0;
     for (int d = d0; d < d1; ++d) {
-        const bool take_a = (ea >= 0) & ((eb < 0) | !reg_less<NW>(kb, fb, ka, fa));
+        const bool take_a = va & (!vb | !reg_less<NW>(kb, fb, ka, fa));
         const int e = take_a ? ea : eb;
         const int f = take_a ? fa : fb;
         Key<NW> k;
 #pragma unroll
         for (int q = 0; q < NW; ++q) k.w[q] = take_a ? ka.w[q] : kb.w[q];
-        out[d] = uint16_t(e);
+        out[d] = make_ent(e, f);
         const int first = (f == 1) & !(have & (pf == 1) & reg_eq<NW>(k, pk));
         c += first;
         cnt[d] = uint16_t(c | (first << 15));
         if constexpr (SPLIT) {
-            const int fn = first & (e >= o1);
-            cn += fn;
-            cntn[d] = uint16_t(cn | (fn << 15));
+            const int fnew = first & (e >= o1);
+            cn += fnew;
+            cntn[d] = uint16_t(cn | (fnew << 15));
         }
         pk = k;
         pf = f;
         have = true;
         // the next head of the side taken
-        const int kk = take_a ? ++i : ++j;
-        const uint16_t* sp = take_a ? A.ptr : B.ptr;
-        const int sb = take_a ? A.base : B.base, sn = take_a ? A.n : B.n;
-        int en = -1;
-        if (kk < sn) en = sp ? int(sp[kk]) : sb + kk;
-        const int el = en >= 0 ? en : 0;
-        const Key<NW> kn = keys.get(el);
-        const int fnx = flags[el];
+        const int kq = take_a ? ++i : ++j;
+        const bool valid = kq < (take_a ? A.n : B.n);
+        const int kk = valid ? kq : 0;
+        int e1, f1, e2, f2;
+        seq_at<true>(A, flags, take_a ? kk : 0, e1, f1);
+        seq_at<false>(B, flags, take_a ? 0 : kk, e2, f2);
+        const int en = take_a ? e1 : e2;
+        const int fn = take_a ? f1 : f2;
+        const Key<NW> kn = keys.get(en);
         if (take_a) {
             ea = en;
+            fa = fn;
             ka = kn;
-            fa = fnx;
+            va = valid;
         } else {
             eb = en;
+            fb = fn;
             kb = kn;
-            fb = fnx;
+            vb = valid;
         }
     }
     return c | (cn << 16);
@@ -659,7 +705,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     extern __shared__ __align__(16) unsigned char smem[];
     const SKeys<NW> s_key{reinterpret_cast<uint64_t*>(smem)};
     uint8_t* s_flag = smem + size_t(tmax) * NW * 8;
-    uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_flag + ((tmax + 15) & ~15));  // merged pos -> element
+    uint16_t* s_perm = reinterpret_cast<uint16_t*>(s_flag + ((tmax + 15) & ~15));  // merged pos -> entry
     uint16_t* s_lv1 = s_perm + tmax;   // first merge level; then the per-thread counts of firsts
     uint16_t* s_lv2 = s_lv1 + tmax;    // second merge level
     uint16_t* s_cnt = s_lv1;           // after level 2: running count of firsts | first << 15
@@ -670,6 +716,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     __shared__ int s_warp[kTileThreads / 32], s_warpn[kTileThreads / 32];
     __shared__ int s_ceil;
     __shared__ __align__(16) TileDesc<NW> s_d;
+    __shared__ uint32_t s_ft[kSubMerges][kFrontiers];
     const int* s_start = s_d.start;
     const int* s_off = s_d.off;
     const int* s_lo = s_d.lo;
@@ -712,6 +759,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
             s_key.set(e, k);
             s_flag[e] = uint8_t(f);
         }
+        frontier_table(s_d.sc, s_d.nsp, s_ft, tid);
         __syncthreads();
 
         // 2. merged order: pairwise merge tree (runs 0+1, 2+3) -> (0123) -> (01234) in shared
@@ -725,29 +773,28 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
             auto ident = [](int base, int len) { return Seq{nullptr, base, len}; };
             auto arr = [](const uint16_t* x, int len) { return Seq{x, 0, len}; };
             const int per4 = (n0123 + kTileThreads - 1) / kTileThreads;
-            const int nsp = s_d.nsp;
             int lo, hi;
             int d0 = min(tid * per4, n0123), d1 = min(d0 + per4, n0123);
             if (d0 < n01) {
-                frontier_bounds(s_d.sc, nsp, 0, 1, 2, d0, o1, o2 - o1, lo, hi);
-                merge_range<NW>(s_key, s_flag, ident(0, o1), ident(o1, o2 - o1), d0, min(d1, n01), s_lv1, lo, hi);
+                frontier_bounds(s_ft[SM_01], d0, o1, o2 - o1, lo, hi);
+                merge_range<NW, false, false>(s_key, s_flag, ident(0, o1), ident(o1, o2 - o1), d0, min(d1, n01), s_lv1, lo, hi);
             }
             if (d1 > n01) {
                 const int e0 = max(d0, n01) - n01;
-                frontier_bounds(s_d.sc, nsp, 2, 3, 4, e0, o3 - o2, o4 - o3, lo, hi);
-                merge_range<NW>(s_key, s_flag, ident(o2, o3 - o2), ident(o3, o4 - o3), e0, d1 - n01, s_lv1 + n01, lo,
+                frontier_bounds(s_ft[SM_23], e0, o3 - o2, o4 - o3, lo, hi);
+                merge_range<NW, false, false>(s_key, s_flag, ident(o2, o3 - o2), ident(o3, o4 - o3), e0, d1 - n01, s_lv1 + n01, lo,
                                 hi);
             }
             __syncthreads();
             if (d0 < d1) {
-                frontier_bounds(s_d.sc, nsp, 0, 2, 4, d0, n01, n0123 - n01, lo, hi);
-                merge_range<NW>(s_key, s_flag, arr(s_lv1, n01), arr(s_lv1 + n01, n0123 - n01), d0, d1, s_lv2, lo, hi);
+                frontier_bounds(s_ft[SM_0123], d0, n01, n0123 - n01, lo, hi);
+                merge_range<NW, true, true>(s_key, s_flag, arr(s_lv1, n01), arr(s_lv1 + n01, n0123 - n01), d0, d1, s_lv2, lo, hi);
             }
             __syncthreads();
             d0 = min(tid * per, n);
             d1 = min(d0 + per, n);
             if (d0 < d1) {
-                frontier_bounds(s_d.sc, nsp, 0, 4, 5, d0, n0123, n - o4, lo, hi);
+                frontier_bounds(s_ft[SM_ALL], d0, n0123, n - o4, lo, hi);
                 const int c = merge_range_first<NW, SPLIT>(s_key, s_flag, arr(s_lv2, n0123), ident(o4, n - o4), d0,
                                                            d1, s_perm, s_cnt, s_cntn, o1, s_d.has_pred != 0, s_pred,
                                                            s_d.pred_flag, lo, hi);
@@ -811,11 +858,15 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
         //    new keys (and H rows, or the new part) at first occurrences, and every element's
         //    index map (its group's output: the running count at its merged position)
         int ceil_local = 0;
+        // q / per as a multiply and shift: exact for q < 2^kEntBits and per <= 13 (the error of the
+        // rounded-up reciprocal stays below 1 / per)
+        const uint32_t per_inv = (65536u + uint32_t(per) - 1u) / uint32_t(per);
         for (int q = tid; q < n; q += kTileThreads) {
-            const int owner = q / per;
+            const int owner = int((uint32_t(q) * per_inv) >> 16);
             const unsigned raw = s_cnt[q];
             const int c = int(raw & 0x7fffu) + s_thr[owner] + s_warp[owner >> 5];  // firsts in the tile up to q
-            const int e = s_perm[q];
+            const int ent = s_perm[q];
+            const int e = ent & kEntMask;
             if (e >= n) {  // every position is written by level 3: cannot happen
                 raise_status(status, PACES_ERR_BADARG);
                 continue;
@@ -858,7 +909,7 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
 #pragma unroll
                 for (int qq = 1; qq < kRuns; ++qq) j += (e >= s_off[qq]);
                 const int64_t src = int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]);
-                const int f = s_flag[e];
+                const int f = ent >> kEntBits;
                 ceil_local += (f == 2);
                 if (src < out.map_cap) out.maps[int64_t(j) * out.map_cap + src] = f == 1 ? int(u) : -1;
             }
