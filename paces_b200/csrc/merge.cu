@@ -1,5 +1,6 @@
 // Structured k-way merge kernels (see merge.cuh for the design).
 #include "kernels.cuh"
+#include "tc.cuh"
 
 namespace paces {
 
@@ -31,10 +32,8 @@ __device__ __forceinline__ int run_source(const ModelDev& m, const MergeWs& ws, 
 // Element `src` of X as it appears in run j of block p: key and order flag
 // (0 = floor hole, 1 = real, 2 = ceiling hole).
 template <int NW>
-__device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __restrict__ X,
-                                         const uint64_t* __restrict__ Y, const MergeWs& ws, int p, int j,
-                                         int64_t src, Key<NW>& k, int& flag) {
-    k = load_key<NW>(j == RUN_SELF ? X : Y, src);
+__device__ __forceinline__ void run_transform(const ModelDev& m, const MergeWs& ws, int p, int j, int64_t src,
+                                              Key<NW>& k, int& flag) {
     flag = 1;
     if (ws.keep && j != RUN_SELF && src < ws.keep_cap && !__ldg(ws.keep + j * ws.keep_cap + src)) flag = 2;
     const int kind = ws.run_kind[j];
@@ -63,6 +62,14 @@ __device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __re
             }
         }
     }
+}
+
+template <int NW>
+__device__ __forceinline__ void run_elem(const ModelDev& m, const uint64_t* __restrict__ X,
+                                         const uint64_t* __restrict__ Y, const MergeWs& ws, int p, int j,
+                                         int64_t src, Key<NW>& k, int& flag) {
+    k = load_key<NW>(j == RUN_SELF ? X : Y, src);
+    run_transform<NW>(m, ws, p, j, src, k, flag);
 }
 
 template <int NW>
@@ -717,6 +724,8 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     __shared__ int s_ceil;
     __shared__ __align__(16) TileDesc<NW> s_d;
     __shared__ uint32_t s_ft[kSubMerges][kFrontiers];
+    __shared__ __align__(8) uint64_t s_mbar;  // completion of the tile's bulk copies
+    __shared__ int s_abort;
     const int* s_start = s_d.start;
     const int* s_off = s_d.off;
     const int* s_lo = s_d.lo;
@@ -731,8 +740,11 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
     if (tid == 0) {
         s_t = atomicAdd(&ws.counters[2], 1);
         s_ceil = 0;
+        s_abort = 0;
+        if constexpr (NW % 2 == 0) tc::mbar_init(tc::smem_addr(&s_mbar), 1);
     }
     __syncthreads();
+    uint32_t parity = 0;  // phase of s_mbar
     for (;;) {
         const int t = s_t;
         if (t >= ntiles) break;
@@ -748,16 +760,52 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
 #pragma unroll
         for (int q = 0; q < NW; ++q) s_pred.w[q] = s_d.pred[q];
 
-        // 1. load the tile's segments (transforms applied on the fly)
-        for (int e = tid; e < n; e += kTileThreads) {
-            int j = 0;
+        // 1. the tile's segments into shared memory, transforms applied
+        if constexpr (NW % 2 == 0) {
+            // keys of 16-byte multiples: one bulk copy per run segment (completion on the
+            // mbarrier, bounded wait), then the transforms in place
+            const uint32_t mb = tc::smem_addr(&s_mbar);
+            if (tid == 0 && n > 0) {
+                // the block's reads of the previous tile's keys precede the copies' writes
+                tc::fence_proxy_async();
+                tc::mbar_expect_tx(mb, uint32_t(n) * uint32_t(NW * 8));
+                for (int j = 0; j < kRuns; ++j) {
+                    const int len = s_off[j + 1] - s_off[j];
+                    if (len <= 0) continue;
+                    const uint64_t* src = (j == RUN_SELF ? X : Y) + (int64_t(s_lo[j]) + s_start[j]) * NW;
+                    tc::bulk_g2s(tc::smem_addr(s_key.w + size_t(s_off[j]) * NW), src, uint32_t(len) * (NW * 8), mb);
+                }
+            }
+            if (n > 0) {
+                if (!tc::mbar_wait(mb, parity) && lane == 0) s_abort = 1;
+                parity ^= 1u;
+            }
+            for (int e = tid; e < n; e += kTileThreads) {
+                int j = 0;
 #pragma unroll
-            for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
-            Key<NW> k;
-            int f;
-            run_elem<NW>(m, X, Y, ws, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
-            s_key.set(e, k);
-            s_flag[e] = uint8_t(f);
+                for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
+                int kind = ws.run_kind[0];
+#pragma unroll
+                for (int q = 1; q < kRuns; ++q) kind = j == q ? ws.run_kind[q] : kind;
+                int f = 1;
+                if (kind == RK_UP || kind == RK_DOWN || (ws.keep && j != RUN_SELF)) {
+                    Key<NW> k = s_key.get(e);
+                    run_transform<NW>(m, ws, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
+                    s_key.set(e, k);
+                }
+                s_flag[e] = uint8_t(f);
+            }
+        } else {
+            for (int e = tid; e < n; e += kTileThreads) {
+                int j = 0;
+#pragma unroll
+                for (int q = 1; q < kRuns; ++q) j += (e >= s_off[q]);
+                Key<NW> k;
+                int f;
+                run_elem<NW>(m, X, Y, ws, p, j, int64_t(s_lo[j]) + s_start[j] + (e - s_off[j]), k, f);
+                s_key.set(e, k);
+                s_flag[e] = uint8_t(f);
+            }
         }
         frontier_table(s_d.sc, s_d.nsp, s_ft, tid);
         __syncthreads();
@@ -924,9 +972,15 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
                 s_ceil = 0;
             }
         }
-        // every thread has read this tile's ticket and descriptor: draw the next one
-        if (tid == 0) s_t = atomicAdd(&ws.counters[2], 1);
+        // every thread has read this tile's ticket and descriptor: draw the next one (none
+        // after a copy that did not complete in time)
+        if (tid == 0) s_t = s_abort ? ntiles : atomicAdd(&ws.counters[2], 1);
         __syncthreads();
+    }
+    if (s_abort && tid == 0) {
+        // wait (bounded) for the late copy before the block's shared memory is released
+        raise_status(status, PACES_ERR_TIMEOUT);
+        tc::mbar_wait(tc::smem_addr(&s_mbar), parity ^ 1u);
     }
     // the block that finishes last writes the block offsets and the totals: every block makes
     // its tiles' words and counts visible before it takes its exit ticket
