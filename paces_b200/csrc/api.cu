@@ -92,6 +92,7 @@ struct Layout {
     size_t aw, keep;  // kept amplitudes of the truncation, proposal keep mask [kRuns][cap]
     size_t maps_e, keysN, blkN, n2b;  // split expansion: its maps, the new part, new part -> output
     size_t maps_x;                    // lattices: maps of the assembly's passes 2 and 3
+    size_t diag;                      // diagnostics folded by the first Taylor sweep (diag_group)
 };
 
 Layout make_layout(const paces_ctx* c, int64_t cap) {
@@ -149,6 +150,7 @@ Layout make_layout(const paces_ctx* c, int64_t cap) {
     l.keysN = take(ucap * nw * 8);
     l.blkN = take(size_t(L + 1) * 4);
     l.n2b = take(ucap * 4);
+    l.diag = take(diag_doubles(cap) * 8);
     l.total = off;
     return l;
 }
@@ -226,7 +228,14 @@ TaylorWs taylor_ws(const paces_ctx* c, const Layout& l, void* ws) {
     w.barrier = at<unsigned>(ws, l.v_bar);
     w.wait_ns = c->test_wait_ns ? c->test_wait_ns : kWaitLimitNs;
     w.skip_block = c->test_skip_block;
+    w.diag = nullptr;
     return w;
+}
+
+// The post-adaptation diagnostics come out of the Taylor launch's first sweep when the step
+// propagates by the Taylor series; otherwise (no propagation, Lanczos) from their own pass.
+bool diag_in_taylor(const paces_step_params* prm) {
+    return prm->diagnostics && prm->evolve && prm->lanczos_order == 0;
 }
 
 // Output rows the assembly can flag in the Taylor term buffer (one byte each).
@@ -574,8 +583,8 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
                                        p.new_b->blk, p.target, remap_ws(l, ws), status, c->num_sms, st),
                        "step/remap");
     mark(4);
-    // 5. post-adaptation diagnostics
-    if (prm->diagnostics) {
+    // 5. post-adaptation diagnostics (unless the Taylor launch folds them)
+    if (prm->diagnostics && !diag_in_taylor(prm)) {
         ObsTarget t{&rec->post_adapt_norm, &rec->post_adapt_energy_re, &rec->post_adapt_energy_im, nullptr, nullptr};
         PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, with_h(c, p.h), p.new_b->keys, p.new_b->blk, p.h->nbr,
                                                  p.h->cap, p.h->meta, p.target, PACES_OBS_NORM | PACES_OBS_ENERGY,
@@ -595,6 +604,11 @@ int step_back(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
     auto mark = [&](int i) {
         if (marks && c->profiling) cudaEventRecord(c->ev[i], st);
     };
+    if (diag_in_taylor(prm)) {
+        ObsTarget t{&rec->post_adapt_norm, &rec->post_adapt_energy_re, &rec->post_adapt_energy_im, nullptr, nullptr};
+        PACES_CHECK_LAUNCH(c, launch_diag_final(at<double>(p.ws, p.l.diag), p.new_b->blk, c->m.L, p.l.cap, t, st),
+                           "step/diagnostics");
+    }
     if (prm->evolve && prm->renormalize) {
         ObsTarget t{&rec->norm, nullptr, nullptr, nullptr, nullptr};
         PACES_CHECK_LAUNCH(c, launch_observables(c->nw, c64, with_h(c, p.h), p.new_b->keys, p.new_b->blk, p.h->nbr, p.h->cap,
@@ -1202,10 +1216,11 @@ int paces_step(paces_ctx* c, const paces_basis* old_b, const void* old_psi, pace
                                                  c->num_sms, st),
                                "step/lanczos");
         } else {
+            TaylorWs tw = taylor_ws(c, p.l, ws);
+            if (diag_in_taylor(prm)) tw.diag = at<double>(ws, p.l.diag);
             PACES_CHECK_LAUNCH(c, launch_taylor(c->precision == PACES_C64, with_h(c, h), new_b->blk, h->nbr, h->cap,
-                                                h->meta, p.target, new_psi, prm->dt, prm->m_star, prm->tol,
-                                                taylor_ws(c, p.l, ws), o, &rec->status, c->num_sms, c->taylor_bps,
-                                                c->taylor_variant, st),
+                                                h->meta, p.target, new_psi, prm->dt, prm->m_star, prm->tol, tw, o,
+                                                &rec->status, c->num_sms, c->taylor_bps, c->taylor_variant, st),
                                "step/taylor");
         }
     }
@@ -1452,6 +1467,7 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
             ti.sq = c->d_sq;
             ti.sqf = c->d_sqf;
             ti.status = &p.rec->status;
+            ti.diag = diag_in_taylor(prm) ? at<double>(p.ws, p.l.diag) : nullptr;
             ti.out = TaylorOut{&p.rec->converged, &p.rec->final_m, &p.rec->c1_plus_c2, &p.rec->term_ratio};
             ti.dt = prm->dt;
             ti.tol = prm->tol;

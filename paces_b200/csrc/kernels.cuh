@@ -49,8 +49,46 @@ struct TaylorWs {
     unsigned* barrier;   // [2]
     uint64_t wait_ns;    // grid-barrier wait limit (kWaitLimitNs unless a test shortens it)
     int skip_block;      // test hook: this block skips its first grid-barrier arrival (-1: none)
+    double* diag;        // null, or [diag_groups(rows)][3]: see diag_group
 };
 int taylor_max_grid(bool c64, int num_sms);
+
+// ---- diagnostics of the input state, from the first Taylor sweep ---------------------------
+// The first sweep of the series forms (H v)_r for every row, so the post-adaptation norm and
+// energy <v|H|v> come out of it: each warp folds the rows of one 32-row group (row 32 g + l on
+// lane l, in every kernel and schedule) with a fixed butterfly, and diag_final sums the groups
+// in a fixed order.  The result depends on the rows only -- not on the grid, the row schedule
+// or whether the trajectory runs alone or in a batch.
+constexpr int kDiagGroup = 32;
+constexpr int kDiagChunk = 2048;  // groups per block of the first reduction
+__host__ __device__ inline int64_t diag_groups(int64_t rows) { return (rows + kDiagGroup - 1) / kDiagGroup; }
+inline int64_t diag_chunks(int64_t rows) { return (diag_groups(rows) + kDiagChunk - 1) / kDiagChunk; }
+// doubles of a diag buffer for up to `cap` rows: the group sums, then the chunk sums
+inline size_t diag_doubles(int64_t cap) { return size_t(diag_groups(cap) + diag_chunks(cap)) * 3; }
+
+// Called by all 32 lanes of a warp for the group whose row 32 g + lane this lane holds
+// (valid: the row exists; a, y: v_r and (H v)_r).
+template <typename C>
+__device__ __forceinline__ void diag_group(double* __restrict__ diag, int64_t g, bool valid, const C& a, const C& y) {
+    double n2 = 0.0, er = 0.0, ei = 0.0;
+    if (valid) {
+        const double ar = double(a.x), ai = double(a.y), yr = double(y.x), yi = double(y.y);
+        n2 = fma(ar, ar, __dmul_rn(ai, ai));
+        er = fma(ar, yr, __dmul_rn(ai, yi));
+        ei = fma(ar, yi, -__dmul_rn(ai, yr));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n2 = __dadd_rn(n2, __shfl_xor_sync(0xffffffffu, n2, o));
+        er = __dadd_rn(er, __shfl_xor_sync(0xffffffffu, er, o));
+        ei = __dadd_rn(ei, __shfl_xor_sync(0xffffffffu, ei, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        diag[g * 3] = n2;
+        diag[g * 3 + 1] = er;
+        diag[g * 3 + 2] = ei;
+    }
+}
 
 // ---- Lanczos ----------------------------------------------------------------------------
 constexpr int kMaxLanczosOrder = PACES_MAX_LANCZOS_ORDER;
@@ -117,6 +155,7 @@ struct TaylorItem {
     const double* sq;          // [kSqrtTable] sqrt(k) * g, fp64
     const float* sqf;          // [kSqrtTable] the same rounded to fp32
     int* status;               // the trajectory's status word
+    double* diag;              // null, or the trajectory's diag buffer (first-sweep diagnostics)
     TaylorOut out;
     double dt, tol, eps_sys, hbar_omega, delta_eps, J;
     int L, has_site_eps, m_star, pad;
@@ -145,6 +184,9 @@ struct ObsTarget {
     double* n_exc;       // [L] or null
     double* n_pho;       // [L] or null
 };
+// Norm and energy from a diag buffer filled by the first sweep of a Taylor launch (rows:
+// blk[L]; cap: the buffer's row capacity).  Two launches.
+int launch_diag_final(const double* diag, const int* blk, int L, int64_t cap, const ObsTarget& out, cudaStream_t st);
 constexpr int kObsGridPerSm = 4;
 inline int obs_max_grid(int num_sms) { return num_sms * kObsGridPerSm; }
 int launch_observables(int nw, bool c64, const ModelDev& m, const uint64_t* keys, const int* blk,

@@ -305,6 +305,54 @@ __global__ void __launch_bounds__(256) obs_final_kernel(int L, int nb_e, const d
     }
 }
 
+// Diagnostics from a diag buffer (diag_group): block c sums the groups [c kDiagChunk,
+// (c+1) kDiagChunk) -- thread t its eight consecutive groups in order, then the warps'
+// butterflies and the eight warp sums in order -- into the chunk sums that follow the groups.
+__global__ void __launch_bounds__(256) diag_chunk_kernel(const double* __restrict__ groups, double* __restrict__ chunks,
+                                                        const int* __restrict__ blk, int L) {
+    __shared__ double s_w[8][3];
+    const int64_t ng = diag_groups(blk[L]);
+    const int64_t c = blockIdx.x;
+    if (c * kDiagChunk >= ng) return;
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t g0 = c * kDiagChunk + int64_t(threadIdx.x) * (kDiagChunk / 256);
+#pragma unroll
+    for (int k = 0; k < kDiagChunk / 256; ++k) {
+        const int64_t g = g0 + k;
+        if (g < ng) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) v[q] = __dadd_rn(v[q], groups[g * 3 + q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] = __dadd_rn(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
+        if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5][q] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double acc = 0.0;
+        for (int w = 0; w < 8; ++w) acc = __dadd_rn(acc, s_w[w][threadIdx.x]);
+        chunks[c * 3 + threadIdx.x] = acc;
+    }
+}
+
+// The chunk sums in order: norm (square root of the sum of |v|^2) and energy.
+__global__ void diag_final_kernel(const double* __restrict__ chunks, const int* __restrict__ blk, int L, ObsTarget t) {
+    if (threadIdx.x >= 3) return;
+    const int64_t nch = (diag_groups(blk[L]) + kDiagChunk - 1) / kDiagChunk;
+    double acc = 0.0;
+    for (int64_t c = 0; c < nch; ++c) acc = __dadd_rn(acc, chunks[c * 3 + threadIdx.x]);
+    if (threadIdx.x == 0) {
+        if (t.norm) *t.norm = sqrt(acc);
+    } else if (threadIdx.x == 1) {
+        if (t.energy_re) *t.energy_re = acc;
+    } else {
+        if (t.energy_im) *t.energy_im = acc;
+    }
+}
+
 // y = H x on every row of the basis (total_ham, paces/core/time_evolution.py:382-400).
 template <bool C64>
 __global__ void __launch_bounds__(kOThreads) apply_h_kernel(ModelDev m, const int* __restrict__ blk,
@@ -565,6 +613,15 @@ int launch_obs_t(const ModelDev& m, const uint64_t* keys, const int* blk, const 
 }
 
 }  // namespace
+
+int launch_diag_final(const double* diag, const int* blk, int L, int64_t cap, const ObsTarget& out, cudaStream_t st) {
+    if (!diag || cap < 0) return PACES_ERR_BADARG;
+    double* chunks = const_cast<double*>(diag) + diag_groups(cap) * 3;
+    const int64_t nch = diag_chunks(cap);
+    diag_chunk_kernel<<<unsigned(nch > 0 ? nch : 1), 256, 0, st>>>(diag, chunks, blk, L);
+    diag_final_kernel<<<1, 32, 0, st>>>(chunks, blk, L, out);
+    return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
+}
 
 int launch_observables(int nw, bool c64, const ModelDev& m, const uint64_t* keys, const int* blk,
                        const int* nbr, int64_t nbr_cap, const uint32_t* meta, const void* psi,

@@ -129,17 +129,42 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
             dst[r] = t;
             res[r] = rr;
         };
+        const bool diag = j == 0 && ws.diag != nullptr;  // first sweep: fold the input's diagnostics
+        const int wid = threadIdx.x >> 5;
         if constexpr (!BULK) {
             // two rows per thread per pass: all loads of both rows precede the stores
             const int64_t stride = int64_t(gridDim.x) * kTThreads;
-            int64_t r = int64_t(blockIdx.x) * kTThreads + threadIdx.x;
-            for (; r + stride < S; r += 2 * stride) {
-                const C y0 = hrow(r), y1 = hrow(r + stride);
-                const C a0 = rin[r], a1 = rin[r + stride];
-                finish(r, y0, a0);
-                finish(r + stride, y1, a1);
+            if (!diag) {
+                int64_t r = int64_t(blockIdx.x) * kTThreads + threadIdx.x;
+                for (; r + stride < S; r += 2 * stride) {
+                    const C y0 = hrow(r), y1 = hrow(r + stride);
+                    const C a0 = rin[r], a1 = rin[r + stride];
+                    finish(r, y0, a0);
+                    finish(r + stride, y1, a1);
+                }
+                if (r < S) finish(r, hrow(r), rin[r]);
+            } else {
+                // the same rows, in a loop every lane of a warp runs together (warp-uniform
+                // bounds), so that each warp folds its 32-row groups
+                const int lane = threadIdx.x & 31;
+                for (int64_t rb = int64_t(blockIdx.x) * kTThreads + (threadIdx.x & ~31); rb < S; rb += 2 * stride) {
+                    const int64_t r0 = rb + lane, r1 = rb + stride + lane;
+                    const bool v0 = r0 < S, v1 = r1 < S;
+                    C y0{}, y1{}, a0{}, a1{};
+                    if (v0) {
+                        y0 = hrow(r0);
+                        a0 = rin[r0];
+                    }
+                    if (v1) {
+                        y1 = hrow(r1);
+                        a1 = rin[r1];
+                    }
+                    if (v0) finish(r0, y0, a0);
+                    if (v1) finish(r1, y1, a1);
+                    diag_group(ws.diag, rb >> 5, v0, a0, y0);
+                    if (rb + stride < S) diag_group(ws.diag, (rb + stride) >> 5, v1, a1, y1);
+                }
             }
-            if (r < S) finish(r, hrow(r), rin[r]);
         } else {
             constexpr uint32_t kCB = chunk_bytes<C64>();
             constexpr uint32_t kOffMeta = kChunk * 16, kOffRin = kOffMeta + kChunk * 4,
@@ -197,10 +222,28 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                     }
                     finish(r0 + t0, y0, srin[t0]);
                     finish(r0 + t1, y1, srin[t1]);
+                    if (diag) {
+                        diag_group(ws.diag, (r0 >> 5) + wid, true, srin[t0], y0);
+                        diag_group(ws.diag, (r0 >> 5) + kTWarps + wid, true, srin[t1], y1);
+                    }
                 } else {
                     // the last, partial chunk: direct loads
-                    if (r0 + t0 < S) finish(r0 + t0, hrow(r0 + t0), rin[r0 + t0]);
-                    if (r0 + t1 < S) finish(r0 + t1, hrow(r0 + t1), rin[r0 + t1]);
+                    const bool v0 = r0 + t0 < S, v1 = r0 + t1 < S;
+                    C y0{}, y1{}, a0{}, a1{};
+                    if (v0) {
+                        y0 = hrow(r0 + t0);
+                        a0 = rin[r0 + t0];
+                        finish(r0 + t0, y0, a0);
+                    }
+                    if (v1) {
+                        y1 = hrow(r0 + t1);
+                        a1 = rin[r0 + t1];
+                        finish(r0 + t1, y1, a1);
+                    }
+                    if (diag) {  // groups with at least one row (warp-uniform)
+                        if (r0 + 32 * wid < S) diag_group(ws.diag, (r0 >> 5) + wid, v0, a0, y0);
+                        if (r0 + kTThreads + 32 * wid < S) diag_group(ws.diag, (r0 >> 5) + kTWarps + wid, v1, a1, y1);
+                    }
                 }
                 __syncthreads();  // the buffer is free for the copy issued next iteration
                 if (s_abort) break;

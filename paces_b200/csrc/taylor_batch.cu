@@ -6,14 +6,16 @@
 // (:382-400), run once per trajectory; the reference has no batching.
 //
 // Design.  The rows of all trajectories form one index space (trajectory t owns rows
-// [off[t], off[t+1]), off computed on the device from every basis' blk[L], so the host
-// never reads a size).  Each term is one sweep over that space in warp units of 64 rows
-// (two per lane, all loads before the stores), assigned grid-stride so the rows of the
-// trajectories still running are spread over every SM.  A unit inside one trajectory
-// takes the fast path: lanes keep running maxima of |term|^2, |res|^2, |v|^2 and a
-// non-finite flag for the warp's current trajectory and fold them into shared memory
-// only when the trajectory changes.  A unit that straddles trajectories (at most one per
-// boundary) folds row by row.  Blocks then fold into per-trajectory global maxima with
+// [off[t], off[t] + rows_t), off computed on the device from every basis' blk[L] rounded up
+// to a multiple of the 64-row unit, so the host never reads a size and no unit straddles two
+// trajectories).  Each term is one sweep over that space in warp units of 64 rows (two per
+// lane, all loads before the stores), assigned grid-stride so the rows of the trajectories
+// still running are spread over every SM.  Lanes keep running maxima of |term|^2, |res|^2,
+// |v|^2 and a non-finite flag for the warp's current trajectory and fold them into shared
+// memory only when the trajectory changes.  Row 64 u + l of a trajectory sits on lane l of
+// its unit, as in the single-trajectory kernel's 32-row groups, so the first sweep folds the
+// input's diagnostics (diag_group) exactly as that kernel does.  Blocks then fold into
+// per-trajectory global maxima with
 // atomicMax on the fp64 bit patterns (non-negative doubles order like their bits), which
 // is exact and order-independent, so each trajectory's stop decision -- taken by every
 // block from the same global maxima -- and its arithmetic are bit-identical to the
@@ -43,6 +45,7 @@ taylor_batch_kernel(const __grid_constant__ TaylorBatch bt, TaylorBatchWs ws) {
     using C = typename std::conditional<C64, float2, double2>::type;
     using R = typename std::conditional<C64, float, double>::type;
     __shared__ long long s_off[kMaxBatch + 1];
+    __shared__ long long s_rows[kMaxBatch];
     __shared__ unsigned long long s_max[kMaxBatch][4];
     __shared__ double s_c1[kMaxBatch], s_c1c2[kMaxBatch], s_ratio[kMaxBatch], s_cd[kMaxBatch];
     __shared__ int s_active[kMaxBatch];
@@ -52,7 +55,8 @@ taylor_batch_kernel(const __grid_constant__ TaylorBatch bt, TaylorBatchWs ws) {
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < n; i += kBThreads) {
         const TaylorItem& I = bt.items[i];
-        s_off[i + 1] = I.blk[I.L];
+        s_rows[i] = I.blk[I.L];
+        s_off[i + 1] = (s_rows[i] + kUnit - 1) / kUnit * kUnit;
         s_active[i] = 1;
         s_c1[i] = s_c1c2[i] = s_ratio[i] = 0.0;
 #pragma unroll
@@ -133,48 +137,37 @@ taylor_batch_kernel(const __grid_constant__ TaylorBatch bt, TaylorBatchWs ws) {
         for (long long u = gwarp; u < units; u += nwarps) {
             const long long base = u * kUnit;
             while (s_off[it + 1] <= base) ++it;
-            const long long end = base + kUnit < rows ? base + kUnit : rows;
-            if (s_off[it + 1] >= end) {
-                // fast path: the whole unit is rows of trajectory `it`
-                if (!s_active[it]) continue;
-                if (it != cur) {
-                    flush();
-                    cur = it;
-                }
-                const TaylorItem& I = bt.items[it];
-                const double cd = s_cd[it];
-                const long long r0 = base + lane, r1 = base + 32 + lane;
-                const long long l0 = r0 - s_off[it], l1 = r1 - s_off[it];
-                if (r1 < end) {
-                    C y0, a0, y1, a1;
-                    load_row(I, l0, y0, a0);
-                    load_row(I, l1, y1, a1);
-                    finish_row(I, cd, l0, y0, a0, cm);
-                    finish_row(I, cd, l1, y1, a1, cm);
-                } else if (r0 < end) {
-                    C y0, a0;
-                    load_row(I, l0, y0, a0);
-                    finish_row(I, cd, l0, y0, a0, cm);
-                }
-            } else {
-                // slow path: the unit crosses a trajectory boundary; fold row by row
-#pragma unroll 1
-                for (int h = 0; h < 2; ++h) {
-                    const long long r = base + h * 32 + lane;
-                    if (r >= end) continue;
-                    int i = it;
-                    while (s_off[i + 1] <= r) ++i;
-                    if (!s_active[i]) continue;
-                    const TaylorItem& I = bt.items[i];
-                    const long long l = r - s_off[i];
-                    double mx[4] = {0.0, 0.0, 0.0, 0.0};
-                    C y, a;
-                    load_row(I, l, y, a);
-                    finish_row(I, s_cd[i], l, y, a, mx);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        if (mx[k] > 0.0) atomicMax(&s_max[i][k], dbits(mx[k]));
-                }
+            // the whole unit is rows (or padding) of trajectory `it`
+            if (!s_active[it]) continue;
+            if (it != cur) {
+                flush();
+                cur = it;
+            }
+            const TaylorItem& I = bt.items[it];
+            const double cd = s_cd[it];
+            const long long l0 = base - s_off[it] + lane, l1 = l0 + 32;
+            const long long nr = s_rows[it];
+            if (first && I.diag) {
+                // the first sweep with the diagnostics (groups with at least one row; warp-uniform)
+                const bool v0 = l0 < nr, v1 = l1 < nr;
+                C y0{}, a0{}, y1{}, a1{};
+                if (v0) load_row(I, l0, y0, a0);
+                if (v1) load_row(I, l1, y1, a1);
+                const long long g = (base - s_off[it]) >> 5;
+                if (g * 32 < nr) diag_group(I.diag, g, v0, a0, y0);
+                if ((g + 1) * 32 < nr) diag_group(I.diag, g + 1, v1, a1, y1);
+                if (v0) finish_row(I, cd, l0, y0, a0, cm);
+                if (v1) finish_row(I, cd, l1, y1, a1, cm);
+            } else if (l1 < nr) {
+                C y0, a0, y1, a1;
+                load_row(I, l0, y0, a0);
+                load_row(I, l1, y1, a1);
+                finish_row(I, cd, l0, y0, a0, cm);
+                finish_row(I, cd, l1, y1, a1, cm);
+            } else if (l0 < nr) {
+                C y0, a0;
+                load_row(I, l0, y0, a0);
+                finish_row(I, cd, l0, y0, a0, cm);
             }
         }
         flush();
