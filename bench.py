@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="step without CUDA-graph replay")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--merge-stride", type=int, default=0, help="plain: this merge stride instead of tuning it")
+    ap.add_argument("--assemble-stride", type=int, default=0,
+                    help="plain, with --merge-stride: the assembly's own stride (default: the same)")
     ap.add_argument("--batch", type=int, default=64, help="trajectories of the batched workload")
     ap.add_argument("--seed", type=int, default=0, help="seed of the batched workload's draws")
     ap.add_argument("--streams", type=int, default=8, help="streams of the batched step")
@@ -395,10 +397,10 @@ def run_ours(a):
     tuning = None
     if a.merge_stride:
         from paces_b200 import autotune
-        autotune.set_tuning(eng, merge_stride=a.merge_stride)
+        autotune.set_tuning(eng, merge_stride=a.merge_stride, assemble_stride=a.assemble_stride or None)
         t = autotune.get_tuning(eng)
-        tuning = {"merge_stride": t.merge_stride, "taylor_blocks_per_sm": t.taylor_blocks_per_sm,
-                  "taylor_variant": t.taylor_variant}
+        tuning = {"merge_stride": t.merge_stride, "assemble_stride": t.assemble_stride,
+                  "taylor_blocks_per_sm": t.taylor_blocks_per_sm, "taylor_variant": t.taylor_variant}
     elif not a.no_tune:
         from paces_b200 import autotune
         tuning = autotune.tune(tr, a.dt)

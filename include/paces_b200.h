@@ -266,9 +266,9 @@ int paces_set_profiling(paces_ctx *ctx, int32_t on);
 int paces_stage_times(paces_ctx *ctx, float *ms);
 /* Number of kernels paces_step has enqueued on this context so far. */
 unsigned long long paces_kernel_launches(const paces_ctx *ctx);
-/* Launch shapes (no counterpart in the reference): the merge tiles' splitter stride
- * (tile size = 13 * stride elements), the Taylor kernel's blocks per SM and its row
- * schedule.  Results do
+/* Launch shapes (no counterpart in the reference): the merge tiles' splitter strides
+ * (tile size = 17 * stride elements; one for the expansions, one for the assembly), the
+ * Taylor kernel's blocks per SM and its row schedule.  Results do
  * not depend on them; paces_b200.autotune picks them by timing the live workload.
  * paces_get_tuning also reports the allowed ranges; paces_set_tuning rejects values
  * outside them with PACES_ERR_BADARG. */
@@ -279,7 +279,8 @@ typedef struct paces_tuning {
     int32_t merge_stride_max;          /* read only */
     int32_t taylor_blocks_per_sm_max;  /* read only */
     int32_t taylor_variant;            /* 0: rows read directly; 1: 512-row chunks prefetched by bulk copies */
-    int32_t reserved[2];
+    int32_t assemble_stride;           /* the assembly's stride, same range; 0 on set: merge_stride */
+    int32_t reserved[1];
 } paces_tuning;
 int paces_get_tuning(const paces_ctx *ctx, paces_tuning *t);
 int paces_set_tuning(paces_ctx *ctx, const paces_tuning *t);

@@ -130,7 +130,8 @@ class Tuning(ctypes.Structure):
         ("merge_stride_max", ctypes.c_int32),
         ("taylor_blocks_per_sm_max", ctypes.c_int32),
         ("taylor_variant", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("assemble_stride", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 

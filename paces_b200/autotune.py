@@ -3,14 +3,16 @@
 These shapes change the speed of a step but never its results (each trajectory's
 arithmetic and ordering are fixed by the data, not by the tiling):
 
-* the merge tiles' splitter stride (tile = 13 * stride elements): larger tiles spend less
-  on splitters and look-back, smaller ones fit more blocks per SM;
+* the merge tiles' splitter strides (tile = 17 * stride elements), one for the expansions
+  and one for the assembly: larger tiles spend less on splitters and look-back, smaller ones
+  fit more blocks per SM;
 * the persistent Taylor kernel's blocks per SM (its grid) and its row schedule (rows read
   directly, or 512-row chunks prefetched into shared memory by bulk TMA copies).
 
 `tune(trajectory, dt)` times candidates on the live workload -- eager steps with the
-library's stage events -- and keeps, shape by shape, the fastest (merge stride by the
-expand + assemble time, Taylor blocks by the Taylor time).  `tune_batch` does the same for
+library's stage events -- and keeps, shape by shape, the fastest (the expansion stride by
+the expand time and the assembly stride by the assemble time of the same trials, Taylor
+blocks by the Taylor time).  `tune_batch` does the same for
 a TrajectoryBatch with its phase times.  Choices are cached per (GPU name, key words,
 precision, log2 of the basis size) in memory and in a JSON file
 ($PACES_TUNE_CACHE, default ~/.cache/paces_b200/tuning.json), so a later run of the same
@@ -31,7 +33,7 @@ CACHE_PATH = os.environ.get("PACES_TUNE_CACHE",
                             os.path.join(os.path.expanduser("~"), ".cache", "paces_b200", "tuning.json"))
 _memory: dict = {}
 VARIANTS = [0, 1]  # Taylor row schedules: direct, bulk-prefetched
-SHAPES = ("merge_stride", "taylor_blocks_per_sm", "taylor_variant")
+SHAPES = ("merge_stride", "taylor_blocks_per_sm", "taylor_variant", "assemble_stride")
 
 
 def get_tuning(eng) -> nat.Tuning:
@@ -40,10 +42,15 @@ def get_tuning(eng) -> nat.Tuning:
     return t
 
 
-def set_tuning(eng, merge_stride=None, taylor_blocks_per_sm=None, taylor_variant=None):
+def set_tuning(eng, merge_stride=None, taylor_blocks_per_sm=None, taylor_variant=None, assemble_stride=None):
+    """Set the given shapes, keeping the others; a merge_stride given without assemble_stride
+    sets both strides."""
     t = get_tuning(eng)
     if merge_stride is not None:
         t.merge_stride = int(merge_stride)
+        t.assemble_stride = int(merge_stride if assemble_stride is None else assemble_stride)
+    elif assemble_stride is not None:
+        t.assemble_stride = int(assemble_stride)
     if taylor_blocks_per_sm is not None:
         t.taylor_blocks_per_sm = int(taylor_blocks_per_sm)
     if taylor_variant is not None:
@@ -60,9 +67,14 @@ def bps_candidates(t: nat.Tuning):
     return [0] + list(range(1, t.taylor_blocks_per_sm_max))
 
 
+# bumped when the kernels' tiling changes, so that choices cached for other tiles are not reused
+CACHE_LAYOUT = 2
+
+
 def _key(eng, states):
     name = torch.cuda.get_device_name(eng.device)
-    return f"{name}|nw{eng.nw}|{'c64' if eng.c64 else 'c128'}|s{int(round(math.log2(max(states, 1))))}"
+    return (f"v{CACHE_LAYOUT}|{name}|nw{eng.nw}|{'c64' if eng.c64 else 'c128'}"
+            f"|s{int(round(math.log2(max(states, 1))))}")
 
 
 def _load_file():
@@ -95,26 +107,37 @@ def _lookup(key, use_cache):
 
 
 def _search(apply, measure, strides, bpss, variants, measure_taylor=None):
-    """Coordinate search: the stride by its stages' time, then the Taylor schedule and grid
-    by the Taylor time.  The strides are timed in two passes, the second in reverse order,
-    and each keeps its faster pass: a basis that still grows during the search then favours
-    no end of the candidate list.  measure_taylor (when given) times the Taylor candidates
-    on one fixed input, so that no candidate is judged on a step with fewer terms."""
-    timings = {"merge_stride": {}, "taylor": {}}
+    """Coordinate search: the strides by their stages' times, then the Taylor schedule and
+    grid by the Taylor time.  Every stride trial runs both merges at that stride; when
+    measure() reports the expand and assemble stages apart, each merge keeps its own fastest
+    stride, else one stride serves both.  The strides are timed in two passes, the second in
+    reverse order, and each keeps its faster pass: a basis that still grows during the search
+    then favours no end of the candidate list.  measure_taylor (when given) times the Taylor
+    candidates on one fixed input, so that no candidate is judged on a step with fewer
+    terms.  apply(expansion stride, assembly stride, blocks per SM, variant)."""
+    timings = {"merge_stride": {}, "assemble_stride": {}, "taylor": {}}
+    split = True
     for order in (list(strides), list(reversed(strides))):
         for s in order:
-            apply(s, 0, variants[0])
-            ms = measure()["merge"]
-            timings["merge_stride"][s] = min(ms, timings["merge_stride"].get(s, ms))
+            apply(s, s, 0, variants[0])
+            m = measure()
+            split = split and "expand" in m and "assemble" in m
+            e, a = (m["expand"], m["assemble"]) if split else (m["merge"], 0.0)
+            timings["merge_stride"][s] = min(e, timings["merge_stride"].get(s, e))
+            timings["assemble_stride"][s] = min(a, timings["assemble_stride"].get(s, a))
     best_s = min(timings["merge_stride"], key=timings["merge_stride"].get)
+    best_a = min(timings["assemble_stride"], key=timings["assemble_stride"].get) if split else best_s
+    if not split:
+        del timings["assemble_stride"]
     for v in variants:
         for b in bpss:
-            apply(best_s, b, v)
+            apply(best_s, best_a, b, v)
             timings["taylor"][(v, b)] = measure_taylor() if measure_taylor else measure()["taylor"]
     best_v, best_b = min(timings["taylor"], key=timings["taylor"].get)
-    apply(best_s, best_b, best_v)
+    apply(best_s, best_a, best_b, best_v)
     timings["taylor"] = {f"variant{v}_bps{b}": ms for (v, b), ms in timings["taylor"].items()}
-    return {"merge_stride": best_s, "taylor_blocks_per_sm": best_b, "taylor_variant": best_v, "timings_ms": timings}
+    return {"merge_stride": best_s, "assemble_stride": best_a, "taylor_blocks_per_sm": best_b,
+            "taylor_variant": best_v, "timings_ms": timings}
 
 
 def tune(tr, dt, steps=2, use_cache=True):
@@ -125,7 +148,8 @@ def tune(tr, dt, steps=2, use_cache=True):
     key = _key(eng, tr.basis.count())
     hit = _lookup(key, use_cache)
     if hit is not None:
-        set_tuning(eng, hit["merge_stride"], hit["taylor_blocks_per_sm"], hit.get("taylor_variant"))
+        set_tuning(eng, hit["merge_stride"], hit["taylor_blocks_per_sm"], hit.get("taylor_variant"),
+                   assemble_stride=hit.get("assemble_stride"))
         return dict(hit, cached=True)
     t0 = get_tuning(eng)
     use_graph, tr.use_graph = tr.use_graph, False
@@ -133,11 +157,12 @@ def tune(tr, dt, steps=2, use_cache=True):
 
     def measure():
         tr.step(evolve=True, dt=dt)  # first step after a change: not timed
-        acc = {"merge": 0.0, "taylor": 0.0}
+        acc = {"expand": 0.0, "assemble": 0.0, "taylor": 0.0}
         for _ in range(steps):
             tr.step(evolve=True, dt=dt)
             st = eng.stage_times()
-            acc["merge"] += st["expand"] + st["assemble"]
+            acc["expand"] += st["expand"]
+            acc["assemble"] += st["assemble"]
             acc["taylor"] += st["taylor"]
         return {k: v / steps for k, v in acc.items()}
 
@@ -158,8 +183,8 @@ def tune(tr, dt, steps=2, use_cache=True):
         return best
 
     try:
-        choice = _search(lambda s, b, v: set_tuning(eng, s, b, v), measure, stride_candidates(t0), bps_candidates(t0),
-                         VARIANTS, measure_taylor=measure_taylor)
+        choice = _search(lambda s, a, b, v: set_tuning(eng, s, b, v, assemble_stride=a), measure,
+                         stride_candidates(t0), bps_candidates(t0), VARIANTS, measure_taylor=measure_taylor)
     finally:
         eng.set_profiling(False)
         tr.use_graph = use_graph
@@ -177,13 +202,14 @@ def tune_batch(batch, dt, steps=2, use_cache=True):
     key = "batch|" + _key(engs[0], total) + f"|n{len(engs)}"
     hit = _lookup(key, use_cache)
 
-    def apply(s, b, v=None):
+    def apply(s, a, b, v=None):
         for e in engs:
             t = get_tuning(e)
-            set_tuning(e, min(max(s, t.merge_stride_min), t.merge_stride_max), b, v)
+            clamp = lambda x: min(max(x, t.merge_stride_min), t.merge_stride_max)
+            set_tuning(e, clamp(s), b, v, assemble_stride=clamp(a))
 
     if hit is not None:
-        apply(hit["merge_stride"], hit["taylor_blocks_per_sm"])
+        apply(hit["merge_stride"], hit.get("assemble_stride", hit["merge_stride"]), hit["taylor_blocks_per_sm"])
         return dict(hit, cached=True)
     t0 = get_tuning(engs[0])
     use_graph, batch.use_graph = batch.use_graph, False

@@ -17,7 +17,8 @@ struct paces_ctx {
     int device;
     int num_sms;
     int taylor_grid;
-    int merge_stride;  // tuning: elements per splitter of the merge tiles
+    int merge_stride;     // tuning: elements per splitter of the expansions' merge tiles
+    int assemble_stride;  // tuning: the same for the assembly
     int taylor_bps;    // tuning: Taylor blocks per SM (0 = as many as fit)
     int taylor_variant;  // tuning: 0 direct rows, 1 bulk-prefetched chunks
     int* d_status;  // device status word for the stage entry points (start of the constants block)
@@ -342,7 +343,7 @@ int merge_all_channels(paces_ctx* c, bool assemble, const Layout& l, void* ws, c
             mo.maps = pass_maps[k];
             mo.map_cap = l.cap;
         }
-        const int rc = launch_merge(c->nw, assemble ? MERGE_ASSEMBLE : MERGE_EXPAND, c->merge_stride, c->m,
+        const int rc = launch_merge(c->nw, assemble ? MERGE_ASSEMBLE : MERGE_EXPAND, assemble ? c->assemble_stride : c->merge_stride, c->m,
                                     k == 0 ? X.keys : prev->keys, k == 0 ? X.blk : prev->blk,
                                     k == 0 ? nullptr : X.keys, k == 0 ? nullptr : X.blk, mws, mo,
                                     k == 0 ? ceiling : nullptr, 0, status, c->num_sms, st);
@@ -567,7 +568,7 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
         // the propagation; S bytes)
         mo.self_flag = at<uint8_t>(ws, l.v_TA);
         if (mo.cap > self_flag_cap(c, l)) mo.cap = self_flag_cap(c, l);
-        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, cur->keys, cur->blk,
+        PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->assemble_stride, c->m, cur->keys, cur->blk,
                                            split ? nbasis.keys : nullptr, split ? nbasis.blk : nullptr, merge_ws(c, l, ws),
                                            mo, &rec->ceiling_hits, split ? 1 : 0, status, c->num_sms, st),
                            "step/assemble");
@@ -747,6 +748,7 @@ int paces_create(const paces_model_desc* d, paces_ctx** out) {
     }
     c->taylor_grid = taylor_max_grid(c->precision == PACES_C64, c->num_sms);
     c->merge_stride = merge_default_stride(c->nw);
+    c->assemble_stride = merge_default_assemble_stride(c->nw);
     c->taylor_bps = 0;
     c->taylor_variant = 1;
     c->test_wait_ns = 0;
@@ -842,6 +844,7 @@ int paces_get_tuning(const paces_ctx* c, paces_tuning* t) {
     if (!c || !t) return PACES_ERR_BADARG;
     std::memset(t, 0, sizeof(*t));
     t->merge_stride = c->merge_stride;
+    t->assemble_stride = c->assemble_stride;
     t->merge_stride_max = merge_stride(c->nw);
     t->merge_stride_min = kMinMergeStride;
     t->taylor_blocks_per_sm = c->taylor_bps;
@@ -855,12 +858,17 @@ int paces_set_tuning(paces_ctx* c, const paces_tuning* t) {
     if (t->merge_stride < kMinMergeStride || t->merge_stride > merge_stride(c->nw) || t->merge_stride % 16)
         return fail(c, PACES_ERR_BADARG, "merge_stride %d: a multiple of 16 in [%d, %d]", t->merge_stride,
                     kMinMergeStride, merge_stride(c->nw));
+    const int as = t->assemble_stride ? t->assemble_stride : t->merge_stride;
+    if (as < kMinMergeStride || as > merge_stride(c->nw) || as % 16)
+        return fail(c, PACES_ERR_BADARG, "assemble_stride %d: 0 or a multiple of 16 in [%d, %d]", t->assemble_stride,
+                    kMinMergeStride, merge_stride(c->nw));
     if (t->taylor_blocks_per_sm < 0 || t->taylor_blocks_per_sm > c->taylor_grid / c->num_sms)
         return fail(c, PACES_ERR_BADARG, "taylor_blocks_per_sm %d: 0..%d", t->taylor_blocks_per_sm,
                     c->taylor_grid / c->num_sms);
     if (t->taylor_variant < 0 || t->taylor_variant > 1)
         return fail(c, PACES_ERR_BADARG, "taylor_variant %d: 0 or 1", t->taylor_variant);
     c->merge_stride = t->merge_stride;
+    c->assemble_stride = as;
     c->taylor_bps = t->taylor_blocks_per_sm;
     c->taylor_variant = t->taylor_variant;
     return PACES_OK;
@@ -953,7 +961,7 @@ int paces_assemble(paces_ctx* c, const paces_basis* in, paces_basis* out, paces_
                            "assemble");
         return PACES_OK;
     }
-    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->merge_stride, c->m, in->keys, in->blk, nullptr, nullptr,
+    PACES_CHECK_LAUNCH(c, launch_merge(c->nw, MERGE_ASSEMBLE, c->assemble_stride, c->m, in->keys, in->blk, nullptr, nullptr,
                                        merge_ws(c, l, ws), mo, dev_ceiling_hits, 0,
                                        c->d_status, c->num_sms, reinterpret_cast<cudaStream_t>(stream)),
                        "assemble");

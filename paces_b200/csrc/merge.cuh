@@ -124,14 +124,19 @@ struct MergeOut {
 // (the images of the rest are already in this expansion's output).
 enum MergeMode : int { MERGE_EXPAND = 0, MERGE_ASSEMBLE = 1, MERGE_EXPAND_SPLIT = 2 };
 
-// Tiling constants by key width.  merge_stride(nw) is the largest stride (the tile's shared
-// memory stays below ~100 KB); any multiple of 16 down to kMinMergeStride works
-// (paces_set_tuning), smaller tiles trading splitter work for more resident blocks.
-// merge_default_stride(nw) is the untuned choice: four blocks per SM for 1-2 key words.
+// Tiling constants by key width.  merge_stride(nw) is the largest stride (a tile's element
+// indices fit 12 bits); any multiple of 16 down to kMinMergeStride works (paces_set_tuning),
+// smaller tiles trading splitter work for more resident blocks.  The untuned choices for one
+// or two key words, measured on the 2^22 chain: stride 160 for the expansions (three blocks
+// per SM), 192 for the assembly.
 __host__ __device__ constexpr int merge_stride(int nw) { return nw <= 2 ? 240 : (nw <= 4 ? 128 : 64); }
 __host__ __device__ constexpr int merge_default_stride(int nw) { return nw <= 2 ? 160 : (nw <= 4 ? 128 : 64); }
+__host__ __device__ constexpr int merge_default_assemble_stride(int nw) { return nw <= 2 ? 192 : (nw <= 4 ? 128 : 64); }
 constexpr int kMinMergeStride = 64;
-constexpr int kMergeGroup = 8;
+// Splitter intervals per tile: 12 measured faster than 8, 10, 14 and 16 on the 2^22 chain
+// (larger tiles spread each thread's merge-path searches over more elements; smaller ones fit
+// more blocks per SM).
+constexpr int kMergeGroup = 12;
 // A tile holds the merged range of kMergeGroup consecutive splitters; every run contributes
 // fewer than (its splitters in the range + 1) * stride elements, so at most
 // (kMergeGroup + kRuns) * stride elements in total.
@@ -144,7 +149,7 @@ inline int64_t merge_split_cap(int64_t in_cap, int nw, int L) {
 }
 inline int64_t merge_tile_cap(int64_t split_cap, int L) { return split_cap / kMergeGroup + L + 8; }
 // Bytes of one tile descriptor (any key width).
-constexpr size_t merge_desc_bytes() { return 256; }
+constexpr size_t merge_desc_bytes() { return 320; }
 
 // X feeds the self run, Y (null: X) the four image runs.  ceiling_out (optional) receives the
 // number of ceiling holes of the up run, or has it added (ceiling_add).  An assembly with

@@ -190,7 +190,7 @@ int remap_static_tile_cap() { return int((kStaticRemapBytes - kStaticHeaderBytes
 
 // The array's device address belongs to a CUDA context: the cache below is keyed on the
 // context current at the call (the device's primary context, or one the host created), read
-// through the driver's cuCtxGetCurrent.
+// through the CUDA driver API's cuCtxGetCurrent.
 using CtxGetCurrentFn = int (*)(void**);
 
 void* current_context() {

@@ -1,4 +1,4 @@
-"""Launch shapes (merge stride, Taylor grid) change speed only: every shape the tuner may
+"""Launch shapes (merge strides, Taylor grid) change speed only: every shape the tuner may
 pick gives bit-identical trajectories, and the tuner returns one of them."""
 
 import numpy as np
@@ -9,11 +9,11 @@ from tests import gpu_helpers
 pytestmark = pytest.mark.gpu
 
 
-def _run(precision, stride=None, bps=None, variant=None, steps=8):
+def _run(precision, stride=None, bps=None, variant=None, steps=8, astride=None):
     from paces_b200 import autotune
     eng = gpu_helpers.engine_for(16, 16, 1.0, cap=1 << 14, precision=precision, periodic=True)
     if stride is not None or bps is not None or variant is not None:
-        autotune.set_tuning(eng, stride, bps, variant)
+        autotune.set_tuning(eng, stride, bps, variant, assemble_stride=astride)
     tr, _ = gpu_helpers.grown_trajectory(eng, 16, 20000)
     recs = [tr.step(evolve=True, dt=0.05) for _ in range(steps)]
     n = tr.basis.count()
@@ -25,8 +25,9 @@ def _run(precision, stride=None, bps=None, variant=None, steps=8):
 @pytest.mark.parametrize("precision", ["c128", "c64"])
 def test_results_do_not_depend_on_launch_shapes(precision):
     ref = _run(precision, variant=0)
-    for stride, bps, variant in ((64, 1, 0), (96, 2, 1), (160, 0, 1), (240, 1, 1), (128, 0, 0)):
-        got = _run(precision, stride, bps, variant)
+    for stride, bps, variant, astride in ((64, 1, 0, None), (96, 2, 1, None), (160, 0, 1, None), (240, 1, 1, None),
+                                          (128, 0, 0, None), (128, 0, 1, 224), (224, 1, 0, 80)):
+        got = _run(precision, stride, bps, variant, astride=astride)
         for a, b in zip(ref[0], got[0]):
             assert (a.n_states, a.final_m, a.converged) == (b.n_states, b.final_m, b.converged)
             assert list(a.n_exc) == list(b.n_exc) and list(a.n_pho) == list(b.n_pho)
@@ -40,9 +41,15 @@ def test_out_of_range_shapes_are_rejected():
     eng = gpu_helpers.engine_for(8, 16, 1.0, cap=1 << 10)
     t = autotune.get_tuning(eng)
     assert t.merge_stride == 160 and t.merge_stride_max == 240 and t.merge_stride_min == 64
+    assert t.assemble_stride == 192
     for bad in (48, 250, 72):
         with pytest.raises(nat.PacesError):
             autotune.set_tuning(eng, merge_stride=bad)
+        with pytest.raises(nat.PacesError):
+            autotune.set_tuning(eng, assemble_stride=bad)
+    autotune.set_tuning(eng, merge_stride=128, assemble_stride=208)
+    t = autotune.get_tuning(eng)
+    assert (t.merge_stride, t.assemble_stride) == (128, 208)
     with pytest.raises(nat.PacesError):
         autotune.set_tuning(eng, taylor_blocks_per_sm=t.taylor_blocks_per_sm_max + 1)
     with pytest.raises(nat.PacesError):
@@ -60,7 +67,9 @@ def test_tuner_picks_an_allowed_shape(tmp_path, monkeypatch):
     t = autotune.get_tuning(eng)
     assert not choice["cached"]
     assert t.merge_stride == choice["merge_stride"] and t.taylor_blocks_per_sm == choice["taylor_blocks_per_sm"]
+    assert t.assemble_stride == choice["assemble_stride"]
     assert set(choice["timings_ms"]["merge_stride"]) == set(autotune.stride_candidates(t))
+    assert set(choice["timings_ms"]["assemble_stride"]) == set(autotune.stride_candidates(t))
     assert t.taylor_variant == choice["taylor_variant"] in (0, 1)
     again = autotune.tune(tr, 0.05, steps=1)
     assert again["cached"] and again["merge_stride"] == choice["merge_stride"]
