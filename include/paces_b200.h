@@ -322,10 +322,9 @@ int paces_remap(paces_ctx *ctx, const paces_basis *old_b, const void *old_psi,
  * through CuPy's pool on every call).  For callers that cannot allocate device memory
  * at all: a host application that owns the whole device through its own memory pool, or
  * a latency-critical loop that must not call cudaMalloc (it can synchronise the device).
- * The scratch is a 256 KiB array in the library's static device memory, held by every
+ * The scratch is a 512 KiB array in the library's static device memory, held by every
  * GPU that loads the library until the process exits; it bounds the two bases together
- * to about 64M states (2048 per remap tile for keys of 1-2 words, 1024 for 3-4, 512
- * beyond).  Capacities beyond that return PACES_ERR_CAPACITY before anything is
+ * to about 64M states (1024 per remap tile for keys of 1-4 words, 512 beyond).  Capacities beyond that return PACES_ERR_CAPACITY before anything is
  * launched.  The first call in each CUDA context (a device's primary context, or one the
  * host made current) looks up the array's device address in that context: make it before
  * any stream capture.  A context destroyed and replaced by a new one at the same handle

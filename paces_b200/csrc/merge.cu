@@ -906,8 +906,10 @@ merge_tile_kernel(ModelDev m, const uint64_t* __restrict__ X, const uint64_t* __
         //    new keys (and H rows, or the new part) at first occurrences, and every element's
         //    index map (its group's output: the running count at its merged position)
         int ceil_local = 0;
-        // q / per as a multiply and shift: exact for q < 2^kEntBits and per <= 13 (the error of the
-        // rounded-up reciprocal stays below 1 / per)
+        // q / per as a multiply and shift: exact for q < 2^kEntBits and per <= 16, which covers
+        // every tile (n <= 4080 over 256 threads); the rounded-up reciprocal's error stays below
+        // 1 / per, and every (q, per) pair in that range was checked
+        static_assert(merge_tmax(merge_stride(1)) <= 16 * kTileThreads, "per <= 16");
         const uint32_t per_inv = (65536u + uint32_t(per) - 1u) / uint32_t(per);
         for (int q = tid; q < n; q += kTileThreads) {
             const int owner = int((uint32_t(q) * per_inv) >> 16);

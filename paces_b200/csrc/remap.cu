@@ -170,16 +170,16 @@ int launch_remap_t(const ModelDev& m, const uint64_t* ok, const int* ob, const v
                    int num_sms, cudaStream_t st) {
     remap_split_kernel<NW><<<grid_for(int64_t(ws.tile_cap) * 2, 256, num_sms * 2), 256, 0, st>>>(m, ok, ob, nk, nb, ws,
                                                                                                 remap_tile(NW), status);
-    remap_tile_kernel<NW, C64><<<grid_for(ws.tile_cap, 1, num_sms * 4), kRThreads, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi,
+    remap_tile_kernel<NW, C64><<<grid_for(ws.tile_cap, 1, num_sms * 8), kRThreads, 0, st>>>(m, ok, ob, opsi, nk, nb, npsi,
                                                                                             ws);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
 // Scratch of the workspace-free remap (paces_remap_noalloc): block tile offsets, the tile
-// counter and two splits per tile, 256 KiB in total.  Every GPU that loads the library
+// counter and two splits per tile, 512 KiB in total.  Every GPU that loads the library
 // holds one copy until the process exits.  Nothing in it has to start at zero: the split
 // kernel rewrites the offsets, the counter and every split it uses.
-constexpr size_t kStaticRemapBytes = size_t(256) << 10;
+constexpr size_t kStaticRemapBytes = size_t(512) << 10;
 constexpr size_t kStaticHeaderBytes = 1024;  // tile_off[kMaxSites+1] and counters
 
 }  // namespace
