@@ -338,15 +338,20 @@ __global__ void __launch_bounds__(256) diag_chunk_kernel(const double* __restric
     }
 }
 
-// The chunk sums in order: norm (square root of the sum of |v|^2) and energy.
-__global__ void diag_final_kernel(const double* __restrict__ chunks, const int* __restrict__ blk, int L, ObsTarget t) {
-    if (threadIdx.x >= 3) return;
+// The chunk sums in a fixed order -- warp q sums value q: lane l the chunks l, l + 32, ... in
+// order, then the butterfly -- into the norm (square root of the sum of |v|^2) and energy.
+__global__ void __launch_bounds__(96) diag_final_kernel(const double* __restrict__ chunks, const int* __restrict__ blk,
+                                                        int L, ObsTarget t) {
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t nch = (diag_groups(blk[L]) + kDiagChunk - 1) / kDiagChunk;
     double acc = 0.0;
-    for (int64_t c = 0; c < nch; ++c) acc = __dadd_rn(acc, chunks[c * 3 + threadIdx.x]);
-    if (threadIdx.x == 0) {
+    for (int64_t c = lane; c < nch; c += 32) acc = __dadd_rn(acc, chunks[c * 3 + q]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+    if (lane != 0) return;
+    if (q == 0) {
         if (t.norm) *t.norm = sqrt(acc);
-    } else if (threadIdx.x == 1) {
+    } else if (q == 1) {
         if (t.energy_re) *t.energy_re = acc;
     } else {
         if (t.energy_im) *t.energy_im = acc;
@@ -619,7 +624,7 @@ int launch_diag_final(const double* diag, const int* blk, int L, int64_t cap, co
     double* chunks = const_cast<double*>(diag) + diag_groups(cap) * 3;
     const int64_t nch = diag_chunks(cap);
     diag_chunk_kernel<<<unsigned(nch > 0 ? nch : 1), 256, 0, st>>>(diag, chunks, blk, L);
-    diag_final_kernel<<<1, 32, 0, st>>>(chunks, blk, L, out);
+    diag_final_kernel<<<1, 96, 0, st>>>(chunks, blk, L, out);
     return cudaGetLastError() == cudaSuccess ? PACES_OK : PACES_ERR_CUDA;
 }
 
