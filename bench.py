@@ -810,7 +810,7 @@ def run_batched(a):
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": a.precision,
             "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "kernel": "taylor_batch_kernel", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": batch_taylor_kernel(batch), "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "algorithmic_bytes": taylor_alg, "launch_ms": taylor_ms},
             "phase_ms": {k: v / n_prof for k, v in phase.items()},
@@ -947,6 +947,15 @@ def run_learned(a):
 # --------------------------------------------------------------------------------------------
 # long chain: N=64 rings with site-energy disorder, realizations batched in one launch
 # --------------------------------------------------------------------------------------------
+def batch_taylor_kernel(batch):
+    """The Taylor kernel a batch step runs: one persistent launch for all, or the single-trajectory
+    kernel per trajectory when every trajectory has room for PACES_BATCH_SINGLE_CAP states."""
+    from paces_b200 import _native as nat
+    if all(t.basis.cap >= nat.BATCH_SINGLE_CAP for t in batch.trajs):
+        return f"taylor_kernel x{len(batch.trajs)}"
+    return "taylor_batch_kernel"
+
+
 def longchain_site_eps(seed, nchain, sigma):
     """Site energies of disorder realization `seed`: numpy.random.default_rng(seed).normal(0, sigma, N)."""
     return np.random.default_rng(seed).normal(0.0, sigma, nchain)
@@ -1070,7 +1079,7 @@ def run_longchain(a):
             "unit": "trajectory-steps/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": a.precision, "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "kernel": "taylor_batch_kernel", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": batch_taylor_kernel(batch), "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "launch_ms": taylor_ms},
             "phase_ms": {k: v / n_prof for k, v in phase.items()}, "compare": compare,

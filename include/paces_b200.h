@@ -80,6 +80,7 @@ enum paces_precision {
 #define PACES_MAX_SITES 128
 /* largest ExpmParams.lanczos_order (Krylov vectors: order + 1) */
 #define PACES_MAX_LANCZOS_ORDER 63
+#define PACES_BATCH_SINGLE_CAP (1 << 25)
 
 typedef struct paces_model_desc {
     int32_t nchain;            /* number of sites L (1D chain), 1 <= L <= 128 */
@@ -429,8 +430,10 @@ int paces_mlp_adam(float *master, float *m1, float *m2, float *grads, int32_t t,
  * The per-trajectory truncation, enlargement, assembly, remap and observables are spread
  * over the batch's own streams (forked from and joined back into `stream`, so the whole
  * call can be captured into one CUDA graph); the Taylor series of every trajectory runs
- * in ONE persistent cooperative launch.  Each trajectory's results are bit-identical to
- * paces_step on the same inputs.  All contexts share one precision and device.  Item
+ * in ONE persistent cooperative launch -- unless every evolving trajectory's new basis
+ * has room for PACES_BATCH_SINGLE_CAP states or more, when each runs through paces_step's
+ * kernel in turn (its schedule streams long row ranges faster).  Each trajectory's results
+ * are bit-identical to paces_step on the same inputs.  All contexts share one precision and device.  Item
  * errors land in each record's status; a non-OK return names the item in
  * paces_batch_last_error. */
 typedef struct paces_batch paces_batch;

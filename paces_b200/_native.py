@@ -32,6 +32,7 @@ C128 = 0
 C64 = 1
 MAX_SITES = 128
 MAX_LANCZOS_ORDER = 63
+BATCH_SINGLE_CAP = 1 << 25  # PACES_BATCH_SINGLE_CAP
 OBS_NORM, OBS_ENERGY, OBS_SITES = 1, 2, 4
 WEIGHT_NONE, WEIGHT_COHERENCE, WEIGHT_NORM, WEIGHT_HAM_ONES = 0, 1, 2, 3
 

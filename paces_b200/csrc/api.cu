@@ -1452,8 +1452,30 @@ int paces_batch_step(paces_batch* b, const paces_batch_item* items, int32_t n, p
     }
     if (!join()) return bfail(PACES_ERR_CUDA, "join: %s", cudaGetErrorString(cudaGetLastError()));
     mark(1);
-    // 2. one persistent launch for every trajectory's Taylor series
-    if (n_evolve > 0) {
+    // 2. the Taylor series.  Batches of large trajectories (every evolving one with room for at
+    //    least kBatchSingleCap states) run them one after the other through the single-trajectory
+    //    kernel, whose bulk-copy schedule streams long row ranges faster (0.85 against 0.61 of
+    //    HBM on 64M-row trajectories); otherwise one persistent launch serves all.  Both give
+    //    the same results.  Test hooks on the batch keep the batched launch.
+    bool per_item = n_evolve > 0 && b->test_wait_ns == 0 && b->test_skip_block < 0;
+    for (int i = 0; i < n && per_item; ++i)
+        if (items[i].params->evolve && plans[i].new_b->cap < kBatchSingleCap) per_item = false;
+    if (per_item) {
+        for (int i = 0; i < n; ++i) {
+            const paces_step_params* prm = items[i].params;
+            if (!prm->evolve) continue;
+            paces_ctx* c = items[i].ctx;
+            StepPlan& p = plans[i];
+            TaylorWs tw = taylor_ws(c, p.l, p.ws);
+            if (diag_in_taylor(prm)) tw.diag = at<double>(p.ws, p.l.diag);
+            TaylorOut o{&p.rec->converged, &p.rec->final_m, &p.rec->c1_plus_c2, &p.rec->term_ratio};
+            if (launch_taylor(c->precision == PACES_C64, with_h(c, p.h), p.new_b->blk, p.h->nbr, p.h->cap, p.h->meta,
+                              p.target, p.new_psi, prm->dt, prm->m_star, prm->tol, tw, o, &p.rec->status, c->num_sms,
+                              c->taylor_bps, c->taylor_variant, st) != PACES_OK)
+                return bfail(PACES_ERR_CUDA, "item %d: Taylor: %s", i, cudaGetErrorString(cudaGetLastError()));
+            launches += 1;
+        }
+    } else if (n_evolve > 0) {
         TaylorBatch& bt = *b->desc;
         bt.n = 0;
         bt.max_m_star = 0;

@@ -141,6 +141,9 @@ int launch_lookahead(bool c64, const ModelDev& m, const int* blk, const int* nbr
 
 // ---- batched Taylor: many trajectories in one persistent launch ---------------------------
 constexpr int kMaxBatch = 128;  // trajectories per launch (the descriptors travel as kernel parameters)
+// batches whose every evolving trajectory has room for at least this many states step their
+// Taylor series through the single-trajectory kernel, one launch per trajectory
+constexpr int64_t kBatchSingleCap = PACES_BATCH_SINGLE_CAP;
 constexpr int kSqrtTable = 260; // sqrt(k) * g for k < 260 (occupations up to 255, plus one)
 // One trajectory of a batched Taylor launch: its H (neighbour table + metadata), vectors,
 // model constants and where its results go.  Field names follow ModelDev so the row

@@ -96,3 +96,38 @@ def test_batch_grows_buffers_and_repeats_the_step():
         for a, b in zip(ra[i], rb[i]):
             _same(a, b)
         assert np.array_equal(sa[i][1], sb[i][1])
+
+
+def test_large_trajectories_step_through_the_single_kernel():
+    """Batches whose every trajectory has room for 2^25 states or more run their Taylor
+    series through the single-trajectory kernel, one launch each (the capacity decides, so
+    small bases in large buffers take that path too): the records and states stay those of
+    stepping each trajectory alone."""
+    from paces_b200.engine import TrajectoryBatch
+    steps = 6
+    specs = SPECS[:2]
+    ra, sa = [], []
+    for big in (False, True):
+        runs = []
+        for nchain, dim, g, w0, m, periodic, initpos, dt, seed in specs:
+            eng = gpu_helpers.engine_for(nchain, dim, g, cap=(1 << 25) if big else (1 << 14), precision="c64",
+                                         periodic=periodic, hbar_omega=w0)
+            tr, _ = gpu_helpers.grown_trajectory(eng, nchain, m, initpos=initpos, dim=dim)
+            runs.append((tr, dt, eng))
+        if big:
+            batch = TrajectoryBatch([tr for tr, _, _ in runs], n_streams=2)
+            recs = [[] for _ in runs]
+            for _ in range(steps):
+                for i, r in enumerate(batch.step(evolve=True, dt=[dt for _, dt, _ in runs])):
+                    recs[i].append(r)
+            rb, sb = recs, [_state(tr) for tr, _, _ in runs]
+            batch.close()
+        else:
+            ra = [[tr.step(evolve=True, dt=dt) for _ in range(steps)] for tr, dt, _ in runs]
+            sa = [_state(tr) for tr, _, _ in runs]
+        for _, _, eng in runs:
+            eng.close()
+    for i in range(len(specs)):
+        for a, b in zip(ra[i], rb[i]):
+            _same(a, b)
+        assert np.array_equal(sa[i][0], sb[i][0]) and np.array_equal(sa[i][1], sb[i][1])
