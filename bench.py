@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--open-chain", action="store_true", help="open boundaries (the reference's only mode)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-serial", action="store_true",
+                    help="e2e: copy the new state out and the next input in one after the other")
     ap.add_argument("--no-learned", action="store_true",
                     help="plain: skip the learned form over the metric's window (training takes ~a minute)")
     ap.add_argument("--ref-steps", type=int, default=3,
@@ -621,63 +623,88 @@ def compare_precisions(a, dev, dist, total=WINDOW_TO, window_from=WINDOW_FROM, l
 
 
 def run_e2e(a, eng, tr, barrier, dist):
+    """The C ABI with the state in pinned host memory: every step copies its input state in
+    and its new state (and record) out.  The new state is the next step's input, so each
+    chunk of it goes back in as soon as it has landed on the host, on a second copy stream:
+    the two directions of the link run at once (--e2e-serial: one after the other)."""
     import torch
     e = eng
     cs = 8 if a.precision == "c64" else 16
     cap = e.cap
-    hk = [torch.empty((cap, e.nw), dtype=torch.int64).pin_memory() for _ in range(2)]
-    hb = [torch.empty(e.L + 1, dtype=torch.int32).pin_memory() for _ in range(2)]
-    hp = [torch.empty(cap, dtype=e.cdtype).pin_memory() for _ in range(2)]
+    hk = torch.empty((cap, e.nw), dtype=torch.int64).pin_memory()
+    hb = torch.empty(e.L + 1, dtype=torch.int32).pin_memory()
+    hp = torch.empty(cap, dtype=e.cdtype).pin_memory()
     # with the look-ahead weighting the state includes the basis' neighbour table
     table = bool(tr.weighting)
     if table:
-        hn = [torch.empty((cap, 4), dtype=torch.int32).pin_memory() for _ in range(2)]
-        hm = [torch.empty(cap, dtype=torch.int32).pin_memory() for _ in range(2)]
-    b, v = tr.basis, tr.psis[tr.cur]
-    n = b.count()
-    hk[0][:n].copy_(b.keys[:n])
-    hb[0].copy_(b.blk)
-    hp[0][:n].copy_(v[:n])
-    if table:
-        hn[0][:n].copy_(tr.h.nbr[:n])
-        hm[0][:n].copy_(tr.h.meta[:n])
-    cur = 0
+        hn = torch.empty((cap, 4), dtype=torch.int32).pin_memory()
+        hm = torch.empty(cap, dtype=torch.int32).pin_memory()
+
+    def pairs(n):
+        """(device, host) views of the current state, whole rows."""
+        b, v = tr.basis, tr.psis[tr.cur]
+        out = [(b.keys[:n], hk[:n]), (b.blk, hb), (v[:n], hp[:n])]
+        if table:
+            out += [(tr.h.nbr[:n], hn[:n]), (tr.h.meta[:n], hm[:n])]
+        return out
+
+    def nbytes(n):
+        return n * (e.nw * 8 + cs) + (e.L + 1) * 4 + (n * 20 if table else 0)
+
+    n = tr.basis.count()
+    for dev, host in pairs(n):
+        host.copy_(dev)
+    main = torch.cuda.current_stream()
+    s_out, s_in = torch.cuda.Stream(), torch.cuda.Stream()
+    chunk = 32 << 20  # bytes per copy
     h2d = d2h = 0
     barrier()
-    stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(a.steps):
-        db, dv = tr.basis, tr.psis[tr.cur]
-        db.keys[:n].copy_(hk[cur][:n], non_blocking=True)
-        db.blk.copy_(hb[cur], non_blocking=True)
-        dv[:n].copy_(hp[cur][:n], non_blocking=True)
-        h2d += n * (e.nw * 8 + cs) + (e.L + 1) * 4
-        if table:
-            tr.h.nbr[:n].copy_(hn[cur][:n], non_blocking=True)
-            tr.h.meta[:n].copy_(hm[cur][:n], non_blocking=True)
-            h2d += n * 20
+    ev0.record(main)
+    for dev, host in pairs(n):  # the first step's input
+        dev.copy_(host, non_blocking=True)
+    h2d += nbytes(n)
+    for k in range(a.steps):
         rec = tr.step(evolve=True, dt=a.dt)
         n = rec.n_states
-        nb, nv = tr.basis, tr.psis[tr.cur]
-        nxt = 1 - cur
-        hk[nxt][:n].copy_(nb.keys[:n], non_blocking=True)
-        hb[nxt].copy_(nb.blk, non_blocking=True)
-        hp[nxt][:n].copy_(nv[:n], non_blocking=True)
-        d2h += n * (e.nw * 8 + cs) + (e.L + 1) * 4 + ctypes.sizeof(type(rec))
-        if table:
-            hn[nxt][:n].copy_(tr.h.nbr[:n], non_blocking=True)
-            hm[nxt][:n].copy_(tr.h.meta[:n], non_blocking=True)
-            d2h += n * 20
-        torch.cuda.current_stream().synchronize()
-        cur = nxt
-    ev1.record(stream)
+        d2h += nbytes(n) + ctypes.sizeof(type(rec))
+        nxt = k + 1 < a.steps  # the new state goes back in as the next step's input
+        if a.e2e_serial:
+            for dev, host in pairs(n):
+                host.copy_(dev, non_blocking=True)
+            if nxt:
+                for dev, host in pairs(n):
+                    dev.copy_(host, non_blocking=True)
+        else:
+            s_out.wait_stream(main)
+            s_in.wait_stream(main)
+            for dev, host in pairs(n):
+                if dev.shape[0] == 0:
+                    continue
+                row_bytes = dev.element_size() * (dev.shape[1] if dev.dim() > 1 else 1)
+                rows = max(1, chunk // row_bytes)
+                for r0 in range(0, dev.shape[0], rows):
+                    with torch.cuda.stream(s_out):
+                        host[r0:r0 + rows].copy_(dev[r0:r0 + rows], non_blocking=True)
+                    if nxt:
+                        landed = torch.cuda.Event()
+                        landed.record(s_out)
+                        s_in.wait_event(landed)
+                        with torch.cuda.stream(s_in):
+                            dev[r0:r0 + rows].copy_(host[r0:r0 + rows], non_blocking=True)
+            main.wait_stream(s_out)
+            main.wait_stream(s_in)
+        if nxt:
+            h2d += nbytes(n)
+        main.synchronize()  # the host holds the new state
+    ev1.record(main)
     ev1.synchronize()
     ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     world = 1 if dist is None else dist.get_world_size()
     return {"value": a.steps * world / (ms / 1e3), "unit": "time-steps/s",
             "h2d_bytes_per_step": h2d // a.steps, "d2h_bytes_per_step": d2h // a.steps,
-            "api": "paces_step (C ABI) with the state in pinned host memory"}
+            "api": "paces_step (C ABI) with the state in pinned host memory"
+                   + ("" if a.e2e_serial else "; each step's new state streams out and back in on two copy streams")}
 
 # --------------------------------------------------------------------------------------------
 # batched workload: independent trajectories advanced together
