@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-serial", action="store_true",
                     help="e2e: copy the new state out and the next input in one after the other")
+    ap.add_argument("--e2e-chunk-mb", type=int, default=32, help="e2e: MB per copy of the streamed state")
     ap.add_argument("--no-learned", action="store_true",
                     help="plain: skip the learned form over the metric's window (training takes ~a minute)")
     ap.add_argument("--ref-steps", type=int, default=3,
@@ -656,7 +657,7 @@ def run_e2e(a, eng, tr, barrier, dist):
         host.copy_(dev)
     main = torch.cuda.current_stream()
     s_out, s_in = torch.cuda.Stream(), torch.cuda.Stream()
-    chunk = 32 << 20  # bytes per copy
+    chunk = max(1, a.e2e_chunk_mb) << 20  # bytes per copy
     h2d = d2h = 0
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
