@@ -436,7 +436,14 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
             }
         }
         // pass 2: ranks among the kept states, block starts, copies; four slices of 32 per
-        // round, their key loads in flight together
+        // round, their key loads in flight together.  Exciton blocks start in few of the
+        // warp's segments: a warp whose segment holds no block start skips their search.
+        bool starts = false;
+        for (int p = lane; p < L; p += 32) {
+            const int64_t b0 = s_blk[p];
+            starts |= b0 >= i0 + q_lo && b0 < i0 + q_hi && b0 < s_blk[p + 1];
+        }
+        starts = __any_sync(0xffffffffu, starts);
         constexpr int kU = 4;
         for (int qb = q_lo; qb < q_hi; qb += 32 * kU) {
             bool keep[kU];
@@ -468,7 +475,7 @@ __global__ void __launch_bounds__(256) trunc_write_kernel(ModelDev m, const uint
                     H += __popc(bh);
                 }
                 // block starts among these 32 states: the number of kept states before them
-                for (int p0 = 0; p0 < L; p0 += 32) {
+                for (int p0 = 0; starts && p0 < L; p0 += 32) {
                     const int p = p0 + lane;
                     const int e = p < L ? int(int64_t(s_blk[p]) - (i0 + q0)) : -1;
                     const long long o = __shfl_sync(0xffffffffu, out[u], (e >= 0 && e < 32) ? e : 0);
