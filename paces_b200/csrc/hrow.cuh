@@ -85,7 +85,7 @@ __device__ __forceinline__ float2 h_row_c64_nb(const P& m, const float* sq, floa
     const float d = float(diag_value(m, meta));
     const float ja = nb.x >= 0 ? J : 0.f, jb = nb.y >= 0 ? J : 0.f;
     const float cd = nb.z >= 0 ? sq[n] : 0.f, cu = nb.w >= 0 ? sq[n + 1] : 0.f;
-    float2 y = make_float2(d * xr.x, d * xr.y);
+    float2 y = make_float2(__fmul_rn(d, xr.x), __fmul_rn(d, xr.y));
     y.x = fmaf(ja, xa.x, y.x);
     y.y = fmaf(ja, xa.y, y.y);
     y.x = fmaf(jb, xb.x, y.x);
@@ -152,7 +152,7 @@ __device__ __forceinline__ float2 h_row_c64_x(const ModelDev& m, const float* sq
                                               float2 xr, const float2* __restrict__ x) {
     const int n = int((meta >> 8) & 0xffu);
     const float d = float(diag_value(m, meta));
-    float2 y = make_float2(d * xr.x, d * xr.y);
+    float2 y = make_float2(__fmul_rn(d, xr.x), __fmul_rn(d, xr.y));
     for (int t = 0; t < 2; ++t) {
         const float Jt = float(t == 0 ? m.J : m.J2);
         for (int e = 0; e < m.hop_n[t]; ++e) {

@@ -57,28 +57,40 @@ int taylor_max_grid(bool c64, int num_sms);
 
 // ---- diagnostics of the input state, from the first Taylor sweep ---------------------------
 // The first sweep of the series forms (H v)_r for every row, so the post-adaptation norm and
-// energy <v|H|v> come out of it: each warp folds the rows of one 32-row group (row 32 g + l on
-// lane l, in every kernel and schedule) with a fixed butterfly, and diag_final sums the groups
-// in a fixed order.  The result depends on the rows only -- not on the grid, the row schedule
-// or whether the trajectory runs alone or in a batch.
-constexpr int kDiagGroup = 32;
+// energy <v|H|v> come out of it: each warp folds the rows of one 64-row group (rows 64 g + l and
+// 64 g + 32 + l on lane l, in every kernel and schedule: the lane adds its two rows, then a fixed
+// butterfly), and diag_final sums the groups in a fixed order.  The result depends on the rows
+// only -- not on the grid, the row schedule or whether the trajectory runs alone or in a batch.
+constexpr int kDiagGroup = 64;
 constexpr int kDiagChunk = 2048;  // groups per block of the first reduction
 __host__ __device__ inline int64_t diag_groups(int64_t rows) { return (rows + kDiagGroup - 1) / kDiagGroup; }
 inline int64_t diag_chunks(int64_t rows) { return (diag_groups(rows) + kDiagChunk - 1) / kDiagChunk; }
 // doubles of a diag buffer for up to `cap` rows: the group sums, then the chunk sums
 inline size_t diag_doubles(int64_t cap) { return size_t(diag_groups(cap) + diag_chunks(cap)) * 3; }
 
-// Called by all 32 lanes of a warp for the group whose row 32 g + lane this lane holds
-// (valid: the row exists; a, y: v_r and (H v)_r).
+// |v_r|^2, Re and Im of conj(v_r) (H v)_r of one row (zero when it does not exist).
 template <typename C>
-__device__ __forceinline__ void diag_group(double* __restrict__ diag, int64_t g, bool valid, const C& a, const C& y) {
-    double n2 = 0.0, er = 0.0, ei = 0.0;
+__device__ __forceinline__ void diag_row(bool valid, const C& a, const C& y, double& n2, double& er, double& ei) {
+    n2 = er = ei = 0.0;
     if (valid) {
         const double ar = double(a.x), ai = double(a.y), yr = double(y.x), yi = double(y.y);
         n2 = fma(ar, ar, __dmul_rn(ai, ai));
         er = fma(ar, yr, __dmul_rn(ai, yi));
         ei = fma(ar, yi, -__dmul_rn(ai, yr));
     }
+}
+
+// Called by all 32 lanes of a warp for group g, whose rows 64 g + lane (valid0: it exists; a0,
+// y0: v_r and (H v)_r) and 64 g + 32 + lane (valid1, a1, y1) this lane holds.
+template <typename C>
+__device__ __forceinline__ void diag_group(double* __restrict__ diag, int64_t g, bool valid0, const C& a0,
+                                           const C& y0, bool valid1, const C& a1, const C& y1) {
+    double n2, er, ei, n2b, erb, eib;
+    diag_row(valid0, a0, y0, n2, er, ei);
+    diag_row(valid1, a1, y1, n2b, erb, eib);
+    n2 = __dadd_rn(n2, n2b);
+    er = __dadd_rn(er, erb);
+    ei = __dadd_rn(ei, eib);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         n2 = __dadd_rn(n2, __shfl_xor_sync(0xffffffffu, n2, o));

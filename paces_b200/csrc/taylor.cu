@@ -113,17 +113,19 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
         auto finish = [&](int64_t r, const C& y, const C& a) {
             C t, rr;
             if constexpr (C64) {
-                t = make_float2(c * y.y, -(c * y.x));
-                rr = make_float2(a.x + t.x, a.y + t.y);
-                mx[0] = fmax(mx[0], double(fmaf(t.x, t.x, t.y * t.y)));
-                mx[1] = fmax(mx[1], double(fmaf(rr.x, rr.x, rr.y * rr.y)));
-                if (j == 0) mx[2] = fmax(mx[2], double(fmaf(a.x, a.x, a.y * a.y)));
+                // separate roundings (no contraction into an FMA): every kernel and schedule that
+                // runs these rows -- direct, bulk, batched -- must round them alike
+                t = make_float2(__fmul_rn(c, y.y), -__fmul_rn(c, y.x));
+                rr = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
+                mx[0] = fmax(mx[0], double(fmaf(t.x, t.x, __fmul_rn(t.y, t.y))));
+                mx[1] = fmax(mx[1], double(fmaf(rr.x, rr.x, __fmul_rn(rr.y, rr.y))));
+                if (j == 0) mx[2] = fmax(mx[2], double(fmaf(a.x, a.x, __fmul_rn(a.y, a.y))));
             } else {
                 t = make_double2(__dmul_rn(cd, y.y), -__dmul_rn(cd, y.x));
                 rr = make_double2(__dadd_rn(a.x, t.x), __dadd_rn(a.y, t.y));
-                mx[0] = fmax(mx[0], fma(t.x, t.x, t.y * t.y));
-                mx[1] = fmax(mx[1], fma(rr.x, rr.x, rr.y * rr.y));
-                if (j == 0) mx[2] = fmax(mx[2], fma(a.x, a.x, a.y * a.y));
+                mx[0] = fmax(mx[0], fma(t.x, t.x, __dmul_rn(t.y, t.y)));
+                mx[1] = fmax(mx[1], fma(rr.x, rr.x, __dmul_rn(rr.y, rr.y)));
+                if (j == 0) mx[2] = fmax(mx[2], fma(a.x, a.x, __dmul_rn(a.y, a.y)));
             }
             if (!(isfinite(double(rr.x)) && isfinite(double(rr.y)))) mx[3] = 1.0;
             dst[r] = t;
@@ -144,11 +146,12 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                 }
                 if (r < S) finish(r, hrow(r), rin[r]);
             } else {
-                // the same rows, in a loop every lane of a warp runs together (warp-uniform
-                // bounds), so that each warp folds its 32-row groups
+                // every row once, in 64-row units per warp (rows u + lane and u + 32 + lane, a
+                // warp-uniform loop), so that each warp folds its 64-row groups
                 const int lane = threadIdx.x & 31;
-                for (int64_t rb = int64_t(blockIdx.x) * kTThreads + (threadIdx.x & ~31); rb < S; rb += 2 * stride) {
-                    const int64_t r0 = rb + lane, r1 = rb + stride + lane;
+                const int64_t ustride = int64_t(gridDim.x) * kTWarps * kDiagGroup;
+                for (int64_t ub = (int64_t(blockIdx.x) * kTWarps + wid) * kDiagGroup; ub < S; ub += ustride) {
+                    const int64_t r0 = ub + lane, r1 = ub + 32 + lane;
                     const bool v0 = r0 < S, v1 = r1 < S;
                     C y0{}, y1{}, a0{}, a1{};
                     if (v0) {
@@ -161,8 +164,7 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                     }
                     if (v0) finish(r0, y0, a0);
                     if (v1) finish(r1, y1, a1);
-                    diag_group(ws.diag, rb >> 5, v0, a0, y0);
-                    if (rb + stride < S) diag_group(ws.diag, (rb + stride) >> 5, v1, a1, y1);
+                    diag_group(ws.diag, ub / kDiagGroup, v0, a0, y0, v1, a1, y1);
                 }
             }
         } else {
@@ -194,7 +196,10 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                 const int64_t cn = c + gridDim.x;
                 if (threadIdx.x == 0 && cn < nch && full(cn)) issue(cn, b ^ 1);
                 const int64_t r0 = c * kChunk;
-                const int t0 = threadIdx.x, t1 = threadIdx.x + kTThreads;
+                // chunk rows of this thread: t and t + 256, or in the first sweep with the
+                // diagnostics 64 w + lane and 64 w + 32 + lane (warp w's 64-row group)
+                const int t0 = diag ? kDiagGroup * wid + (threadIdx.x & 31) : threadIdx.x;
+                const int t1 = diag ? t0 + 32 : threadIdx.x + kTThreads;
                 if (full(c)) {
                     if (!tc::mbar_wait(tc::smem_addr(&s_mbar[b]), (parity >> b) & 1u)) s_abort = 1;
                     parity ^= 1u << b;
@@ -222,10 +227,7 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                     }
                     finish(r0 + t0, y0, srin[t0]);
                     finish(r0 + t1, y1, srin[t1]);
-                    if (diag) {
-                        diag_group(ws.diag, (r0 >> 5) + wid, true, srin[t0], y0);
-                        diag_group(ws.diag, (r0 >> 5) + kTWarps + wid, true, srin[t1], y1);
-                    }
+                    if (diag) diag_group(ws.diag, r0 / kDiagGroup + wid, true, srin[t0], y0, true, srin[t1], y1);
                 } else {
                     // the last, partial chunk: direct loads
                     const bool v0 = r0 + t0 < S, v1 = r0 + t1 < S;
@@ -240,10 +242,8 @@ taylor_kernel(ModelDev m, const int* __restrict__ blk, const int* __restrict__ n
                         a1 = rin[r0 + t1];
                         finish(r0 + t1, y1, a1);
                     }
-                    if (diag) {  // groups with at least one row (warp-uniform)
-                        if (r0 + 32 * wid < S) diag_group(ws.diag, (r0 >> 5) + wid, v0, a0, y0);
-                        if (r0 + kTThreads + 32 * wid < S) diag_group(ws.diag, (r0 >> 5) + kTWarps + wid, v1, a1, y1);
-                    }
+                    if (diag && r0 + kDiagGroup * wid < S)  // groups with at least one row (warp-uniform)
+                        diag_group(ws.diag, r0 / kDiagGroup + wid, v0, a0, y0, v1, a1, y1);
                 }
                 __syncthreads();  // the buffer is free for the copy issued next iteration
                 if (s_abort) break;

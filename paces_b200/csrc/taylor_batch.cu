@@ -12,9 +12,9 @@
 // lane, all loads before the stores), assigned grid-stride so the rows of the trajectories
 // still running are spread over every SM.  Lanes keep running maxima of |term|^2, |res|^2,
 // |v|^2 and a non-finite flag for the warp's current trajectory and fold them into shared
-// memory only when the trajectory changes.  Row 64 u + l of a trajectory sits on lane l of
-// its unit, as in the single-trajectory kernel's 32-row groups, so the first sweep folds the
-// input's diagnostics (diag_group) exactly as that kernel does.  Blocks then fold into
+// memory only when the trajectory changes.  Rows 64 u + l and 64 u + 32 + l of a trajectory
+// sit on lane l of its unit, as in the single-trajectory kernel's 64-row groups, so the first
+// sweep folds the input's diagnostics (diag_group) exactly as that kernel does.  Blocks then fold into
 // per-trajectory global maxima with
 // atomicMax on the fp64 bit patterns (non-negative doubles order like their bits), which
 // is exact and order-independent, so each trajectory's stop decision -- taken by every
@@ -104,17 +104,18 @@ taylor_batch_kernel(const __grid_constant__ TaylorBatch bt, TaylorBatchWs ws) {
             C t, rr;
             if constexpr (C64) {
                 const R c = R(cd);
-                t = make_float2(c * y.y, -(c * y.x));
-                rr = make_float2(a.x + t.x, a.y + t.y);
-                mx[0] = fmax(mx[0], double(fmaf(t.x, t.x, t.y * t.y)));
-                mx[1] = fmax(mx[1], double(fmaf(rr.x, rr.x, rr.y * rr.y)));
-                if (first) mx[2] = fmax(mx[2], double(fmaf(a.x, a.x, a.y * a.y)));
+                // separate roundings, as the single-trajectory kernel (no contraction into an FMA)
+                t = make_float2(__fmul_rn(c, y.y), -__fmul_rn(c, y.x));
+                rr = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
+                mx[0] = fmax(mx[0], double(fmaf(t.x, t.x, __fmul_rn(t.y, t.y))));
+                mx[1] = fmax(mx[1], double(fmaf(rr.x, rr.x, __fmul_rn(rr.y, rr.y))));
+                if (first) mx[2] = fmax(mx[2], double(fmaf(a.x, a.x, __fmul_rn(a.y, a.y))));
             } else {
                 t = make_double2(__dmul_rn(cd, y.y), -__dmul_rn(cd, y.x));
                 rr = make_double2(__dadd_rn(a.x, t.x), __dadd_rn(a.y, t.y));
-                mx[0] = fmax(mx[0], fma(t.x, t.x, t.y * t.y));
-                mx[1] = fmax(mx[1], fma(rr.x, rr.x, rr.y * rr.y));
-                if (first) mx[2] = fmax(mx[2], fma(a.x, a.x, a.y * a.y));
+                mx[0] = fmax(mx[0], fma(t.x, t.x, __dmul_rn(t.y, t.y)));
+                mx[1] = fmax(mx[1], fma(rr.x, rr.x, __dmul_rn(rr.y, rr.y)));
+                if (first) mx[2] = fmax(mx[2], fma(a.x, a.x, __dmul_rn(a.y, a.y)));
             }
             if (!(isfinite(double(rr.x)) && isfinite(double(rr.y)))) mx[3] = 1.0;
             dst[l] = t;
@@ -148,14 +149,13 @@ taylor_batch_kernel(const __grid_constant__ TaylorBatch bt, TaylorBatchWs ws) {
             const long long l0 = base - s_off[it] + lane, l1 = l0 + 32;
             const long long nr = s_rows[it];
             if (first && I.diag) {
-                // the first sweep with the diagnostics (groups with at least one row; warp-uniform)
+                // the first sweep with the diagnostics: the unit is one 64-row group (it holds at
+                // least one row, since the padding is shorter than a unit)
                 const bool v0 = l0 < nr, v1 = l1 < nr;
                 C y0{}, a0{}, y1{}, a1{};
                 if (v0) load_row(I, l0, y0, a0);
                 if (v1) load_row(I, l1, y1, a1);
-                const long long g = (base - s_off[it]) >> 5;
-                if (g * 32 < nr) diag_group(I.diag, g, v0, a0, y0);
-                if ((g + 1) * 32 < nr) diag_group(I.diag, g + 1, v1, a1, y1);
+                diag_group(I.diag, (base - s_off[it]) / kDiagGroup, v0, a0, y0, v1, a1, y1);
                 if (v0) finish_row(I, cd, l0, y0, a0, cm);
                 if (v1) finish_row(I, cd, l1, y1, a1, cm);
             } else if (l1 < nr) {
