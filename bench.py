@@ -1063,6 +1063,7 @@ def run_longchain(a):
             phase[k] += v
     launches_per_step = (batch.kernel_launches() - l0) / n_prof
     batch.set_profiling(False)
+    taylor_kernel = batch_taylor_kernel(batch)  # before the trajectories are released
     batch.close()
     for t in trajs:
         t.eng.close()
@@ -1107,7 +1108,7 @@ def run_longchain(a):
             "unit": "trajectory-steps/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": a.precision, "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "kernel": batch_taylor_kernel(batch), "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": taylor_kernel, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "launch_ms": taylor_ms},
             "phase_ms": {k: v / n_prof for k, v in phase.items()}, "compare": compare,
