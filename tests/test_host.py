@@ -112,3 +112,20 @@ def test_replica_timing_takes_the_max_over_ranks():
     port = _free_port()
     mp.start_processes(_replica_worker, args=(2, port, out), nprocs=2, start_method="spawn")
     assert dict(out) == {0: 11.0, 1: 11.0}
+
+
+def test_bench_names_the_batch_taylor_kernel():
+    """bench.py's roofline label follows paces_batch_step's choice: the single-trajectory
+    kernel per trajectory when every trajectory has room for PACES_BATCH_SINGLE_CAP states."""
+    import types
+    import bench
+    from paces_b200 import _native as nat
+    def batch(*caps):
+        return types.SimpleNamespace(trajs=[types.SimpleNamespace(basis=types.SimpleNamespace(cap=c)) for c in caps])
+    big = nat.BATCH_SINGLE_CAP
+    assert bench.batch_taylor_kernel(batch(big, big, 2 * big, big)) == "taylor_kernel x4"
+    assert bench.batch_taylor_kernel(batch(big, big - 1)) == "taylor_batch_kernel"
+    assert bench.batch_taylor_kernel(batch(1 << 14)) == "taylor_batch_kernel"
+    header = open(os.path.join(os.path.dirname(__file__), "..", "include", "paces_b200.h")).read()
+    m = re.search(r"#define PACES_BATCH_SINGLE_CAP \(1 << (\d+)\)", header)
+    assert m and (1 << int(m.group(1))) == big
