@@ -627,7 +627,10 @@ def run_e2e(a, eng, tr, barrier, dist):
     """The C ABI with the state in pinned host memory: every step copies its input state in
     and its new state (and record) out.  The new state is the next step's input, so each
     chunk of it goes back in as soon as it has landed on the host, on a second copy stream:
-    the two directions of the link run at once (--e2e-serial: one after the other)."""
+    the two directions of the link run at once.  The new basis (and table) starts out as soon
+    as the step has built it (paces_step_params.basis_ready), while the remap, the
+    propagation and the observables run; the amplitudes follow when the step ends.
+    --e2e-serial: one copy after the other, after the step."""
     import torch
     e = eng
     cs = 8 if a.precision == "c64" else 16
@@ -641,13 +644,19 @@ def run_e2e(a, eng, tr, barrier, dist):
         hn = torch.empty((cap, 4), dtype=torch.int32).pin_memory()
         hm = torch.empty(cap, dtype=torch.int32).pin_memory()
 
-    def pairs(n):
-        """(device, host) views of the current state, whole rows."""
-        b, v = tr.basis, tr.psis[tr.cur]
-        out = [(b.keys[:n], hk[:n]), (b.blk, hb), (v[:n], hp[:n])]
+    def basis_pairs(n, b=None, h=None):
+        """(device, host) views of the basis part of the state (keys, table), whole rows;
+        the block offsets travel on their own."""
+        b = tr.basis if b is None else b
+        h = tr.h if h is None else h
+        out = [(b.keys[:n], hk[:n])]
         if table:
-            out += [(tr.h.nbr[:n], hn[:n]), (tr.h.meta[:n], hm[:n])]
+            out += [(h.nbr[:n], hn[:n]), (h.meta[:n], hm[:n])]
         return out
+
+    def pairs(n):
+        """(device, host) views of the whole current state."""
+        return [(tr.basis.blk, hb), (tr.psis[tr.cur][:n], hp[:n])] + basis_pairs(n)
 
     def nbytes(n):
         return n * (e.nw * 8 + cs) + (e.L + 1) * 4 + (n * 20 if table else 0)
@@ -658,6 +667,28 @@ def run_e2e(a, eng, tr, barrier, dist):
     main = torch.cuda.current_stream()
     s_out, s_in = torch.cuda.Stream(), torch.cuda.Stream()
     chunk = max(1, a.e2e_chunk_mb) << 20  # bytes per copy
+    basis_ready = torch.cuda.Event()
+    basis_ready.record(main)  # creates the event the steps record
+
+    def stream_out_in(dev, host, back, after=None):
+        """dev -> host in chunks on s_out; with `back`, each chunk returns to dev on s_in
+        once it has landed (and, with `after`, not before that event)."""
+        if dev.shape[0] == 0:
+            return
+        row_bytes = dev.element_size() * (dev.shape[1] if dev.dim() > 1 else 1)
+        rows = max(1, chunk // row_bytes)
+        if back and after is not None:
+            s_in.wait_event(after)
+        for r0 in range(0, dev.shape[0], rows):
+            with torch.cuda.stream(s_out):
+                host[r0:r0 + rows].copy_(dev[r0:r0 + rows], non_blocking=True)
+            if back:
+                landed = torch.cuda.Event()
+                landed.record(s_out)
+                s_in.wait_event(landed)
+                with torch.cuda.stream(s_in):
+                    dev[r0:r0 + rows].copy_(host[r0:r0 + rows], non_blocking=True)
+
     h2d = d2h = 0
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -666,35 +697,48 @@ def run_e2e(a, eng, tr, barrier, dist):
         dev.copy_(host, non_blocking=True)
     h2d += nbytes(n)
     for k in range(a.steps):
-        rec = tr.step(evolve=True, dt=a.dt)
-        n = rec.n_states
-        d2h += nbytes(n) + ctypes.sizeof(type(rec))
         nxt = k + 1 < a.steps  # the new state goes back in as the next step's input
         if a.e2e_serial:
+            rec = tr.step(evolve=True, dt=a.dt)
+            n = rec.n_states
             for dev, host in pairs(n):
                 host.copy_(dev, non_blocking=True)
             if nxt:
                 for dev, host in pairs(n):
                     dev.copy_(host, non_blocking=True)
         else:
-            s_out.wait_stream(main)
-            s_in.wait_stream(main)
-            for dev, host in pairs(n):
-                if dev.shape[0] == 0:
-                    continue
-                row_bytes = dev.element_size() * (dev.shape[1] if dev.dim() > 1 else 1)
-                rows = max(1, chunk // row_bytes)
-                for r0 in range(0, dev.shape[0], rows):
-                    with torch.cuda.stream(s_out):
-                        host[r0:r0 + rows].copy_(dev[r0:r0 + rows], non_blocking=True)
-                    if nxt:
-                        landed = torch.cuda.Event()
-                        landed.record(s_out)
-                        s_in.wait_event(landed)
-                        with torch.cuda.stream(s_in):
-                            dev[r0:r0 + rows].copy_(host[r0:r0 + rows], non_blocking=True)
+            nbas, npsi, nh = tr.step_begin(a.dt, basis_ready)
+            done = torch.cuda.Event()
+            done.record(main)
+            # the new basis' size, as soon as the basis is final
+            s_out.wait_event(basis_ready)
+            with torch.cuda.stream(s_out):
+                hb.copy_(nbas.blk, non_blocking=True)
+            sized = torch.cuda.Event()
+            sized.record(s_out)
+            sized.synchronize()
+            n = int(hb[e.L])
+            # the basis goes out while the step runs on; nothing goes back in before the
+            # step has ended (its observables read the keys)
+            if nxt:
+                s_in.wait_event(done)
+                with torch.cuda.stream(s_in):
+                    nbas.blk.copy_(hb, non_blocking=True)
+            for dev, host in basis_pairs(n, nbas, nh):
+                stream_out_in(dev, host, nxt)
+            s_out.wait_event(done)
+            stream_out_in(npsi[:n], hp[:n], nxt)
             main.wait_stream(s_out)
             main.wait_stream(s_in)
+            rec, repeated = tr.step_end()
+            if repeated:  # a capacity overflow ran the step again in other buffers
+                n = rec.n_states
+                for dev, host in pairs(n):
+                    host.copy_(dev, non_blocking=True)
+                if nxt:
+                    for dev, host in pairs(n):
+                        dev.copy_(host, non_blocking=True)
+        d2h += nbytes(n) + ctypes.sizeof(type(rec))
         if nxt:
             h2d += nbytes(n)
         main.synchronize()  # the host holds the new state
@@ -705,7 +749,8 @@ def run_e2e(a, eng, tr, barrier, dist):
     return {"value": a.steps * world / (ms / 1e3), "unit": "time-steps/s",
             "h2d_bytes_per_step": h2d // a.steps, "d2h_bytes_per_step": d2h // a.steps,
             "api": "paces_step (C ABI) with the state in pinned host memory"
-                   + ("" if a.e2e_serial else "; each step's new state streams out and back in on two copy streams")}
+                   + ("" if a.e2e_serial else "; the new basis streams out from the moment the step has built it, "
+                      "the amplitudes when it ends, and each chunk goes back in on a second copy stream")}
 
 # --------------------------------------------------------------------------------------------
 # batched workload: independent trajectories advanced together

@@ -165,6 +165,13 @@ typedef struct paces_step_params {
     int32_t reserved1;
     void *krylov;
     size_t krylov_bytes;
+    /* NULL, or a CUDA event (cudaEvent_t) that the step records on its stream as soon as
+     * new_b (keys, block offsets) and h are final, after the assembly and before the remap
+     * and the propagation, which no longer write them.  Another stream that waits on it can
+     * copy the new basis to the host while the propagation runs.  Under stream capture
+     * the record is an external event node, recorded at every replay.  A step that fails
+     * before that point does not record it. */
+    void *basis_ready;
 } paces_step_params;
 
 /* Written on the device by paces_step; the caller copies it back (one transfer per step). */

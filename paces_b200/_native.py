@@ -90,6 +90,7 @@ class StepParams(ctypes.Structure):
         ("reserved1", ctypes.c_int32),
         ("krylov", ctypes.c_void_p),
         ("krylov_bytes", ctypes.c_size_t),
+        ("basis_ready", ctypes.c_void_p),
     ]
 
 

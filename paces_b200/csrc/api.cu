@@ -579,6 +579,15 @@ int step_front(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
                                "step/neighbours");
     }
     mark(3);
+    // the new basis and its table are final: a caller may start copying them out
+    if (prm->basis_ready) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess ||
+            cudaEventRecordWithFlags(static_cast<cudaEvent_t>(prm->basis_ready), st,
+                                     cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                         : cudaEventRecordDefault) != cudaSuccess)
+            return cuda_fail(c, "step/basis_ready");
+    }
     // 4. amplitudes into the new basis
     PACES_CHECK_LAUNCH(c, launch_remap(c->nw, c64, c->m, p.old_b->keys, p.old_b->blk, p.old_psi, p.new_b->keys,
                                        p.new_b->blk, p.target, remap_ws(l, ws), status, c->num_sms, st),
@@ -638,7 +647,7 @@ int step_back(paces_ctx* c, StepPlan& p, cudaStream_t st, bool marks) {
 
 extern "C" {
 
-int paces_version(void) { return 10200; }
+int paces_version(void) { return 10300; }
 
 int paces_hop_channels(const paces_ctx* c) { return c ? c->m.nhop : 0; }
 

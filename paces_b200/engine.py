@@ -724,6 +724,46 @@ class Trajectory:
         self.last = rec
         return rec
 
+    def step_begin(self, dt, basis_ready):
+        """Enqueue one evolving step on the current stream without waiting for it (no CUDA
+        graph).  `basis_ready` is a torch.cuda.Event that has been recorded at least once
+        (so that its CUDA event exists): the step records it again as soon as the new
+        basis and its neighbour table are final, before the remap and the propagation,
+        which only read them.  Returns the new slot's (basis, amplitudes, table); the
+        amplitudes are final when the step is.  step_end() completes the step."""
+        if getattr(self, "_pending", None) is not None:
+            raise RuntimeError("step_begin: the previous step_begin has not been ended")
+        if not basis_ready.cuda_event:
+            raise ValueError("step_begin: record basis_ready once before passing it")
+        nxt = 1 - self.cur
+        prm = self.params(True, dt)
+        prm.basis_ready = basis_ready.cuda_event
+        self.eng.step(self.bases[self.cur], self.psis[self.cur], self.bases[nxt], self.psis[nxt], self.hs[nxt], prm,
+                      sync=False)
+        self._pending = (nxt, float(dt))
+        return self.bases[nxt], self.psis[nxt], self.hs[nxt]
+
+    def step_end(self):
+        """Wait for the step of step_begin and return (record, repeated).  On a capacity
+        overflow the buffers grow and the step runs again through step() (its inputs are
+        read only, so the repeat is exact); repeated is then True, the new state lives in
+        other buffers and what was copied out after basis_ready is void."""
+        if getattr(self, "_pending", None) is None:
+            raise RuntimeError("step_end without step_begin")
+        nxt, dt = self._pending
+        self._pending = None
+        rec = self.eng.read_record()
+        if rec.status == nat.ERR_CAPACITY:
+            self._regrow()
+            return self.step(evolve=True, dt=dt), True
+        if rec.status != nat.PACES_OK:
+            raise nat.PacesError(rec.status, "paces_step")
+        self.cur = nxt
+        self.step_index += 1
+        self._h_valid = True
+        self.last = rec
+        return rec, False
+
 
 class TrajectoryBatch:
     """Independent trajectories (each its own Engine: model, key width, dt, maxstates)

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 def test_workspace_query_without_a_device():
     from paces_b200 import _native
     lib = _native.load()
-    assert lib.paces_version() == 10200
+    assert lib.paces_version() == 10300
     assert lib.paces_create(None, None) == 5  # PACES_ERR_BADARG, no device touched
 
 
@@ -129,3 +129,35 @@ def test_bench_names_the_batch_taylor_kernel():
     header = open(os.path.join(os.path.dirname(__file__), "..", "include", "paces_b200.h")).read()
     m = re.search(r"#define PACES_BATCH_SINGLE_CAP \(1 << (\d+)\)", header)
     assert m and (1 << int(m.group(1))) == big
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every ctypes mirror of a struct in include/paces_b200.h has the C compiler's size and
+    field offsets (gcc on the header alone; no device)."""
+    import ctypes
+    import shutil
+    import subprocess
+    from paces_b200 import _native as nat
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not found")
+    mirrors = {"paces_model_desc": nat.ModelDesc, "paces_basis": nat.Basis, "paces_hmat": nat.HMat,
+               "paces_step_params": nat.StepParams, "paces_step_record": nat.StepRecord,
+               "paces_expm_info": nat.ExpmInfo, "paces_tuning": nat.Tuning, "paces_batch_item": nat.BatchItem}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "paces_b200.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, *_ in py._fields_:
+            lines.append(f'    printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["    return 0;", "}"]
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in filter(None, out):
+        cname, what, v = ln.split()
+        got[(cname, what)] = int(v)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, *_ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
