@@ -134,3 +134,28 @@ def test_periodic_symmetric_start_observables():
     agree with the oracle at every step although mirror-image ties at the cut may keep a
     different one of two equal states."""
     _run(16, 1.5, 1.0, None, 4096, 50, [0], [1.0], check_keys=False)
+
+
+# the wide keys: 4-bit fields fill nchain / 16 uint64 words, so these rings run the merge,
+# truncation, remap and observables kernels at four to eight key words (eight is the
+# maximum); site disorder breaks the mirror symmetry, so the keys compare at every step.
+# The first case is the long-chain workload's model (N=64, g=2, sigma 0.5, dt 0.025) at a
+# small maxstates.
+WIDE_CASES = [
+    (64, 2.0, 1.0, 5, 4096, 30, [0], [1.0], 0.025),
+    (80, 1.5, 1.0, 6, 2048, 25, [0], [1.0], 0.05),
+    (96, 1.5, 0.8, 7, 2048, 25, [3], [1.0], 0.05),
+    (112, 2.0, 1.0, 8, 2048, 25, [0], [1.0], 0.05),
+    (128, 1.5, 1.0, 9, 2048, 25, [64], [1.0], 0.05),
+]
+
+
+@pytest.mark.parametrize("nchain,g,w0,seed,maxstates,steps,sites,amps,dt", WIDE_CASES,
+                         ids=[f"n{c[0]}_nw{c[0] // 16}" for c in WIDE_CASES])
+def test_wide_keys_trajectory_bit_exact(nchain, g, w0, seed, maxstates, steps, sites, amps, dt):
+    from paces_b200.engine import Engine, ModelParams
+    eng = Engine(ModelParams(nchain=nchain, max_ho_dims=[16] * nchain, g=g, periodic=True), cap=64)
+    assert eng.nw == nchain // 16
+    eng.close()
+    saturated = _run(nchain, g, w0, seed, maxstates, steps, sites, amps, dt=dt)
+    assert saturated >= steps // 2
