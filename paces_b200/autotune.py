@@ -56,6 +56,7 @@ def set_tuning(eng, merge_stride=None, taylor_blocks_per_sm=None, taylor_variant
     if taylor_variant is not None:
         t.taylor_variant = int(taylor_variant)
     nat.check(eng.lib.paces_set_tuning(eng.ctx, t), eng.ctx, "set_tuning")
+    eng.tuning_epoch += 1  # graphs captured under the old shapes are not replayed
 
 
 def stride_candidates(t: nat.Tuning):

@@ -122,6 +122,9 @@ class Engine:
             nat.check(self.lib.paces_create(ctypes.byref(desc), ctypes.byref(ctx)), None, "paces_create")
         self.ctx = ctx
         self.nw = self.lib.paces_key_words(ctx)
+        # bumped by every change of the launch shapes: CUDA graphs captured under other shapes
+        # are not replayed
+        self.tuning_epoch = 0
         self.nhop = int(self.lib.paces_hop_channels(ctx))  # hopping channels (1: the chain)
         self.ref_words = self.lib.paces_ref_words(ctx)
         self.cap = 0
@@ -606,7 +609,7 @@ class Trajectory:
         return g, prm
 
     def _graph_step(self, dt):
-        key = (self.cur, float(dt),
+        key = (self.cur, float(dt), self.eng.tuning_epoch,
                None if self.proposal is None else (self.proposal[0].data_ptr(), float(self.proposal[1])))
         if key not in self._graphs:
             self._graphs[key] = self._capture(dt)
@@ -861,7 +864,7 @@ class TrajectoryBatch:
         graphed = self.use_graph and evolve and all(t.shuffle_seed is None for t in self.trajs)
         for _ in range(12):
             if graphed:
-                key = (tuple(t.cur for t in self.trajs), dts)
+                key = (tuple(t.cur for t in self.trajs), dts, tuple(t.eng.tuning_epoch for t in self.trajs))
                 if key not in self._graphs:
                     self._graphs[key] = self._capture(dts)
                 self._graphs[key][0].replay()

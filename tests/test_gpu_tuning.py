@@ -74,3 +74,39 @@ def test_tuner_picks_an_allowed_shape(tmp_path, monkeypatch):
     again = autotune.tune(tr, 0.05, steps=1)
     assert again["cached"] and again["merge_stride"] == choice["merge_stride"]
     eng.close()
+
+
+def test_graphs_follow_the_launch_shapes():
+    """A change of launch shapes (set_tuning, or a cached choice the tuner applies) makes the
+    next graph step capture anew, for a trajectory and for a batch: no replay runs under the
+    shapes it was captured with after they changed."""
+    from paces_b200 import autotune
+    from paces_b200.engine import TrajectoryBatch
+    trs = []
+    for _ in range(3):
+        eng = gpu_helpers.engine_for(16, 16, 1.0, cap=1 << 14, precision="c64", periodic=True)
+        tr, _ = gpu_helpers.grown_trajectory(eng, 16, 20000, graph=True)
+        trs.append(tr)
+    tr = trs[0]
+    for _ in range(2):
+        tr.step(evolve=True, dt=0.05)
+    before = set(tr._graphs)
+    assert len(before) == 2
+    epoch = tr.eng.tuning_epoch
+    autotune.set_tuning(tr.eng, 240, assemble_stride=240)
+    assert tr.eng.tuning_epoch == epoch + 1
+    tr.step(evolve=True, dt=0.05)
+    new = set(tr._graphs) - before
+    assert len(new) == 1 and all(k[2] == tr.eng.tuning_epoch for k in new)
+
+    batch = TrajectoryBatch(trs[1:], n_streams=2, graph=True)
+    for _ in range(2):
+        batch.step(evolve=True, dt=0.05)
+    before = set(batch._graphs)
+    assert len(before) == 2
+    autotune.set_tuning(trs[2].eng, 240, assemble_stride=240)
+    batch.step(evolve=True, dt=0.05)
+    new = set(batch._graphs) - before
+    assert len(new) == 1
+    assert all(k[2] == tuple(t.eng.tuning_epoch for t in trs[1:]) for k in new)
+    batch.close()
