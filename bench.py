@@ -769,6 +769,29 @@ def batched_specs(seed, n):
             for i in range(n)]
 
 
+def warm_up_batch(batch, trajs, warmup, dt, headroom=1.6, extra=30):
+    """Untimed batch steps before the timed ones.  An overflow in the timed steps would run
+    that batch step again and capture its graphs anew, so every trajectory first gets room
+    for `headroom` times its states, and the warm-up goes on (at most `extra` more steps)
+    until `warmup` steps in a row have run without a repeat.  Returns the steps taken."""
+    grown = False
+    for t in trajs:
+        need = int(headroom * t.last.n_states) + 64
+        if t.eng.cap < need:
+            t._regrow(need / t.eng.cap)
+            grown = True
+    if grown:
+        batch._graphs = {}
+    steps = quiet = 0
+    want = max(warmup, 1)
+    while steps < max(warmup, 0) or (quiet < want and steps < max(warmup, 0) + extra):
+        r0 = batch.repeats
+        batch.step(evolve=True, dt=dt)
+        steps += 1
+        quiet = quiet + 1 if batch.repeats == r0 else 0
+    return steps
+
+
 def run_batched(a):
     import torch
     from paces_b200 import _native as nat
@@ -805,8 +828,8 @@ def run_batched(a):
     if not a.no_tune:
         from paces_b200 import autotune
         tuning = autotune.tune_batch(batch, a.dt)
-    for _ in range(max(a.warmup, 0)):
-        batch.step(evolve=True, dt=a.dt)
+    warm_up_batch(batch, trajs, a.warmup, a.dt)
+    repeats0 = batch.repeats
 
     def barrier():
         torch.cuda.synchronize()
@@ -826,6 +849,7 @@ def run_batched(a):
         ev1.synchronize()
     ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     clocks = clk.summary()
+    repeated_timed = batch.repeats - repeats0
     barrier()
 
     # phase split (eager batch steps with events) and the batched Taylor launch
@@ -888,6 +912,7 @@ def run_batched(a):
                          "algorithmic_bytes": taylor_alg, "launch_ms": taylor_ms},
             "phase_ms": {k: v / n_prof for k, v in phase.items()},
             "sequential_ms_per_step": seq_ms, "batched_speedup": seq_ms / (ms / a.steps),
+            "repeated_steps_timed": repeated_timed,
             "clocks": clocks, "gpu_launches": int(round(launches_per_step * a.steps)), "cpu_baseline": None,
             "e2e": None,
         }

@@ -795,6 +795,7 @@ class TrajectoryBatch:
             nat.check(self.lib.paces_batch_create(len(trajs), int(n_streams), ctypes.byref(h)), None, "batch_create")
         self.handle = h
         self.rec_host = torch.zeros((len(trajs), ctypes.sizeof(nat.StepRecord)), dtype=torch.uint8).pin_memory()
+        self.repeats = 0  # batch steps run again after a capacity overflow
 
     def _dts(self, dt):
         if isinstance(dt, (int, float)):
@@ -876,6 +877,7 @@ class TrajectoryBatch:
                 for i in grow:
                     self.trajs[i]._regrow()
                 self._graphs = {}
+                self.repeats += 1
                 continue
             break
         for i, r in enumerate(recs):

@@ -161,3 +161,48 @@ def test_ctypes_structs_match_the_header(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, *_ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_batch_warm_up_runs_until_no_step_repeats():
+    """bench.warm_up_batch: trajectories short of room grow first (and the batch drops its
+    graphs); the warm-up takes at least `warmup` steps and goes on until that many in a row
+    ran without a capacity repeat, within the extra steps allowed."""
+    import sys
+    sys.path.insert(0, REPO)
+    import bench
+
+    class Rec:
+        def __init__(self, n):
+            self.n_states = n
+
+    class Eng:
+        def __init__(self, cap):
+            self.cap = cap
+
+    class Traj:
+        def __init__(self, cap, n):
+            self.eng, self.last, self.grown = Eng(cap), Rec(n), []
+
+        def _regrow(self, factor):
+            self.grown.append(factor)
+            self.eng.cap = int(self.eng.cap * factor)
+
+    class Batch:
+        def __init__(self, repeat_at):
+            self.repeats, self.n, self.repeat_at, self._graphs = 0, 0, set(repeat_at), {"g": 1}
+
+        def step(self, evolve, dt):
+            self.n += 1
+            if self.n in self.repeat_at:
+                self.repeats += 1
+
+    trajs = [Traj(1000, 900), Traj(10000, 100)]
+    b = Batch(repeat_at=[2, 5])
+    assert bench.warm_up_batch(b, trajs, 3, 0.05) == 8  # repeats at 2 and 5: quiet from 6 to 8
+    assert trajs[0].eng.cap >= 1.6 * 900 and trajs[0].grown and not trajs[1].grown
+    assert b._graphs == {}
+    b = Batch(repeat_at=range(1, 100))
+    assert bench.warm_up_batch(b, [Traj(10000, 10)], 3, 0.05, extra=5) == 8  # bounded
+    b = Batch(repeat_at=[])
+    assert bench.warm_up_batch(b, [Traj(10000, 10)], 3, 0.05) == 3
+    assert b._graphs == {"g": 1}
